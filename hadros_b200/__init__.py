@@ -1,0 +1,250 @@
+"""hadros_b200 — B200-native HADROS per-pixel image pipeline.
+
+Python face of the C ABI in include/hadros_b200.h (the library
+hadros_b200/lib/libhadros_b200.so, built by ``python -m hadros_b200.build``).
+The compute path is the CUDA library; there is no CPU fallback: without the
+built library or a B200, the calls raise.
+
+    import hadros_b200 as hb
+    sig = hb.SigmaTable.load("data/sigma/sigma_nuN_CC_GBW.dat")
+    p = hb.params(nx=32, ny=32, profile="gaussian", source="inner_ring")
+    with hb.Context(0) as ctx:
+        img = ctx.image(p, sig)          # dict of numpy arrays, pixel = j*nx + i
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import abi
+from .abi import (FATE_CAPTURED, FATE_ESCAPED, FATE_TRUNCATED, PRECISION_FP64,
+                  PRECISION_MIXED, PROFILES, SOURCES, SPECTRA, HadrosImageOut,
+                  HadrosParams, HadrosStats)
+
+__all__ = ["lib", "HadrosError", "params", "SigmaTable", "Context", "spectral_bins",
+           "HadrosParams", "PRECISION_FP64", "PRECISION_MIXED", "PROFILES", "SOURCES",
+           "SPECTRA", "FATE_ESCAPED", "FATE_CAPTURED", "FATE_TRUNCATED"]
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libhadros_b200.so"
+_LIB = None
+
+
+class HadrosError(RuntimeError):
+    """A HADROS_E_* status from the library, with hadros_last_error()'s text."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+        self.message = message
+
+
+def lib() -> C.CDLL:
+    """Load libhadros_b200.so (raises if it was not built)."""
+    global _LIB
+    if _LIB is None:
+        path = Path(os.environ.get("HADROS_B200_LIB", LIB_PATH))
+        if not path.exists():
+            raise ImportError(f"{path} not found: build it with `python -m hadros_b200.build`")
+        L = C.CDLL(str(path))
+        for name, (res, args) in abi.SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        if L.hadros_abi_version() != abi.ABI_VERSION:
+            raise ImportError("libhadros_b200.so ABI version does not match hadros_b200/abi.py")
+        _LIB = L
+    return _LIB
+
+
+def _check(status: int) -> None:
+    if status != abi.OK:
+        raise HadrosError(status, lib().hadros_last_error().decode())
+
+
+def _kind(table, value, parser: str) -> int:
+    if isinstance(value, str):
+        k = C.c_int32()
+        _check(getattr(lib(), parser)(value.encode(), C.byref(k)))
+        return k.value
+    return int(value)
+
+
+_DEG = {"theta_obs_deg": "theta_obs_rad", "funnel_theta_deg": "funnel_theta_rad",
+        "src_theta_width_deg": "src_theta_width_rad", "src_funnel_theta_deg": "src_funnel_theta_rad",
+        "src_gradient_dtheta_deg": "src_gradient_dtheta_rad"}
+
+
+def params(**kw) -> HadrosParams:
+    """hadros_params_default() with overrides.
+
+    Accepts every hadros_params field, the model names ``profile``, ``source``,
+    ``spectral`` (reference spellings and aliases), ``precision`` as
+    "fp64"/"mixed", and ``*_deg`` forms of the angle fields (converted as the
+    reference apps do: value * M_PI / 180.0).
+    """
+    p = HadrosParams()
+    lib().hadros_params_default(C.byref(p))
+    for key, val in kw.items():
+        if key == "profile":
+            p.profile_kind = _kind(PROFILES, val, "hadros_parse_profile")
+        elif key == "source":
+            p.source_kind = _kind(SOURCES, val, "hadros_parse_source")
+        elif key == "spectral":
+            p.spectral_kind = _kind(SPECTRA, val, "hadros_parse_spectral")
+        elif key == "precision":
+            p.precision = {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}.get(val, val)
+        elif key in _DEG:
+            setattr(p, _DEG[key], float(val) * math.pi / 180.0)
+        elif hasattr(p, key):
+            setattr(p, key, val)
+        else:
+            raise TypeError(f"unknown hadros_params field {key!r}")
+    return p
+
+
+class SigmaTable:
+    """sigma_CC(E) table handle (SigmaTable, src/sigma_table.cpp)."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+
+    @classmethod
+    def load(cls, path) -> "SigmaTable":
+        h = C.c_void_p()
+        _check(lib().hadros_sigma_load(str(path).encode(), C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_arrays(cls, E_GeV, sigma_cm2, sigma_GeV2=None) -> "SigmaTable":
+        E = np.ascontiguousarray(E_GeV, dtype=np.float64)
+        s = np.ascontiguousarray(sigma_cm2, dtype=np.float64)
+        g = None if sigma_GeV2 is None else np.ascontiguousarray(sigma_GeV2, dtype=np.float64)
+        if E.shape != s.shape or (g is not None and g.shape != E.shape):
+            raise ValueError("E, sigma arrays must have the same length")
+        h = C.c_void_p()
+        _check(lib().hadros_sigma_from_arrays(E.ctypes.data, None if g is None else g.ctypes.data,
+                                              s.ctypes.data, int(E.size), C.byref(h)))
+        return cls(h.value)
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise HadrosError(abi.E_STATE, "sigma table was closed")
+        return self._h
+
+    def info(self) -> tuple[int, float, float]:
+        n, lo, hi = C.c_int32(), C.c_double(), C.c_double()
+        _check(lib().hadros_sigma_info(self.handle, C.byref(n), C.byref(lo), C.byref(hi)))
+        return n.value, lo.value, hi.value
+
+    def sigma_cm2(self, E: float) -> float:
+        out = C.c_double()
+        _check(lib().hadros_sigma_eval_cm2(self.handle, float(E), C.byref(out)))
+        return out.value
+
+    def close(self) -> None:
+        if self._h:
+            lib().hadros_sigma_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def n_bins_of(p: HadrosParams) -> int:
+    return 1 if p.spectral_kind == 0 else max(int(p.n_bins), 1)
+
+
+def spectral_bins(p: HadrosParams, sigma: SigmaTable) -> dict:
+    """The bins integrate_kerr_ray_spectral uses: E_mid, dE, weight, valid."""
+    B = n_bins_of(p)
+    E, d, w = (np.zeros(B) for _ in range(3))
+    v = np.zeros(B, dtype=np.int8)
+    n = C.c_int32()
+    _check(lib().hadros_spectral_bins(C.byref(p), sigma.handle, E.ctypes.data, d.ctypes.data,
+                                      w.ctypes.data, v.ctypes.data, C.byref(n)))
+    return {"E_mid": E[:n.value], "dE": d[:n.value], "weight": w[:n.value], "valid": v[:n.value]}
+
+
+OUTPUTS = ("tau", "P_surv", "I_obs", "fate", "steps", "attempts", "tau_E", "I_E")
+
+
+class Context:
+    """A CUDA device context (hadros_ctx): one stream and its buffers."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().hadros_ctx_create(int(device), C.byref(h)))
+        self._h = h
+        self.device = device
+
+    def close(self) -> None:
+        if self._h:
+            lib().hadros_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise HadrosError(abi.E_STATE, "context was closed")
+        return self._h
+
+    def stats(self) -> dict:
+        s = HadrosStats()
+        _check(lib().hadros_ctx_stats(self.handle, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in s._fields_}
+
+    def set_attempt_budget(self, attempts_per_ray: int) -> None:
+        _check(lib().hadros_ctx_set_attempt_budget(self.handle, int(attempts_per_ray)))
+
+    def image(self, p: HadrosParams, sigma: SigmaTable, pixel_ids=None,
+              outputs=OUTPUTS) -> dict:
+        """Trace an image (or a pixel list) into host numpy arrays."""
+        B = n_bins_of(p)
+        P = int(p.nx) * int(p.ny) if pixel_ids is None else len(pixel_ids)
+        fdt = np.float32 if p.precision == PRECISION_MIXED else np.float64
+        shapes = {"tau": (P, np.float64), "P_surv": (P, np.float64), "I_obs": (P, np.float64),
+                  "fate": (P, np.int8), "steps": (P, np.int32), "attempts": (P, np.int32),
+                  "tau_E": ((P, B), fdt), "I_E": ((P, B), fdt)}
+        res = {k: np.zeros(shapes[k][0], dtype=shapes[k][1]) for k in outputs}
+        out = HadrosImageOut()
+        for k, arr in res.items():
+            setattr(out, k, arr.ctypes.data)
+        if pixel_ids is None:
+            _check(lib().hadros_image(self.handle, C.byref(p), sigma.handle, C.byref(out)))
+        else:
+            ids = np.ascontiguousarray(pixel_ids, dtype=np.int32)
+            _check(lib().hadros_image_pixels(self.handle, C.byref(p), sigma.handle,
+                                             ids.ctypes.data, int(ids.size), C.byref(out)))
+        return res
+
+    def image_device(self, p: HadrosParams, sigma: SigmaTable, out: dict, stream=None) -> None:
+        """Enqueue an image into device buffers (torch tensors or raw pointers)."""
+        o = HadrosImageOut()
+        for k, v in out.items():
+            setattr(o, k, v if isinstance(v, int) else v.data_ptr())
+        st = None if stream is None else C.c_void_p(stream if isinstance(stream, int)
+                                                    else stream.cuda_stream)
+        _check(lib().hadros_image_device(self.handle, C.byref(p), sigma.handle, C.byref(o), st))
+
+    def synchronize(self) -> None:
+        _check(lib().hadros_ctx_synchronize(self.handle))

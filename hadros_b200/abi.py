@@ -1,0 +1,143 @@
+"""ctypes mirror of include/hadros_b200.h (structures and constants only).
+
+Importing this module loads nothing; hadros_b200.lib() loads the library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+ABI_VERSION = 1
+
+OK, E_ARG, E_IO, E_CUDA, E_RANGE, E_TIMEOUT, E_NOMEM, E_STATE = range(8)
+
+PROFILES = ("gaussian", "powerlaw", "gaussian_funnel", "powerlaw_funnel",
+            "gaussian_envelope", "powerlaw_envelope", "powerlaw_funnel_envelope",
+            "collapsar_ndaf_like")
+SOURCES = ("inner_ring", "funnel_wall", "jet_base", "shock_layer", "density_weighted")
+SPECTRA = ("monochromatic", "powerlaw", "powerlaw_cutoff")
+
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+FATE_ESCAPED, FATE_CAPTURED, FATE_TRUNCATED = 0, 1, 2
+
+
+class HadrosParams(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("nx", C.c_int32), ("ny", C.c_int32),
+        ("max_steps", C.c_int32),
+        ("profile_kind", C.c_int32),
+        ("source_kind", C.c_int32),
+        ("spectral_kind", C.c_int32),
+        ("n_bins", C.c_int32),
+        ("precision", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("a_spin", C.c_double),
+        ("r_obs_rg", C.c_double),
+        ("theta_obs_rad", C.c_double),
+        ("fov_deg", C.c_double),
+        ("r_max_rg", C.c_double),
+        ("h", C.c_double),
+        ("tolerance", C.c_double),
+        ("Enu_obs_GeV", C.c_double),
+        ("M_bh_msun", C.c_double),
+        ("rho0_gcm3", C.c_double),
+        ("r0_rg", C.c_double),
+        ("sigma_r_rg", C.c_double),
+        ("H_over_R", C.c_double),
+        ("radial_power", C.c_double),
+        ("funnel_depletion", C.c_double),
+        ("funnel_theta_rad", C.c_double),
+        ("envelope_rho0_gcm3", C.c_double),
+        ("envelope_alpha", C.c_double),
+        ("torus_r_min_rg", C.c_double),
+        ("torus_r_max_rg", C.c_double),
+        ("rho_floor_gcm3", C.c_double),
+        ("src_r_center_rg", C.c_double),
+        ("src_sigma_r_rg", C.c_double),
+        ("src_theta_width_rad", C.c_double),
+        ("src_powerlaw", C.c_double),
+        ("src_emax_GeV", C.c_double),
+        ("src_norm", C.c_double),
+        ("src_funnel_theta_rad", C.c_double),
+        ("src_density_power_q", C.c_double),
+        ("src_radial_power_s", C.c_double),
+        ("src_rho_ref_gcm3", C.c_double),
+        ("src_cutoff_min", C.c_double),
+        ("src_cutoff_max", C.c_double),
+        ("src_gradient_dr_rg", C.c_double),
+        ("src_gradient_dtheta_rad", C.c_double),
+        ("spec_gamma", C.c_double),
+        ("spec_ecut_GeV", C.c_double),
+        ("spec_e_min_GeV", C.c_double),
+        ("spec_e_max_GeV", C.c_double),
+    ]
+
+    def copy(self) -> "HadrosParams":
+        q = HadrosParams()
+        C.memmove(C.byref(q), C.byref(self), C.sizeof(HadrosParams))
+        return q
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class HadrosImageOut(C.Structure):
+    _fields_ = [
+        ("tau", C.c_void_p),
+        ("P_surv", C.c_void_p),
+        ("I_obs", C.c_void_p),
+        ("fate", C.c_void_p),
+        ("steps", C.c_void_p),
+        ("attempts", C.c_void_p),
+        ("tau_E", C.c_void_p),
+        ("I_E", C.c_void_p),
+    ]
+
+
+class HadrosStats(C.Structure):
+    _fields_ = [
+        ("kernel_ms", C.c_double),
+        ("total_ms", C.c_double),
+        ("rays", C.c_int64),
+        ("accepted_steps", C.c_int64),
+        ("attempts", C.c_int64),
+        ("launches", C.c_int32),
+        ("aborted_rays", C.c_int32),
+    ]
+
+
+# Every function the header declares: name -> (restype, argtypes).
+P = C.POINTER
+SIGNATURES = {
+    "hadros_abi_version": (C.c_int32, []),
+    "hadros_status_string": (C.c_char_p, [C.c_int32]),
+    "hadros_last_error": (C.c_char_p, []),
+    "hadros_params_default": (None, [P(HadrosParams)]),
+    "hadros_params_validate": (C.c_int32, [P(HadrosParams)]),
+    "hadros_parse_profile": (C.c_int32, [C.c_char_p, P(C.c_int32)]),
+    "hadros_parse_source": (C.c_int32, [C.c_char_p, P(C.c_int32)]),
+    "hadros_parse_spectral": (C.c_int32, [C.c_char_p, P(C.c_int32)]),
+    "hadros_profile_name": (C.c_char_p, [C.c_int32]),
+    "hadros_source_name": (C.c_char_p, [C.c_int32]),
+    "hadros_spectral_name": (C.c_char_p, [C.c_int32]),
+    "hadros_sigma_load": (C.c_int32, [C.c_char_p, P(C.c_void_p)]),
+    "hadros_sigma_from_arrays": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                             P(C.c_void_p)]),
+    "hadros_sigma_info": (C.c_int32, [C.c_void_p, P(C.c_int32), P(C.c_double), P(C.c_double)]),
+    "hadros_sigma_eval_cm2": (C.c_int32, [C.c_void_p, C.c_double, P(C.c_double)]),
+    "hadros_sigma_destroy": (None, [C.c_void_p]),
+    "hadros_spectral_bins": (C.c_int32, [P(HadrosParams), C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, P(C.c_int32)]),
+    "hadros_ctx_create": (C.c_int32, [C.c_int32, P(C.c_void_p)]),
+    "hadros_ctx_destroy": (None, [C.c_void_p]),
+    "hadros_ctx_stats": (C.c_int32, [C.c_void_p, P(HadrosStats)]),
+    "hadros_ctx_set_attempt_budget": (C.c_int32, [C.c_void_p, C.c_int64]),
+    "hadros_image": (C.c_int32, [C.c_void_p, P(HadrosParams), C.c_void_p, P(HadrosImageOut)]),
+    "hadros_image_pixels": (C.c_int32, [C.c_void_p, P(HadrosParams), C.c_void_p, C.c_void_p,
+                                        C.c_int32, P(HadrosImageOut)]),
+    "hadros_image_device": (C.c_int32, [C.c_void_p, P(HadrosParams), C.c_void_p,
+                                        P(HadrosImageOut), C.c_void_p]),
+    "hadros_ctx_synchronize": (C.c_int32, [C.c_void_p]),
+}

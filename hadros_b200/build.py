@@ -1,0 +1,102 @@
+"""Builds the in-tree CUDA library hadros_b200/lib/libhadros_b200.so for sm_100a.
+
+    python -m hadros_b200.build          # incremental
+    python -m hadros_b200.build --force  # rebuild everything
+
+The trace kernel is compiled with --fmad=false (no contraction of a*b+c into
+an FMA) so that its FP64 arithmetic rounds like the reference's x86-64 build;
+FMAs the mixed-precision transfer wants are written as explicit intrinsics.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+LIB_DIR = PKG / "lib"
+BUILD_DIR = PKG / "_build"
+LIB = LIB_DIR / "libhadros_b200.so"
+REPO = PKG.parent
+INCLUDE = REPO / "include"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC",
+              "-Xptxas", "-v"]
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra"]
+
+CU_SOURCES = ["hadros_trace.cu"]
+CXX_SOURCES = ["hadros_host.cpp"]
+HEADERS = ["hadros_internal.h", "hadros_physics.cuh"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found: the hadros_b200 CUDA library cannot be built")
+
+
+def _cuda_home() -> Path:
+    return Path(_nvcc()).resolve().parent.parent
+
+
+def _stale(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def _run(cmd: list[str], log: list[str], verbose: bool) -> None:
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    log.append(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError(f"build step failed: {' '.join(cmd[:3])} ...")
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile the CUDA kernels and the C-ABI host code; returns the .so path."""
+    BUILD_DIR.mkdir(exist_ok=True)
+    LIB_DIR.mkdir(exist_ok=True)
+    nvcc = _nvcc()
+    cuda_inc = _cuda_home() / "include"
+    headers = [CSRC / h for h in HEADERS] + [INCLUDE / "hadros_b200.h"]
+    objs: list[Path] = []
+    log: list[str] = []
+    for src in CU_SOURCES:
+        obj = BUILD_DIR / (Path(src).stem + ".o")
+        if force or _stale(obj, [CSRC / src] + headers):
+            _run([nvcc, *ARCH, *NVCC_FLAGS, "-I", str(INCLUDE), "-c", str(CSRC / src),
+                  "-o", str(obj)], log, verbose)
+        objs.append(obj)
+    for src in CXX_SOURCES:
+        obj = BUILD_DIR / (Path(src).stem + ".o")
+        if force or _stale(obj, [CSRC / src] + headers):
+            _run(["g++", *CXX_FLAGS, "-I", str(INCLUDE), "-I", str(cuda_inc), "-c",
+                  str(CSRC / src), "-o", str(obj)], log, verbose)
+        objs.append(obj)
+    if force or _stale(LIB, objs):
+        _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fPIC",
+              "-o", str(LIB), *map(str, objs)], log, verbose)
+    (BUILD_DIR / "build.log").write_text("\n".join(log))
+    return LIB
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("-v", "--verbose", action="store_true")
+    a = ap.parse_args()
+    print(build(force=a.force, verbose=a.verbose))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,705 @@
+// hadros_host.cpp — the C ABI (include/hadros_b200.h): parameters, model
+// names, sigma tables, device contexts and the image calls.
+//
+// No function lets a C++ exception or a CUDA error escape: every entry point
+// returns a status code and leaves a message for hadros_last_error().
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <new>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "hadros_internal.h"
+
+using namespace hadros;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int32_t fail(int32_t code, const std::string& msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+int32_t ok()
+{
+    g_last_error.clear();
+    return HADROS_OK;
+}
+
+const char* const kProfileNames[8] = {"gaussian", "powerlaw", "gaussian_funnel", "powerlaw_funnel",
+                                      "gaussian_envelope", "powerlaw_envelope",
+                                      "powerlaw_funnel_envelope", "collapsar_ndaf_like"};
+const char* const kSourceNames[5] = {"inner_ring", "funnel_wall", "jet_base", "shock_layer",
+                                     "density_weighted"};
+const char* const kSpectralNames[3] = {"monochromatic", "powerlaw", "powerlaw_cutoff"};
+
+std::atomic<uint64_t> g_sigma_serial{1};
+
+}  // namespace
+
+// A device context: one stream, device buffers grown on demand, the sigma
+// table last uploaded, and the statistics of the last call.
+struct hadros_ctx {
+    int device = 0;
+    int n_sm = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t attempt_budget = 0;
+    hadros_stats stats{};
+    std::string err;
+    bool failed = false;
+
+    // device buffers
+    void* d_cams = nullptr; size_t cams_cap = 0;
+    void* d_bins = nullptr; size_t bins_cap = 0;
+    void* d_pix = nullptr; size_t pix_cap = 0;
+    void* d_out = nullptr; size_t out_cap = 0;
+    unsigned long long* d_counters = nullptr;
+    void* d_sig = nullptr; size_t sig_cap = 0;
+    const hadros_sigma* sig_key = nullptr;
+    uint64_t sig_serial = 0;
+    SigmaDev sig_dev{};
+};
+
+namespace {
+
+int32_t cuda_fail(hadros_ctx* ctx, cudaError_t e, const char* what)
+{
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    if (ctx) {
+        ctx->err = m;
+        if (e != cudaErrorMemoryAllocation) ctx->failed = true;
+    }
+    return fail(e == cudaErrorMemoryAllocation ? HADROS_E_NOMEM : HADROS_E_CUDA, m);
+}
+
+int32_t grow(hadros_ctx* ctx, void** buf, size_t* cap, size_t need, const char* what)
+{
+    if (need <= *cap && *buf) return HADROS_OK;
+    if (*buf) {
+        cudaFree(*buf);
+        *buf = nullptr;
+        *cap = 0;
+    }
+    size_t n = need < 256 ? 256 : need;
+    cudaError_t e = cudaMalloc(buf, n);
+    if (e != cudaSuccess) {
+        *buf = nullptr;
+        return cuda_fail(ctx, e, what);
+    }
+    *cap = n;
+    return HADROS_OK;
+}
+
+bool finite_all(std::initializer_list<double> v)
+{
+    for (double x : v)
+        if (!std::isfinite(x)) return false;
+    return true;
+}
+
+// Device copy of a sigma table: E, S, lnE, lnS (double), lx (float), seg
+// (float4), each 256-byte aligned.
+int32_t upload_sigma(hadros_ctx* ctx, const hadros_sigma* s, uint64_t serial)
+{
+    if (ctx->sig_key == s && ctx->sig_serial == serial && ctx->d_sig) return HADROS_OK;
+    const SigmaHost& h = s->h;
+    const size_t n = h.E.size();
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t oE = 0, oS = al(oE + 8 * n), olnE = al(oS + 8 * n), olnS = al(olnE + 8 * n),
+                 olx = al(olnS + 8 * n), oseg = al(olx + 4 * n), total = al(oseg + 16 * n);
+    int32_t rc = grow(ctx, &ctx->d_sig, &ctx->sig_cap, total, "sigma table allocation");
+    if (rc) return rc;
+    std::vector<unsigned char> blob(total, 0);
+    std::memcpy(blob.data() + oE, h.E.data(), 8 * n);
+    std::memcpy(blob.data() + oS, h.s_cm2.data(), 8 * n);
+    std::memcpy(blob.data() + olnE, h.lnE.data(), 8 * n);
+    std::memcpy(blob.data() + olnS, h.lnS.data(), 8 * n);
+    std::memcpy(blob.data() + olx, h.lx.data(), 4 * n);
+    std::memcpy(blob.data() + oseg, h.seg.data(), 16 * n);
+    cudaError_t e = cudaMemcpy(ctx->d_sig, blob.data(), total, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "sigma table upload");
+    unsigned char* base = static_cast<unsigned char*>(ctx->d_sig);
+    SigmaDev& d = ctx->sig_dev;
+    d.n = static_cast<int32_t>(n);
+    d.E_min = h.E.front();
+    d.E_max = h.E.back();
+    d.sigma_scale = h.sigma_scale;
+    d.E = reinterpret_cast<const double*>(base + oE);
+    d.S = reinterpret_cast<const double*>(base + oS);
+    d.lnE = reinterpret_cast<const double*>(base + olnE);
+    d.lnS = reinterpret_cast<const double*>(base + olnS);
+    d.lx = reinterpret_cast<const float*>(base + olx);
+    d.seg = reinterpret_cast<const float*>(base + oseg);
+    ctx->sig_key = s;
+    ctx->sig_serial = serial;
+    return HADROS_OK;
+}
+
+}  // namespace
+
+namespace {
+uint64_t sigma_serial(const hadros_sigma* s) { return s->serial; }
+}  // namespace
+
+extern "C" {
+
+int32_t hadros_abi_version(void) { return HADROS_ABI_VERSION; }
+
+const char* hadros_status_string(int32_t status)
+{
+    switch (status) {
+    case HADROS_OK: return "ok";
+    case HADROS_E_ARG: return "invalid argument";
+    case HADROS_E_IO: return "i/o error";
+    case HADROS_E_CUDA: return "CUDA error";
+    case HADROS_E_RANGE: return "energy outside sigma table range";
+    case HADROS_E_TIMEOUT: return "attempt budget exhausted";
+    case HADROS_E_NOMEM: return "out of memory";
+    case HADROS_E_STATE: return "invalid handle or state";
+    default: return "unknown status";
+    }
+}
+
+const char* hadros_last_error(void) { return g_last_error.c_str(); }
+
+void hadros_params_default(hadros_params* p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->struct_size = sizeof(hadros_params);
+    // KerrCamera arguments of compute_kerr_geodesics (apps/compute_kerr_geodesics.cpp:26-34)
+    p->a_spin = 0.9;
+    p->r_obs_rg = 60.0;
+    p->theta_obs_rad = M_PI * 74.0 / 180.0;
+    p->fov_deg = 45.0;
+    p->nx = 100;
+    p->ny = 100;
+    p->r_max_rg = 120.0;
+    p->h = 0.001;
+    p->tolerance = 1.0e-6;   // include/kerr_geodesic.hpp:12
+    p->max_steps = 200000;   // src/kerr_camera.cpp:222
+    // compute_kerr_image_from_cache argv defaults (apps/compute_kerr_image_from_cache.cpp:33-55)
+    p->Enu_obs_GeV = 1.0e9;
+    p->M_bh_msun = 3.0;
+    p->rho0_gcm3 = 1.0e10;
+    p->r0_rg = 10.0;
+    p->sigma_r_rg = 5.0;
+    p->H_over_R = 0.01;
+    p->profile_kind = HADROS_PROFILE_GAUSSIAN;
+    p->radial_power = 2.0;
+    p->funnel_depletion = 0.0;
+    p->funnel_theta_rad = 15.0 * M_PI / 180.0;
+    p->envelope_rho0_gcm3 = 0.0;
+    p->envelope_alpha = 2.5;
+    p->torus_r_min_rg = 4.0;
+    p->torus_r_max_rg = 60.0;
+    p->rho_floor_gcm3 = 1.0e-99;
+    // UHESourceParams defaults (include/radiative_transfer.hpp:45-62)
+    p->source_kind = HADROS_SOURCE_INNER_RING;
+    p->src_r_center_rg = 3.5;
+    p->src_sigma_r_rg = 1.0;
+    p->src_theta_width_rad = 8.0 * 3.141592653589793238462643383279502884 / 180.0;
+    p->src_powerlaw = 2.0;
+    p->src_emax_GeV = 1.0e12;
+    p->src_norm = 1.0;
+    p->src_funnel_theta_rad = 20.0 * 3.141592653589793238462643383279502884 / 180.0;
+    p->src_density_power_q = 1.0;
+    p->src_radial_power_s = 2.0;
+    p->src_rho_ref_gcm3 = -1.0;
+    p->src_cutoff_min = 0.0;
+    p->src_cutoff_max = 1.0e2;
+    p->src_gradient_dr_rg = 0.1;
+    p->src_gradient_dtheta_rad = 1.0 * 3.141592653589793238462643383279502884 / 180.0;
+    // UHESpectralParams defaults (include/radiative_transfer.hpp:29-35)
+    p->spectral_kind = HADROS_SPECTRAL_MONOCHROMATIC;
+    p->spec_gamma = 2.0;
+    p->spec_ecut_GeV = 1.0e12;
+    p->spec_e_min_GeV = 1.0e5;
+    p->spec_e_max_GeV = 1.0e12;
+    p->n_bins = 8;
+    p->precision = HADROS_PRECISION_FP64;
+}
+
+int32_t hadros_params_validate(const hadros_params* p)
+{
+    if (!p) return fail(HADROS_E_ARG, "params is NULL");
+    if (p->struct_size != sizeof(hadros_params))
+        return fail(HADROS_E_ARG, "params.struct_size does not match this library (use hadros_params_default)");
+    if (p->nx <= 0 || p->ny <= 0)
+        return fail(HADROS_E_ARG, "nx and ny must be positive");
+    if (static_cast<int64_t>(p->nx) * p->ny > 2147483647LL)
+        return fail(HADROS_E_ARG, "nx*ny exceeds 2^31-1 pixels");
+    if (p->max_steps <= 0) return fail(HADROS_E_ARG, "max_steps must be positive");
+    if (p->profile_kind < 0 || p->profile_kind > 7) return fail(HADROS_E_ARG, "profile_kind out of range");
+    if (p->source_kind < 0 || p->source_kind > 4) return fail(HADROS_E_ARG, "source_kind out of range");
+    if (p->spectral_kind < 0 || p->spectral_kind > 2) return fail(HADROS_E_ARG, "spectral_kind out of range");
+    if (p->precision != HADROS_PRECISION_FP64 && p->precision != HADROS_PRECISION_MIXED)
+        return fail(HADROS_E_ARG, "precision must be HADROS_PRECISION_FP64 or HADROS_PRECISION_MIXED");
+    if (p->spectral_kind != HADROS_SPECTRAL_MONOCHROMATIC && (p->n_bins > kMaxBins))
+        return fail(HADROS_E_ARG, "n_bins must be <= 256");
+    if (!(p->h > 0.0) || !std::isfinite(p->h)) return fail(HADROS_E_ARG, "step h must be positive and finite");
+    if (!(p->tolerance > 0.0) || !std::isfinite(p->tolerance))
+        return fail(HADROS_E_ARG, "tolerance must be positive and finite");
+    if (!finite_all({p->a_spin, p->r_obs_rg, p->theta_obs_rad, p->fov_deg, p->r_max_rg,
+                     p->Enu_obs_GeV, p->M_bh_msun}))
+        return fail(HADROS_E_ARG, "camera parameters must be finite");
+    return ok();
+}
+
+int32_t hadros_parse_profile(const char* name, int32_t* kind)
+{   // src/torus_profile.cpp:44-91
+    if (!name || !kind) return fail(HADROS_E_ARG, "NULL argument");
+    const std::string n(name);
+    int32_t k = -1;
+    if (n == "gaussian" || n == "torus" || n == "gaussian_torus") k = 0;
+    else if (n == "powerlaw" || n == "powerlaw_disk") k = 1;
+    else if (n == "funnel" || n == "gaussian_funnel") k = 2;
+    else if (n == "powerlaw_funnel") k = 3;
+    else if (n == "gaussian_envelope") k = 4;
+    else if (n == "powerlaw_envelope") k = 5;
+    else if (n == "powerlaw_funnel_envelope") k = 6;
+    else if (n == "collapsar_ndaf_like" || n == "collapsar_ndaf") k = 7;
+    if (k < 0)
+        return fail(HADROS_E_ARG,
+                    "Unknown density profile '" + n +
+                        "'. Use gaussian, powerlaw, gaussian_funnel, powerlaw_funnel, "
+                        "gaussian_envelope, powerlaw_envelope, powerlaw_funnel_envelope, "
+                        "or collapsar_ndaf_like.");
+    *kind = k;
+    return ok();
+}
+
+int32_t hadros_parse_source(const char* name, int32_t* kind)
+{   // src/radiative_transfer.cpp:80-112
+    if (!name || !kind) return fail(HADROS_E_ARG, "NULL argument");
+    const std::string n(name);
+    int32_t k = -1;
+    if (n == "inner_ring" || n == "INNER_RING" || n == "ring") k = 0;
+    else if (n == "funnel_wall" || n == "FUNNEL_WALL") k = 1;
+    else if (n == "jet_base" || n == "JET_BASE") k = 2;
+    else if (n == "shock_layer" || n == "SHOCK_LAYER") k = 3;
+    else if (n == "density_weighted" || n == "DENSITY_WEIGHTED") k = 4;
+    if (k < 0)
+        return fail(HADROS_E_ARG, "Unknown UHE source model '" + n +
+                                      "'. Use inner_ring, funnel_wall, jet_base, shock_layer, or density_weighted.");
+    *kind = k;
+    return ok();
+}
+
+int32_t hadros_parse_spectral(const char* name, int32_t* kind)
+{   // src/radiative_transfer.cpp:132-156
+    if (!name || !kind) return fail(HADROS_E_ARG, "NULL argument");
+    const std::string n(name);
+    int32_t k = -1;
+    if (n == "monochromatic" || n == "MONOCHROMATIC" || n == "mono") k = 0;
+    else if (n == "powerlaw" || n == "POWERLAW" || n == "power_law") k = 1;
+    else if (n == "powerlaw_cutoff" || n == "POWERLAW_CUTOFF" || n == "power_law_cutoff") k = 2;
+    if (k < 0)
+        return fail(HADROS_E_ARG, "Unknown UHE spectral model '" + n +
+                                      "'. Use monochromatic, powerlaw, or powerlaw_cutoff.");
+    *kind = k;
+    return ok();
+}
+
+const char* hadros_profile_name(int32_t kind) { return (kind >= 0 && kind < 8) ? kProfileNames[kind] : nullptr; }
+const char* hadros_source_name(int32_t kind) { return (kind >= 0 && kind < 5) ? kSourceNames[kind] : nullptr; }
+const char* hadros_spectral_name(int32_t kind) { return (kind >= 0 && kind < 3) ? kSpectralNames[kind] : nullptr; }
+
+// ---- sigma tables --------------------------------------------------------
+
+static int32_t sigma_finish(std::vector<double>& E, std::vector<double>& g2, std::vector<double>& cm2,
+                            hadros_sigma** out)
+{   // src/sigma_table.cpp:38-53
+    if (E.size() < 2)
+        return fail(HADROS_E_IO, "Sigma table must contain at least two valid data lines.");
+    for (size_t i = 1; i < E.size(); ++i)
+        if (E[i] <= E[i - 1])
+            return fail(HADROS_E_IO, "Energy grid in sigma table must be strictly increasing.");
+    if (E.size() > static_cast<size_t>(kMaxSigma))
+        return fail(HADROS_E_ARG, "sigma table has more than 4096 rows");
+    hadros_sigma* box = new (std::nothrow) hadros_sigma();
+    if (!box) return fail(HADROS_E_NOMEM, "out of host memory");
+    box->serial = g_sigma_serial.fetch_add(1);
+    box->h.E.swap(E);
+    box->h.s_GeV2.swap(g2);
+    box->h.s_cm2.swap(cm2);
+    prepare_sigma(box->h);
+    *out = box;
+    return ok();
+}
+
+int32_t hadros_sigma_load(const char* path, hadros_sigma** out)
+{   // SigmaTable::SigmaTable (src/sigma_table.cpp:9-53)
+    if (!path || !out) return fail(HADROS_E_ARG, "NULL argument");
+    *out = nullptr;
+    std::ifstream in(path);
+    if (!in) return fail(HADROS_E_IO, std::string("Could not open sigma table: ") + path);
+    std::vector<double> E, g2, cm2;
+    std::string line;
+    while (std::getline(in, line)) {
+        if (line.empty()) continue;
+        if (line[0] == '#') continue;
+        std::istringstream iss(line);
+        double e, sg, sc;
+        if (!(iss >> e >> sg >> sc)) continue;
+        if (e <= 0.0 || sg <= 0.0 || sc <= 0.0) continue;
+        E.push_back(e);
+        g2.push_back(sg);
+        cm2.push_back(sc);
+    }
+    return sigma_finish(E, g2, cm2, out);
+}
+
+int32_t hadros_sigma_from_arrays(const double* E_GeV, const double* sigma_GeV2, const double* sigma_cm2,
+                                 int32_t n, hadros_sigma** out)
+{
+    if (!E_GeV || !sigma_cm2 || !out || n < 0) return fail(HADROS_E_ARG, "NULL argument or negative n");
+    *out = nullptr;
+    std::vector<double> E, g2, cm2;
+    for (int32_t i = 0; i < n; ++i) {
+        const double sg = sigma_GeV2 ? sigma_GeV2[i] : 1.0;
+        if (E_GeV[i] <= 0.0 || sg <= 0.0 || sigma_cm2[i] <= 0.0) continue;
+        E.push_back(E_GeV[i]);
+        g2.push_back(sigma_GeV2 ? sg : 0.0);
+        cm2.push_back(sigma_cm2[i]);
+    }
+    return sigma_finish(E, g2, cm2, out);
+}
+
+int32_t hadros_sigma_info(const hadros_sigma* s, int32_t* n, double* E_min, double* E_max)
+{
+    if (!s) return fail(HADROS_E_STATE, "sigma handle is NULL");
+    if (n) *n = static_cast<int32_t>(s->h.E.size());
+    if (E_min) *E_min = s->h.E.front();
+    if (E_max) *E_max = s->h.E.back();
+    return ok();
+}
+
+int32_t hadros_sigma_eval_cm2(const hadros_sigma* s, double x, double* out)
+{   // SigmaTable::log_interp (src/sigma_table.cpp:81-124)
+    if (!s || !out) return fail(HADROS_E_ARG, "NULL argument");
+    const auto& xs = s->h.E;
+    const auto& ys = s->h.s_cm2;
+    if (x <= 0.0) return fail(HADROS_E_RANGE, "Interpolation energy must be positive.");
+    if (x < xs.front() || x > xs.back()) return fail(HADROS_E_RANGE, "Requested energy outside sigma table range.");
+    auto it = std::lower_bound(xs.begin(), xs.end(), x);
+    if (it == xs.begin()) { *out = ys.front(); return ok(); }
+    if (it == xs.end()) { *out = ys.back(); return ok(); }
+    const size_t i = static_cast<size_t>(it - xs.begin());
+    const double lx = std::log(x), lx1 = std::log(xs[i - 1]), lx2 = std::log(xs[i]);
+    const double ly1 = std::log(ys[i - 1]), ly2 = std::log(ys[i]);
+    const double t = (lx - lx1) / (lx2 - lx1);
+    *out = std::exp(ly1 + t * (ly2 - ly1));
+    return ok();
+}
+
+void hadros_sigma_destroy(hadros_sigma* s)
+{
+    delete s;
+}
+
+int32_t hadros_spectral_bins(const hadros_params* p, const hadros_sigma* s, double* E_mid, double* dE,
+                             double* weight, int8_t* valid, int32_t* n_bins_out)
+{
+    int32_t rc = hadros_params_validate(p);
+    if (rc) return rc;
+    if (!s) return fail(HADROS_E_STATE, "sigma handle is NULL");
+    DevCam cam;
+    std::vector<DevBin> bins;
+    std::string err;
+    rc = build_cam(*p, s->h, cam, bins, err);
+    if (rc) return fail(rc, err);
+    for (size_t b = 0; b < bins.size(); ++b) {
+        if (E_mid) E_mid[b] = bins[b].E_mid;
+        if (dE) dE[b] = bins[b].dE;
+        if (weight) weight[b] = bins[b].w;
+        if (valid) valid[b] = static_cast<int8_t>(bins[b].valid);
+    }
+    if (n_bins_out) *n_bins_out = static_cast<int32_t>(bins.size());
+    return ok();
+}
+
+// ---- contexts -----------------------------------------------------------------
+
+int32_t hadros_ctx_create(int32_t device, hadros_ctx** out)
+{
+    if (!out) return fail(HADROS_E_ARG, "NULL argument");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count <= 0) return fail(HADROS_E_CUDA, "no CUDA device available");
+    if (device < 0 || device >= count) return fail(HADROS_E_ARG, "device index out of range");
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaSetDevice");
+    cudaDeviceProp prop{};
+    e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceProperties");
+    if (prop.major != 10 || prop.minor != 0)
+        return fail(HADROS_E_CUDA, std::string("this library is built for sm_100a (B200); device is ") + prop.name);
+    hadros_ctx* ctx = new (std::nothrow) hadros_ctx();
+    if (!ctx) return fail(HADROS_E_NOMEM, "out of host memory");
+    ctx->device = device;
+    ctx->n_sm = prop.multiProcessorCount;
+    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&ctx->ev0)) != cudaSuccess || (e = cudaEventCreate(&ctx->ev1)) != cudaSuccess ||
+        (e = cudaMalloc(reinterpret_cast<void**>(&ctx->d_counters), 4 * sizeof(unsigned long long))) != cudaSuccess) {
+        hadros_ctx_destroy(ctx);
+        return cuda_fail(nullptr, e, "context setup");
+    }
+    *out = ctx;
+    return ok();
+}
+
+void hadros_ctx_destroy(hadros_ctx* ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->d_cams);
+    cudaFree(ctx->d_bins);
+    cudaFree(ctx->d_pix);
+    cudaFree(ctx->d_out);
+    cudaFree(ctx->d_counters);
+    cudaFree(ctx->d_sig);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int32_t hadros_ctx_stats(const hadros_ctx* ctx, hadros_stats* out)
+{
+    if (!ctx || !out) return fail(HADROS_E_STATE, "NULL argument");
+    *out = ctx->stats;
+    return ok();
+}
+
+int32_t hadros_ctx_set_attempt_budget(hadros_ctx* ctx, int64_t attempts_per_ray)
+{
+    if (!ctx) return fail(HADROS_E_STATE, "context is NULL");
+    if (attempts_per_ray < 0) return fail(HADROS_E_ARG, "budget must be >= 0");
+    ctx->attempt_budget = attempts_per_ray;
+    return ok();
+}
+
+}  // extern "C"
+
+namespace {
+
+// Shared body of the image calls.  dev_out holds DEVICE pointers.
+int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s,
+                  const int32_t* pixel_ids_host, int32_t n_pixels, const hadros_image_out& dev_out,
+                  cudaStream_t st, bool time_kernel)
+{
+    if (!ctx) return fail(HADROS_E_STATE, "context is NULL");
+    if (ctx->failed) return fail(HADROS_E_STATE, "context is in a failed state: " + ctx->err);
+    if (!s) return fail(HADROS_E_STATE, "sigma handle is NULL");
+    int32_t rc = hadros_params_validate(p);
+    if (rc) return rc;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+
+    DevCam cam;
+    std::vector<DevBin> bins;
+    std::string err;
+    rc = build_cam(*p, s->h, cam, bins, err);
+    if (rc) return fail(rc, err);
+    const int64_t P = pixel_ids_host ? n_pixels : static_cast<int64_t>(p->nx) * p->ny;
+    if (pixel_ids_host) {
+        const int64_t total = static_cast<int64_t>(p->nx) * p->ny;
+        for (int32_t k = 0; k < n_pixels; ++k)
+            if (pixel_ids_host[k] < 0 || pixel_ids_host[k] >= total)
+                return fail(HADROS_E_ARG, "pixel id out of range");
+    }
+    cam.item_begin = 0;
+    cam.item_end = P;
+    cam.out_offset = 0;
+    cam.binout_offset = 0;
+
+    if ((rc = upload_sigma(ctx, s, sigma_serial(s)))) return rc;
+    if ((rc = grow(ctx, &ctx->d_cams, &ctx->cams_cap, sizeof(DevCam), "camera table"))) return rc;
+    if ((rc = grow(ctx, &ctx->d_bins, &ctx->bins_cap, sizeof(DevBin) * bins.size(), "bin table"))) return rc;
+    if ((e = cudaMemcpyAsync(ctx->d_cams, &cam, sizeof(DevCam), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return cuda_fail(ctx, e, "camera upload");
+    if ((e = cudaMemcpyAsync(ctx->d_bins, bins.data(), sizeof(DevBin) * bins.size(), cudaMemcpyHostToDevice, st)) !=
+        cudaSuccess)
+        return cuda_fail(ctx, e, "bin upload");
+    const int32_t* d_pix = nullptr;
+    if (pixel_ids_host && n_pixels > 0) {
+        if ((rc = grow(ctx, &ctx->d_pix, &ctx->pix_cap, sizeof(int32_t) * n_pixels, "pixel list"))) return rc;
+        if ((e = cudaMemcpyAsync(ctx->d_pix, pixel_ids_host, sizeof(int32_t) * n_pixels, cudaMemcpyHostToDevice,
+                                 st)) != cudaSuccess)
+            return cuda_fail(ctx, e, "pixel list upload");
+        d_pix = static_cast<const int32_t*>(ctx->d_pix);
+    }
+    if ((e = cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(unsigned long long), st)) != cudaSuccess)
+        return cuda_fail(ctx, e, "counter reset");
+
+    TraceArgs A{};
+    A.cams = static_cast<const DevCam*>(ctx->d_cams);
+    A.n_cams = 1;
+    A.max_bins = cam.n_bins;
+    A.total_items = P;
+    A.pixel_ids = d_pix;
+    A.bins = static_cast<const DevBin*>(ctx->d_bins);
+    A.sig = ctx->sig_dev;
+    A.tau = dev_out.tau;
+    A.P_surv = dev_out.P_surv;
+    A.I_obs = dev_out.I_obs;
+    A.fate = dev_out.fate;
+    A.steps = dev_out.steps;
+    A.attempts = dev_out.attempts;
+    A.tau_E = dev_out.tau_E;
+    A.I_E = dev_out.I_E;
+    A.counters = ctx->d_counters;
+    A.attempt_budget = ctx->attempt_budget > 0 ? ctx->attempt_budget
+                                               : static_cast<int64_t>(p->max_steps) * 51 + 1;
+
+    if (P > 0) {
+        if (time_kernel) cudaEventRecord(ctx->ev0, st);
+        rc = launch_trace(A, p->precision, ctx->n_sm, st, err);
+        if (rc) {
+            ctx->err = err;
+            return fail(rc, err);
+        }
+        if (time_kernel) cudaEventRecord(ctx->ev1, st);
+    }
+    ctx->stats.rays = P;
+    ctx->stats.launches = P > 0 ? 1 : 0;
+    return HADROS_OK;
+}
+
+// Finish a synchronous call: wait, read counters, fill stats.
+int32_t finish_sync(hadros_ctx* ctx, bool timed)
+{
+    unsigned long long c[4] = {0, 0, 0, 0};
+    cudaError_t e = cudaMemcpyAsync(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "trace kernel");
+    ctx->stats.accepted_steps = static_cast<int64_t>(c[1]);
+    ctx->stats.attempts = static_cast<int64_t>(c[2]);
+    ctx->stats.aborted_rays = static_cast<int32_t>(c[3]);
+    if (timed && ctx->stats.rays > 0) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.kernel_ms = ms;
+    }
+    if (c[3] > 0)
+        return fail(HADROS_E_TIMEOUT, std::to_string(c[3]) + " rays exceeded the attempt budget");
+    return ok();
+}
+
+int32_t image_host(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s, const int32_t* pix,
+                   int32_t n_pix, const hadros_image_out* out)
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    if (!ctx) return fail(HADROS_E_STATE, "context is NULL");
+    if (!out) return fail(HADROS_E_ARG, "output struct is NULL");
+    int32_t rc = hadros_params_validate(p);
+    if (rc) return rc;
+    if (!s) return fail(HADROS_E_STATE, "sigma handle is NULL");
+    const int64_t P = pix ? n_pix : static_cast<int64_t>(p->nx) * p->ny;
+    const int64_t B = p->spectral_kind == HADROS_SPECTRAL_MONOCHROMATIC ? 1 : std::max(p->n_bins, 1);
+    const size_t fsz = p->precision == HADROS_PRECISION_MIXED ? 4 : 8;
+    // device staging: tau, P, I (8B), steps, attempts (4B), fate (1B), tau_E, I_E
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    size_t o = 0;
+    const size_t o_tau = o; o = al(o + (out->tau ? 8 * P : 0));
+    const size_t o_P = o; o = al(o + (out->P_surv ? 8 * P : 0));
+    const size_t o_I = o; o = al(o + (out->I_obs ? 8 * P : 0));
+    const size_t o_st = o; o = al(o + (out->steps ? 4 * P : 0));
+    const size_t o_at = o; o = al(o + (out->attempts ? 4 * P : 0));
+    const size_t o_f = o; o = al(o + (out->fate ? P : 0));
+    const size_t o_tE = o; o = al(o + (out->tau_E ? fsz * P * B : 0));
+    const size_t o_IE = o; o = al(o + (out->I_E ? fsz * P * B : 0));
+    if ((rc = grow(ctx, &ctx->d_out, &ctx->out_cap, o, "output buffers"))) return rc;
+    unsigned char* base = static_cast<unsigned char*>(ctx->d_out);
+    hadros_image_out d{};
+    d.tau = out->tau ? reinterpret_cast<double*>(base + o_tau) : nullptr;
+    d.P_surv = out->P_surv ? reinterpret_cast<double*>(base + o_P) : nullptr;
+    d.I_obs = out->I_obs ? reinterpret_cast<double*>(base + o_I) : nullptr;
+    d.steps = out->steps ? reinterpret_cast<int32_t*>(base + o_st) : nullptr;
+    d.attempts = out->attempts ? reinterpret_cast<int32_t*>(base + o_at) : nullptr;
+    d.fate = out->fate ? reinterpret_cast<int8_t*>(base + o_f) : nullptr;
+    d.tau_E = out->tau_E ? static_cast<void*>(base + o_tE) : nullptr;
+    d.I_E = out->I_E ? static_cast<void*>(base + o_IE) : nullptr;
+    rc = run_image(ctx, p, s, pix, n_pix, d, ctx->stream, true);
+    if (rc) return rc;
+    struct Cp { void* h; const void* d; size_t n; } cps[8] = {
+        {out->tau, d.tau, 8 * size_t(P)}, {out->P_surv, d.P_surv, 8 * size_t(P)},
+        {out->I_obs, d.I_obs, 8 * size_t(P)}, {out->steps, d.steps, 4 * size_t(P)},
+        {out->attempts, d.attempts, 4 * size_t(P)}, {out->fate, d.fate, size_t(P)},
+        {out->tau_E, d.tau_E, fsz * size_t(P * B)}, {out->I_E, d.I_E, fsz * size_t(P * B)}};
+    for (auto& c : cps) {
+        if (!c.h || c.n == 0) continue;
+        cudaError_t e = cudaMemcpyAsync(c.h, c.d, c.n, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "output download");
+    }
+    rc = finish_sync(ctx, true);
+    ctx->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t hadros_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s, const hadros_image_out* out)
+{
+    try {
+        return image_host(ctx, p, s, nullptr, 0, out);
+    } catch (const std::exception& ex) {
+        return fail(HADROS_E_NOMEM, ex.what());
+    }
+}
+
+int32_t hadros_image_pixels(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s,
+                            const int32_t* pixel_ids, int32_t n_pixels, const hadros_image_out* out)
+{
+    if (!pixel_ids || n_pixels < 0) return fail(HADROS_E_ARG, "pixel list is NULL or negative length");
+    try {
+        return image_host(ctx, p, s, pixel_ids, n_pixels, out);
+    } catch (const std::exception& ex) {
+        return fail(HADROS_E_NOMEM, ex.what());
+    }
+}
+
+int32_t hadros_image_device(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s,
+                            const hadros_image_out* dev_out, void* stream)
+{
+    if (!dev_out) return fail(HADROS_E_ARG, "output struct is NULL");
+    try {
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : (ctx ? ctx->stream : nullptr);
+        const int32_t rc = run_image(ctx, p, s, nullptr, 0, *dev_out, st, false);
+        return rc ? rc : ok();
+    } catch (const std::exception& ex) {
+        return fail(HADROS_E_NOMEM, ex.what());
+    }
+}
+
+int32_t hadros_ctx_synchronize(hadros_ctx* ctx)
+{
+    if (!ctx) return fail(HADROS_E_STATE, "context is NULL");
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "synchronize");
+    unsigned long long c[4] = {0, 0, 0, 0};
+    e = cudaMemcpy(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "counter read");
+    ctx->stats.accepted_steps = static_cast<int64_t>(c[1]);
+    ctx->stats.attempts = static_cast<int64_t>(c[2]);
+    ctx->stats.aborted_rays = static_cast<int32_t>(c[3]);
+    if (c[3] > 0) return fail(HADROS_E_TIMEOUT, std::to_string(c[3]) + " rays exceeded the attempt budget");
+    return ok();
+}
+
+}  // extern "C"

@@ -1,0 +1,117 @@
+// hadros_internal.h — structures shared by the C-ABI host code and the
+// sm_100a trace kernel.  Not part of the public ABI.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/hadros_b200.h"
+#include "hadros_physics.cuh"
+
+namespace hadros {
+
+constexpr int kTPB = 128;        // threads per block of the trace kernel
+constexpr int kMaxBins = 256;    // per-camera spectral bins
+constexpr int kMaxSigma = 4096;  // sigma table rows staged in shared memory
+
+// Per-camera constants, computed once on the host with the host libm (so the
+// observer-side quantities are the reference's own values bit for bit).
+struct DevCam {
+    // camera and integrator (src/kerr_camera.cpp:79-186, kerr_geodesic.cpp)
+    double a;
+    double r_obs, th_obs, tan_half;
+    double r_max, h0, h_min, tol;
+    double r_stop;                    // r_+ + 1e-3
+    double g_tt, g_tph, g_rr, g_thth, g_phph;
+    double sq_grr, sq_gthth, sq_gphph;
+    double alpha_obs, omega_obs, pt_contra;
+    double c0[15];                    // RKF45 stage coefficients at h = h0
+    // transfer (src/radiative_transfer.cpp:457-685)
+    double rt_skip;                   // r_+(clamped a) + 1e-3
+    double rg_cm;
+    Torus torus;
+    Source src;
+    int32_t nx, ny, max_steps, n_bins;
+    int32_t mono;
+    int32_t bin_offset;               // first row in the bin tables
+    int64_t item_begin;               // first work item of this camera
+    int64_t item_end;
+    int64_t out_offset;               // first output row
+    int64_t binout_offset;            // first per-bin output element
+};
+
+// Per-bin constants (one row per camera bin).
+struct DevBin {
+    double E_mid;       // bin centre energy (monochromatic: Enu_obs)
+    double dE;          // bin width (1 for monochromatic)
+    double w;           // aggregation weight w(E_mid)*dE (1 for monochromatic)
+    double w0;          // spectral_weight(E_mid): scale of the FP32 intensity
+    double gg_lo, gg_hi;// E_mid/gg in [E_min, E_max]  <=>  gg in [gg_lo, gg_hi]
+    float lnE;          // log(E_mid)
+    float kcut;         // E_mid / E_cut (or / E_max for monochromatic), 0 if none
+    float gamma;        // spectral index of the ratio w(E)/w(E_mid)
+    int32_t valid;      // counted in the spectral aggregates
+};
+
+// Sigma table staged in shared memory.  FP64 arrays follow SigmaTable::
+// log_interp (src/sigma_table.cpp:81-124); the FP32 segment form is the
+// mixed-precision lookup sigma = sigma_scale * s1[k] * exp(t * dly[k]).
+struct SigmaDev {
+    int32_t n;
+    double E_min, E_max, sigma_scale;
+    const double* E;     // [n]
+    const double* S;     // [n]  sigma_cm2
+    const double* lnE;   // [n]  log(E_k)
+    const double* lnS;   // [n]  log(sigma_k)
+    const float* lx;     // [n]  (float)log(E_k)
+    const float* seg;    // [4n] per segment k>=1: lx1, 1/(lx2-lx1), s1, dly
+};
+
+struct TraceArgs {
+    const DevCam* cams;
+    int32_t n_cams;
+    int32_t max_bins;
+    int64_t total_items;
+    const int32_t* pixel_ids;   // optional list (single camera)
+    const DevBin* bins;
+    SigmaDev sig;
+    // outputs (device); any may be null
+    double* tau;
+    double* P_surv;
+    double* I_obs;
+    int8_t* fate;
+    int32_t* steps;
+    int32_t* attempts;
+    void* tau_E;
+    void* I_E;
+    // scratch
+    unsigned long long* counters;   // [0] work cursor, [1] steps, [2] attempts, [3] aborted
+    int64_t attempt_budget;
+};
+
+// Host-side handle of an uploaded sigma table.
+struct SigmaHost {
+    std::vector<double> E, s_GeV2, s_cm2;
+    std::vector<double> lnE, lnS;
+    std::vector<float> lx, seg;
+    double sigma_scale = 1.0;
+};
+
+// Camera plan building (host, hadros_trace.cu).
+int build_cam(const hadros_params& p, const SigmaHost& sig, DevCam& cam,
+              std::vector<DevBin>& bins, std::string& err);
+void prepare_sigma(SigmaHost& s);
+
+// Kernel launch (hadros_trace.cu).  `stream` is a cudaStream_t.
+int launch_trace(const TraceArgs& args, int precision, int n_sm, void* stream,
+                 std::string& err);
+size_t trace_smem_bytes(int precision, int sig_n, int max_bins);
+
+}  // namespace hadros
+
+// hadros_sigma is the public opaque handle.
+struct hadros_sigma {
+    hadros::SigmaHost h;
+    uint64_t serial = 0;   // distinguishes handles that reuse an address
+};

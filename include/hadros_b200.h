@@ -1,0 +1,289 @@
+/*
+ * hadros_b200.h — C ABI of the B200-native HADROS per-pixel image pipeline.
+ *
+ * The pipeline is the one HADROS runs per pixel: Kerr camera ray setup,
+ * RKF45 null-geodesic integration in Boyer-Lindquist coordinates, DIS optical
+ * depth tau_E = sum n_b sigma_CC(E_local) dl and UHE radiative transfer
+ * I_E += g^3 j(r, theta, E_local) exp(-tau_E) dl per spectral bin.
+ *
+ * In the reference these stages are C++ classes driven by command-line
+ * executables (no library API):
+ *   KerrCamera::trace_pixel                  src/kerr_camera.cpp:188-283
+ *   KerrGeodesic::step_adaptive              src/kerr_geodesic.cpp:194-329
+ *   SigmaTable                               src/sigma_table.cpp:9-124
+ *   TorusProfile::rho                        src/torus_profile.cpp:261-272
+ *   radiative_transfer::integrate_kerr_ray_spectral
+ *                                            src/radiative_transfer.cpp:687-780
+ *   executables compute_kerr_geodesics + compute_kerr_image_from_cache
+ *   (CPU) and compute_kerr_image_cuda (GPU).
+ * This header replaces that boundary with plain C: POD parameters, caller-owned
+ * output buffers, integer status codes and a per-thread error message.
+ *
+ * Conventions
+ *  - Pixel p = j * nx + i, i in [0, nx) along alpha (u), j in [0, ny) along
+ *    beta (v); the reference's KIMG row order (apps/compute_kerr_image_cuda.cu:
+ *    279-332).
+ *  - No function throws or aborts; every entry point returns HADROS_OK (0) or
+ *    a HADROS_E_* code and leaves a message for hadros_last_error().
+ *  - A hadros_ctx owns one CUDA stream and its device buffers; one context is
+ *    used by one host thread at a time. Distinct contexts may run concurrently.
+ *  - A hadros_sigma handle is immutable after creation and may be shared.
+ */
+#ifndef HADROS_B200_H
+#define HADROS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HADROS_ABI_VERSION 1
+
+/* Status codes.  The reference reports errors by throwing std::runtime_error
+ * (e.g. src/torus_profile.cpp:85-90, src/sigma_table.cpp:14-16) or by exiting
+ * with code 1/2 (apps/compute_kerr_image_cuda.cu:2607-2610, :1822). */
+enum hadros_status {
+    HADROS_OK = 0,
+    HADROS_E_ARG = 1,     /* bad argument, unknown model name, bad sizes   */
+    HADROS_E_IO = 2,      /* file missing, unreadable or malformed          */
+    HADROS_E_CUDA = 3,    /* CUDA runtime error or no usable device         */
+    HADROS_E_RANGE = 4,   /* energy outside the sigma table                 */
+    HADROS_E_TIMEOUT = 5, /* device attempt budget exhausted (rays aborted) */
+    HADROS_E_NOMEM = 6,   /* host or device allocation failed               */
+    HADROS_E_STATE = 7    /* null handle or call on a failed context        */
+};
+
+/* Density morphologies, in the order of DensityProfileKind
+ * (include/torus_profile.hpp:6-15). */
+enum hadros_profile_kind {
+    HADROS_PROFILE_GAUSSIAN = 0,
+    HADROS_PROFILE_POWERLAW = 1,
+    HADROS_PROFILE_GAUSSIAN_FUNNEL = 2,
+    HADROS_PROFILE_POWERLAW_FUNNEL = 3,
+    HADROS_PROFILE_GAUSSIAN_ENVELOPE = 4,
+    HADROS_PROFILE_POWERLAW_ENVELOPE = 5,
+    HADROS_PROFILE_POWERLAW_FUNNEL_ENVELOPE = 6,
+    HADROS_PROFILE_COLLAPSAR_NDAF_LIKE = 7
+};
+
+/* UHE source morphologies (include/radiative_transfer.hpp:37-43). */
+enum hadros_source_kind {
+    HADROS_SOURCE_INNER_RING = 0,
+    HADROS_SOURCE_FUNNEL_WALL = 1,
+    HADROS_SOURCE_JET_BASE = 2,
+    HADROS_SOURCE_SHOCK_LAYER = 3,
+    HADROS_SOURCE_DENSITY_WEIGHTED = 4
+};
+
+/* UHE spectral models (include/radiative_transfer.hpp:23-27). */
+enum hadros_spectral_kind {
+    HADROS_SPECTRAL_MONOCHROMATIC = 0,
+    HADROS_SPECTRAL_POWERLAW = 1,
+    HADROS_SPECTRAL_POWERLAW_CUTOFF = 2
+};
+
+/* Arithmetic of the transfer stage.  The geodesic is FP64 in both. */
+enum hadros_precision {
+    HADROS_PRECISION_FP64 = 0,  /* every stage FP64, reference operation order */
+    HADROS_PRECISION_MIXED = 1  /* FP64 geodesic; FP32 Kahan tau and I per bin */
+};
+
+/* Ray fate.  The reference keeps only `captured` (include/ray.hpp:25); a ray
+ * that hits the step cap has captured == false (src/kerr_camera.cpp:222). */
+enum hadros_fate {
+    HADROS_FATE_ESCAPED = 0,   /* r >= r_max after more than 10 steps     */
+    HADROS_FATE_CAPTURED = 1,  /* r <= r_+ + 1e-3                          */
+    HADROS_FATE_TRUNCATED = 2  /* step cap reached first ("neither")      */
+};
+
+/* All parameters of one camera/image.  Fill with hadros_params_default()
+ * and override fields.  Angles are radians except fov_deg, which KerrCamera
+ * takes in degrees (src/kerr_camera.cpp:79-98). */
+typedef struct hadros_params {
+    uint32_t struct_size;    /* = sizeof(hadros_params); set by _default   */
+    int32_t nx, ny;          /* image size                                  */
+    int32_t max_steps;       /* step cap; reference hard-codes 200000      */
+    int32_t profile_kind;    /* enum hadros_profile_kind                    */
+    int32_t source_kind;     /* enum hadros_source_kind                     */
+    int32_t spectral_kind;   /* enum hadros_spectral_kind                   */
+    int32_t n_bins;          /* spectral bins (ignored for monochromatic)  */
+    int32_t precision;       /* enum hadros_precision                       */
+    int32_t reserved0;
+
+    /* camera and integrator: KerrCamera(a, r_obs, theta_obs, fov_deg, nx,
+     * ny, r_max, h) with KerrGeodesic tolerance (include/kerr_geodesic.hpp:
+     * 10-13; the CPU image path uses the default 1e-6). */
+    double a_spin;
+    double r_obs_rg;
+    double theta_obs_rad;
+    double fov_deg;
+    double r_max_rg;
+    double h;
+    double tolerance;
+
+    /* observed energy (monochromatic) and black-hole mass */
+    double Enu_obs_GeV;
+    double M_bh_msun;
+
+    /* TorusProfile constructor arguments (include/torus_profile.hpp:19-33) */
+    double rho0_gcm3;
+    double r0_rg;
+    double sigma_r_rg;
+    double H_over_R;
+    double radial_power;
+    double funnel_depletion;
+    double funnel_theta_rad;
+    double envelope_rho0_gcm3;
+    double envelope_alpha;
+    double torus_r_min_rg;
+    double torus_r_max_rg;
+    double rho_floor_gcm3;
+
+    /* UHESourceParams (include/radiative_transfer.hpp:45-62) */
+    double src_r_center_rg;
+    double src_sigma_r_rg;
+    double src_theta_width_rad;
+    double src_powerlaw;
+    double src_emax_GeV;
+    double src_norm;
+    double src_funnel_theta_rad;
+    double src_density_power_q;
+    double src_radial_power_s;
+    double src_rho_ref_gcm3;
+    double src_cutoff_min;
+    double src_cutoff_max;
+    double src_gradient_dr_rg;
+    double src_gradient_dtheta_rad;
+
+    /* UHESpectralParams (include/radiative_transfer.hpp:29-35) */
+    double spec_gamma;
+    double spec_ecut_GeV;
+    double spec_e_min_GeV;
+    double spec_e_max_GeV;
+} hadros_params;
+
+/* Caller-owned outputs.  Any pointer may be NULL (that output is skipped).
+ * Per-pixel arrays hold nx*ny entries (or n_pixels for the pixel-list call);
+ * per-bin arrays hold that many rows of n_bins entries (1 for
+ * monochromatic), float in HADROS_PRECISION_MIXED and double in FP64.
+ * tau/P_surv/I_obs are integrate_kerr_ray_spectral's aggregates
+ * (src/radiative_transfer.cpp:687-780); tau_E/I_E are integrate_kerr_ray
+ * at each bin's E_mid (src/radiative_transfer.cpp:457-685). */
+typedef struct hadros_image_out {
+    double* tau;
+    double* P_surv;
+    double* I_obs;
+    int8_t* fate;       /* enum hadros_fate                                */
+    int32_t* steps;     /* accepted steps = RayPath::points.size()         */
+    int32_t* attempts;  /* RKF45 attempts (>= steps)                       */
+    void* tau_E;
+    void* I_E;
+} hadros_image_out;
+
+/* Run statistics of the last image/batch call on a context. */
+typedef struct hadros_stats {
+    double kernel_ms;        /* device time of the trace kernel(s)          */
+    double total_ms;         /* host wall time of the whole call            */
+    int64_t rays;
+    int64_t accepted_steps;  /* sum of steps                                */
+    int64_t attempts;        /* sum of attempts                             */
+    int32_t launches;        /* kernels this library launched in the call  */
+    int32_t aborted_rays;    /* rays stopped by the attempt budget          */
+} hadros_stats;
+
+/* ---- library info, names and parameters --------------------------------- */
+
+int32_t hadros_abi_version(void);
+const char* hadros_status_string(int32_t status);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* hadros_last_error(void);
+
+/* Reference defaults: KerrCamera args of compute_kerr_geodesics
+ * (apps/compute_kerr_geodesics.cpp:26-34), argv defaults of
+ * compute_kerr_image_from_cache (apps/compute_kerr_image_from_cache.cpp:
+ * 33-55), tolerance 1e-6, max_steps 200000, UHESourceParams/UHESpectralParams
+ * member defaults. */
+void hadros_params_default(hadros_params* p);
+/* Validate sizes, kinds and finiteness; HADROS_E_ARG with a message. */
+int32_t hadros_params_validate(const hadros_params* p);
+
+/* Name -> kind with the reference's aliases and error text
+ * (src/torus_profile.cpp:44-91, src/radiative_transfer.cpp:80-156). */
+int32_t hadros_parse_profile(const char* name, int32_t* kind);
+int32_t hadros_parse_source(const char* name, int32_t* kind);
+int32_t hadros_parse_spectral(const char* name, int32_t* kind);
+const char* hadros_profile_name(int32_t kind);
+const char* hadros_source_name(int32_t kind);
+const char* hadros_spectral_name(int32_t kind);
+
+/* ---- sigma_CC(E) table (SigmaTable, src/sigma_table.cpp) ------------------ */
+
+typedef struct hadros_sigma hadros_sigma;
+
+/* Parse a 3-column "E_GeV sigma_GeV^-2 sigma_cm2" file: '#' and empty lines
+ * and non-positive rows skipped, >= 2 rows, strictly increasing E
+ * (src/sigma_table.cpp:9-53). */
+int32_t hadros_sigma_load(const char* path, hadros_sigma** out);
+/* Same validation from arrays (sigma_GeV2 may be NULL). */
+int32_t hadros_sigma_from_arrays(const double* E_GeV, const double* sigma_GeV2,
+                                 const double* sigma_cm2, int32_t n,
+                                 hadros_sigma** out);
+int32_t hadros_sigma_info(const hadros_sigma* s, int32_t* n, double* E_min,
+                          double* E_max);
+/* SigmaTable::sigma_cm2: log-log interpolation, HADROS_E_RANGE outside
+ * [E_min, E_max] (src/sigma_table.cpp:81-124).  Host-side. */
+int32_t hadros_sigma_eval_cm2(const hadros_sigma* s, double E_GeV, double* out);
+void hadros_sigma_destroy(hadros_sigma* s);
+
+/* Spectral bins integrate_kerr_ray_spectral uses (src/radiative_transfer.cpp:
+ * 711-737): *n_bins_out entries of E_mid, dE, weight and valid (weight > 0
+ * and finite).  Monochromatic: one bin at Enu_obs_GeV, dE = weight = 1.
+ * Arrays must hold max(n_bins, 1) entries; any may be NULL. */
+int32_t hadros_spectral_bins(const hadros_params* p, const hadros_sigma* s,
+                             double* E_mid, double* dE, double* weight,
+                             int8_t* valid, int32_t* n_bins_out);
+
+/* ---- device contexts and the image call ----------------------------------- */
+
+typedef struct hadros_ctx hadros_ctx;
+
+/* Create a context on CUDA device `device` (its own non-blocking stream).
+ * HADROS_E_CUDA when the device or the kernels for sm_100a are unusable. */
+int32_t hadros_ctx_create(int32_t device, hadros_ctx** out);
+void hadros_ctx_destroy(hadros_ctx* ctx);
+int32_t hadros_ctx_stats(const hadros_ctx* ctx, hadros_stats* out);
+/* Upper bound on RKF45 attempts per ray before the ray is aborted with
+ * HADROS_E_TIMEOUT (0 = max_steps * 51, the most step_adaptive can take). */
+int32_t hadros_ctx_set_attempt_budget(hadros_ctx* ctx, int64_t attempts_per_ray);
+
+/* Whole image.  Replaces compute_kerr_geodesics + compute_kerr_image_from_
+ * cache (apps/compute_kerr_geodesics.cpp:24-146, apps/compute_kerr_image_
+ * from_cache.cpp:31-722) and compute_kerr_image_cuda's in-line mode
+ * (apps/compute_kerr_image_cuda.cu:2239-2611).  Outputs are HOST buffers;
+ * the call returns when they are filled. */
+int32_t hadros_image(hadros_ctx* ctx, const hadros_params* p,
+                     const hadros_sigma* s, const hadros_image_out* out);
+
+/* Subset of pixels (ids j*nx+i); outputs indexed by list position.  The
+ * oracle harness's trace_pixel-over-a-subset, used for strided CPU baselines
+ * and for judging a random pixel subset. */
+int32_t hadros_image_pixels(hadros_ctx* ctx, const hadros_params* p,
+                            const hadros_sigma* s, const int32_t* pixel_ids,
+                            int32_t n_pixels, const hadros_image_out* out);
+
+/* Whole image into DEVICE buffers on `stream` (a cudaStream_t, NULL = the
+ * context's stream).  Asynchronous: returns after enqueueing.  For callers
+ * that keep results in HBM (batched scans, benchmarks). */
+int32_t hadros_image_device(hadros_ctx* ctx, const hadros_params* p,
+                            const hadros_sigma* s,
+                            const hadros_image_out* dev_out, void* stream);
+/* Wait for the context's work and report the first deferred error. */
+int32_t hadros_ctx_synchronize(hadros_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HADROS_B200_H */

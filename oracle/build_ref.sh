@@ -1,0 +1,23 @@
+#!/usr/bin/env bash
+# Builds oracle/_ref/libhadros_ref.so: the reference's own hot-path sources,
+# compiled where they lie (read-only, unmodified) with the reference Makefile's
+# flags (-O3 -std=c++17 -fopenmp, no -march), plus oracle/ref_driver.cpp.
+# Test infrastructure only; outputs go to oracle/_ref/ (git-ignored).
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+set -euo pipefail
+here="$(cd "$(dirname "$0")" && pwd)"
+ref="${1:-/root/reference}"
+out="$here/_ref"
+if [ ! -d "$ref/src" ]; then
+    echo "build_ref: no reference sources at $ref; skipping" >&2
+    exit 0
+fi
+mkdir -p "$out"
+srcs=""
+for f in kerr_metric kerr_geodesic kerr_camera sigma_table torus_profile \
+         radiative_transfer mev_neutrino_physics; do
+    srcs="$srcs $ref/src/$f.cpp"
+done
+g++ -O3 -std=c++17 -fopenmp -fPIC -shared -I"$ref/include" \
+    -o "$out/libhadros_ref.so" $srcs "$here/ref_driver.cpp"
+echo "built $out/libhadros_ref.so"
