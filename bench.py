@@ -1,0 +1,389 @@
+#!/usr/bin/env python
+"""bench.py — pixel-bins/s of the HADROS per-pixel image pipeline on B200.
+
+A step traces one image of the workload (default: the 512x512 mixed-precision
+image with 8 powerlaw_cutoff bins, hadros_b200.workloads.mixed_512) through
+the trace kernel.  One process per GPU; each GPU traces its own image per step
+(pixels are independent, no data-path collective: weak scaling).
+
+  value       device-timed throughput, outputs resident in HBM (CUDA events
+              around K steps, L2 flushed between steps, max over ranks)
+  e2e         the same metric through the C-ABI call a user makes
+              (hadros_image: parameters host->device, image device->host)
+  roofline    the trace kernel's FP64 arithmetic rate against the measured
+              FP64 peak (cuBLAS DGEMM on this GPU, measured in the same run)
+  cpu_baseline the reference CPU code (or the oracle port) on the host cores
+              over a strided pixel subset of the same image
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+# Algorithmic FP64 work, counted from the reference formulas with their
+# duplicate inverse-metric evaluations removed (+,-,*,/ = 1 flop; FMA = 2;
+# transcendentals not counted): one RKF45 attempt = 6 RHS (192 each) + stage
+# inputs + y4/y5 + error = 1573 flop; one accepted step's ZAMO interval and
+# redshift = 52 flop.  Per point 44 flop and per point-bin 16 flop of transfer.
+F_ATT, F_GEO, F_PT, F_PB = 1573, 52, 44, 16
+FP64_PEAK_DATASHEET_TFLOPS = 37.0
+WORKLOAD_DESC = ("512x512 px x 8 powerlaw_cutoff bins (1e5-1e12 GeV), a=0.998, i=17 deg, "
+                 "powerlaw_funnel_envelope, funnel_wall source, r_obs 60 M, fov 25 deg, h0 0.01, "
+                 "FP64 RKF45 geodesics + FP32 Kahan transfer")
+
+
+def env_int(name: str, default: int) -> int:
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+# --------------------------------------------------------------------------- CPU baseline
+
+def cpu_sample(params_kw: dict, stride: int, threads: int) -> dict:
+    """Time the reference CPU implementation (oracle/_ref, or the oracle port)
+    on every `stride`-th pixel in i and j of the image."""
+    import hadros_b200 as hb
+    from hadros_b200 import workloads as W
+    from oracle import pyoracle as O
+    E, g2, s = W.synthetic_sigma_arrays()
+    p = hb.params(**params_kw)
+    ids = W.strided_pixels(p.nx, p.ny, stride)
+    B = 1 if p.spectral_kind == 0 else p.n_bins
+    kind = "reference" if O.ref_available() else "port"
+    t0 = time.perf_counter()
+    if kind == "reference":
+        O.ref_image(p, E, g2, s, pixel_ids=ids, threads=threads, per_bin=False)
+    else:
+        O.oracle_image(p, E, s, pixel_ids=ids, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": ids.size * B / dt, "seconds": dt, "rays": int(ids.size), "kind": kind,
+            "cores": threads, "stride": stride}
+
+
+def describe_cpu(c: dict, nx: int, ny: int) -> str:
+    what = ("reference CPU code built from its sources (KerrCamera::trace_pixel + "
+            "integrate_kerr_ray_spectral, MeV block as shipped)" if c["kind"] == "reference"
+            else "CPU oracle port (oracle/hadros_oracle.c)")
+    return (f"every {c['stride']}th pixel in i and j of the {nx}x{ny} image ({c['rays']} rays), "
+            f"{what}, OpenMP {c['cores']} threads, {c['seconds']:.1f} s")
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_arm(args) -> None:
+    """--impl reference: the reference's own CPU implementation on the host cores."""
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return
+    from hadros_b200 import workloads as W
+    kw = W.mixed_512()
+    threads = host_threads()
+    stride = 48
+    for _ in range(args.warmup):
+        cpu_sample(kw, stride, threads)
+    times, last = [], None
+    for _ in range(args.steps):
+        last = cpu_sample(kw, stride, threads)
+        times.append(last["seconds"])
+    per_step = sum(times) / len(times)
+    value = last["rays"] * kw["n_bins"] / per_step
+    line = {
+        "impl": "reference", "metric": "pixel-bins/sec", "value": value, "unit": "pixel-bins/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "mixed_512: " + WORKLOAD_DESC,
+                   "sample": f"every {stride}th pixel in i and j ({last['rays']} rays) per step"},
+        "cpu_baseline": {"value": value, "unit": "pixel-bins/s", "cores": threads,
+                         "kind": last["kind"], "sample": describe_cpu(last, 512, 512)},
+        "e2e": {"value": value, "unit": "pixel-bins/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-i", str(self.idx), "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.file.flush()
+        rows = []
+        try:
+            text = Path(self.file.name).read_text()
+            for r in csv.reader(io.StringIO(text)):
+                if len(r) >= 9:
+                    rows.append([x.strip() for x in r])
+        finally:
+            os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "", 1).isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "", 1).isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        load = sorted(sm)[len(sm) // 4:] if sm else []
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+# --------------------------------------------------------------------------- GPU arm
+
+def fp64_peak_tflops(torch, device) -> float:
+    """cuBLAS DGEMM 8192^3 on this GPU, best of 5 (CUDA events)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def read_traffic() -> tuple[float | None, str | None]:
+    """DRAM bytes per trace-kernel launch from a committed ncu summary."""
+    f = ROOT / "profiles" / "ncu_traffic.json"
+    if not f.exists():
+        return None, None
+    d = json.loads(f.read_text())
+    return d.get("bytes_per_launch"), d.get("source")
+
+
+def gpu_arm(args) -> None:
+    import torch
+
+    import hadros_b200 as hb
+    from hadros_b200 import workloads as W
+
+    rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=device)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    kw = W.mixed_512()
+    p = hb.params(**kw)
+    E, g2, s = W.synthetic_sigma_arrays()
+    sig = hb.SigmaTable.from_arrays(E, s, g2)
+    ctx = hb.Context(local)
+    P, B = p.nx * p.ny, p.n_bins
+    f32 = p.precision == hb.PRECISION_MIXED
+    out = {
+        "tau": torch.empty(P, dtype=torch.float64, device=device),
+        "P_surv": torch.empty(P, dtype=torch.float64, device=device),
+        "I_obs": torch.empty(P, dtype=torch.float64, device=device),
+        "fate": torch.empty(P, dtype=torch.int8, device=device),
+        "steps": torch.empty(P, dtype=torch.int32, device=device),
+        "attempts": torch.empty(P, dtype=torch.int32, device=device),
+        "tau_E": torch.empty(P * B, dtype=torch.float32 if f32 else torch.float64, device=device),
+        "I_E": torch.empty(P * B, dtype=torch.float64, device=device),
+    }
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)   # > 126 MB L2
+    # a non-default stream: the library launches on it, the events bracket it
+    stream = torch.cuda.Stream(device=device)
+    torch.cuda.set_stream(stream)
+
+    for _ in range(args.warmup):
+        ctx.image_device(p, sig, out, stream)
+        flush.zero_()
+    ctx.synchronize()
+    barrier()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    gpu_index = local
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        try:
+            gpu_index = int(vis.split(",")[local])
+        except (ValueError, IndexError):
+            gpu_index = local
+    launches = 0
+    with ClockSampler(gpu_index) as clocks:
+        t_start.record(stream)
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            ctx.image_device(p, sig, out, stream)
+            launches += ctx.stats()["launches"]
+            ev[k][1].record(stream)
+            flush.zero_()
+        t_end.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    clk = clocks.summary()
+    ctx.synchronize()
+    elapsed = t_start.elapsed_time(t_end) / 1e3
+    kernel_ms = [a.elapsed_time(b) for a, b in ev]
+    elapsed_max = max_over_ranks(elapsed)
+    per_step = elapsed_max / args.steps
+    value = world * P * B / per_step
+
+    attempts = float(out["attempts"].to(torch.int64).sum().item())
+    steps_sum = float(out["steps"].to(torch.int64).sum().item())
+    flop64 = attempts * F_ATT + steps_sum * F_GEO
+    flop32 = steps_sum * (F_PT + B * F_PB)
+    kern_s = statistics.mean(kernel_ms) / 1e3
+    peak = fp64_peak_tflops(torch, device)
+    achieved = flop64 / kern_s / 1e12
+    traffic, traffic_src = read_traffic()
+
+    # e2e through the C-ABI call with host buffers (hadros_image)
+    barrier()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    e2e_kernel_ms = []
+    for _ in range(args.steps):
+        ctx.image(p, sig)
+        st = ctx.stats()
+        h2d, d2h = st["h2d_bytes"], st["d2h_bytes"]
+        e2e_kernel_ms.append(st["kernel_ms"])
+    e2e_s = max_over_ranks(time.perf_counter() - t0) / args.steps
+    e2e_value = world * P * B / e2e_s
+
+    fates = torch.bincount(out["fate"].to(torch.int64), minlength=3).tolist()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        c = cpu_sample(kw, 24, host_threads())
+        cpu = {"value": c["value"], "unit": "pixel-bins/s", "cores": c["cores"], "kind": c["kind"],
+               "sample": describe_cpu(c, p.nx, p.ny)}
+    total_steps = sum_over_ranks(steps_sum)
+    if rank == 0:
+        line = {
+            "metric": "pixel-bins/sec", "value": value, "unit": "pixel-bins/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64+f32", "data": "synthetic",
+            "config": {"workload": "mixed_512: " + WORKLOAD_DESC,
+                       "per_gpu": "one 512x512x8 image per GPU per step",
+                       "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"independent images, {world} GPU(s), no collective"},
+            "rays_per_s": world * P / per_step,
+            "accepted_steps_per_s": total_steps / per_step,
+            "fates": {"escaped": fates[0], "captured": fates[1], "truncated": fates[2]},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 "
+                                        f"(datasheet {FP64_PEAK_DATASHEET_TFLOPS} TFLOP/s)",
+                         "flop64_per_launch": flop64, "flop32_per_launch": flop32,
+                         "kernel_ms": statistics.mean(kernel_ms),
+                         "traffic": traffic, "traffic_source": traffic_src},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "pixel-bins/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
+                    "kernel_ms": statistics.mean(e2e_kernel_ms)},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["hadros", "reference"], default="hadros")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

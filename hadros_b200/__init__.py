@@ -224,7 +224,7 @@ class Context:
         fdt = np.float32 if p.precision == PRECISION_MIXED else np.float64
         shapes = {"tau": (P, np.float64), "P_surv": (P, np.float64), "I_obs": (P, np.float64),
                   "fate": (P, np.int8), "steps": (P, np.int32), "attempts": (P, np.int32),
-                  "tau_E": ((P, B), fdt), "I_E": ((P, B), fdt)}
+                  "tau_E": ((P, B), fdt), "I_E": ((P, B), np.float64)}
         res = {k: np.zeros(shapes[k][0], dtype=shapes[k][1]) for k in outputs}
         out = HadrosImageOut()
         for k, arr in res.items():

@@ -103,6 +103,8 @@ class HadrosStats(C.Structure):
         ("rays", C.c_int64),
         ("accepted_steps", C.c_int64),
         ("attempts", C.c_int64),
+        ("h2d_bytes", C.c_int64),
+        ("d2h_bytes", C.c_int64),
         ("launches", C.c_int32),
         ("aborted_rays", C.c_int32),
     ]

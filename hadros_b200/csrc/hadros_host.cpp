@@ -527,6 +527,7 @@ int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s
     cam.out_offset = 0;
     cam.binout_offset = 0;
 
+    const bool sigma_new = !(ctx->sig_key == s && ctx->sig_serial == sigma_serial(s) && ctx->d_sig);
     if ((rc = upload_sigma(ctx, s, sigma_serial(s)))) return rc;
     if ((rc = grow(ctx, &ctx->d_cams, &ctx->cams_cap, sizeof(DevCam), "camera table"))) return rc;
     if ((rc = grow(ctx, &ctx->d_bins, &ctx->bins_cap, sizeof(DevBin) * bins.size(), "bin table"))) return rc;
@@ -535,8 +536,11 @@ int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s
     if ((e = cudaMemcpyAsync(ctx->d_bins, bins.data(), sizeof(DevBin) * bins.size(), cudaMemcpyHostToDevice, st)) !=
         cudaSuccess)
         return cuda_fail(ctx, e, "bin upload");
+    int64_t h2d = static_cast<int64_t>(sizeof(DevCam) + sizeof(DevBin) * bins.size());
+    if (sigma_new) h2d += static_cast<int64_t>(ctx->sig_cap);
     const int32_t* d_pix = nullptr;
     if (pixel_ids_host && n_pixels > 0) {
+        h2d += static_cast<int64_t>(sizeof(int32_t)) * n_pixels;
         if ((rc = grow(ctx, &ctx->d_pix, &ctx->pix_cap, sizeof(int32_t) * n_pixels, "pixel list"))) return rc;
         if ((e = cudaMemcpyAsync(ctx->d_pix, pixel_ids_host, sizeof(int32_t) * n_pixels, cudaMemcpyHostToDevice,
                                  st)) != cudaSuccess)
@@ -561,7 +565,7 @@ int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s
     A.steps = dev_out.steps;
     A.attempts = dev_out.attempts;
     A.tau_E = dev_out.tau_E;
-    A.I_E = dev_out.I_E;
+    A.I_E = static_cast<double*>(dev_out.I_E);
     A.counters = ctx->d_counters;
     A.attempt_budget = ctx->attempt_budget > 0 ? ctx->attempt_budget
                                                : static_cast<int64_t>(p->max_steps) * 51 + 1;
@@ -577,6 +581,8 @@ int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s
     }
     ctx->stats.rays = P;
     ctx->stats.launches = P > 0 ? 1 : 0;
+    ctx->stats.h2d_bytes = h2d;
+    ctx->stats.d2h_bytes = 0;
     return HADROS_OK;
 }
 
@@ -621,7 +627,7 @@ int32_t image_host(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* 
     const size_t o_at = o; o = al(o + (out->attempts ? 4 * P : 0));
     const size_t o_f = o; o = al(o + (out->fate ? P : 0));
     const size_t o_tE = o; o = al(o + (out->tau_E ? fsz * P * B : 0));
-    const size_t o_IE = o; o = al(o + (out->I_E ? fsz * P * B : 0));
+    const size_t o_IE = o; o = al(o + (out->I_E ? 8 * P * B : 0));
     if ((rc = grow(ctx, &ctx->d_out, &ctx->out_cap, o, "output buffers"))) return rc;
     unsigned char* base = static_cast<unsigned char*>(ctx->d_out);
     hadros_image_out d{};
@@ -639,13 +645,16 @@ int32_t image_host(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* 
         {out->tau, d.tau, 8 * size_t(P)}, {out->P_surv, d.P_surv, 8 * size_t(P)},
         {out->I_obs, d.I_obs, 8 * size_t(P)}, {out->steps, d.steps, 4 * size_t(P)},
         {out->attempts, d.attempts, 4 * size_t(P)}, {out->fate, d.fate, size_t(P)},
-        {out->tau_E, d.tau_E, fsz * size_t(P * B)}, {out->I_E, d.I_E, fsz * size_t(P * B)}};
+        {out->tau_E, d.tau_E, fsz * size_t(P * B)}, {out->I_E, d.I_E, 8 * size_t(P * B)}};
+    int64_t d2h = 4 * sizeof(unsigned long long);
     for (auto& c : cps) {
         if (!c.h || c.n == 0) continue;
+        d2h += static_cast<int64_t>(c.n);
         cudaError_t e = cudaMemcpyAsync(c.h, c.d, c.n, cudaMemcpyDeviceToHost, ctx->stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "output download");
     }
     rc = finish_sync(ctx, true);
+    ctx->stats.d2h_bytes = d2h;
     ctx->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rc;
 }

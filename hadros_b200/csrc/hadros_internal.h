@@ -83,8 +83,8 @@ struct TraceArgs {
     int8_t* fate;
     int32_t* steps;
     int32_t* attempts;
-    void* tau_E;
-    void* I_E;
+    void* tau_E;        // float (mixed) or double (fp64)
+    double* I_E;
     // scratch
     unsigned long long* counters;   // [0] work cursor, [1] steps, [2] attempts, [3] aborted
     int64_t attempt_budget;

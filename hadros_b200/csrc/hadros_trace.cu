@@ -226,10 +226,12 @@ int build_cam(const hadros_params& p, const SigmaHost& sig, DevCam& cam,
                 b.valid = (b.w <= 0.0 || !std::isfinite(b.w)) ? 0 : 1;
                 ratio_consts(b);
             } else {
-                b.E_mid = 1.0;   // harmless placeholder: no valid bin
+                // empty band: the reference computes no bin (RTResult{} defaults)
+                b.E_mid = 0.0;
                 b.valid = 0;
-                ratio_consts(b);
                 b.w0 = 0.0;
+                b.gg_lo = std::numeric_limits<double>::infinity();
+                b.gg_hi = -std::numeric_limits<double>::infinity();
             }
             bb.push_back(b);
         }
@@ -350,7 +352,7 @@ __host__ __device__ inline SmemLayout smem_layout(int precision, int n, int max_
     L.off_seg = o; o += sizeof(float) * 4 * n;
     o = (o + 15) & ~size_t(15);
     L.off_acc = o;
-    o += (precision == HADROS_PRECISION_MIXED ? 4 * sizeof(float) : 2 * sizeof(double)) *
+    o += (precision == HADROS_PRECISION_MIXED ? 5 * sizeof(float) : 2 * sizeof(double)) *
          size_t(kTPB) * size_t(max_bins);
     L.total = o;
     return L;
@@ -390,6 +392,7 @@ __global__ void __launch_bounds__(kTPB) trace_kernel(const TraceArgs A)
     float* accTc = accT + size_t(kTPB) * A.max_bins;
     float* accI = accTc + size_t(kTPB) * A.max_bins;
     float* accIc = accI + size_t(kTPB) * A.max_bins;
+    float* accS = accIc + size_t(kTPB) * A.max_bins;
 
     int phase = kNeedRay;
     // ray state
@@ -457,6 +460,7 @@ __global__ void __launch_bounds__(kTPB) trace_kernel(const TraceArgs A)
                     if (MIXED) {
                         accT[b * kTPB] = 0.0f; accTc[b * kTPB] = 0.0f;
                         accI[b * kTPB] = 0.0f; accIc[b * kTPB] = 0.0f;
+                        accS[b * kTPB] = 0.0f;
                     } else {
                         accT64[b * kTPB] = 0.0; accI64[b * kTPB] = 0.0;
                     }
@@ -483,7 +487,9 @@ __global__ void __launch_bounds__(kTPB) trace_kernel(const TraceArgs A)
                     double tb, ib;
                     if (MIXED) {
                         tb = static_cast<double>(accT[b * kTPB]);
-                        ib = static_cast<double>(accI[b * kTPB]) * bins[b].w0;
+                        // I = (I_s - c) * exp(-S) * w(E_mid)
+                        ib = (static_cast<double>(accI[b * kTPB]) - static_cast<double>(accIc[b * kTPB])) *
+                             exp(-static_cast<double>(accS[b * kTPB])) * bins[b].w0;
                     } else {
                         tb = accT64[b * kTPB];
                         ib = accI64[b * kTPB];
@@ -491,11 +497,10 @@ __global__ void __launch_bounds__(kTPB) trace_kernel(const TraceArgs A)
                     const long long e = cam->binout_offset + local * B + b;
                     if (MIXED) {
                         if (A.tau_E) static_cast<float*>(A.tau_E)[e] = static_cast<float>(tb);
-                        if (A.I_E) static_cast<float*>(A.I_E)[e] = static_cast<float>(ib);
                     } else {
                         if (A.tau_E) static_cast<double*>(A.tau_E)[e] = tb;
-                        if (A.I_E) static_cast<double*>(A.I_E)[e] = ib;
                     }
+                    if (A.I_E) A.I_E[e] = ib;
                     if (cam->mono) {
                         t_out = tb; p_out = exp(-tb); i_out = ib;
                     } else if (bins[b].valid) {   // radiative_transfer.cpp:752-769
@@ -554,18 +559,43 @@ __global__ void __launch_bounds__(kTPB) trace_kernel(const TraceArgs A)
                 const double C = emissivity_factor(cam->src, cam->torus, r, th, rho);
                 const double g3 = pow(g, 3.0);
                 if (MIXED) {
+                    // FP32 transfer.  Each bin's intensity is kept as a Kahan sum
+                    // I_s scaled by exp(S): every contribution K w(E_loc)/w(E_mid)
+                    // exp(-tau) enters as exp(e) with e = ln(...) - tau + S, and S is
+                    // re-anchored when the sum is empty or a term would exceed e^40,
+                    // so intensities behind optically thick gas (exp(-tau) far below
+                    // FP32's range) keep their relative precision.
                     const double zp = 1.0 / gg;   // E_local / E_mid
                     const float lnzp = static_cast<float>(log(zp));
                     const float zm1 = static_cast<float>(zp - 1.0);
-                    const float K = static_cast<float>(g3 * C * dl_cm);
+                    const double Kd = g3 * C * dl_cm;
+                    const bool emit = Kd > 0.0;
+                    const float lnK = emit ? static_cast<float>(log(Kd)) : 0.0f;
                     const bool have_tau = !(rho <= 0.0);
                     const float nbdl = static_cast<float>((rho / kMuG) * dl_cm * sig_scale);
                     for (int b = 0; b < B; ++b) {
                         const DevBin& bn = bins[b];
                         float T = accT[b * kTPB], Tc = accTc[b * kTPB];
-                        float I = accI[b * kTPB], Ic = accIc[b * kTPB];
-                        const float ratio = __expf(-bn.gamma * lnzp - bn.kcut * zm1);
-                        kahan_add(I, Ic, K * ratio * __expf(-T));
+                        if (emit && bn.E_mid > 0.0) {
+                            float I = accI[b * kTPB], Ic = accIc[b * kTPB], S = accS[b * kTPB];
+                            const float arg = lnK - bn.gamma * lnzp - bn.kcut * zm1;
+                            // ln of this contribution; below -800 it is under FP64's
+                            // range (the reference adds an exact or subnormal zero)
+                            const double x = static_cast<double>(arg) -
+                                             (static_cast<double>(T) - static_cast<double>(Tc));
+                            if (x >= -800.0) {
+                                double e = x + static_cast<double>(S);
+                                if (I == 0.0f || e > 40.0) {
+                                    const float shrink = (I == 0.0f) ? 0.0f : __expf(static_cast<float>(-e));
+                                    I *= shrink;
+                                    Ic *= shrink;
+                                    S = static_cast<float>(-x);   // |S| < ~900: exact to 1e-4
+                                    e = x + static_cast<double>(S);
+                                }
+                                kahan_add(I, Ic, __expf(static_cast<float>(e)));
+                                accI[b * kTPB] = I; accIc[b * kTPB] = Ic; accS[b * kTPB] = S;
+                            }
+                        }
                         if (have_tau && gg >= bn.gg_lo && gg <= bn.gg_hi) {
                             const float lnE = bn.lnE + lnzp;
                             int lo = 0, cnt = n_sig;   // lower_bound over lx
@@ -578,9 +608,8 @@ __global__ void __launch_bounds__(kTPB) trace_kernel(const TraceArgs A)
                             const float4 sg = sseg[k];
                             const float t = (lnE - sg.x) * sg.y;
                             kahan_add(T, Tc, nbdl * (sg.z * __expf(t * sg.w)));
+                            accT[b * kTPB] = T; accTc[b * kTPB] = Tc;
                         }
-                        accT[b * kTPB] = T; accTc[b * kTPB] = Tc;
-                        accI[b * kTPB] = I; accIc[b * kTPB] = Ic;
                     }
                 } else {
                     for (int b = 0; b < B; ++b) {

@@ -167,7 +167,8 @@ typedef struct hadros_params {
 /* Caller-owned outputs.  Any pointer may be NULL (that output is skipped).
  * Per-pixel arrays hold nx*ny entries (or n_pixels for the pixel-list call);
  * per-bin arrays hold that many rows of n_bins entries (1 for
- * monochromatic), float in HADROS_PRECISION_MIXED and double in FP64.
+ * monochromatic): tau_E is float in HADROS_PRECISION_MIXED and double in FP64,
+ * I_E is always double (intensities span far more than FP32's range).
  * tau/P_surv/I_obs are integrate_kerr_ray_spectral's aggregates
  * (src/radiative_transfer.cpp:687-780); tau_E/I_E are integrate_kerr_ray
  * at each bin's E_mid (src/radiative_transfer.cpp:457-685). */
@@ -189,6 +190,8 @@ typedef struct hadros_stats {
     int64_t rays;
     int64_t accepted_steps;  /* sum of steps                                */
     int64_t attempts;        /* sum of attempts                             */
+    int64_t h2d_bytes;       /* host->device bytes copied by the call       */
+    int64_t d2h_bytes;       /* device->host bytes copied by the call       */
     int32_t launches;        /* kernels this library launched in the call  */
     int32_t aborted_rays;    /* rays stopped by the attempt budget          */
 } hadros_stats;

@@ -105,8 +105,10 @@ def oracle_image(p, sig_E, sig_cm2, pixel_ids=None, threads: int = 0) -> dict:
     return out
 
 
-def ref_image(p, sig_E, sig_gev2, sig_cm2, pixel_ids=None, threads: int = 0) -> dict:
-    """The reference's own code (KerrCamera::trace_pixel + integrate_kerr_ray_spectral)."""
+def ref_image(p, sig_E, sig_gev2, sig_cm2, pixel_ids=None, threads: int = 0,
+              per_bin: bool = True) -> dict:
+    """The reference's own code (KerrCamera::trace_pixel + integrate_kerr_ray_spectral).
+    per_bin=False skips the extra per-bin integrate_kerr_ray calls (timing runs)."""
     from hadros_b200.workloads import write_sigma_file
     L = ref_lib()
     ids = None if pixel_ids is None else np.ascontiguousarray(pixel_ids, dtype=np.int32)
@@ -118,8 +120,9 @@ def ref_image(p, sig_E, sig_gev2, sig_cm2, pixel_ids=None, threads: int = 0) -> 
         write_sigma_file(path, sig_E, sig_gev2, sig_cm2)
         rc = L.ref_image(C.addressof(p), path.encode(), None if ids is None else ids.ctypes.data,
                          0 if ids is None else int(ids.size),
-                         *(out[k].ctypes.data for k in ("tau", "P_surv", "I_obs", "fate", "steps",
-                                                         "tau_E", "I_E")),
+                         *(out[k].ctypes.data for k in ("tau", "P_surv", "I_obs", "fate", "steps")),
+                         out["tau_E"].ctypes.data if per_bin else None,
+                         out["I_E"].ctypes.data if per_bin else None,
                          int(threads))
     if rc < 0:
         raise RuntimeError(f"reference ref_image failed ({rc})")

@@ -1,0 +1,84 @@
+"""Generates the golden fixtures in tests/golden/*.npz from the REFERENCE itself.
+
+Each case runs the reference's own code (KerrCamera::trace_pixel +
+radiative_transfer::integrate_kerr_ray_spectral, built from the reference
+sources by oracle/build_ref.sh into oracle/_ref/libhadros_ref.so) and stores
+its per-pixel outputs together with the parameters.  Run it where the
+reference sources are available:
+
+    oracle/build_ref.sh && python tests/golden/make_golden.py
+
+The fixtures pin the CPU oracle (tests/test_oracle.py) and are what the GPU
+parity tests compare against on machines without the reference.
+"""
+from __future__ import annotations
+
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent.parent))
+
+import hadros_b200 as hb  # noqa: E402
+from hadros_b200 import workloads as W  # noqa: E402
+from oracle import pyoracle as O  # noqa: E402
+
+
+def cases() -> dict[str, dict]:
+    c: dict[str, dict] = {}
+    # The 32x32 plain tracer, whole image.
+    c["plain_tracer_32"] = W.plain_tracer_32()
+    # The 512x512 mixed-precision configuration, sampled at 16x16 (same
+    # camera, coarser pixel grid), FP64 arithmetic.
+    c["mixed_cfg_16_fp64"] = W.mixed_512(nx=16, ny=16, precision="fp64")
+    # every density profile x every source morphology, 4x4, 4 cutoff bins
+    for prof in hb.PROFILES:
+        for src in hb.SOURCES:
+            c[f"matrix_{prof}_{src}"] = W.mixed_512(nx=4, ny=4, precision="fp64", profile=prof,
+                                                    source=src, h=0.05, n_bins=4)
+    # spectral models
+    c["spectral_powerlaw"] = W.mixed_512(nx=6, ny=6, precision="fp64", spectral="powerlaw",
+                                         h=0.05, n_bins=5)
+    c["spectral_mono_jet"] = W.mixed_512(nx=6, ny=6, precision="fp64", spectral="monochromatic",
+                                         source="jet_base", Enu_obs_GeV=3.0e7, h=0.05)
+    # edge cases
+    c["edge_one_pixel"] = W.plain_tracer_32(nx=1, ny=1)
+    c["edge_ragged_3x5"] = W.mixed_512(nx=3, ny=5, precision="fp64", h=0.05)
+    c["edge_step_cap_40"] = W.mixed_512(nx=4, ny=4, precision="fp64", max_steps=40)
+    c["edge_cap_11"] = W.mixed_512(nx=3, ny=3, precision="fp64", max_steps=11)
+    c["edge_one_bin"] = W.mixed_512(nx=4, ny=4, precision="fp64", n_bins=1, h=0.05)
+    c["edge_empty_band"] = W.mixed_512(nx=3, ny=3, precision="fp64", spec_e_min_GeV=1.0e13,
+                                       spec_e_max_GeV=1.0e14, h=0.05)
+    c["edge_energy_below_table"] = W.plain_tracer_32(nx=4, ny=4, Enu_obs_GeV=1.0e3, fov_deg=25.0,
+                                                     r_obs_rg=60.0, r_max_rg=120.0, h=0.05)
+    c["edge_schwarzschild"] = W.mixed_512(nx=4, ny=4, precision="fp64", a_spin=0.0, h=0.05)
+    c["edge_zero_floor_gauss"] = W.plain_tracer_32(nx=4, ny=4, rho_floor_gcm3=0.0, r_obs_rg=60.0, fov_deg=25.0,
+                                                   r_max_rg=120.0, h=0.05)
+    c["edge_source_guard"] = W.mixed_512(nx=3, ny=3, precision="fp64", source="inner_ring",
+                                         src_sigma_r_rg=0.0, h=0.05)
+    c["edge_equatorial_wide"] = W.mixed_512(nx=5, ny=5, precision="fp64", theta_obs_deg=89.0,
+                                            fov_deg=60.0, h=0.05, a_spin=0.7)
+    c["edge_polar"] = W.mixed_512(nx=3, ny=3, precision="fp64", theta_obs_deg=2.0, h=0.05)
+    return c
+
+
+def main() -> None:
+    if not O.ref_available():
+        raise SystemExit("oracle/_ref/libhadros_ref.so missing: run oracle/build_ref.sh first")
+    E, g2, s = W.synthetic_sigma_arrays()
+    np.savez(HERE / "sigma_synthetic.npz", E=E, sigma_GeV2=g2, sigma_cm2=s)
+    for name, kw in cases().items():
+        p = hb.params(**kw)
+        out = O.ref_image(p, E, g2, s)
+        meta = {k: (v if not isinstance(v, (np.floating, np.integer)) else v.item())
+                for k, v in kw.items()}
+        np.savez_compressed(HERE / f"{name}.npz", params=json.dumps(meta), **out)
+        print(f"{name}: steps {out['steps'].min()}..{out['steps'].max()} "
+              f"fates {np.bincount(out['fate'], minlength=3).tolist()}", flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,84 @@
+"""CUDA path (through the C ABI) against the reference: golden fixtures made by
+the reference itself and the CPU oracle live.  Needs a B200."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden
+from parity import RTOL_FP64, RTOL_MIXED, assert_parity
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_fp64_matches_reference(hb, gpu_ctx, sigma_table, name):
+    kw, ref = load_golden(name)
+    got = gpu_ctx.image(hb.params(**dict(kw, precision="fp64")), sigma_table)
+    assert_parity(got, ref, RTOL_FP64, f"{name}/fp64")
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_mixed_matches_reference(hb, gpu_ctx, sigma_table, name):
+    kw, ref = load_golden(name)
+    got = gpu_ctx.image(hb.params(**dict(kw, precision="mixed")), sigma_table)
+    assert got["tau_E"].dtype == np.float32
+    assert_parity(got, ref, RTOL_MIXED, f"{name}/mixed", p_absolute=True)
+
+
+def test_pixel_list_equals_image_rows(hb, gpu_ctx, sigma_table):
+    from hadros_b200 import workloads as W
+    p = hb.params(**W.mixed_512(nx=12, ny=10, h=0.05))
+    full = gpu_ctx.image(p, sigma_table)
+    ids = np.array([0, 119, 7, 55, 55, 64], dtype=np.int32)
+    sub = gpu_ctx.image(p, sigma_table, pixel_ids=ids)
+    for k in full:
+        np.testing.assert_array_equal(sub[k], full[k][ids], err_msg=k)
+
+
+def test_random_cameras_vs_live_oracle(hb, gpu_ctx, sigma_table, sigma_arrays):
+    from hadros_b200 import workloads as W
+    from oracle import pyoracle as O
+    E, _, s = sigma_arrays
+    rng = np.random.default_rng(2026)
+    for k in range(8):
+        kw = W.mixed_512(nx=int(rng.integers(1, 7)), ny=int(rng.integers(1, 7)),
+                         h=float(rng.uniform(0.02, 0.08)), a_spin=float(rng.uniform(0.0, 0.998)),
+                         theta_obs_deg=float(rng.uniform(5.0, 85.0)),
+                         fov_deg=float(rng.uniform(5.0, 40.0)),
+                         profile=int(rng.integers(0, 8)), source=int(rng.integers(0, 5)),
+                         spectral=int(rng.integers(0, 3)), n_bins=int(rng.integers(1, 17)),
+                         rho0_gcm3=float(10.0 ** rng.uniform(8, 12)), precision="fp64")
+        p = hb.params(**kw)
+        ref = O.oracle_image(p, E, s)
+        assert_parity(gpu_ctx.image(p, sigma_table), ref, RTOL_FP64, f"random {k}/fp64")
+        p.precision = hb.PRECISION_MIXED
+        assert_parity(gpu_ctx.image(p, sigma_table), ref, RTOL_MIXED, f"random {k}/mixed",
+                      p_absolute=True)
+
+
+def test_attempt_budget_returns_timeout_and_context_survives(hb, gpu_ctx, sigma_table):
+    """The device-side bound on work per ray ends rays with HADROS_E_TIMEOUT;
+    the context stays usable for the next call."""
+    from hadros_b200 import workloads as W
+    p = hb.params(**W.mixed_512(nx=4, ny=4, h=0.05, precision="fp64"))
+    gpu_ctx.set_attempt_budget(100)
+    try:
+        with pytest.raises(hb.HadrosError) as e:
+            gpu_ctx.image(p, sigma_table)
+        assert e.value.status == 5
+    finally:
+        gpu_ctx.set_attempt_budget(0)
+    again = gpu_ctx.image(p, sigma_table)
+    assert np.all(again["steps"] > 100)
+
+
+def test_stats_count_the_work(hb, gpu_ctx, sigma_table):
+    from hadros_b200 import workloads as W
+    p = hb.params(**W.mixed_512(nx=5, ny=3, h=0.05))
+    img = gpu_ctx.image(p, sigma_table)
+    st = gpu_ctx.stats()
+    assert st["rays"] == 15 and st["launches"] == 1
+    assert st["accepted_steps"] == int(img["steps"].sum())
+    assert st["attempts"] == int(img["attempts"].sum())
+    assert st["kernel_ms"] > 0.0
