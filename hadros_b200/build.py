@@ -21,6 +21,8 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 BUILD_DIR = PKG / "_build"
 LIB = LIB_DIR / "libhadros_b200.so"
+BIN_DIR = PKG / "bin"
+CLI = BIN_DIR / "compute_kerr_image"
 REPO = PKG.parent
 INCLUDE = REPO / "include"
 
@@ -30,7 +32,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra"]
 
 CU_SOURCES = ["hadros_trace.cu"]
-CXX_SOURCES = ["hadros_host.cpp"]
+CXX_SOURCES = ["hadros_host.cpp", "hadros_formats.cpp"]
 HEADERS = ["hadros_internal.h", "hadros_physics.cuh"]
 
 
@@ -86,6 +88,11 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if force or _stale(LIB, objs):
         _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fPIC",
               "-o", str(LIB), *map(str, objs)], log, verbose)
+    BIN_DIR.mkdir(exist_ok=True)
+    main_src = CSRC / "compute_kerr_image_main.cpp"
+    if force or _stale(CLI, [main_src, LIB, INCLUDE / "hadros_b200.h"]):
+        _run(["g++", *CXX_FLAGS, "-I", str(INCLUDE), "-o", str(CLI), str(main_src),
+              "-L", str(LIB_DIR), "-lhadros_b200", "-Wl,-rpath,$ORIGIN/../lib"], log, verbose)
     (BUILD_DIR / "build.log").write_text("\n".join(log))
     return LIB
 

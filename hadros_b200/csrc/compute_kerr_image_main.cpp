@@ -1,0 +1,214 @@
+// compute_kerr_image — drop-in command-line front end of libhadros_b200.
+//
+// Positional arguments 1-44 have the order and meaning of the reference GPU
+// executable (apps/compute_kerr_image_cuda.cu:2303-2358, usage at :2222-2235):
+//   ENU ASPIN MBH_MSUN TORUS_RHO0 TORUS_R0 TORUS_SIGMA TORUS_H_OVER_R
+//   SOURCE_R SOURCE_SIGMA SOURCE_THETA_DEG SOURCE_POWERLAW SOURCE_EMAX SOURCE_NORM
+//   MEV_ENU MEV_NORM CAM_THETA_DEG CAM_R_OBS CAM_FOV CAM_NX CAM_NY CAM_R_MAX CAM_STEP
+//   GPU_TILE GPU_STEPS_PER_LAUNCH GPU_MAX_STEPS GPU_TOL
+//   [PROFILE RADIAL_POWER FUNNEL_DEPLETION FUNNEL_THETA_DEG ENVELOPE_RHO0
+//    ENVELOPE_ALPHA R_MIN R_MAX RHO_FLOOR SOURCE_MODEL SOURCE_FUNNEL_THETA_DEG
+//    SOURCE_DENSITY_Q SOURCE_RADIAL_S SOURCE_GRADIENT_DR SOURCE_GRADIENT_DTHETA_DEG
+//    SOURCE_RHO_REF SOURCE_CUTOFF_MIN SOURCE_CUTOFF_MAX]
+// GPU_TILE and GPU_STEPS_PER_LAUNCH are accepted and ignored: one persistent
+// launch traces the whole image.  GPU_TOL defaults to the CPU image path's
+// RKF45 tolerance 1e-6 (include/kerr_geodesic.hpp:12).
+//
+// Named options (anywhere): --sigma=FILE (default
+// data/sigma/sigma_nuN_CC_GBW.dat, as the reference hard-codes at :2366),
+// --spectral=MODEL --gamma=G --ecut=E --emin=E --emax=E --nbins=N (the CPU
+// app's spectral arguments, apps/compute_kerr_image_from_cache.cpp:271-288),
+// --precision=fp64|mixed, --device=N, --outdir=DIR (default output/images).
+//
+// Writes DIR/<name>.bin (KIMG) and DIR/<name>.dat with the reference's file
+// name (apps/compute_kerr_image_cuda.cu:2108-2128) and prints the reference's
+// "Saved:" and "CUDA timing:" lines.  Errors go to stderr with exit code 1.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hadros_b200.h"
+
+namespace {
+
+constexpr double PI = 3.141592653589793238462643383279502884;
+
+void usage(const char* argv0)
+{
+    std::fprintf(stderr,
+                 "Usage:\n  %s ENU ASPIN MBH_MSUN TORUS_RHO0 TORUS_R0 TORUS_SIGMA TORUS_H_OVER_R"
+                 " SOURCE_R SOURCE_SIGMA SOURCE_THETA_DEG SOURCE_POWERLAW SOURCE_EMAX SOURCE_NORM"
+                 " MEV_ENU MEV_NORM CAM_THETA_DEG CAM_R_OBS CAM_FOV CAM_NX CAM_NY CAM_R_MAX CAM_STEP"
+                 " GPU_TILE GPU_STEPS_PER_LAUNCH GPU_MAX_STEPS GPU_TOL"
+                 " [PROFILE RADIAL_POWER FUNNEL_DEPLETION FUNNEL_THETA_DEG"
+                 " ENVELOPE_RHO0 ENVELOPE_ALPHA R_MIN R_MAX RHO_FLOOR"
+                 " SOURCE_MODEL SOURCE_FUNNEL_THETA_DEG SOURCE_DENSITY_Q"
+                 " SOURCE_RADIAL_S SOURCE_GRADIENT_DR SOURCE_GRADIENT_DTHETA_DEG"
+                 " SOURCE_RHO_REF SOURCE_CUTOFF_MIN SOURCE_CUTOFF_MAX]\n"
+                 "  options: --sigma=FILE --spectral=MODEL --gamma=G --ecut=E --emin=E --emax=E"
+                 " --nbins=N --precision=fp64|mixed --device=N --outdir=DIR\n",
+                 argv0);
+}
+
+int die(const char* what)
+{
+    std::fprintf(stderr, "%s: %s\n", what, hadros_last_error());
+    return 1;
+}
+
+}  // namespace
+
+int main(int argc, char** argv)
+{
+    std::vector<std::string> pos;
+    std::string sigma_path = "data/sigma/sigma_nuN_CC_GBW.dat", outdir = "output/images";
+    std::string spectral, precision;
+    double gamma = NAN, ecut = NAN, emin = NAN, emax = NAN;
+    int nbins = -1, device = 0;
+    for (int k = 1; k < argc; ++k) {
+        std::string a(argv[k]);
+        if (a.rfind("--", 0) == 0) {
+            const size_t eq = a.find('=');
+            const std::string key = a.substr(2, eq == std::string::npos ? std::string::npos : eq - 2);
+            const std::string val = eq == std::string::npos ? "" : a.substr(eq + 1);
+            if (key == "sigma") sigma_path = val;
+            else if (key == "outdir") outdir = val;
+            else if (key == "spectral") spectral = val;
+            else if (key == "precision") precision = val;
+            else if (key == "gamma") gamma = std::atof(val.c_str());
+            else if (key == "ecut") ecut = std::atof(val.c_str());
+            else if (key == "emin") emin = std::atof(val.c_str());
+            else if (key == "emax") emax = std::atof(val.c_str());
+            else if (key == "nbins") nbins = std::atoi(val.c_str());
+            else if (key == "device") device = std::atoi(val.c_str());
+            else if (key == "help") { usage(argv[0]); return 0; }
+            else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); usage(argv[0]); return 1; }
+        } else {
+            pos.push_back(a);
+        }
+    }
+    auto has = [&](size_t i) { return pos.size() >= i; };
+    auto f = [&](size_t i) { return std::atof(pos[i - 1].c_str()); };
+    auto n = [&](size_t i) { return std::atoi(pos[i - 1].c_str()); };
+
+    hadros_params p;
+    hadros_params_default(&p);
+    // compute_kerr_image_cuda defaults (apps/compute_kerr_image_cuda.cu:2250-2297)
+    p.Enu_obs_GeV = 1.0e9; p.a_spin = 0.9; p.M_bh_msun = 3.0;
+    p.rho0_gcm3 = 1.0e-2; p.r0_rg = 10.0; p.sigma_r_rg = 5.0; p.H_over_R = 0.25;
+    p.profile_kind = HADROS_PROFILE_GAUSSIAN; p.radial_power = 2.0; p.funnel_depletion = 0.0;
+    p.funnel_theta_rad = 15.0 * PI / 180.0; p.envelope_rho0_gcm3 = 0.0; p.envelope_alpha = 2.5;
+    p.torus_r_min_rg = 4.0; p.torus_r_max_rg = 60.0; p.rho_floor_gcm3 = 1.0e-99;
+    p.src_r_center_rg = 3.5; p.src_sigma_r_rg = 1.0; p.src_theta_width_rad = 15.0 * PI / 180.0;
+    p.src_powerlaw = 2.0; p.src_emax_GeV = 1.0e12; p.src_norm = 1.0;
+    p.source_kind = HADROS_SOURCE_INNER_RING; p.src_funnel_theta_rad = 20.0 * PI / 180.0;
+    p.src_density_power_q = 1.0; p.src_radial_power_s = 2.0; p.src_rho_ref_gcm3 = -1.0;
+    p.src_cutoff_min = 0.0; p.src_cutoff_max = 1.0e2; p.src_gradient_dr_rg = 0.1;
+    p.src_gradient_dtheta_rad = 1.0 * PI / 180.0;
+    double mev_E = 10.0, mev_norm = 1.0;
+    p.r_obs_rg = 60.0; p.theta_obs_rad = 80.0 * PI / 180.0; p.fov_deg = 25.0;
+    p.nx = 100; p.ny = 100; p.r_max_rg = 120.0; p.h = 0.001; p.tolerance = 1.0e-6;
+    p.max_steps = 200000;
+    int tile = 32, steps_per_launch = 128;
+
+    if (has(1)) p.Enu_obs_GeV = f(1);
+    if (has(2)) p.a_spin = f(2);
+    if (has(3)) p.M_bh_msun = f(3);
+    if (has(4)) p.rho0_gcm3 = f(4);
+    if (has(5)) p.r0_rg = f(5);
+    if (has(6)) p.sigma_r_rg = f(6);
+    if (has(7)) p.H_over_R = f(7);
+    if (has(8)) p.src_r_center_rg = f(8);
+    if (has(9)) p.src_sigma_r_rg = f(9);
+    if (has(10)) p.src_theta_width_rad = f(10) * PI / 180.0;
+    if (has(11)) p.src_powerlaw = f(11);
+    if (has(12)) p.src_emax_GeV = f(12);
+    if (has(13)) p.src_norm = f(13);
+    if (has(14)) mev_E = f(14);
+    if (has(15)) mev_norm = f(15);
+    if (has(16)) p.theta_obs_rad = f(16) * PI / 180.0;
+    if (has(17)) p.r_obs_rg = f(17);
+    if (has(18)) p.fov_deg = f(18);
+    if (has(19)) p.nx = n(19);
+    if (has(20)) p.ny = n(20);
+    if (has(21)) p.r_max_rg = f(21);
+    if (has(22)) p.h = f(22);
+    if (has(23)) tile = n(23);
+    if (has(24)) steps_per_launch = n(24);
+    if (has(25)) p.max_steps = n(25);
+    if (has(26)) p.tolerance = f(26);
+    if (has(27) && hadros_parse_profile(pos[26].c_str(), &p.profile_kind)) return die("profile");
+    if (has(28)) p.radial_power = f(28);
+    if (has(29)) p.funnel_depletion = f(29);
+    if (has(30)) p.funnel_theta_rad = f(30) * PI / 180.0;
+    if (has(31)) p.envelope_rho0_gcm3 = f(31);
+    if (has(32)) p.envelope_alpha = f(32);
+    if (has(33)) p.torus_r_min_rg = f(33);
+    if (has(34)) p.torus_r_max_rg = f(34);
+    if (has(35)) p.rho_floor_gcm3 = f(35);
+    if (has(36) && hadros_parse_source(pos[35].c_str(), &p.source_kind)) return die("source model");
+    if (has(37)) p.src_funnel_theta_rad = f(37) * PI / 180.0;
+    if (has(38)) p.src_density_power_q = f(38);
+    if (has(39)) p.src_radial_power_s = f(39);
+    if (has(40)) p.src_gradient_dr_rg = f(40);
+    if (has(41)) p.src_gradient_dtheta_rad = f(41) * PI / 180.0;
+    if (has(42)) p.src_rho_ref_gcm3 = f(42);
+    if (has(43)) p.src_cutoff_min = f(43);
+    if (has(44)) p.src_cutoff_max = f(44);
+    if (!spectral.empty() && hadros_parse_spectral(spectral.c_str(), &p.spectral_kind)) return die("spectral model");
+    if (!std::isnan(gamma)) p.spec_gamma = gamma;
+    if (!std::isnan(ecut)) p.spec_ecut_GeV = ecut;
+    if (!std::isnan(emin)) p.spec_e_min_GeV = emin;
+    if (!std::isnan(emax)) p.spec_e_max_GeV = emax;
+    if (nbins > 0) p.n_bins = nbins;
+    if (precision == "mixed") p.precision = HADROS_PRECISION_MIXED;
+    else if (!precision.empty() && precision != "fp64") { usage(argv[0]); return 1; }
+
+    if (p.nx <= 0 || p.ny <= 0 || tile <= 0 || steps_per_launch <= 0 || p.max_steps <= 0) {
+        usage(argv[0]);   // apps/compute_kerr_image_cuda.cu:2360-2364
+        return 1;
+    }
+    if (hadros_params_validate(&p)) return die("parameters");
+
+    hadros_sigma* sig = nullptr;
+    if (hadros_sigma_load(sigma_path.c_str(), &sig)) return die("sigma table");
+    hadros_ctx* ctx = nullptr;
+    if (hadros_ctx_create(device, &ctx)) return die("CUDA");
+    const size_t P = static_cast<size_t>(p.nx) * p.ny;
+    std::vector<double> tau(P), Ps(P), I(P);
+    std::vector<int8_t> fate(P);
+    std::vector<int32_t> steps(P);
+    hadros_image_out out{};
+    out.tau = tau.data();
+    out.P_surv = Ps.data();
+    out.I_obs = I.data();
+    out.fate = fate.data();
+    out.steps = steps.data();
+    std::printf("Grid: %d x %d\n", p.nx, p.ny);
+    const auto t0 = std::chrono::steady_clock::now();
+    if (hadros_image(ctx, &p, sig, &out)) return die("trace");
+    const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    hadros_stats st{};
+    hadros_ctx_stats(ctx, &st);
+
+    char name_bin[512], name_dat[512];
+    if (hadros_image_filename(&p, 0, nullptr, mev_E, mev_norm, ".bin", name_bin, sizeof(name_bin)) ||
+        hadros_image_filename(&p, 0, nullptr, mev_E, mev_norm, ".dat", name_dat, sizeof(name_dat)))
+        return die("file name");
+    const std::string bin_path = outdir + "/" + name_bin, dat_path = outdir + "/" + name_dat;
+    if (hadros_write_kimg(bin_path.c_str(), &p, mev_E, mev_norm, tau.data(), Ps.data(), I.data(), fate.data()))
+        return die("write");
+    if (hadros_write_dat(dat_path.c_str(), &p, "GBW", mev_E, mev_norm, tau.data(), Ps.data(), I.data(), fate.data()))
+        return die("write");
+    std::printf("Saved: %s\nSaved: %s\n", bin_path.c_str(), dat_path.c_str());
+    std::printf("CUDA timing: %g s, %g rays/s, tiles=1, advance launches=%d, accepted steps=%lld\n", elapsed,
+                static_cast<double>(P) / std::max(elapsed, 1.0e-300), st.launches,
+                static_cast<long long>(st.accepted_steps));
+    hadros_ctx_destroy(ctx);
+    hadros_sigma_destroy(sig);
+    return 0;
+}

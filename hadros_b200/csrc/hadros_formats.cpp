@@ -1,0 +1,210 @@
+// hadros_formats.cpp — the reference's image file formats and file names.
+//
+//  * 13-column text image (.dat): '#'-metadata header, then one row per pixel
+//    "i j alpha beta tau P_surv I captured tau_mev P_surv_mev I_mev r_nu
+//    leakage" in pixel order j*nx+i, %.8e for reals
+//    (apps/compute_kerr_image_from_cache.cpp:512-653,
+//    apps/compute_kerr_image_cuda.cu:2509-2586);
+//  * KIMG binary (.bin): "<7i4d" header (magic 0x4B494D47, version 1,
+//    backend, nx, ny, ncols = 13, reserved, E_GeV, E_MeV, MeV norm,
+//    theta_deg) and nx*ny rows of 13 little-endian doubles
+//    (apps/compute_kerr_image_cuda.cu:279-332, read by scripts/plot_kerr_image.py:
+//    108-150);
+//  * output file names (apps/compute_kerr_image_cuda.cu:2108-2128 and
+//    apps/compute_kerr_image_from_cache.cpp:477-500), which the Python drivers
+//    re-derive to find the image.
+// The MeV thermal channel is not computed by this library: its five columns
+// carry RTResult's defaults (tau 0, P 1, I 0, r_nu -1, leakage 1).
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "hadros_internal.h"
+
+namespace {
+
+int32_t ferr(int32_t code, const std::string& m) { return hadros::set_error(code, m); }
+
+// make_tag (apps/compute_kerr_image_cuda.cu:377-386): printf, then
+// '+' -> '_', '-' -> 'm', '.' -> 'p'.
+std::string make_tag(const char* fmt, double v)
+{
+    char buf[64];
+    std::snprintf(buf, sizeof(buf), fmt, v);
+    std::string t(buf);
+    for (char& ch : t) {
+        if (ch == '+') ch = '_';
+        else if (ch == '-') ch = 'm';
+        else if (ch == '.') ch = 'p';
+    }
+    return t;
+}
+
+// make_compact_scientific_tag (:388-403): "%.0e" with the exponent's sign and
+// leading zeros dropped ("1e+10" -> "1e10", "1e-02" -> "1e-2").
+std::string compact_sci(double v)
+{
+    char buf[64];
+    std::snprintf(buf, sizeof(buf), "%.0e", v);
+    std::string t(buf);
+    const size_t e = t.find('e');
+    if (e == std::string::npos) return t;
+    return t.substr(0, e) + "e" + std::to_string(std::atoi(t.c_str() + e + 1));
+}
+
+const char* const kProfile[8] = {"gaussian", "powerlaw", "gaussian_funnel", "powerlaw_funnel",
+                                 "gaussian_envelope", "powerlaw_envelope",
+                                 "powerlaw_funnel_envelope", "collapsar_ndaf_like"};
+const char* const kSource[5] = {"inner_ring", "funnel_wall", "jet_base", "shock_layer",
+                                "density_weighted"};
+const char* const kSpectral[3] = {"monochromatic", "powerlaw", "powerlaw_cutoff"};
+
+double rad2deg(double r) { return r * 180.0 / M_PI; }
+
+double pixel_u(const hadros_params* p, int i)
+{   // src/kerr_camera.cpp:196-200 (alpha_rg, beta_rg)
+    const double fov_rad = p->fov_deg * M_PI / 180.0;
+    return (2.0 * (i + 0.5) / p->nx - 1.0) * std::tan(0.5 * fov_rad);
+}
+
+double pixel_v(const hadros_params* p, int j)
+{
+    const double fov_rad = p->fov_deg * M_PI / 180.0;
+    return (2.0 * (j + 0.5) / p->ny - 1.0) * std::tan(0.5 * fov_rad);
+}
+
+bool kinds_ok(const hadros_params* p)
+{
+    return p && p->profile_kind >= 0 && p->profile_kind < 8 && p->source_kind >= 0 &&
+           p->source_kind < 5 && p->spectral_kind >= 0 && p->spectral_kind < 3 && p->nx > 0 &&
+           p->ny > 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t hadros_image_filename(const hadros_params* p, int32_t style, const char* dis_model,
+                              double mev_E_MeV, double mev_norm, const char* ext, char* buf,
+                              int32_t buflen)
+{
+    if (!kinds_ok(p) || !buf || buflen <= 0 || !ext) return ferr(HADROS_E_ARG, "bad argument");
+    const std::string profile = kProfile[p->profile_kind];
+    std::string name;
+    if (style == 0) {
+        // compute_kerr_image_cuda in-line mode (apps/compute_kerr_image_cuda.cu:2108-2128)
+        name = "kerr_image_cuda_rho0_torus_" + compact_sci(p->rho0_gcm3) +
+               (profile == "gaussian" ? "" : "_Profile_" + profile) +
+               (p->source_kind == HADROS_SOURCE_INNER_RING ? "" : std::string("_Source_") + kSource[p->source_kind]) +
+               "_Enu_" + make_tag("%.0e", p->Enu_obs_GeV) + "_MeVEnu_" + make_tag("%.0e", mev_E_MeV) +
+               "_MeVNorm_" + make_tag("%.0e", mev_norm) + "_CamTheta_" +
+               make_tag("%.1f", rad2deg(p->theta_obs_rad));
+    } else {
+        // compute_kerr_image_from_cache (apps/compute_kerr_image_from_cache.cpp:477-500)
+        name = std::string("kerr_image_cuda_cache_") + (dis_model && *dis_model ? dis_model : "GBW") +
+               "_rho0_torus_" + compact_sci(p->rho0_gcm3) +
+               (profile == "gaussian" ? "" : "_Profile_" + profile) +
+               (p->source_kind == HADROS_SOURCE_INNER_RING ? "" : std::string("_Source_") + kSource[p->source_kind]) +
+               (p->spectral_kind == HADROS_SPECTRAL_MONOCHROMATIC ? "" : std::string("_Spectrum_") + kSpectral[p->spectral_kind]) +
+               "_Enu_" + make_tag("%.0e", p->Enu_obs_GeV) + "_MeVEnu_" + make_tag("%.0e", mev_E_MeV) +
+               "_MeVNorm_" + make_tag("%.0e", mev_norm) + "_CamTheta_" +
+               make_tag("%.1f", rad2deg(p->theta_obs_rad));
+    }
+    name += ext;
+    if (static_cast<int32_t>(name.size()) + 1 > buflen) return ferr(HADROS_E_ARG, "buffer too small");
+    std::memcpy(buf, name.c_str(), name.size() + 1);
+    return HADROS_OK;
+}
+
+int32_t hadros_write_dat(const char* path, const hadros_params* p, const char* dis_model,
+                         double mev_E_MeV, double mev_norm, const double* tau, const double* P_surv,
+                         const double* I_obs, const int8_t* fate)
+{
+    if (!path || !kinds_ok(p) || !tau || !P_surv || !I_obs || !fate)
+        return ferr(HADROS_E_ARG, "bad argument");
+    hadros::set_error(HADROS_OK, "");
+    FILE* f = std::fopen(path, "w");
+    if (!f) return ferr(HADROS_E_IO, std::string("Could not open ") + path);
+    // metadata header: apps/compute_kerr_image_from_cache.cpp:512-597 (ostream
+    // default formatting = %g)
+    const char* prof = kProfile[p->profile_kind];
+    const char* src = kSource[p->source_kind];
+    std::fprintf(f, "# profile_type %s\n# rho0 %g\n# rho0_gcm3 %g\n# r0 %g\n# r0_rg %g\n", prof,
+                 p->rho0_gcm3, p->rho0_gcm3, p->r0_rg, p->r0_rg);
+    std::fprintf(f, "# sigma_r %g\n# sigma_r_rg %g\n# H_over_R %g\n# radial_power %g\n", p->sigma_r_rg,
+                 p->sigma_r_rg, p->H_over_R, p->radial_power);
+    std::fprintf(f, "# funnel_depletion %g\n# funnel_theta_deg %g\n# rho_floor %g\n# rho_floor_gcm3 %g\n",
+                 p->funnel_depletion, rad2deg(p->funnel_theta_rad), p->rho_floor_gcm3, p->rho_floor_gcm3);
+    std::fprintf(f, "# envelope_rho0 %g\n# envelope_rho0_gcm3 %g\n# envelope_alpha %g\n", p->envelope_rho0_gcm3,
+                 p->envelope_rho0_gcm3, p->envelope_alpha);
+    std::fprintf(f, "# R_min %g\n# R_min_rg %g\n# R_max %g\n# R_max_rg %g\n# spin %g\n", p->torus_r_min_rg,
+                 p->torus_r_min_rg, p->torus_r_max_rg, p->torus_r_max_rg, p->a_spin);
+    std::fprintf(f, "# observer_distance %g\n# observer_distance_rg %g\n", p->r_obs_rg, p->r_obs_rg);
+    std::fprintf(f, "# observer_inclination %g\n# observer_inclination_deg %g\n", rad2deg(p->theta_obs_rad),
+                 rad2deg(p->theta_obs_rad));
+    std::fprintf(f, "# DIS_model %s\n# use_F3 1\n", dis_model && *dis_model ? dis_model : "GBW");
+    std::fprintf(f, "# source_model %s\n# source_r_rg %g\n# source_sigma_rg %g\n# source_theta_deg %g\n", src,
+                 p->src_r_center_rg, p->src_sigma_r_rg, rad2deg(p->src_theta_width_rad));
+    std::fprintf(f, "# source_powerlaw %g\n# source_emax_GeV %g\n# source_norm %g\n", p->src_powerlaw,
+                 p->src_emax_GeV, p->src_norm);
+    std::fprintf(f, "# source_funnel_theta_deg %g\n# source_rho_ref %g\n# rho_ref %g\n",
+                 rad2deg(p->src_funnel_theta_rad), p->src_rho_ref_gcm3, p->src_rho_ref_gcm3);
+    std::fprintf(f, "# source_q %g\n# source_s %g\n# source_density_power_q %g\n# source_radial_power_s %g\n",
+                 p->src_density_power_q, p->src_radial_power_s, p->src_density_power_q, p->src_radial_power_s);
+    std::fprintf(f, "# source_cutoff_min %g\n# source_cutoff_max %g\n# source_gradient_dr_rg %g\n",
+                 p->src_cutoff_min, p->src_cutoff_max, p->src_gradient_dr_rg);
+    std::fprintf(f, "# source_gradient_dtheta_deg %g\n", rad2deg(p->src_gradient_dtheta_rad));
+    std::fprintf(f, "# spectral_model %s\n# spectral_gamma %g\n# spectral_ecut_GeV %g\n",
+                 kSpectral[p->spectral_kind], p->spec_gamma, p->spec_ecut_GeV);
+    std::fprintf(f, "# spectral_E_min_GeV %g\n# spectral_E_max_GeV %g\n# spectral_N_bins %d\n", p->spec_e_min_GeV,
+                 p->spec_e_max_GeV, p->n_bins);
+    std::fprintf(f, "# MEV_ENERGY_MEV %g\n# MEV_NORM %g\n# MEV_CUDA_STATUS not_computed\n", mev_E_MeV, mev_norm);
+    std::fprintf(f, "# step_cap %d\n# rkf45_tolerance %g\n# camera_step_rg %g\n# camera_fov_deg %g\n",
+                 p->max_steps, p->tolerance, p->h, p->fov_deg);
+    std::fprintf(f, "# precision %s\n# backend hadros_b200\n",
+                 p->precision == HADROS_PRECISION_MIXED ? "mixed_fp64_geodesic_fp32_transfer" : "fp64");
+    std::fprintf(f, "# i j alpha beta tau_uhe P_surv_uhe I_obs_uhe captured "
+                    "tau_mev P_surv_mev I_obs_mev r_neutrinosphere_rg leakage_mev\n");
+    for (int j = 0; j < p->ny; ++j) {
+        const double v = pixel_v(p, j);
+        for (int i = 0; i < p->nx; ++i) {
+            const size_t k = static_cast<size_t>(j) * p->nx + i;
+            std::fprintf(f, "%d %d %.8e %.8e %.8e %.8e %.8e %d %.8e %.8e %.8e %.8e %.8e\n", i, j, pixel_u(p, i), v,
+                         tau[k], P_surv[k], I_obs[k], fate[k] == HADROS_FATE_CAPTURED ? 1 : 0, 0.0, 1.0, 0.0,
+                         -1.0, 1.0);
+        }
+    }
+    const bool ok = std::ferror(f) == 0;
+    std::fclose(f);
+    return ok ? HADROS_OK : ferr(HADROS_E_IO, std::string("write failed: ") + path);
+}
+
+int32_t hadros_write_kimg(const char* path, const hadros_params* p, double mev_E_MeV, double mev_norm,
+                          const double* tau, const double* P_surv, const double* I_obs, const int8_t* fate)
+{
+    if (!path || !kinds_ok(p) || !tau || !P_surv || !I_obs || !fate)
+        return ferr(HADROS_E_ARG, "bad argument");
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return ferr(HADROS_E_IO, std::string("Could not open binary output file: ") + path);
+    const int32_t hdr_i[7] = {0x4B494D47, 1, 2, p->nx, p->ny, 13, 0};
+    const double hdr_d[4] = {p->Enu_obs_GeV, mev_E_MeV, mev_norm, rad2deg(p->theta_obs_rad)};
+    std::fwrite(hdr_i, sizeof(hdr_i), 1, f);
+    std::fwrite(hdr_d, sizeof(hdr_d), 1, f);
+    for (int j = 0; j < p->ny; ++j) {
+        const double v = pixel_v(p, j);
+        for (int i = 0; i < p->nx; ++i) {
+            const size_t k = static_cast<size_t>(j) * p->nx + i;
+            const double row[13] = {static_cast<double>(i), static_cast<double>(j), pixel_u(p, i), v, tau[k],
+                                    P_surv[k], I_obs[k], fate[k] == HADROS_FATE_CAPTURED ? 1.0 : 0.0,
+                                    0.0, 1.0, 0.0, -1.0, 1.0};
+            std::fwrite(row, sizeof(row), 1, f);
+        }
+    }
+    const bool ok = std::ferror(f) == 0;
+    std::fclose(f);
+    return ok ? HADROS_OK : ferr(HADROS_E_IO, std::string("write failed: ") + path);
+}
+
+}  // extern "C"

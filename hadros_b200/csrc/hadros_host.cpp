@@ -47,6 +47,8 @@ std::atomic<uint64_t> g_sigma_serial{1};
 
 }  // namespace
 
+int32_t hadros::set_error(int32_t code, const std::string& msg) { return fail(code, msg); }
+
 // A device context: one stream, device buffers grown on demand, the sigma
 // table last uploaded, and the statistics of the last call.
 struct hadros_ctx {

@@ -108,6 +108,9 @@ int launch_trace(const TraceArgs& args, int precision, int n_sm, void* stream,
                  std::string& err);
 size_t trace_smem_bytes(int precision, int sig_n, int max_bins);
 
+// Record the calling thread's hadros_last_error() message; returns `code`.
+int32_t set_error(int32_t code, const std::string& msg);
+
 }  // namespace hadros
 
 // hadros_sigma is the public opaque handle.

@@ -285,6 +285,29 @@ int32_t hadros_image_device(hadros_ctx* ctx, const hadros_params* p,
 /* Wait for the context's work and report the first deferred error. */
 int32_t hadros_ctx_synchronize(hadros_ctx* ctx);
 
+/* ---- the reference's image files (host only) ------------------------------ */
+
+/* Output file name the reference apps use, so scripts that re-derive it find
+ * the image: style 0 = compute_kerr_image_cuda in-line mode
+ * (apps/compute_kerr_image_cuda.cu:2108-2128), style 1 =
+ * compute_kerr_image_from_cache (apps/compute_kerr_image_from_cache.cpp:
+ * 477-500; dis_model NULL -> "GBW").  `ext` is appended (".dat", ".bin").
+ * The name has no directory part. */
+int32_t hadros_image_filename(const hadros_params* p, int32_t style, const char* dis_model,
+                              double mev_E_MeV, double mev_norm, const char* ext, char* buf,
+                              int32_t buflen);
+/* 13-column text image with the reference's '#' metadata header
+ * (apps/compute_kerr_image_from_cache.cpp:512-653); rows in j*nx+i order;
+ * the MeV columns carry RTResult's defaults (the MeV channel is not
+ * computed).  Arrays hold nx*ny entries. */
+int32_t hadros_write_dat(const char* path, const hadros_params* p, const char* dis_model,
+                         double mev_E_MeV, double mev_norm, const double* tau,
+                         const double* P_surv, const double* I_obs, const int8_t* fate);
+/* KIMG binary image (apps/compute_kerr_image_cuda.cu:279-332). */
+int32_t hadros_write_kimg(const char* path, const hadros_params* p, double mev_E_MeV,
+                          double mev_norm, const double* tau, const double* P_surv,
+                          const double* I_obs, const int8_t* fate);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,137 @@
+"""The reference's image files: names, 13-column text image and KIMG binary,
+written by the library from host arrays (no GPU)."""
+from __future__ import annotations
+
+import ctypes as C
+import struct
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_golden
+
+
+def fname(hb, p, style, ext, dis=None, mev_E=10.0, mev_norm=1.0):
+    buf = C.create_string_buffer(512)
+    rc = hb.lib().hadros_image_filename(C.byref(p), style, dis, mev_E, mev_norm, ext.encode(), buf, 512)
+    assert rc == 0
+    return buf.value.decode()
+
+
+def test_filenames_match_reference_validation_targets(hb):
+    """Names the reference Makefile's validate_small_cuda target compares
+    (Makefile:686-687: ENU 1e5, TORUS_RHO0 1e-2, CAM_THETA_DEG 80, MeV 10/1)."""
+    p = hb.params(Enu_obs_GeV=1e5, rho0_gcm3=1e-2, theta_obs_deg=80.0)
+    assert fname(hb, p, 1, ".dat", b"GBW") == (
+        "kerr_image_cuda_cache_GBW_rho0_torus_1e-2_Enu_1e_05_MeVEnu_1e_01_MeVNorm_1e_00_CamTheta_80p0.dat")
+    q = hb.params(Enu_obs_GeV=1e5, rho0_gcm3=1e-2, theta_obs_deg=80.0, profile="powerlaw_funnel_envelope")
+    assert fname(hb, q, 1, ".dat", b"GBW") == (
+        "kerr_image_cuda_cache_GBW_rho0_torus_1e-2_Profile_powerlaw_funnel_envelope_Enu_1e_05_"
+        "MeVEnu_1e_01_MeVNorm_1e_00_CamTheta_80p0.dat")
+    r = hb.params(Enu_obs_GeV=1e9, rho0_gcm3=1e11, theta_obs_deg=17.0, source="funnel_wall",
+                  spectral="powerlaw_cutoff")
+    assert fname(hb, r, 0, ".bin") == (
+        "kerr_image_cuda_rho0_torus_1e11_Source_funnel_wall_Enu_1e_09_MeVEnu_1e_01_MeVNorm_1e_00_"
+        "CamTheta_17p0.bin")
+    assert fname(hb, r, 1, ".dat", b"IIM") == (
+        "kerr_image_cuda_cache_IIM_rho0_torus_1e11_Source_funnel_wall_Spectrum_powerlaw_cutoff_"
+        "Enu_1e_09_MeVEnu_1e_01_MeVNorm_1e_00_CamTheta_17p0.dat")
+
+
+def _write(hb, tmp_path, kw, ref):
+    p = hb.params(**kw)
+    arrs = [np.ascontiguousarray(ref[k]) for k in ("tau", "P_surv", "I_obs", "fate")]
+    dat, kimg = tmp_path / "img.dat", tmp_path / "img.bin"
+    L = hb.lib()
+    assert L.hadros_write_dat(str(dat).encode(), C.byref(p), b"GBW", 10.0, 1.0,
+                              *(a.ctypes.data for a in arrs)) == 0
+    assert L.hadros_write_kimg(str(kimg).encode(), C.byref(p), 10.0, 1.0,
+                               *(a.ctypes.data for a in arrs)) == 0
+    return p, dat, kimg
+
+
+def test_dat_and_kimg_layout(hb, tmp_path):
+    kw, ref = load_golden("edge_ragged_3x5")
+    p, dat, kimg = _write(hb, tmp_path, kw, ref)
+    text = dat.read_text().splitlines()
+    assert text[0] == "# profile_type powerlaw_funnel_envelope"
+    assert "# source_model funnel_wall" in text
+    assert "# spectral_model powerlaw_cutoff" in text
+    assert text[[i for i, l in enumerate(text) if not l.startswith("#")][0] - 1].startswith(
+        "# i j alpha beta tau_uhe P_surv_uhe I_obs_uhe captured")
+    d = np.loadtxt(dat, comments="#")
+    assert d.shape == (15, 13)
+    np.testing.assert_array_equal(d[:, 0], np.tile(np.arange(3), 5))
+    np.testing.assert_array_equal(d[:, 1], np.repeat(np.arange(5), 3))
+    np.testing.assert_allclose(d[:, 4], ref["tau"], rtol=1e-8)
+    np.testing.assert_allclose(d[:, 6], ref["I_obs"], rtol=1e-8)
+    np.testing.assert_array_equal(d[:, 7], (ref["fate"] == 1).astype(float))
+    np.testing.assert_array_equal(d[:, 8:], np.tile([0.0, 1.0, 0.0, -1.0, 1.0], (15, 1)))
+    with open(kimg, "rb") as f:
+        h = struct.Struct("<7i4d")
+        magic, version, backend, nx, ny, ncols, res, E, Emev, norm, th = h.unpack(f.read(h.size))
+        payload = np.fromfile(f, dtype="<f8")
+    assert (magic, version, nx, ny, ncols) == (0x4B494D47, 1, 3, 5, 13)
+    assert th == pytest.approx(17.0)
+    rows = payload.reshape(15, 13)
+    np.testing.assert_array_equal(rows[:, 4], ref["tau"])
+    np.testing.assert_array_equal(rows[:, 6], ref["I_obs"])
+    np.testing.assert_allclose(rows[:, :4], d[:, :4], rtol=1e-8)
+
+
+def test_alpha_beta_are_reference_camera_coordinates(hb, tmp_path):
+    import math
+    kw, ref = load_golden("edge_ragged_3x5")
+    p, dat, kimg = _write(hb, tmp_path, kw, ref)
+    rows = np.fromfile(kimg, dtype="<f8", offset=struct.calcsize("<7i4d")).reshape(15, 13)
+    t = math.tan(0.5 * (p.fov_deg * math.pi / 180.0))
+    for row in rows:
+        i, j = int(row[0]), int(row[1])
+        assert row[2] == (2.0 * (i + 0.5) / p.nx - 1.0) * t
+        assert row[3] == (2.0 * (j + 0.5) / p.ny - 1.0) * t
+
+
+def test_compare_module_matches_reference_script(hb, tmp_path):
+    """hadros_b200.compare's aggregates equal the reference comparer's."""
+    script = Path("/root/reference/scripts/compare_cuda_cpu_metrics.py")
+    kw, ref = load_golden("edge_ragged_3x5")
+    _, dat_a, _ = _write(hb, tmp_path, kw, ref)
+    ref2 = dict(ref)
+    ref2["tau"] = ref["tau"] * (1 + 1e-7)
+    d2 = tmp_path / "b"
+    d2.mkdir()
+    _, dat_b, _ = _write(hb, d2, kw, ref2)
+    ours = tmp_path / "ours.txt"
+    from hadros_b200 import compare
+    assert compare.main([str(ours), "case", str(dat_a), str(dat_b)]) == 0
+    got = {l.split()[0]: l.split()[1:] for l in ours.read_text().splitlines()
+           if l and not l.startswith(("#", "[", "cpu_", "gpu_", "per_"))}
+    assert float(got["mean_tau"][2]) == pytest.approx(1e-7, rel=1e-2)
+    if not script.exists():
+        pytest.skip("reference comparer not present here")
+    theirs = tmp_path / "theirs.txt"
+    subprocess.run([sys.executable, str(script), str(theirs), "case", str(dat_a), str(dat_b)],
+                   check=True, capture_output=True)
+    ref_m = {l.split()[0]: l.split()[1:] for l in theirs.read_text().splitlines()
+             if l and not l.startswith(("#", "[", "cpu_", "cuda_"))}
+    for k in ("mean_tau", "max_tau", "mean_P_surv", "total_intensity", "valid_rays"):
+        assert got[k] == ref_m[k], k
+
+
+def test_cli_usage_and_errors():
+    cli = ROOT / "hadros_b200" / "bin" / "compute_kerr_image"
+    if not cli.exists():
+        pytest.skip("CLI not built")
+    r = subprocess.run([str(cli), "1e9", "0.9", "3", "1e-2", "10", "5", "0.25", "3.5", "1", "15", "2",
+                        "1e12", "1", "10", "1", "80", "60", "25", "0", "10"],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "Usage" in r.stderr
+    r = subprocess.run([str(cli), "--sigma=/nonexistent.dat"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Could not open sigma table" in r.stderr
+    r = subprocess.run([str(cli), "1e9", "0.9", "3", "1e-2", "10", "5", "0.25", "3.5", "1", "15", "2",
+                        "1e12", "1", "10", "1", "80", "60", "25", "4", "4", "120", "0.01", "32", "128",
+                        "200000", "1e-6", "no_such_profile"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Unknown density profile 'no_such_profile'" in r.stderr
