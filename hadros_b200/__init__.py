@@ -95,6 +95,8 @@ def params(**kw) -> HadrosParams:
             p.source_kind = _kind(SOURCES, val, "hadros_parse_source")
         elif key == "spectral":
             p.spectral_kind = _kind(SPECTRA, val, "hadros_parse_spectral")
+        elif key == "fast":
+            p.fast_geodesic = 1 if val else 0
         elif key == "precision":
             p.precision = {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}.get(val, val)
         elif key in _DEG:

@@ -32,7 +32,7 @@ class HadrosParams(C.Structure):
         ("spectral_kind", C.c_int32),
         ("n_bins", C.c_int32),
         ("precision", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("fast_geodesic", C.c_int32),
         ("a_spin", C.c_double),
         ("r_obs_rg", C.c_double),
         ("theta_obs_rad", C.c_double),

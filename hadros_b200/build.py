@@ -3,9 +3,9 @@
     python -m hadros_b200.build          # incremental
     python -m hadros_b200.build --force  # rebuild everything
 
-The trace kernel is compiled with --fmad=false (no contraction of a*b+c into
-an FMA) so that its FP64 arithmetic rounds like the reference's x86-64 build;
-FMAs the mixed-precision transfer wants are written as explicit intrinsics.
+The reference-arithmetic trace kernel is compiled with --fmad=false (no
+contraction of a*b+c into an FMA) so that its FP64 arithmetic rounds like the
+reference's x86-64 build; the fast-geodesic variant is compiled with FMA.
 """
 from __future__ import annotations
 
@@ -27,13 +27,14 @@ REPO = PKG.parent
 INCLUDE = REPO / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC",
-              "-Xptxas", "-v"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra"]
 
-CU_SOURCES = ["hadros_trace.cu"]
+# (source, extra nvcc flags): the reference-arithmetic kernel must not contract
+# a*b+c into FMAs; the fast-geodesic kernel does.
+CU_SOURCES = [("hadros_trace.cu", ["--fmad=false"]), ("hadros_trace_fast.cu", ["--fmad=true"])]
 CXX_SOURCES = ["hadros_host.cpp", "hadros_formats.cpp"]
-HEADERS = ["hadros_internal.h", "hadros_physics.cuh"]
+HEADERS = ["hadros_internal.h", "hadros_physics.cuh", "hadros_trace_kernel.cuh"]
 
 
 def _nvcc() -> str:
@@ -73,10 +74,10 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     headers = [CSRC / h for h in HEADERS] + [INCLUDE / "hadros_b200.h"]
     objs: list[Path] = []
     log: list[str] = []
-    for src in CU_SOURCES:
+    for src, extra in CU_SOURCES:
         obj = BUILD_DIR / (Path(src).stem + ".o")
         if force or _stale(obj, [CSRC / src] + headers):
-            _run([nvcc, *ARCH, *NVCC_FLAGS, "-I", str(INCLUDE), "-c", str(CSRC / src),
+            _run([nvcc, *ARCH, *NVCC_FLAGS, *extra, "-I", str(INCLUDE), "-c", str(CSRC / src),
                   "-o", str(obj)], log, verbose)
         objs.append(obj)
     for src in CXX_SOURCES:

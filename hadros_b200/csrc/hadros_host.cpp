@@ -246,6 +246,8 @@ int32_t hadros_params_validate(const hadros_params* p)
     if (p->profile_kind < 0 || p->profile_kind > 7) return fail(HADROS_E_ARG, "profile_kind out of range");
     if (p->source_kind < 0 || p->source_kind > 4) return fail(HADROS_E_ARG, "source_kind out of range");
     if (p->spectral_kind < 0 || p->spectral_kind > 2) return fail(HADROS_E_ARG, "spectral_kind out of range");
+    if (p->fast_geodesic != 0 && p->fast_geodesic != 1)
+        return fail(HADROS_E_ARG, "fast_geodesic must be 0 or 1");
     if (p->precision != HADROS_PRECISION_FP64 && p->precision != HADROS_PRECISION_MIXED)
         return fail(HADROS_E_ARG, "precision must be HADROS_PRECISION_FP64 or HADROS_PRECISION_MIXED");
     if (p->spectral_kind != HADROS_SPECTRAL_MONOCHROMATIC && (p->n_bins > kMaxBins))
@@ -569,6 +571,7 @@ int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s
     A.tau_E = dev_out.tau_E;
     A.I_E = static_cast<double*>(dev_out.I_E);
     A.counters = ctx->d_counters;
+    A.fast_geodesic = p->fast_geodesic;
     A.attempt_budget = ctx->attempt_budget > 0 ? ctx->attempt_budget
                                                : static_cast<int64_t>(p->max_steps) * 51 + 1;
 

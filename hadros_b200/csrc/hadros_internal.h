@@ -88,6 +88,7 @@ struct TraceArgs {
     // scratch
     unsigned long long* counters;   // [0] work cursor, [1] steps, [2] attempts, [3] aborted
     int64_t attempt_budget;
+    int32_t fast_geodesic;          // 1: geo_rhs_fast (hadros_trace_fast.cu)
 };
 
 // Host-side handle of an uploaded sigma table.
@@ -106,6 +107,8 @@ void prepare_sigma(SigmaHost& s);
 // Kernel launch (hadros_trace.cu).  `stream` is a cudaStream_t.
 int launch_trace(const TraceArgs& args, int precision, int n_sm, void* stream,
                  std::string& err);
+int launch_trace_fast(const TraceArgs& args, int precision, int n_sm, void* stream,
+                      std::string& err);
 size_t trace_smem_bytes(int precision, int sig_n, int max_bins);
 
 // Record the calling thread's hadros_last_error() message; returns `code`.

@@ -1,0 +1,12 @@
+// hadros_trace_fast.cu — the trace kernel with the fast geodesic arithmetic
+// (hadros_trace_kernel.cuh: geo_rhs_fast), compiled with FMA contraction.
+#include "hadros_trace_kernel.cuh"
+
+namespace hadros {
+
+int launch_trace_fast(const TraceArgs& args, int precision, int n_sm, void* stream, std::string& err)
+{
+    return launch_variant<1>(args, precision, n_sm, static_cast<cudaStream_t>(stream), err);
+}
+
+}  // namespace hadros

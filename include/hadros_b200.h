@@ -84,7 +84,10 @@ enum hadros_spectral_kind {
     HADROS_SPECTRAL_POWERLAW_CUTOFF = 2
 };
 
-/* Arithmetic of the transfer stage.  The geodesic is FP64 in both. */
+/* Arithmetic of the transfer stage.  The geodesic is FP64 in both.
+ * Independently, hadros_params.fast_geodesic = 1 evaluates the same RKF45 /
+ * centred-difference geodesic with fewer FP64 divisions and transcendentals
+ * and with FMA contraction: same algorithm, different rounding. */
 enum hadros_precision {
     HADROS_PRECISION_FP64 = 0,  /* every stage FP64, reference operation order */
     HADROS_PRECISION_MIXED = 1  /* FP64 geodesic; FP32 Kahan tau and I per bin */
@@ -110,7 +113,7 @@ typedef struct hadros_params {
     int32_t spectral_kind;   /* enum hadros_spectral_kind                   */
     int32_t n_bins;          /* spectral bins (ignored for monochromatic)  */
     int32_t precision;       /* enum hadros_precision                       */
-    int32_t reserved0;
+    int32_t fast_geodesic;   /* 0: reference arithmetic (default); 1: fast  */
 
     /* camera and integrator: KerrCamera(a, r_obs, theta_obs, fov_deg, nx,
      * ny, r_max, h) with KerrGeodesic tolerance (include/kerr_geodesic.hpp:

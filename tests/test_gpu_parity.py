@@ -82,3 +82,14 @@ def test_stats_count_the_work(hb, gpu_ctx, sigma_table):
     assert st["accepted_steps"] == int(img["steps"].sum())
     assert st["attempts"] == int(img["attempts"].sum())
     assert st["kernel_ms"] > 0.0
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_fast_geodesic_matches_reference(hb, gpu_ctx, sigma_table, name):
+    """fast_geodesic=1: same RKF45 and centred differences with fewer
+    divisions/transcendentals and FMA; fate and steps still exact."""
+    kw, ref = load_golden(name)
+    got = gpu_ctx.image(hb.params(**dict(kw, precision="fp64", fast=True)), sigma_table)
+    assert_parity(got, ref, RTOL_FP64, f"{name}/fast-fp64")
+    got = gpu_ctx.image(hb.params(**dict(kw, precision="mixed", fast=True)), sigma_table)
+    assert_parity(got, ref, RTOL_MIXED, f"{name}/fast-mixed", p_absolute=True)
