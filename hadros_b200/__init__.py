@@ -239,6 +239,32 @@ class Context:
                                              ids.ctypes.data, int(ids.size), C.byref(out)))
         return res
 
+    def batch(self, cams: list, sigma: SigmaTable, outputs=OUTPUTS) -> list[dict]:
+        """Trace many cameras in one launch; returns one dict per camera."""
+        n = len(cams)
+        arr = (HadrosParams * n)(*cams)
+        Ps = [int(c.nx) * int(c.ny) for c in cams]
+        Bs = [n_bins_of(c) for c in cams]
+        P, PB = sum(Ps), sum(a * b for a, b in zip(Ps, Bs))
+        fdt = np.float32 if cams[0].precision == PRECISION_MIXED else np.float64
+        shapes = {"tau": (P, np.float64), "P_surv": (P, np.float64), "I_obs": (P, np.float64),
+                  "fate": (P, np.int8), "steps": (P, np.int32), "attempts": (P, np.int32),
+                  "tau_E": (PB, fdt), "I_E": (PB, np.float64)}
+        res = {k: np.zeros(shapes[k][0], dtype=shapes[k][1]) for k in outputs}
+        out = HadrosImageOut()
+        for k, a in res.items():
+            setattr(out, k, a.ctypes.data)
+        _check(lib().hadros_batch(self.handle, C.addressof(arr), n, sigma.handle, C.byref(out)))
+        per, o, ob = [], 0, 0
+        for Pc, Bc in zip(Ps, Bs):
+            d = {}
+            for k, a in res.items():
+                d[k] = a[ob:ob + Pc * Bc].reshape(Pc, Bc) if k in ("tau_E", "I_E") else a[o:o + Pc]
+            per.append(d)
+            o += Pc
+            ob += Pc * Bc
+        return per
+
     def image_device(self, p: HadrosParams, sigma: SigmaTable, out: dict, stream=None) -> None:
         """Enqueue an image into device buffers (torch tensors or raw pointers)."""
         o = HadrosImageOut()

@@ -591,6 +591,94 @@ int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s
     return HADROS_OK;
 }
 
+
+// Many cameras in one persistent launch.  dev_out holds DEVICE pointers to
+// the concatenated outputs (camera order).
+int32_t run_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, const hadros_sigma* s,
+                  const hadros_image_out& dev_out, cudaStream_t st, bool time_kernel, int64_t* P_total,
+                  int64_t* PB_total)
+{
+    if (!ctx) return fail(HADROS_E_STATE, "context is NULL");
+    if (ctx->failed) return fail(HADROS_E_STATE, "context is in a failed state: " + ctx->err);
+    if (!s) return fail(HADROS_E_STATE, "sigma handle is NULL");
+    if (!cams || n_cams <= 0) return fail(HADROS_E_ARG, "camera list is NULL or empty");
+    for (int32_t c = 0; c < n_cams; ++c) {
+        int32_t rc = hadros_params_validate(&cams[c]);
+        if (rc) return fail(rc, "camera " + std::to_string(c) + ": " + g_last_error);
+        if (cams[c].precision != cams[0].precision || cams[c].fast_geodesic != cams[0].fast_geodesic)
+            return fail(HADROS_E_ARG, "all cameras of a batch need the same precision and fast_geodesic");
+    }
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+    std::vector<DevCam> dc(static_cast<size_t>(n_cams));
+    std::vector<DevBin> bins;
+    std::string err;
+    int64_t items = 0, binout = 0;
+    int32_t max_bins = 1;
+    for (int32_t c = 0; c < n_cams; ++c) {
+        int32_t rc = build_cam(cams[c], s->h, dc[c], bins, err);
+        if (rc) return fail(rc, "camera " + std::to_string(c) + ": " + err);
+        const int64_t P = static_cast<int64_t>(cams[c].nx) * cams[c].ny;
+        dc[c].item_begin = items;
+        dc[c].item_end = items + P;
+        dc[c].out_offset = items;
+        dc[c].binout_offset = binout;
+        items += P;
+        binout += P * dc[c].n_bins;
+        max_bins = std::max(max_bins, dc[c].n_bins);
+    }
+    *P_total = items;
+    *PB_total = binout;
+    int32_t rc;
+    const bool sigma_new = !(ctx->sig_key == s && ctx->sig_serial == sigma_serial(s) && ctx->d_sig);
+    if ((rc = upload_sigma(ctx, s, sigma_serial(s)))) return rc;
+    if ((rc = grow(ctx, &ctx->d_cams, &ctx->cams_cap, sizeof(DevCam) * dc.size(), "camera table"))) return rc;
+    if ((rc = grow(ctx, &ctx->d_bins, &ctx->bins_cap, sizeof(DevBin) * bins.size(), "bin table"))) return rc;
+    if ((e = cudaMemcpyAsync(ctx->d_cams, dc.data(), sizeof(DevCam) * dc.size(), cudaMemcpyHostToDevice, st)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(ctx->d_bins, bins.data(), sizeof(DevBin) * bins.size(), cudaMemcpyHostToDevice, st)) !=
+            cudaSuccess)
+        return cuda_fail(ctx, e, "camera upload");
+    if ((e = cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(unsigned long long), st)) != cudaSuccess)
+        return cuda_fail(ctx, e, "counter reset");
+    TraceArgs A{};
+    A.cams = static_cast<const DevCam*>(ctx->d_cams);
+    A.n_cams = n_cams;
+    A.max_bins = max_bins;
+    A.total_items = items;
+    A.pixel_ids = nullptr;
+    A.bins = static_cast<const DevBin*>(ctx->d_bins);
+    A.sig = ctx->sig_dev;
+    A.tau = dev_out.tau;
+    A.P_surv = dev_out.P_surv;
+    A.I_obs = dev_out.I_obs;
+    A.fate = dev_out.fate;
+    A.steps = dev_out.steps;
+    A.attempts = dev_out.attempts;
+    A.tau_E = dev_out.tau_E;
+    A.I_E = static_cast<double*>(dev_out.I_E);
+    A.counters = ctx->d_counters;
+    int32_t max_cap = 0;
+    for (int32_t c = 0; c < n_cams; ++c) max_cap = std::max(max_cap, cams[c].max_steps);
+    A.attempt_budget = ctx->attempt_budget > 0 ? ctx->attempt_budget : static_cast<int64_t>(max_cap) * 51 + 1;
+    A.fast_geodesic = cams[0].fast_geodesic;
+    if (items > 0) {
+        if (time_kernel) cudaEventRecord(ctx->ev0, st);
+        rc = launch_trace(A, cams[0].precision, ctx->n_sm, st, err);
+        if (rc) {
+            ctx->err = err;
+            return fail(rc, err);
+        }
+        if (time_kernel) cudaEventRecord(ctx->ev1, st);
+    }
+    ctx->stats.rays = items;
+    ctx->stats.launches = items > 0 ? 1 : 0;
+    ctx->stats.h2d_bytes = static_cast<int64_t>(sizeof(DevCam) * dc.size() + sizeof(DevBin) * bins.size()) +
+                           (sigma_new ? static_cast<int64_t>(ctx->sig_cap) : 0);
+    ctx->stats.d2h_bytes = 0;
+    return HADROS_OK;
+}
+
 // Finish a synchronous call: wait, read counters, fill stats.
 int32_t finish_sync(hadros_ctx* ctx, bool timed)
 {
@@ -696,6 +784,81 @@ int32_t hadros_image_device(hadros_ctx* ctx, const hadros_params* p, const hadro
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : (ctx ? ctx->stream : nullptr);
         const int32_t rc = run_image(ctx, p, s, nullptr, 0, *dev_out, st, false);
         return rc ? rc : ok();
+    } catch (const std::exception& ex) {
+        return fail(HADROS_E_NOMEM, ex.what());
+    }
+}
+
+int32_t hadros_batch_device(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, const hadros_sigma* s,
+                            const hadros_image_out* dev_out, void* stream)
+{
+    if (!dev_out) return fail(HADROS_E_ARG, "output struct is NULL");
+    try {
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : (ctx ? ctx->stream : nullptr);
+        int64_t P = 0, PB = 0;
+        const int32_t rc = run_batch(ctx, cams, n_cams, s, *dev_out, st, false, &P, &PB);
+        return rc ? rc : ok();
+    } catch (const std::exception& ex) {
+        return fail(HADROS_E_NOMEM, ex.what());
+    }
+}
+
+int32_t hadros_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, const hadros_sigma* s,
+                     const hadros_image_out* out)
+{
+    if (!ctx) return fail(HADROS_E_STATE, "context is NULL");
+    if (!out || !cams || n_cams <= 0) return fail(HADROS_E_ARG, "NULL argument or empty camera list");
+    try {
+        const auto t0 = std::chrono::steady_clock::now();
+        int64_t P = 0, PB = 0;
+        for (int32_t c = 0; c < n_cams; ++c) {
+            if (hadros_params_validate(&cams[c])) return fail(HADROS_E_ARG, "camera " + std::to_string(c) + ": " + g_last_error);
+            const int64_t pc = static_cast<int64_t>(cams[c].nx) * cams[c].ny;
+            P += pc;
+            PB += pc * (cams[c].spectral_kind == HADROS_SPECTRAL_MONOCHROMATIC ? 1 : std::max(cams[c].n_bins, 1));
+        }
+        const size_t fsz = cams[0].precision == HADROS_PRECISION_MIXED ? 4 : 8;
+        auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+        size_t o = 0;
+        const size_t o_tau = o; o = al(o + (out->tau ? 8 * P : 0));
+        const size_t o_P = o; o = al(o + (out->P_surv ? 8 * P : 0));
+        const size_t o_I = o; o = al(o + (out->I_obs ? 8 * P : 0));
+        const size_t o_st = o; o = al(o + (out->steps ? 4 * P : 0));
+        const size_t o_at = o; o = al(o + (out->attempts ? 4 * P : 0));
+        const size_t o_f = o; o = al(o + (out->fate ? P : 0));
+        const size_t o_tE = o; o = al(o + (out->tau_E ? fsz * PB : 0));
+        const size_t o_IE = o; o = al(o + (out->I_E ? 8 * PB : 0));
+        int32_t rc = grow(ctx, &ctx->d_out, &ctx->out_cap, o, "output buffers");
+        if (rc) return rc;
+        unsigned char* base = static_cast<unsigned char*>(ctx->d_out);
+        hadros_image_out d{};
+        d.tau = out->tau ? reinterpret_cast<double*>(base + o_tau) : nullptr;
+        d.P_surv = out->P_surv ? reinterpret_cast<double*>(base + o_P) : nullptr;
+        d.I_obs = out->I_obs ? reinterpret_cast<double*>(base + o_I) : nullptr;
+        d.steps = out->steps ? reinterpret_cast<int32_t*>(base + o_st) : nullptr;
+        d.attempts = out->attempts ? reinterpret_cast<int32_t*>(base + o_at) : nullptr;
+        d.fate = out->fate ? reinterpret_cast<int8_t*>(base + o_f) : nullptr;
+        d.tau_E = out->tau_E ? static_cast<void*>(base + o_tE) : nullptr;
+        d.I_E = out->I_E ? static_cast<void*>(base + o_IE) : nullptr;
+        int64_t P2 = 0, PB2 = 0;
+        rc = run_batch(ctx, cams, n_cams, s, d, ctx->stream, true, &P2, &PB2);
+        if (rc) return rc;
+        struct Cp { void* h; const void* d; size_t n; } cps[8] = {
+            {out->tau, d.tau, 8 * size_t(P)}, {out->P_surv, d.P_surv, 8 * size_t(P)},
+            {out->I_obs, d.I_obs, 8 * size_t(P)}, {out->steps, d.steps, 4 * size_t(P)},
+            {out->attempts, d.attempts, 4 * size_t(P)}, {out->fate, d.fate, size_t(P)},
+            {out->tau_E, d.tau_E, fsz * size_t(PB)}, {out->I_E, d.I_E, 8 * size_t(PB)}};
+        int64_t d2h = 4 * sizeof(unsigned long long);
+        for (auto& c : cps) {
+            if (!c.h || c.n == 0) continue;
+            d2h += static_cast<int64_t>(c.n);
+            cudaError_t e = cudaMemcpyAsync(c.h, c.d, c.n, cudaMemcpyDeviceToHost, ctx->stream);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "output download");
+        }
+        rc = finish_sync(ctx, true);
+        ctx->stats.d2h_bytes = d2h;
+        ctx->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return rc;
     } catch (const std::exception& ex) {
         return fail(HADROS_E_NOMEM, ex.what());
     }

@@ -13,6 +13,20 @@
 
 namespace hadros {
 
+// Minimum resident blocks per SM asked of the register allocator.
+#ifndef HADROS_MIN_BLOCKS
+#define HADROS_MIN_BLOCKS 1
+#endif
+// Inline the geodesic RHS at its call sites (1) or keep one out-of-line copy (0).
+#ifndef HADROS_RHS_INLINE
+#define HADROS_RHS_INLINE 1
+#endif
+#if HADROS_RHS_INLINE
+#define HADROS_RHS_ATTR __device__ __forceinline__
+#else
+#define HADROS_RHS_ATTR __device__ __noinline__
+#endif
+
 namespace {
 
 // RKF45 weights of y4 and y5 (kerr_geodesic.cpp:310-311), folded at compile
@@ -42,7 +56,7 @@ __device__ __forceinline__ double fd_force(double d00, double d03, double d11, d
 // KerrGeodesic::rhs (kerr_geodesic.cpp:83-135) with sin/cos of theta given.
 // The reference evaluates g^{-1}(r +- eps) and g^{-1}(theta +- eps) once per
 // (mu, nu) pair; they are evaluated once here (identical values).
-__device__ __forceinline__ void geo_rhs(double a, double r, double th, double s, double c,
+HADROS_RHS_ATTR void geo_rhs(double a, double r, double th, double s, double c,
                                         double pr, double pth, double pt, double pph, K5& d)
 {
     M5 gi;
@@ -137,7 +151,7 @@ __device__ __forceinline__ Trig trig_shift(double s, double c, double d)
     return t;
 }
 
-__device__ __forceinline__ void geo_rhs_fast(double a, double r, double th, double s, double c,
+HADROS_RHS_ATTR void geo_rhs_fast(double a, double r, double th, double s, double c,
                                              double pr, double pth, double pt, double pph, K5& d)
 {
     const double a2 = a * a;
@@ -223,7 +237,7 @@ __host__ __device__ inline SmemLayout smem_layout(int precision, int n, int max_
 enum Phase : int { kNeedRay = 0, kStepStart = 1, kAttempt = 2, kDone = 3 };
 
 template <int MIXED, int FAST>
-__global__ void __launch_bounds__(kTPB) trace_kernel(const TraceArgs A)
+__global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const TraceArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int n_sig = A.sig.n;

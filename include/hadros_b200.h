@@ -285,8 +285,22 @@ int32_t hadros_image_pixels(hadros_ctx* ctx, const hadros_params* p,
 int32_t hadros_image_device(hadros_ctx* ctx, const hadros_params* p,
                             const hadros_sigma* s,
                             const hadros_image_out* dev_out, void* stream);
+/* Many cameras in one persistent launch (parameter scans: cameras of
+ * different size, spin, inclination, profile, rho0 and bins).  Outputs are
+ * concatenated in camera order: per-pixel arrays hold sum(nx*ny) entries,
+ * per-bin arrays sum(nx*ny*n_bins).  All cameras share the sigma table and
+ * must share precision and fast_geodesic.  Replaces the reference's serial
+ * per-tile host loop (apps/compute_kerr_image_cuda.cu:2418-2483) repeated per
+ * parameter point by the scan drivers (scripts/run_robustness_scans.py:81-145). */
+int32_t hadros_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams,
+                     const hadros_sigma* s, const hadros_image_out* out);
+int32_t hadros_batch_device(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams,
+                            const hadros_sigma* s, const hadros_image_out* dev_out,
+                            void* stream);
+
 /* Wait for the context's work and report the first deferred error. */
 int32_t hadros_ctx_synchronize(hadros_ctx* ctx);
+
 
 /* ---- the reference's image files (host only) ------------------------------ */
 

@@ -93,3 +93,29 @@ def test_fast_geodesic_matches_reference(hb, gpu_ctx, sigma_table, name):
     assert_parity(got, ref, RTOL_FP64, f"{name}/fast-fp64")
     got = gpu_ctx.image(hb.params(**dict(kw, precision="mixed", fast=True)), sigma_table)
     assert_parity(got, ref, RTOL_MIXED, f"{name}/fast-mixed", p_absolute=True)
+
+
+def test_batch_equals_separate_images(hb, gpu_ctx, sigma_table):
+    """One persistent launch over cameras of different size, spin, inclination,
+    profile, source, spectrum and bin count gives each camera's own image."""
+    from hadros_b200 import workloads as W
+    rng = np.random.default_rng(5)
+    cams = []
+    for k in range(6):
+        cams.append(hb.params(**W.mixed_512(
+            nx=int(rng.integers(1, 9)), ny=int(rng.integers(1, 9)), h=0.05,
+            a_spin=float(rng.uniform(0, 0.998)), theta_obs_deg=float(rng.uniform(5, 85)),
+            profile=k % 8, source=k % 5, spectral=k % 3, n_bins=int(rng.integers(1, 12)),
+            precision="mixed")))
+    got = gpu_ctx.batch(cams, sigma_table)
+    for k, c in enumerate(cams):
+        one = gpu_ctx.image(c, sigma_table)
+        for key in one:
+            np.testing.assert_array_equal(got[k][key], one[key], err_msg=f"camera {k} {key}")
+
+
+def test_batch_rejects_mixed_precisions(hb, gpu_ctx, sigma_table):
+    a = hb.params(nx=2, ny=2, precision="fp64")
+    b = hb.params(nx=2, ny=2, precision="mixed")
+    with pytest.raises(hb.HadrosError, match="same precision"):
+        gpu_ctx.batch([a, b], sigma_table)
