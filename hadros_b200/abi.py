@@ -145,6 +145,8 @@ SIGNATURES = {
     "hadros_batch": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, P(HadrosImageOut)]),
     "hadros_batch_device": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
                                         P(HadrosImageOut), C.c_void_p]),
+    "hadros_image_device_noalloc": (C.c_int32, [P(HadrosParams), C.c_void_p, P(HadrosImageOut),
+                                                C.c_void_p]),
     "hadros_image_filename": (C.c_int32, [P(HadrosParams), C.c_int32, C.c_char_p, C.c_double,
                                           C.c_double, C.c_char_p, C.c_char_p, C.c_int32]),
     "hadros_write_dat": (C.c_int32, [C.c_char_p, P(HadrosParams), C.c_char_p, C.c_double,

@@ -301,6 +301,21 @@ int32_t hadros_batch_device(hadros_ctx* ctx, const hadros_params* cams, int32_t 
 /* Wait for the context's work and report the first deferred error. */
 int32_t hadros_ctx_synchronize(hadros_ctx* ctx);
 
+/* Whole image into DEVICE buffers without allocating any GPU memory.  No
+ * counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (a framework's caching allocator owns the device memory, or a fixed
+ * per-tenant memory budget forbids new allocations): it needs no context,
+ * and its scratch (work counters, camera and bin tables, sigma table) is a
+ * static ~60 KB device array inside this library, held by every GPU that
+ * loads it until the process exits.  Runs on the current device, on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream), with the
+ * reference-arithmetic kernel, and returns when the image is done.  Limits:
+ * at most 1024 sigma rows and 64 spectral bins (else HADROS_E_ARG);
+ * fast_geodesic must be 0.  The first call on a device looks up the array's
+ * address (make it outside stream capture).  All calls share the array:
+ * calls that overlap on the GPU race; serialize them. */
+int32_t hadros_image_device_noalloc(const hadros_params* p, const hadros_sigma* s,
+                                    const hadros_image_out* dev_out, void* stream);
 
 /* ---- the reference's image files (host only) ------------------------------ */
 
