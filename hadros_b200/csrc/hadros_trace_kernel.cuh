@@ -13,9 +13,13 @@
 
 namespace hadros {
 
-// Minimum resident blocks per SM asked of the register allocator.
+// Minimum resident blocks per SM asked of the register allocator.  4 blocks
+// of 128 threads caps the kernel at 128 registers: measured on B200 (256x256
+// mixed camera) 1.72x faster than the uncapped 162 registers / 3 blocks for
+// the reference-arithmetic kernel and 1.31x for the fast one; 5 blocks (96
+// registers) spills more and is slower again.
 #ifndef HADROS_MIN_BLOCKS
-#define HADROS_MIN_BLOCKS 1
+#define HADROS_MIN_BLOCKS 4
 #endif
 // Inline the geodesic RHS at its call sites (1) or keep one out-of-line copy (0).
 #ifndef HADROS_RHS_INLINE
