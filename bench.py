@@ -251,7 +251,7 @@ def gpu_arm(args) -> None:
         return float(t.item())
 
     kw = W.mixed_512()
-    p = hb.params(**kw)
+    p = hb.params(**kw)          # library default: fast geodesic arithmetic
     E, g2, s = W.synthetic_sigma_arrays()
     sig = hb.SigmaTable.from_arrays(E, s, g2)
     ctx = hb.Context(local)

@@ -231,6 +231,7 @@ void hadros_params_default(hadros_params* p)
     p->spec_e_max_GeV = 1.0e12;
     p->n_bins = 8;
     p->precision = HADROS_PRECISION_FP64;
+    p->fast_geodesic = 1;
 }
 
 int32_t hadros_params_validate(const hadros_params* p)

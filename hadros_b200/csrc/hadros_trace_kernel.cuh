@@ -186,14 +186,34 @@ HADROS_RHS_ATTR void geo_rhs_fast(double a, double r, double th, double s, doubl
     }
 }
 
+// sin and cos of th0 + d from those of th0, |d| < 0.05: Taylor series of
+// sin d and cos d to d^9 and d^8 (the next terms are below 3e-20).
+__device__ __forceinline__ void sincos_shift(double s0, double c0, double d, double* s, double* c)
+{
+    const double d2 = d * d;
+    const double cd = 1.0 + d2 * (-1.0 / 2 + d2 * (1.0 / 24 + d2 * (-1.0 / 720 + d2 * (1.0 / 40320))));
+    const double sd = d * (1.0 + d2 * (-1.0 / 6 + d2 * (1.0 / 120 + d2 * (-1.0 / 5040 + d2 * (1.0 / 362880)))));
+    *s = s0 * cd + c0 * sd;
+    *c = c0 * cd - s0 * sd;
+}
+
+// RHS at a stage point.  The fast variant reuses sin/cos of the step's base
+// angle th0 (s0, c0) through sincos_shift when the stage angle is close.
 template <int FAST>
 __device__ __forceinline__ void geo_rhs_sel(double a, double r, double th, double pr, double pth,
-                                            double pt, double pph, K5& d)
+                                            double pt, double pph, K5& d, double th0, double s0,
+                                            double c0)
 {
     double s, c;
-    sincos(th, &s, &c);
-    if (FAST) geo_rhs_fast(a, r, th, s, c, pr, pth, pt, pph, d);
-    else geo_rhs(a, r, th, s, c, pr, pth, pt, pph, d);
+    if (FAST) {
+        const double dt = th - th0;
+        if (fabs(dt) < 0.05) sincos_shift(s0, c0, dt, &s, &c);
+        else sincos(th, &s, &c);
+        geo_rhs_fast(a, r, th, s, c, pr, pth, pt, pph, d);
+    } else {
+        sincos(th, &s, &c);
+        geo_rhs(a, r, th, s, c, pr, pth, pt, pph, d);
+    }
 }
 
 // wrapped_delta_phi (kerr_camera.cpp:31-44)
@@ -284,6 +304,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
     double a = 0.0, r = 0.0, th = 0.0, ph = 0.0, pr = 0.0, pth = 0.0, pt = 0.0, pph = 0.0;
     double r_prev = 0.0, th_prev = 0.0, ph_prev = 0.0, E_obs = 1.0, h = 0.0;
     K5 k1{};
+    double s_base = 0.0, c_base = 1.0;   // sin/cos of theta at the step start
     int fate = HADROS_FATE_TRUNCATED;
 
     while (true) {
@@ -529,6 +550,8 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
             r_prev = r;
             th_prev = th;
             ph_prev = ph;
+            s_base = s;
+            c_base = c;
             h = cam->h0;
             att_in_step = 0;
             phase = kAttempt;
@@ -553,25 +576,25 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
         }
         K5 k2, k3, k4, k5, k6;
         geo_rhs_sel<FAST>(a, r + cf[0] * k1.r, th + cf[0] * k1.th, pr + cf[0] * k1.pr,
-                   pth + cf[0] * k1.pth, pt, pph, k2);
+                   pth + cf[0] * k1.pth, pt, pph, k2, th, s_base, c_base);
         geo_rhs_sel<FAST>(a, r + cf[1] * k1.r + cf[2] * k2.r, th + cf[1] * k1.th + cf[2] * k2.th,
                    pr + cf[1] * k1.pr + cf[2] * k2.pr, pth + cf[1] * k1.pth + cf[2] * k2.pth,
-                   pt, pph, k3);
+                   pt, pph, k3, th, s_base, c_base);
         geo_rhs_sel<FAST>(a, r + cf[3] * k1.r + cf[4] * k2.r + cf[5] * k3.r,
                    th + cf[3] * k1.th + cf[4] * k2.th + cf[5] * k3.th,
                    pr + cf[3] * k1.pr + cf[4] * k2.pr + cf[5] * k3.pr,
-                   pth + cf[3] * k1.pth + cf[4] * k2.pth + cf[5] * k3.pth, pt, pph, k4);
+                   pth + cf[3] * k1.pth + cf[4] * k2.pth + cf[5] * k3.pth, pt, pph, k4, th, s_base, c_base);
         geo_rhs_sel<FAST>(a, r + cf[6] * k1.r + cf[7] * k2.r + cf[8] * k3.r + cf[9] * k4.r,
                    th + cf[6] * k1.th + cf[7] * k2.th + cf[8] * k3.th + cf[9] * k4.th,
                    pr + cf[6] * k1.pr + cf[7] * k2.pr + cf[8] * k3.pr + cf[9] * k4.pr,
                    pth + cf[6] * k1.pth + cf[7] * k2.pth + cf[8] * k3.pth + cf[9] * k4.pth,
-                   pt, pph, k5);
+                   pt, pph, k5, th, s_base, c_base);
         geo_rhs_sel<FAST>(a,
                    r + cf[10] * k1.r + cf[11] * k2.r + cf[12] * k3.r + cf[13] * k4.r + cf[14] * k5.r,
                    th + cf[10] * k1.th + cf[11] * k2.th + cf[12] * k3.th + cf[13] * k4.th + cf[14] * k5.th,
                    pr + cf[10] * k1.pr + cf[11] * k2.pr + cf[12] * k3.pr + cf[13] * k4.pr + cf[14] * k5.pr,
                    pth + cf[10] * k1.pth + cf[11] * k2.pth + cf[12] * k3.pth + cf[13] * k4.pth + cf[14] * k5.pth,
-                   pt, pph, k6);
+                   pt, pph, k6, th, s_base, c_base);
 #define HAD_Y4(f) (A1 * k1.f + A3 * k3.f + A4 * k4.f - A5 * k5.f)
 #define HAD_Y5(f) (B1 * k1.f + B3 * k3.f + B4 * k4.f - B5 * k5.f + B6 * k6.f)
         const double y4r = r + h * HAD_Y4(r), y5r = r + h * HAD_Y5(r);
@@ -603,11 +626,11 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                 const double h0 = cam->h0;
                 K5 q2, q3, q4;
                 geo_rhs_sel<FAST>(a, r + 0.5 * h0 * k1.r, th + 0.5 * h0 * k1.th, pr + 0.5 * h0 * k1.pr,
-                           pth + 0.5 * h0 * k1.pth, pt, pph, q2);
+                           pth + 0.5 * h0 * k1.pth, pt, pph, q2, th, s_base, c_base);
                 geo_rhs_sel<FAST>(a, r + 0.5 * h0 * q2.r, th + 0.5 * h0 * q2.th, pr + 0.5 * h0 * q2.pr,
-                           pth + 0.5 * h0 * q2.pth, pt, pph, q3);
+                           pth + 0.5 * h0 * q2.pth, pt, pph, q3, th, s_base, c_base);
                 geo_rhs_sel<FAST>(a, r + h0 * q3.r, th + h0 * q3.th, pr + h0 * q3.pr, pth + h0 * q3.pth,
-                           pt, pph, q4);
+                           pt, pph, q4, th, s_base, c_base);
                 r += h0 * (k1.r + 2.0 * q2.r + 2.0 * q3.r + q4.r) / 6.0;
                 th += h0 * (k1.th + 2.0 * q2.th + 2.0 * q3.th + q4.th) / 6.0;
                 ph += h0 * (k1.ph + 2.0 * q2.ph + 2.0 * q3.ph + q4.ph) / 6.0;

@@ -113,7 +113,7 @@ typedef struct hadros_params {
     int32_t spectral_kind;   /* enum hadros_spectral_kind                   */
     int32_t n_bins;          /* spectral bins (ignored for monochromatic)  */
     int32_t precision;       /* enum hadros_precision                       */
-    int32_t fast_geodesic;   /* 0: reference arithmetic (default); 1: fast  */
+    int32_t fast_geodesic;   /* 1: fast geodesic arithmetic (default); 0: reference */
 
     /* camera and integrator: KerrCamera(a, r_obs, theta_obs, fov_deg, nx,
      * ny, r_max, h) with KerrGeodesic tolerance (include/kerr_geodesic.hpp:
@@ -206,7 +206,7 @@ const char* hadros_status_string(int32_t status);
 /* Message of the last failing call on this host thread ("" if none). */
 const char* hadros_last_error(void);
 
-/* Reference defaults: KerrCamera args of compute_kerr_geodesics
+/* Reference defaults (and fast_geodesic = 1): KerrCamera args of compute_kerr_geodesics
  * (apps/compute_kerr_geodesics.cpp:26-34), argv defaults of
  * compute_kerr_image_from_cache (apps/compute_kerr_image_from_cache.cpp:
  * 33-55), tolerance 1e-6, max_steps 200000, UHESourceParams/UHESpectralParams

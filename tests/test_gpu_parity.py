@@ -14,14 +14,14 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("name", golden_names())
 def test_fp64_matches_reference(hb, gpu_ctx, sigma_table, name):
     kw, ref = load_golden(name)
-    got = gpu_ctx.image(hb.params(**dict(kw, precision="fp64")), sigma_table)
+    got = gpu_ctx.image(hb.params(**dict(kw, precision="fp64", fast=False)), sigma_table)
     assert_parity(got, ref, RTOL_FP64, f"{name}/fp64")
 
 
 @pytest.mark.parametrize("name", golden_names())
 def test_mixed_matches_reference(hb, gpu_ctx, sigma_table, name):
     kw, ref = load_golden(name)
-    got = gpu_ctx.image(hb.params(**dict(kw, precision="mixed")), sigma_table)
+    got = gpu_ctx.image(hb.params(**dict(kw, precision="mixed", fast=False)), sigma_table)
     assert got["tau_E"].dtype == np.float32
     assert_parity(got, ref, RTOL_MIXED, f"{name}/mixed", p_absolute=True)
 

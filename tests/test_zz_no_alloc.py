@@ -47,9 +47,10 @@ def test_noalloc_matches_ordinary_entry_point_twice(hb, gpu_ctx, sigma_table, pr
     import torch
     from hadros_b200 import workloads as W
     torch.cuda.set_device(0)
-    cases = [W.mixed_512(nx=9, ny=7, h=0.05, precision=precision),
+    # the no-alloc entry point runs the reference-arithmetic kernel (fast=False)
+    cases = [W.mixed_512(nx=9, ny=7, h=0.05, precision=precision, fast=False),
              W.plain_tracer_32(nx=5, ny=6, r_obs_rg=60.0, r_max_rg=120.0, fov_deg=25.0, h=0.05,
-                               precision=precision)]
+                               precision=precision, fast=False)]
     for kw in cases:
         p = hb.params(**kw)
         ref = gpu_ctx.image(p, sigma_table)
@@ -64,11 +65,11 @@ def test_noalloc_rejects_sizes_beyond_its_limits(hb, sigma_table):
     import torch
     torch.cuda.set_device(0)
     out = hb.HadrosImageOut()
-    p = hb.params(spectral="powerlaw_cutoff", n_bins=65, nx=2, ny=2)
+    p = hb.params(spectral="powerlaw_cutoff", n_bins=65, nx=2, ny=2, fast=False)
     rc = hb.lib().hadros_image_device_noalloc(C.byref(p), sigma_table.handle, C.byref(out), None)
     assert rc == 1 and b"64 spectral bins" in hb.lib().hadros_last_error()
     E = np.logspace(4, 12, 1025)
     big = hb.SigmaTable.from_arrays(E, 1e-35 * E ** 0.3)
-    rc = hb.lib().hadros_image_device_noalloc(C.byref(hb.params(nx=2, ny=2)), big.handle,
+    rc = hb.lib().hadros_image_device_noalloc(C.byref(hb.params(nx=2, ny=2, fast=False)), big.handle,
                                                C.byref(out), None)
     assert rc == 1 and b"1024" in hb.lib().hadros_last_error()
