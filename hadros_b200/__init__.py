@@ -178,6 +178,42 @@ def spectral_bins(p: HadrosParams, sigma: SigmaTable) -> dict:
 OUTPUTS = ("tau", "P_surv", "I_obs", "fate", "steps", "attempts", "tau_E", "I_E")
 
 
+def pack_paths(points: np.ndarray, npoints: np.ndarray) -> np.ndarray:
+    """[rows, cap, 7] path buffer -> points packed back to back (cut at cap)."""
+    cap = points.shape[1]
+    return np.concatenate([points[k, :min(int(n), cap)] for k, n in enumerate(npoints)] or
+                          [np.zeros((0, 7))])
+
+
+def write_kgeo(path, p: HadrosParams, npoints, points, pixel_ids=None, fate=None) -> None:
+    """KGEO geodesic cache file (the reference's compute_kerr_geodesics format)."""
+    n = np.ascontiguousarray(npoints, dtype=np.int32)
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    ids = None if pixel_ids is None else np.ascontiguousarray(pixel_ids, dtype=np.int32)
+    fa = None if fate is None else np.ascontiguousarray(fate, dtype=np.int8)
+    _check(lib().hadros_write_kgeo(str(path).encode(), C.byref(p), int(n.size),
+                                   None if ids is None else ids.ctypes.data,
+                                   None if fa is None else fa.ctypes.data, n.ctypes.data,
+                                   pts.ctypes.data if pts.size else None))
+
+
+def read_kgeo(path) -> dict:
+    """Read a KGEO file: nx, ny, a, and per ray pixel id, captured, npoints,
+    alpha, beta, plus the packed points [sum(npoints), 7]."""
+    nx, ny, nr = C.c_int32(), C.c_int32(), C.c_int32()
+    a, npts = C.c_double(), C.c_int64()
+    _check(lib().hadros_kgeo_info(str(path).encode(), C.byref(nx), C.byref(ny), C.byref(a),
+                                  C.byref(nr), C.byref(npts)))
+    R = nr.value
+    out = {"pixel_ids": np.zeros(R, np.int32), "captured": np.zeros(R, np.int8),
+           "npoints": np.zeros(R, np.int32), "alpha": np.zeros(R), "beta": np.zeros(R),
+           "points": np.zeros((npts.value, 7))}
+    _check(lib().hadros_read_kgeo(str(path).encode(), *(out[k].ctypes.data for k in
+                                  ("pixel_ids", "captured", "npoints", "alpha", "beta", "points"))))
+    out.update(nx=nx.value, ny=ny.value, a_spin=a.value)
+    return out
+
+
 class Context:
     """A CUDA device context (hadros_ctx): one stream and its buffers."""
 
@@ -264,6 +300,42 @@ class Context:
             o += Pc
             ob += Pc * Bc
         return per
+
+    def trace_paths(self, p: HadrosParams, pixel_ids=None, max_points: int = 50000) -> dict:
+        """Record every pixel's path points (r, theta, x, y, z, dl, redshift).
+
+        Returns ``points`` [rows, max_points, 7], ``npoints`` and ``fate``."""
+        rows = int(p.nx) * int(p.ny) if pixel_ids is None else len(pixel_ids)
+        pts = np.zeros((rows, max_points, 7))
+        n = np.zeros(rows, dtype=np.int32)
+        f = np.zeros(rows, dtype=np.int8)
+        ids = None if pixel_ids is None else np.ascontiguousarray(pixel_ids, dtype=np.int32)
+        _check(lib().hadros_trace_paths(self.handle, C.byref(p), None if ids is None else ids.ctypes.data,
+                                        0 if ids is None else int(ids.size), int(max_points),
+                                        pts.ctypes.data, n.ctypes.data, f.ctypes.data))
+        return {"points": pts, "npoints": n, "fate": f}
+
+    def transfer_paths(self, p: HadrosParams, sigma: SigmaTable, npoints, points, fate=None,
+                       outputs=("tau", "P_surv", "I_obs", "fate", "steps", "tau_E", "I_E")) -> dict:
+        """Transfer over cached paths: points packed back to back [sum(npoints), 7]."""
+        n = np.ascontiguousarray(npoints, dtype=np.int32)
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 7)
+        if pts.shape[0] != int(n.sum()):
+            raise ValueError("points must hold sum(npoints) rows of 7 doubles")
+        fa = None if fate is None else np.ascontiguousarray(fate, dtype=np.int8)
+        P, B = int(n.size), n_bins_of(p)
+        fdt = np.float32 if p.precision == PRECISION_MIXED else np.float64
+        shapes = {"tau": (P, np.float64), "P_surv": (P, np.float64), "I_obs": (P, np.float64),
+                  "fate": (P, np.int8), "steps": (P, np.int32),
+                  "tau_E": ((P, B), fdt), "I_E": ((P, B), np.float64)}
+        res = {k: np.zeros(shapes[k][0], dtype=shapes[k][1]) for k in outputs}
+        out = HadrosImageOut()
+        for k, a in res.items():
+            setattr(out, k, a.ctypes.data)
+        _check(lib().hadros_transfer_paths(self.handle, C.byref(p), sigma.handle, P, n.ctypes.data,
+                                           None if fa is None else fa.ctypes.data,
+                                           pts.ctypes.data if pts.size else None, C.byref(out)))
+        return res
 
     def image_device(self, p: HadrosParams, sigma: SigmaTable, out: dict, stream=None) -> None:
         """Enqueue an image into device buffers (torch tensors or raw pointers)."""

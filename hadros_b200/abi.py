@@ -147,6 +147,16 @@ SIGNATURES = {
                                         P(HadrosImageOut), C.c_void_p]),
     "hadros_image_device_noalloc": (C.c_int32, [P(HadrosParams), C.c_void_p, P(HadrosImageOut),
                                                 C.c_void_p]),
+    "hadros_trace_paths": (C.c_int32, [C.c_void_p, P(HadrosParams), C.c_void_p, C.c_int32, C.c_int32,
+                                       C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hadros_transfer_paths": (C.c_int32, [C.c_void_p, P(HadrosParams), C.c_void_p, C.c_int32,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, P(HadrosImageOut)]),
+    "hadros_write_kgeo": (C.c_int32, [C.c_char_p, P(HadrosParams), C.c_int32, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]),
+    "hadros_kgeo_info": (C.c_int32, [C.c_char_p, P(C.c_int32), P(C.c_int32), P(C.c_double),
+                                     P(C.c_int32), P(C.c_int64)]),
+    "hadros_read_kgeo": (C.c_int32, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p]),
     "hadros_image_filename": (C.c_int32, [P(HadrosParams), C.c_int32, C.c_char_p, C.c_double,
                                           C.c_double, C.c_char_p, C.c_char_p, C.c_int32]),
     "hadros_write_dat": (C.c_int32, [C.c_char_p, P(HadrosParams), C.c_char_p, C.c_double,

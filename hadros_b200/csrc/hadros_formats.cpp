@@ -207,4 +207,129 @@ int32_t hadros_write_kimg(const char* path, const hadros_params* p, double mev_E
     return ok ? HADROS_OK : ferr(HADROS_E_IO, std::string("write failed: ") + path);
 }
 
+int32_t hadros_write_kgeo(const char* path, const hadros_params* p, int32_t n_rays, const int32_t* pixel_ids,
+                          const int8_t* fate, const int32_t* npoints, const double* points)
+{
+    if (!path || !kinds_ok(p) || n_rays < 0 || (n_rays > 0 && (!npoints || !points)))
+        return ferr(HADROS_E_ARG, "bad argument");
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return ferr(HADROS_E_IO, std::string("Could not open ") + path);
+    const int32_t hdr[4] = {0x4B47454F, 1, p->nx, p->ny};
+    std::fwrite(hdr, sizeof(hdr), 1, f);
+    std::fwrite(&p->a_spin, sizeof(double), 1, f);
+    int64_t off = 0;
+    for (int32_t k = 0; k < n_rays; ++k) {
+        const int32_t pid = pixel_ids ? pixel_ids[k] : k;
+        const int32_t i = pid % p->nx, j = pid / p->nx;
+        unsigned char rh[40] = {0};
+        const int32_t ints[5] = {i * p->ny + j, i, j, (fate && fate[k] == HADROS_FATE_CAPTURED) ? 1 : 0, npoints[k]};
+        const double ab[2] = {pixel_u(p, i), pixel_v(p, j)};
+        std::memcpy(rh, ints, sizeof(ints));
+        std::memcpy(rh + 24, ab, sizeof(ab));
+        std::fwrite(rh, sizeof(rh), 1, f);
+        if (npoints[k] > 0) std::fwrite(points + 7 * off, 56, static_cast<size_t>(npoints[k]), f);
+        off += npoints[k];
+    }
+    const bool ok = std::ferror(f) == 0;
+    std::fclose(f);
+    return ok ? HADROS_OK : ferr(HADROS_E_IO, std::string("write failed: ") + path);
+}
+
+namespace {
+
+// Walk a KGEO file; with sink arrays NULL only counts.
+int32_t kgeo_walk(const char* path, int32_t* nx, int32_t* ny, double* a, int32_t* n_rays, int64_t* n_points,
+                  int32_t* pixel_ids, int8_t* captured, int32_t* npoints, double* alpha, double* beta,
+                  double* points)
+{
+    if (!path) return ferr(HADROS_E_ARG, "path is NULL");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return ferr(HADROS_E_IO, std::string("Could not open geodesic cache ") + path);
+    int32_t hdr[4];
+    double spin = 0.0;
+    if (std::fread(hdr, sizeof(hdr), 1, f) != 1 || std::fread(&spin, sizeof(double), 1, f) != 1) {
+        std::fclose(f);
+        return ferr(HADROS_E_IO, "Invalid binary geodesic cache: short header");
+    }
+    if (hdr[0] != 0x4B47454F) {   // apps/compute_kerr_image_from_cache.cpp:385-389
+        std::fclose(f);
+        return ferr(HADROS_E_IO, "Invalid binary geodesic cache: bad magic number");
+    }
+    if (hdr[1] != 1) {
+        std::fclose(f);
+        return ferr(HADROS_E_IO, "Unsupported binary geodesic cache version: " + std::to_string(hdr[1]));
+    }
+    if (hdr[2] <= 0 || hdr[3] <= 0) {
+        std::fclose(f);
+        return ferr(HADROS_E_IO, "Invalid binary geodesic cache: bad image size");
+    }
+    int32_t rays = 0;
+    int64_t pts = 0;
+    unsigned char rh[40];
+    while (std::fread(rh, sizeof(rh), 1, f) == 1) {
+        int32_t ints[5];
+        double ab[2];
+        std::memcpy(ints, rh, sizeof(ints));
+        std::memcpy(ab, rh + 24, sizeof(ab));
+        if (ints[4] < 0) {   // :666-669
+            std::fclose(f);
+            return ferr(HADROS_E_IO, "Invalid ray with negative number of points");
+        }
+        if (ints[1] < 0 || ints[1] >= hdr[2] || ints[2] < 0 || ints[2] >= hdr[3]) {
+            std::fclose(f);
+            return ferr(HADROS_E_IO, "Invalid binary geodesic cache: pixel index outside the image");
+        }
+        if (pixel_ids) {
+            pixel_ids[rays] = ints[2] * hdr[2] + ints[1];
+            captured[rays] = static_cast<int8_t>(ints[3] != 0);
+            npoints[rays] = ints[4];
+            alpha[rays] = ab[0];
+            beta[rays] = ab[1];
+        }
+        if (ints[4] > 0) {
+            if (points) {
+                if (std::fread(points + 7 * pts, 56, static_cast<size_t>(ints[4]), f) != static_cast<size_t>(ints[4])) {
+                    std::fclose(f);
+                    return ferr(HADROS_E_IO, "Unexpected end of file while reading points");
+                }
+            } else if (std::fseek(f, 56L * ints[4], SEEK_CUR) != 0) {
+                std::fclose(f);
+                return ferr(HADROS_E_IO, "Unexpected end of file while reading points");
+            }
+        }
+        ++rays;
+        pts += ints[4];
+    }
+    // the file must end exactly after the last ray (a short trailing ray
+    // header or a point block cut by the end of the file is an error)
+    std::fseek(f, 0, SEEK_END);
+    const long end = std::ftell(f);
+    std::fclose(f);
+    if (24 + 40LL * rays + 56LL * pts != end) return ferr(HADROS_E_IO, "Unexpected end of file while reading points");
+    if (nx) *nx = hdr[2];
+    if (ny) *ny = hdr[3];
+    if (a) *a = spin;
+    if (n_rays) *n_rays = rays;
+    if (n_points) *n_points = pts;
+    return HADROS_OK;
+}
+
+}  // namespace
+
+int32_t hadros_kgeo_info(const char* path, int32_t* nx, int32_t* ny, double* a_spin, int32_t* n_rays,
+                         int64_t* n_points)
+{
+    return kgeo_walk(path, nx, ny, a_spin, n_rays, n_points, nullptr, nullptr, nullptr, nullptr, nullptr,
+                     nullptr);
+}
+
+int32_t hadros_read_kgeo(const char* path, int32_t* pixel_ids, int8_t* captured, int32_t* npoints,
+                         double* alpha, double* beta, double* points)
+{
+    if (!pixel_ids || !captured || !npoints || !alpha || !beta || !points)
+        return ferr(HADROS_E_ARG, "NULL output array");
+    return kgeo_walk(path, nullptr, nullptr, nullptr, nullptr, nullptr, pixel_ids, captured, npoints, alpha,
+                     beta, points);
+}
+
 }  // extern "C"

@@ -502,6 +502,13 @@ int32_t hadros_ctx_set_attempt_budget(hadros_ctx* ctx, int64_t attempts_per_ray)
 
 namespace {
 
+// Path recording requested by hadros_trace_paths for the next run_image.
+struct PathRec {
+    double* buf;
+    int32_t cap;
+};
+thread_local PathRec g_path_rec{nullptr, 0};
+
 // Shared body of the image calls.  dev_out holds DEVICE pointers.
 int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s,
                   const int32_t* pixel_ids_host, int32_t n_pixels, const hadros_image_out& dev_out,
@@ -573,6 +580,8 @@ int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s
     A.I_E = static_cast<double*>(dev_out.I_E);
     A.counters = ctx->d_counters;
     A.fast_geodesic = p->fast_geodesic;
+    A.paths = g_path_rec.buf;
+    A.path_cap = g_path_rec.cap;
     A.attempt_budget = ctx->attempt_budget > 0 ? ctx->attempt_budget
                                                : static_cast<int64_t>(p->max_steps) * 51 + 1;
 
@@ -854,6 +863,165 @@ int32_t hadros_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams,
             if (!c.h || c.n == 0) continue;
             d2h += static_cast<int64_t>(c.n);
             cudaError_t e = cudaMemcpyAsync(c.h, c.d, c.n, cudaMemcpyDeviceToHost, ctx->stream);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "output download");
+        }
+        rc = finish_sync(ctx, true);
+        ctx->stats.d2h_bytes = d2h;
+        ctx->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return rc;
+    } catch (const std::exception& ex) {
+        return fail(HADROS_E_NOMEM, ex.what());
+    }
+}
+
+int32_t hadros_trace_paths(hadros_ctx* ctx, const hadros_params* p, const int32_t* pixel_ids, int32_t n_pixels,
+                           int32_t max_points, double* points, int32_t* npoints, int8_t* fate)
+{
+    if (!ctx) return fail(HADROS_E_STATE, "context is NULL");
+    if (!points || !npoints || max_points <= 0) return fail(HADROS_E_ARG, "points/npoints NULL or max_points <= 0");
+    int32_t rc = hadros_params_validate(p);
+    if (rc) return rc;
+    const int64_t rows = pixel_ids ? n_pixels : static_cast<int64_t>(p->nx) * p->ny;
+    if (pixel_ids && n_pixels < 0) return fail(HADROS_E_ARG, "negative pixel count");
+    const size_t path_bytes = static_cast<size_t>(rows) * static_cast<size_t>(max_points) * 7 * sizeof(double);
+    try {
+        // a path-only trace: monochromatic, no per-bin outputs
+        hadros_params q = *p;
+        q.spectral_kind = HADROS_SPECTRAL_MONOCHROMATIC;
+        if (!(q.Enu_obs_GeV > 0.0)) q.Enu_obs_GeV = 1.0e9;
+        void* d_paths = nullptr;
+        cudaError_t e = cudaSetDevice(ctx->device);
+        if (e == cudaSuccess) e = cudaMalloc(&d_paths, path_bytes > 0 ? path_bytes : 8);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "path buffer allocation");
+        auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+        const size_t o_st = 0, o_f = al(4 * rows), total = al(o_f + rows);
+        rc = grow(ctx, &ctx->d_out, &ctx->out_cap, total, "output buffers");
+        if (rc) { cudaFree(d_paths); return rc; }
+        unsigned char* base = static_cast<unsigned char*>(ctx->d_out);
+        hadros_image_out d{};
+        d.steps = reinterpret_cast<int32_t*>(base + o_st);
+        d.fate = reinterpret_cast<int8_t*>(base + o_f);
+        // the geometry does not depend on sigma: a fixed two-row table
+        static hadros_sigma* dummy = [] {
+            hadros_sigma* t = new hadros_sigma();
+            t->serial = g_sigma_serial.fetch_add(1);
+            t->h.E = {1.0, 1.0e30};
+            t->h.s_GeV2 = {1.0, 1.0};
+            t->h.s_cm2 = {1.0e-40, 1.0e-40};
+            prepare_sigma(t->h);
+            return t;
+        }();
+        g_path_rec = {static_cast<double*>(d_paths), max_points};
+        rc = run_image(ctx, &q, dummy, pixel_ids, n_pixels, d, ctx->stream, true);
+        g_path_rec = {nullptr, 0};
+        if (!rc) {
+            e = cudaMemcpyAsync(npoints, d.steps, 4 * rows, cudaMemcpyDeviceToHost, ctx->stream);
+            if (e == cudaSuccess && fate) e = cudaMemcpyAsync(fate, d.fate, rows, cudaMemcpyDeviceToHost, ctx->stream);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(points, d_paths, path_bytes, cudaMemcpyDeviceToHost, ctx->stream);
+            if (e != cudaSuccess) rc = cuda_fail(ctx, e, "path download");
+            else rc = finish_sync(ctx, true);
+        }
+        cudaFree(d_paths);
+        return rc;
+    } catch (const std::exception& ex) {
+        g_path_rec = {nullptr, 0};
+        return fail(HADROS_E_NOMEM, ex.what());
+    }
+}
+
+int32_t hadros_transfer_paths(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s, int32_t n_rays,
+                              const int32_t* npoints, const int8_t* fate, const double* points,
+                              const hadros_image_out* out)
+{
+    if (!ctx) return fail(HADROS_E_STATE, "context is NULL");
+    if (ctx->failed) return fail(HADROS_E_STATE, "context is in a failed state: " + ctx->err);
+    if (!s) return fail(HADROS_E_STATE, "sigma handle is NULL");
+    if (!out || !npoints || (!points && n_rays > 0) || n_rays < 0) return fail(HADROS_E_ARG, "NULL argument");
+    int32_t rc = hadros_params_validate(p);
+    if (rc) return rc;
+    const auto t0 = std::chrono::steady_clock::now();
+    try {
+        std::vector<int64_t> offs(static_cast<size_t>(n_rays) + 1, 0);
+        for (int32_t k = 0; k < n_rays; ++k) {
+            if (npoints[k] < 0) return fail(HADROS_E_ARG, "Invalid ray with negative number of points");
+            offs[k + 1] = offs[k] + npoints[k];
+        }
+        const int64_t n_pts = offs.back();
+        DevCam cam;
+        std::vector<DevBin> bins;
+        std::string err;
+        rc = build_cam(*p, s->h, cam, bins, err);
+        if (rc) return fail(rc, err);
+        cam.item_begin = 0;
+        cam.item_end = n_rays;
+        cam.out_offset = 0;
+        cam.binout_offset = 0;
+        const int64_t B = cam.n_bins;
+        const size_t fsz = p->precision == HADROS_PRECISION_MIXED ? 4 : 8;
+        auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+        const int64_t P = n_rays;
+        size_t o = 0;
+        const size_t o_pts = o; o = al(o + 56 * static_cast<size_t>(n_pts));
+        const size_t o_off = o; o = al(o + 8 * offs.size());
+        const size_t o_fin = o; o = al(o + P);
+        const size_t o_tau = o; o = al(o + (out->tau ? 8 * P : 0));
+        const size_t o_P = o; o = al(o + (out->P_surv ? 8 * P : 0));
+        const size_t o_I = o; o = al(o + (out->I_obs ? 8 * P : 0));
+        const size_t o_st = o; o = al(o + (out->steps ? 4 * P : 0));
+        const size_t o_f = o; o = al(o + (out->fate ? P : 0));
+        const size_t o_tE = o; o = al(o + (out->tau_E ? fsz * P * B : 0));
+        const size_t o_IE = o; o = al(o + (out->I_E ? 8 * P * B : 0));
+        if ((rc = grow(ctx, &ctx->d_out, &ctx->out_cap, o, "path buffers"))) return rc;
+        if ((rc = upload_sigma(ctx, s, sigma_serial(s)))) return rc;
+        if ((rc = grow(ctx, &ctx->d_cams, &ctx->cams_cap, sizeof(DevCam), "camera table"))) return rc;
+        if ((rc = grow(ctx, &ctx->d_bins, &ctx->bins_cap, sizeof(DevBin) * bins.size(), "bin table"))) return rc;
+        unsigned char* base = static_cast<unsigned char*>(ctx->d_out);
+        cudaStream_t st = ctx->stream;
+        cudaError_t e = cudaSetDevice(ctx->device);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->d_cams, &cam, sizeof(DevCam), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->d_bins, bins.data(), sizeof(DevBin) * bins.size(), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess && n_pts > 0) e = cudaMemcpyAsync(base + o_pts, points, 56 * static_cast<size_t>(n_pts), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(base + o_off, offs.data(), 8 * offs.size(), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess && fate) e = cudaMemcpyAsync(base + o_fin, fate, P, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "path upload");
+        TraceArgs A{};
+        A.cams = static_cast<const DevCam*>(ctx->d_cams);
+        A.n_cams = 1;
+        A.max_bins = cam.n_bins;
+        A.total_items = P;
+        A.bins = static_cast<const DevBin*>(ctx->d_bins);
+        A.sig = ctx->sig_dev;
+        A.tau = out->tau ? reinterpret_cast<double*>(base + o_tau) : nullptr;
+        A.P_surv = out->P_surv ? reinterpret_cast<double*>(base + o_P) : nullptr;
+        A.I_obs = out->I_obs ? reinterpret_cast<double*>(base + o_I) : nullptr;
+        A.steps = out->steps ? reinterpret_cast<int32_t*>(base + o_st) : nullptr;
+        A.fate = out->fate ? reinterpret_cast<int8_t*>(base + o_f) : nullptr;
+        A.tau_E = out->tau_E ? static_cast<void*>(base + o_tE) : nullptr;
+        A.I_E = out->I_E ? reinterpret_cast<double*>(base + o_IE) : nullptr;
+        A.counters = ctx->d_counters;
+        A.path_offsets = reinterpret_cast<const int64_t*>(base + o_off);
+        A.path_points = reinterpret_cast<const double*>(base + o_pts);
+        A.path_fates = fate ? reinterpret_cast<const int8_t*>(base + o_fin) : nullptr;
+        if (P > 0) {
+            cudaEventRecord(ctx->ev0, st);
+            rc = launch_path_transfer(A, p->precision, ctx->n_sm, st, err);
+            if (rc) { ctx->err = err; return fail(rc, err); }
+            cudaEventRecord(ctx->ev1, st);
+        }
+        ctx->stats.rays = P;
+        ctx->stats.launches = P > 0 ? 1 : 0;
+        ctx->stats.h2d_bytes = static_cast<int64_t>(56 * n_pts + 8 * offs.size() + (fate ? P : 0));
+        struct Cp { void* h; const void* d; size_t n; } cps[7] = {
+            {out->tau, A.tau, 8 * size_t(P)}, {out->P_surv, A.P_surv, 8 * size_t(P)},
+            {out->I_obs, A.I_obs, 8 * size_t(P)}, {out->steps, A.steps, 4 * size_t(P)},
+            {out->fate, A.fate, size_t(P)}, {out->tau_E, A.tau_E, fsz * size_t(P * B)},
+            {out->I_E, A.I_E, 8 * size_t(P * B)}};
+        int64_t d2h = 0;
+        for (auto& c : cps) {
+            if (!c.h || c.n == 0) continue;
+            d2h += static_cast<int64_t>(c.n);
+            e = cudaMemcpyAsync(c.h, c.d, c.n, cudaMemcpyDeviceToHost, st);
             if (e != cudaSuccess) return cuda_fail(ctx, e, "output download");
         }
         rc = finish_sync(ctx, true);

@@ -89,6 +89,13 @@ struct TraceArgs {
     unsigned long long* counters;   // [0] work cursor, [1] steps, [2] attempts, [3] aborted
     int64_t attempt_budget;
     int32_t fast_geodesic;          // 1: geo_rhs_fast (hadros_trace_fast.cu)
+    // path recording (trace kernel): [rows][path_cap][7] PathPoint doubles
+    double* paths;
+    int32_t path_cap;
+    // cached paths (path transfer kernel): points [n][7], ray offsets [rays+1]
+    const int64_t* path_offsets;
+    const double* path_points;
+    const int8_t* path_fates;
 };
 
 // Host-side handle of an uploaded sigma table.
@@ -109,6 +116,8 @@ int launch_trace(const TraceArgs& args, int precision, int n_sm, void* stream,
                  std::string& err);
 int launch_trace_fast(const TraceArgs& args, int precision, int n_sm, void* stream,
                       std::string& err);
+int launch_path_transfer(const TraceArgs& args, int precision, int n_sm, void* stream,
+                         std::string& err);
 size_t trace_smem_bytes(int precision, int sig_n, int max_bins);
 
 // Record the calling thread's hadros_last_error() message; returns `code`.

@@ -259,4 +259,36 @@ int launch_trace(const TraceArgs& args, int precision, int n_sm, void* stream, s
     return launch_variant<0>(args, precision, n_sm, st, err);
 }
 
+namespace {
+
+int launch_paths(const TraceArgs& args, int precision, int n_sm, cudaStream_t st, std::string& err)
+{
+    const size_t smem = smem_layout(precision, args.sig.n, args.max_bins).total;
+    auto kern = (precision == HADROS_PRECISION_MIXED) ? path_transfer_kernel<1> : path_transfer_kernel<0>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTPB, smem);
+    if (e != cudaSuccess || per_sm < 1) {
+        err = std::string("path transfer kernel setup: ") + cudaGetErrorString(e);
+        return HADROS_E_CUDA;
+    }
+    long long grid = static_cast<long long>(n_sm) * per_sm;
+    const long long needed = (args.total_items + kTPB - 1) / kTPB;
+    if (grid > needed) grid = needed > 0 ? needed : 1;
+    kern<<<static_cast<unsigned>(grid), kTPB, smem, st>>>(args);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        err = std::string("path transfer kernel launch: ") + cudaGetErrorString(e);
+        return HADROS_E_CUDA;
+    }
+    return HADROS_OK;
+}
+
+}  // namespace
+
+int launch_path_transfer(const TraceArgs& args, int precision, int n_sm, void* stream, std::string& err)
+{
+    return launch_paths(args, precision, n_sm, static_cast<cudaStream_t>(stream), err);
+}
+
 }  // namespace hadros

@@ -258,6 +258,198 @@ __host__ __device__ inline SmemLayout smem_layout(int precision, int n, int max_
     return L;
 }
 
+// Shared-memory sigma tables of the block.
+struct SmemTables {
+    const double* E;
+    const double* S;
+    const double* lnE;
+    const double* lnS;
+    const float* lx;
+    const float4* seg;
+    int n;
+    double Emin, Emax, scale;
+};
+
+// This thread's column of per-bin accumulators (stride kTPB).
+struct BinAcc {
+    double* T64;
+    double* I64;
+    float* T;
+    float* Tc;
+    float* I;
+    float* Ic;
+    float* S;
+};
+
+// One path point (r, theta, dl, redshift) into every bin: the body of
+// integrate_kerr_ray's point loop (radiative_transfer.cpp:501-672, UHE terms)
+// for all bins at once.  Used by the fused trace kernel and by the kernel
+// over cached paths.
+template <int MIXED>
+__device__ __forceinline__ void transfer_point(const DevCam* cam, const DevBin* bins, int B,
+                                               const SmemTables& tb, const BinAcc& acc, double r,
+                                               double th, double dl, double z)
+{
+    if (r < cam->rt_skip) return;   // radiative_transfer.cpp:501-505
+    const double g = 1.0 / smax(z, 1.0e-300);
+    const double gg = smax(g, 1.0e-300);
+    const double dl_cm = dl * cam->rg_cm;
+    const double rho = torus_rho(cam->torus, r, th);
+    const double C = emissivity_factor(cam->src, cam->torus, r, th, rho);
+    const double g3 = pow(g, 3.0);
+    if (MIXED) {
+        // FP32 transfer.  Each bin's intensity is kept as a Kahan sum
+        // I_s scaled by exp(S): every contribution K w(E_loc)/w(E_mid)
+        // exp(-tau) enters as exp(e) with e = ln(...) - tau + S, and S is
+        // re-anchored when the sum is empty or a term would exceed e^40,
+        // so intensities behind optically thick gas (exp(-tau) far below
+        // FP32's range) keep their relative precision.
+        const double zp = 1.0 / gg;   // E_local / E_mid
+        const float lnzp = static_cast<float>(log(zp));
+        const float zm1 = static_cast<float>(zp - 1.0);
+        const double Kd = g3 * C * dl_cm;
+        const bool emit = Kd > 0.0;
+        const float lnK = emit ? static_cast<float>(log(Kd)) : 0.0f;
+        const bool have_tau = !(rho <= 0.0);
+        const float nbdl = static_cast<float>((rho / kMuG) * dl_cm * tb.scale);
+        for (int b = 0; b < B; ++b) {
+            const DevBin& bn = bins[b];
+            float T = acc.T[b * kTPB], Tc = acc.Tc[b * kTPB];
+            if (emit && bn.E_mid > 0.0) {
+                float I = acc.I[b * kTPB], Ic = acc.Ic[b * kTPB], S = acc.S[b * kTPB];
+                const float arg = lnK - bn.gamma * lnzp - bn.kcut * zm1;
+                // ln of this contribution; below -800 it is under FP64's
+                // range (the reference adds an exact or subnormal zero)
+                const double x = static_cast<double>(arg) -
+                                 (static_cast<double>(T) - static_cast<double>(Tc));
+                if (x >= -800.0) {
+                    double e = x + static_cast<double>(S);
+                    if (I == 0.0f || e > 40.0) {
+                        const float shrink = (I == 0.0f) ? 0.0f : __expf(static_cast<float>(-e));
+                        I *= shrink;
+                        Ic *= shrink;
+                        S = static_cast<float>(-x);   // |S| < ~900: exact to 1e-4
+                        e = x + static_cast<double>(S);
+                    }
+                    kahan_add(I, Ic, __expf(static_cast<float>(e)));
+                    acc.I[b * kTPB] = I; acc.Ic[b * kTPB] = Ic; acc.S[b * kTPB] = S;
+                }
+            }
+            if (have_tau && gg >= bn.gg_lo && gg <= bn.gg_hi) {
+                const float lnE = bn.lnE + lnzp;
+                int lo = 0, cnt = tb.n;   // lower_bound over lx
+                while (cnt > 0) {
+                    const int st = cnt >> 1;
+                    if (tb.lx[lo + st] < lnE) { lo += st + 1; cnt -= st + 1; }
+                    else cnt = st;
+                }
+                const int k = lo < 1 ? 1 : (lo > tb.n - 1 ? tb.n - 1 : lo);
+                const float4 sg = tb.seg[k];
+                const float t = (lnE - sg.x) * sg.y;
+                kahan_add(T, Tc, nbdl * (sg.z * __expf(t * sg.w)));
+                acc.T[b * kTPB] = T; acc.Tc[b * kTPB] = Tc;
+            }
+        }
+    } else {
+        for (int b = 0; b < B; ++b) {
+            const double E_loc = bins[b].E_mid / gg;
+            double jj = 0.0;
+            if (!(E_loc <= 0.0)) jj = C * spectral_weight(cam->src, E_loc);
+            double T = acc.T64[b * kTPB];
+            acc.I64[b * kTPB] += g3 * jj * exp(-T) * dl_cm;
+            if (rho <= 0.0 || E_loc < tb.Emin || E_loc > tb.Emax) continue;
+            // SigmaTable::log_interp (sigma_table.cpp:81-124)
+            int lo = 0, cnt = tb.n;
+            while (cnt > 0) {
+                const int st = cnt >> 1;
+                if (tb.E[lo + st] < E_loc) { lo += st + 1; cnt -= st + 1; }
+                else cnt = st;
+            }
+            double sigma_cm2;
+            if (lo == 0) sigma_cm2 = tb.S[0];
+            else if (lo == tb.n) sigma_cm2 = tb.S[tb.n - 1];
+            else {
+                const double lx = log(E_loc);
+                const double lx1 = tb.lnE[lo - 1], lx2 = tb.lnE[lo];
+                const double ly1 = tb.lnS[lo - 1], ly2 = tb.lnS[lo];
+                const double t = (lx - lx1) / (lx2 - lx1);
+                sigma_cm2 = exp(ly1 + t * (ly2 - ly1));
+            }
+            const double nb = rho / kMuG;
+            T += nb * sigma_cm2 * dl_cm;
+            acc.T64[b * kTPB] = T;
+        }
+    }
+}
+
+// A finished pixel: per-bin outputs, the spectral aggregates of
+// integrate_kerr_ray_spectral (radiative_transfer.cpp:730-769; monochromatic:
+// the single bin), defaults for an empty ray, fate, steps and attempts.
+template <int MIXED>
+__device__ __forceinline__ void finish_pixel(const TraceArgs& A, const DevCam* cam, const DevBin* bins,
+                                             int B, const BinAcc& acc, long long local, int step,
+                                             int fate, long long att_total)
+{
+    const long long orow = cam->out_offset + local;
+    double t_out = 0.0, p_out = 1.0, i_out = 0.0;
+    double wsum = 0.0, tsum = 0.0, psum = 0.0, isum = 0.0;
+    for (int b = 0; b < B; ++b) {
+        double tb, ib;
+        if (MIXED) {
+            tb = static_cast<double>(acc.T[b * kTPB]);
+            // I = (I_s - c) * exp(-S) * w(E_mid)
+            ib = (static_cast<double>(acc.I[b * kTPB]) - static_cast<double>(acc.Ic[b * kTPB])) *
+                 exp(-static_cast<double>(acc.S[b * kTPB])) * bins[b].w0;
+        } else {
+            tb = acc.T64[b * kTPB];
+            ib = acc.I64[b * kTPB];
+        }
+        const long long e = cam->binout_offset + local * B + b;
+        if (MIXED) {
+            if (A.tau_E) static_cast<float*>(A.tau_E)[e] = static_cast<float>(tb);
+        } else {
+            if (A.tau_E) static_cast<double*>(A.tau_E)[e] = tb;
+        }
+        if (A.I_E) A.I_E[e] = ib;
+        if (cam->mono) {
+            t_out = tb; p_out = exp(-tb); i_out = ib;
+        } else if (bins[b].valid) {   // radiative_transfer.cpp:752-769
+            const double w = bins[b].w;
+            wsum += w;
+            tsum += w * tb;
+            psum += w * exp(-tb);
+            isum += ib * bins[b].dE;
+        }
+    }
+    if (!cam->mono && wsum > 0.0) {
+        t_out = tsum / wsum;
+        p_out = psum / wsum;
+        i_out = isum;
+    }
+    if (step == 0) { t_out = 0.0; p_out = 1.0; i_out = 0.0; }
+    if (A.tau) A.tau[orow] = t_out;
+    if (A.P_surv) A.P_surv[orow] = p_out;
+    if (A.I_obs) A.I_obs[orow] = i_out;
+    if (A.fate) A.fate[orow] = static_cast<int8_t>(fate);
+    if (A.steps) A.steps[orow] = step;
+    if (A.attempts) A.attempts[orow] = static_cast<int32_t>(att_total > 2147483647LL ? 2147483647LL : att_total);
+}
+
+// Zero this thread's per-bin accumulators.
+template <int MIXED>
+__device__ __forceinline__ void reset_bins(const BinAcc& acc, int B)
+{
+    for (int b = 0; b < B; ++b) {
+        if (MIXED) {
+            acc.T[b * kTPB] = 0.0f; acc.Tc[b * kTPB] = 0.0f;
+            acc.I[b * kTPB] = 0.0f; acc.Ic[b * kTPB] = 0.0f;
+            acc.S[b * kTPB] = 0.0f;
+        } else {
+            acc.T64[b * kTPB] = 0.0; acc.I64[b * kTPB] = 0.0;
+        }
+    }
+}
+
 enum Phase : int { kNeedRay = 0, kStepStart = 1, kAttempt = 2, kDone = 3 };
 
 template <int MIXED, int FAST>
@@ -293,6 +485,8 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
     float* accI = accTc + size_t(kTPB) * A.max_bins;
     float* accIc = accI + size_t(kTPB) * A.max_bins;
     float* accS = accIc + size_t(kTPB) * A.max_bins;
+    const SmemTables tb{sE, sS, slnE, slnS, slx, sseg, n_sig, sigEmin, sigEmax, sig_scale};
+    const BinAcc acc{accT64, accI64, accT, accTc, accI, accIc, accS};
 
     int phase = kNeedRay;
     // ray state
@@ -357,15 +551,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                 E_obs = -(pt + cam->omega_obs * pph) / cam->alpha_obs;
                 step = 0;
                 att_total = 0;
-                for (int b = 0; b < B; ++b) {
-                    if (MIXED) {
-                        accT[b * kTPB] = 0.0f; accTc[b * kTPB] = 0.0f;
-                        accI[b * kTPB] = 0.0f; accIc[b * kTPB] = 0.0f;
-                        accS[b * kTPB] = 0.0f;
-                    } else {
-                        accT64[b * kTPB] = 0.0; accI64[b * kTPB] = 0.0;
-                    }
-                }
+                reset_bins<MIXED>(acc, B);
                 phase = kStepStart;
             }
 
@@ -380,50 +566,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                 stop = true;
             }
             if (stop) {
-                // ---- finish the pixel: aggregates and stores --------------
-                const long long orow = cam->out_offset + local;
-                double t_out = 0.0, p_out = 1.0, i_out = 0.0;
-                double wsum = 0.0, tsum = 0.0, psum = 0.0, isum = 0.0;
-                for (int b = 0; b < B; ++b) {
-                    double tb, ib;
-                    if (MIXED) {
-                        tb = static_cast<double>(accT[b * kTPB]);
-                        // I = (I_s - c) * exp(-S) * w(E_mid)
-                        ib = (static_cast<double>(accI[b * kTPB]) - static_cast<double>(accIc[b * kTPB])) *
-                             exp(-static_cast<double>(accS[b * kTPB])) * bins[b].w0;
-                    } else {
-                        tb = accT64[b * kTPB];
-                        ib = accI64[b * kTPB];
-                    }
-                    const long long e = cam->binout_offset + local * B + b;
-                    if (MIXED) {
-                        if (A.tau_E) static_cast<float*>(A.tau_E)[e] = static_cast<float>(tb);
-                    } else {
-                        if (A.tau_E) static_cast<double*>(A.tau_E)[e] = tb;
-                    }
-                    if (A.I_E) A.I_E[e] = ib;
-                    if (cam->mono) {
-                        t_out = tb; p_out = exp(-tb); i_out = ib;
-                    } else if (bins[b].valid) {   // radiative_transfer.cpp:752-769
-                        const double w = bins[b].w;
-                        wsum += w;
-                        tsum += w * tb;
-                        psum += w * exp(-tb);
-                        isum += ib * bins[b].dE;
-                    }
-                }
-                if (!cam->mono && wsum > 0.0) {
-                    t_out = tsum / wsum;
-                    p_out = psum / wsum;
-                    i_out = isum;
-                }
-                if (step == 0) { t_out = 0.0; p_out = 1.0; i_out = 0.0; }
-                if (A.tau) A.tau[orow] = t_out;
-                if (A.P_surv) A.P_surv[orow] = p_out;
-                if (A.I_obs) A.I_obs[orow] = i_out;
-                if (A.fate) A.fate[orow] = static_cast<int8_t>(fate);
-                if (A.steps) A.steps[orow] = step;
-                if (A.attempts) A.attempts[orow] = static_cast<int32_t>(att_total > 2147483647LL ? 2147483647LL : att_total);
+                finish_pixel<MIXED>(A, cam, bins, B, acc, local, step, fate, att_total);
                 atomicAdd(&A.counters[1], static_cast<unsigned long long>(step));
                 atomicAdd(&A.counters[2], static_cast<unsigned long long>(att_total));
                 phase = kNeedRay;
@@ -450,99 +593,21 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
             const double alpha = bl_lapse(a, r, s, c);
             const double omega = bl_omega(a, r, s);
             const double z = (-(pt + omega * pph) / alpha) / smax(E_obs, 1.0e-300);
+            if (A.paths && step < A.path_cap) {   // PathPoint record (kerr_camera.cpp:235-273)
+                double sph, cph;
+                sincos(ph, &sph, &cph);
+                double* q = A.paths + ((cam->out_offset + local) * static_cast<long long>(A.path_cap) + step) * 7;
+                q[0] = r;
+                q[1] = th;
+                q[2] = r * s * cph;
+                q[3] = r * s * sph;
+                q[4] = r * c;
+                q[5] = dl;
+                q[6] = z;
+            }
 
             // ---- transfer of this point into every bin ------------------
-            if (!(r < cam->rt_skip)) {   // radiative_transfer.cpp:501-505
-                const double g = 1.0 / smax(z, 1.0e-300);
-                const double gg = smax(g, 1.0e-300);
-                const double dl_cm = dl * cam->rg_cm;
-                const double rho = torus_rho(cam->torus, r, th);
-                const double C = emissivity_factor(cam->src, cam->torus, r, th, rho);
-                const double g3 = pow(g, 3.0);
-                if (MIXED) {
-                    // FP32 transfer.  Each bin's intensity is kept as a Kahan sum
-                    // I_s scaled by exp(S): every contribution K w(E_loc)/w(E_mid)
-                    // exp(-tau) enters as exp(e) with e = ln(...) - tau + S, and S is
-                    // re-anchored when the sum is empty or a term would exceed e^40,
-                    // so intensities behind optically thick gas (exp(-tau) far below
-                    // FP32's range) keep their relative precision.
-                    const double zp = 1.0 / gg;   // E_local / E_mid
-                    const float lnzp = static_cast<float>(log(zp));
-                    const float zm1 = static_cast<float>(zp - 1.0);
-                    const double Kd = g3 * C * dl_cm;
-                    const bool emit = Kd > 0.0;
-                    const float lnK = emit ? static_cast<float>(log(Kd)) : 0.0f;
-                    const bool have_tau = !(rho <= 0.0);
-                    const float nbdl = static_cast<float>((rho / kMuG) * dl_cm * sig_scale);
-                    for (int b = 0; b < B; ++b) {
-                        const DevBin& bn = bins[b];
-                        float T = accT[b * kTPB], Tc = accTc[b * kTPB];
-                        if (emit && bn.E_mid > 0.0) {
-                            float I = accI[b * kTPB], Ic = accIc[b * kTPB], S = accS[b * kTPB];
-                            const float arg = lnK - bn.gamma * lnzp - bn.kcut * zm1;
-                            // ln of this contribution; below -800 it is under FP64's
-                            // range (the reference adds an exact or subnormal zero)
-                            const double x = static_cast<double>(arg) -
-                                             (static_cast<double>(T) - static_cast<double>(Tc));
-                            if (x >= -800.0) {
-                                double e = x + static_cast<double>(S);
-                                if (I == 0.0f || e > 40.0) {
-                                    const float shrink = (I == 0.0f) ? 0.0f : __expf(static_cast<float>(-e));
-                                    I *= shrink;
-                                    Ic *= shrink;
-                                    S = static_cast<float>(-x);   // |S| < ~900: exact to 1e-4
-                                    e = x + static_cast<double>(S);
-                                }
-                                kahan_add(I, Ic, __expf(static_cast<float>(e)));
-                                accI[b * kTPB] = I; accIc[b * kTPB] = Ic; accS[b * kTPB] = S;
-                            }
-                        }
-                        if (have_tau && gg >= bn.gg_lo && gg <= bn.gg_hi) {
-                            const float lnE = bn.lnE + lnzp;
-                            int lo = 0, cnt = n_sig;   // lower_bound over lx
-                            while (cnt > 0) {
-                                const int st = cnt >> 1;
-                                if (slx[lo + st] < lnE) { lo += st + 1; cnt -= st + 1; }
-                                else cnt = st;
-                            }
-                            const int k = lo < 1 ? 1 : (lo > n_sig - 1 ? n_sig - 1 : lo);
-                            const float4 sg = sseg[k];
-                            const float t = (lnE - sg.x) * sg.y;
-                            kahan_add(T, Tc, nbdl * (sg.z * __expf(t * sg.w)));
-                            accT[b * kTPB] = T; accTc[b * kTPB] = Tc;
-                        }
-                    }
-                } else {
-                    for (int b = 0; b < B; ++b) {
-                        const double E_loc = bins[b].E_mid / gg;
-                        double jj = 0.0;
-                        if (!(E_loc <= 0.0)) jj = C * spectral_weight(cam->src, E_loc);
-                        double T = accT64[b * kTPB];
-                        accI64[b * kTPB] += g3 * jj * exp(-T) * dl_cm;
-                        if (rho <= 0.0 || E_loc < sigEmin || E_loc > sigEmax) continue;
-                        // SigmaTable::log_interp (sigma_table.cpp:81-124)
-                        int lo = 0, cnt = n_sig;
-                        while (cnt > 0) {
-                            const int st = cnt >> 1;
-                            if (sE[lo + st] < E_loc) { lo += st + 1; cnt -= st + 1; }
-                            else cnt = st;
-                        }
-                        double sigma_cm2;
-                        if (lo == 0) sigma_cm2 = sS[0];
-                        else if (lo == n_sig) sigma_cm2 = sS[n_sig - 1];
-                        else {
-                            const double lx = log(E_loc);
-                            const double lx1 = slnE[lo - 1], lx2 = slnE[lo];
-                            const double ly1 = slnS[lo - 1], ly2 = slnS[lo];
-                            const double t = (lx - lx1) / (lx2 - lx1);
-                            sigma_cm2 = exp(ly1 + t * (ly2 - ly1));
-                        }
-                        const double nb = rho / kMuG;
-                        T += nb * sigma_cm2 * dl_cm;
-                        accT64[b * kTPB] = T;
-                    }
-                }
-            }
+            transfer_point<MIXED>(cam, bins, B, tb, acc, r, th, dl, z);
 
             // ---- k1 of the coming step_adaptive (shares sin/cos) ------------
             if (FAST) geo_rhs_fast(a, r, th, s, c, pr, pth, pt, pph, k1);
@@ -644,6 +709,57 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
     }
 }
 
+
+// Transfer over cached paths (compute_kerr_image_from_cache,
+// apps/compute_kerr_image_from_cache.cpp:599-711): one thread per ray walks
+// its recorded points (r, theta, x, y, z, dl, redshift) through the same
+// transfer_point as the fused kernel.  Grid-stride over rays.
+template <int MIXED>
+__global__ void __launch_bounds__(kTPB) path_transfer_kernel(const TraceArgs A)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int n_sig = A.sig.n;
+    const SmemLayout L = smem_layout(MIXED ? 1 : 0, n_sig, A.max_bins);
+    double* sE = reinterpret_cast<double*>(smem + L.off_E);
+    double* sS = reinterpret_cast<double*>(smem + L.off_S);
+    double* slnE = reinterpret_cast<double*>(smem + L.off_lnE);
+    double* slnS = reinterpret_cast<double*>(smem + L.off_lnS);
+    float* slx = reinterpret_cast<float*>(smem + L.off_lx);
+    float4* sseg = reinterpret_cast<float4*>(smem + L.off_seg);
+    for (int k = threadIdx.x; k < n_sig; k += blockDim.x) {
+        sE[k] = A.sig.E[k];
+        sS[k] = A.sig.S[k];
+        slnE[k] = A.sig.lnE[k];
+        slnS[k] = A.sig.lnS[k];
+        slx[k] = A.sig.lx[k];
+        sseg[k] = reinterpret_cast<const float4*>(A.sig.seg)[k];
+    }
+    __syncthreads();
+    const int tid = threadIdx.x;
+    double* accT64 = reinterpret_cast<double*>(smem + L.off_acc) + tid;
+    double* accI64 = accT64 + size_t(kTPB) * A.max_bins;
+    float* accT = reinterpret_cast<float*>(smem + L.off_acc) + tid;
+    float* accTc = accT + size_t(kTPB) * A.max_bins;
+    float* accI = accTc + size_t(kTPB) * A.max_bins;
+    float* accIc = accI + size_t(kTPB) * A.max_bins;
+    float* accS = accIc + size_t(kTPB) * A.max_bins;
+    const SmemTables tb{sE, sS, slnE, slnS, slx, sseg, n_sig, A.sig.E_min, A.sig.E_max, A.sig.sigma_scale};
+    const BinAcc acc{accT64, accI64, accT, accTc, accI, accIc, accS};
+    const DevCam* cam = A.cams;
+    const DevBin* bins = A.bins + cam->bin_offset;
+    const int B = cam->n_bins;
+    for (long long ray = static_cast<long long>(blockIdx.x) * kTPB + tid; ray < A.total_items;
+         ray += static_cast<long long>(gridDim.x) * kTPB) {
+        reset_bins<MIXED>(acc, B);
+        const long long k0 = A.path_offsets[ray], k1 = A.path_offsets[ray + 1];
+        for (long long kk = k0; kk < k1; ++kk) {
+            const double* q = A.path_points + kk * 7;
+            transfer_point<MIXED>(cam, bins, B, tb, acc, q[0], q[1], q[5], q[6]);
+        }
+        const int fate = A.path_fates ? A.path_fates[ray] : HADROS_FATE_ESCAPED;
+        finish_pixel<MIXED>(A, cam, bins, B, acc, ray, static_cast<int>(k1 - k0), fate, 0);
+    }
+}
 
 // Occupancy-sized persistent launch of one kernel variant.
 template <int FAST>

@@ -298,6 +298,30 @@ int32_t hadros_batch_device(hadros_ctx* ctx, const hadros_params* cams, int32_t 
                             const hadros_sigma* s, const hadros_image_out* dev_out,
                             void* stream);
 
+/* ---- geodesic cache (compute_kerr_geodesics / --image-from-cache) ---------- */
+
+/* Trace pixels (all: pixel_ids NULL; or a list) and record every path point
+ * as compute_kerr_geodesics stores it: (r, theta, x, y, z, dl_rg, redshift),
+ * KerrCamera::trace_pixel's PathPoint (src/kerr_camera.cpp:235-273).
+ * points: host buffer of rows x max_points x 7 doubles; npoints[k] = the
+ * ray's accepted steps (a value above max_points means the stored path was
+ * cut at max_points); fate may be NULL.  Replaces
+ * apps/compute_kerr_geodesics.cpp:95-138 and the CUDA --geodesic-cache mode
+ * (apps/compute_kerr_image_cuda.cu:1624-1826). */
+int32_t hadros_trace_paths(hadros_ctx* ctx, const hadros_params* p, const int32_t* pixel_ids,
+                           int32_t n_pixels, int32_t max_points, double* points,
+                           int32_t* npoints, int8_t* fate);
+/* Radiative transfer over cached paths: n_rays rays with npoints[k] points
+ * each, packed back to back in `points` (7 doubles per point, as in KGEO);
+ * fate may be NULL (then 0).  Outputs as hadros_image, one row per ray, with
+ * steps = npoints and attempts unused.  p supplies the spin (the cache's),
+ * mass, medium, source, spectrum and precision.  Replaces
+ * apps/compute_kerr_image_from_cache.cpp:599-711 and the CUDA
+ * --image-from-cache mode (apps/compute_kerr_image_cuda.cu:1828-2220). */
+int32_t hadros_transfer_paths(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s,
+                              int32_t n_rays, const int32_t* npoints, const int8_t* fate,
+                              const double* points, const hadros_image_out* out);
+
 /* Wait for the context's work and report the first deferred error. */
 int32_t hadros_ctx_synchronize(hadros_ctx* ctx);
 
@@ -339,6 +363,24 @@ int32_t hadros_write_dat(const char* path, const hadros_params* p, const char* d
 int32_t hadros_write_kimg(const char* path, const hadros_params* p, double mev_E_MeV,
                           double mev_norm, const double* tau, const double* P_surv,
                           const double* I_obs, const int8_t* fate);
+
+/* KGEO geodesic cache files (apps/compute_kerr_geodesics.cpp:14-22, :95-138):
+ * header <int32 magic 0x4B47454F, int32 version 1, int32 nx, int32 ny,
+ * double a>, then per ray a 40-byte header <int32 ray_id, pixel_i, pixel_j,
+ * captured, npoints, 4 pad bytes, double alpha, double beta> and npoints
+ * PathPoints of 7 doubles.  The writer takes the packed layout of
+ * hadros_transfer_paths (ray_id = i*ny + j, alpha/beta from the camera). */
+int32_t hadros_write_kgeo(const char* path, const hadros_params* p, int32_t n_rays,
+                          const int32_t* pixel_ids, const int8_t* fate,
+                          const int32_t* npoints, const double* points);
+/* First pass: sizes of a KGEO file (reference read loop,
+ * apps/compute_kerr_image_from_cache.cpp:374-406, :655-707). */
+int32_t hadros_kgeo_info(const char* path, int32_t* nx, int32_t* ny, double* a_spin,
+                         int32_t* n_rays, int64_t* n_points);
+/* Second pass: per ray pixel id (j*nx+i), captured flag, npoints, alpha,
+ * beta, and the packed points.  Arrays sized from hadros_kgeo_info. */
+int32_t hadros_read_kgeo(const char* path, int32_t* pixel_ids, int8_t* captured,
+                         int32_t* npoints, double* alpha, double* beta, double* points);
 
 #ifdef __cplusplus
 }

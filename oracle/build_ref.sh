@@ -1,5 +1,6 @@
 #!/usr/bin/env bash
-# Builds oracle/_ref/libhadros_ref.so: the reference's own hot-path sources,
+# Builds oracle/_ref/libhadros_ref.so (and the reference's two cache
+# executables): the reference's own hot-path sources,
 # compiled where they lie (read-only, unmodified) with the reference Makefile's
 # flags (-O3 -std=c++17 -fopenmp, no -march), plus oracle/ref_driver.cpp.
 # Test infrastructure only; outputs go to oracle/_ref/ (git-ignored).
@@ -20,4 +21,9 @@ for f in kerr_metric kerr_geodesic kerr_camera sigma_table torus_profile \
 done
 g++ -O3 -std=c++17 -fopenmp -fPIC -shared -I"$ref/include" \
     -o "$out/libhadros_ref.so" $srcs "$here/ref_driver.cpp"
-echo "built $out/libhadros_ref.so"
+# the reference's own cache writer and cache reader executables (file-format
+# compatibility tests)
+for app in compute_kerr_geodesics compute_kerr_image_from_cache; do
+    g++ -O3 -std=c++17 -fopenmp -I"$ref/include" -o "$out/$app" $srcs "$ref/apps/$app.cpp"
+done
+echo "built $out/libhadros_ref.so and reference cache executables"
