@@ -21,9 +21,9 @@ from pathlib import Path
 import numpy as np
 
 from . import abi
-from .abi import (FATE_CAPTURED, FATE_ESCAPED, FATE_TRUNCATED, PRECISION_FP64,
-                  PRECISION_MIXED, PROFILES, SOURCES, SPECTRA, HadrosImageOut,
-                  HadrosParams, HadrosStats)
+from .abi import (FATE_CAPTURED, FATE_ESCAPED, FATE_TRUNCATED, ORDER_COST, ORDER_ROWS,
+                  ORDER_TILES, PRECISION_FP64, PRECISION_MIXED, PROFILES, SOURCES, SPECTRA,
+                  HadrosImageOut, HadrosParams, HadrosSchedule, HadrosStats)
 
 __all__ = ["lib", "HadrosError", "params", "SigmaTable", "Context", "spectral_bins",
            "HadrosParams", "PRECISION_FP64", "PRECISION_MIXED", "PROFILES", "SOURCES",
@@ -337,6 +337,10 @@ class Context:
                                            pts.ctypes.data if pts.size else None, C.byref(out)))
         return res
 
+    def plan(self, cams: list, sigma: SigmaTable, schedule=None) -> "Plan":
+        """Upload a scan once (see hadros_plan_create)."""
+        return Plan(self, cams, sigma, schedule)
+
     def image_device(self, p: HadrosParams, sigma: SigmaTable, out: dict, stream=None) -> None:
         """Enqueue an image into device buffers (torch tensors or raw pointers)."""
         o = HadrosImageOut()
@@ -348,3 +352,66 @@ class Context:
 
     def synchronize(self) -> None:
         _check(lib().hadros_ctx_synchronize(self.handle))
+
+
+def schedule(**kw) -> HadrosSchedule:
+    """hadros_schedule_default() with overrides (blocks_per_sm, order, ...)."""
+    sc = HadrosSchedule()
+    lib().hadros_schedule_default(C.byref(sc))
+    for k, v in kw.items():
+        setattr(sc, k, int(v))
+    return sc
+
+
+def _ptr_stream(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+
+
+class Plan:
+    """A scan uploaded once; launch() only enqueues the kernel (capturable)."""
+
+    def __init__(self, ctx: Context, cams: list, sigma: SigmaTable, sched=None):
+        self.cams = list(cams)
+        arr = (HadrosParams * len(self.cams))(*self.cams)
+        h = C.c_void_p()
+        _check(lib().hadros_plan_create(ctx.handle, C.addressof(arr), len(self.cams), sigma.handle,
+                                        None if sched is None else C.byref(sched), C.byref(h)))
+        self._h = h
+        self.ctx = ctx
+        n, nb, g, b = C.c_int64(), C.c_int64(), C.c_int32(), C.c_int32()
+        _check(lib().hadros_plan_info(h, C.byref(n), C.byref(nb), C.byref(g), C.byref(b)))
+        self.n_pixels, self.n_pixel_bins, self.grid, self.blocks_per_sm = n.value, nb.value, g.value, b.value
+
+    def alloc(self, torch, device=None, outputs=OUTPUTS) -> dict:
+        """Device output tensors for this plan."""
+        P, PB = self.n_pixels, self.n_pixel_bins
+        f32 = self.cams[0].precision == PRECISION_MIXED
+        spec = {"tau": (P, torch.float64), "P_surv": (P, torch.float64), "I_obs": (P, torch.float64),
+                "fate": (P, torch.int8), "steps": (P, torch.int32), "attempts": (P, torch.int32),
+                "tau_E": (PB, torch.float32 if f32 else torch.float64), "I_E": (PB, torch.float64)}
+        return {k: torch.empty(spec[k][0], dtype=spec[k][1], device=device) for k in outputs}
+
+    def launch(self, out: dict, stream=None) -> None:
+        o = HadrosImageOut()
+        for k, v in out.items():
+            setattr(o, k, v if isinstance(v, int) else v.data_ptr())
+        _check(lib().hadros_plan_launch(self._h, C.byref(o), _ptr_stream(stream)))
+
+    def counters(self, stream=None) -> dict:
+        st, at, ab = C.c_int64(), C.c_int64(), C.c_int32()
+        _check(lib().hadros_plan_counters(self._h, _ptr_stream(stream), C.byref(st), C.byref(at),
+                                          C.byref(ab)))
+        return {"accepted_steps": st.value, "attempts": at.value, "aborted": ab.value}
+
+    def close(self) -> None:
+        if self._h:
+            lib().hadros_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -96,6 +96,14 @@ class HadrosImageOut(C.Structure):
     ]
 
 
+ORDER_ROWS, ORDER_TILES, ORDER_COST = 0, 1, 2
+
+
+class HadrosSchedule(C.Structure):
+    _fields_ = [("blocks_per_sm", C.c_int32), ("order", C.c_int32), ("coarse_stride", C.c_int32),
+                ("camera_order", C.c_int32)]
+
+
 class HadrosStats(C.Structure):
     _fields_ = [
         ("kernel_ms", C.c_double),
@@ -147,6 +155,15 @@ SIGNATURES = {
                                         P(HadrosImageOut), C.c_void_p]),
     "hadros_image_device_noalloc": (C.c_int32, [P(HadrosParams), C.c_void_p, P(HadrosImageOut),
                                                 C.c_void_p]),
+    "hadros_schedule_default": (None, [P(HadrosSchedule)]),
+    "hadros_plan_create": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                       P(HadrosSchedule), P(C.c_void_p)]),
+    "hadros_plan_info": (C.c_int32, [C.c_void_p, P(C.c_int64), P(C.c_int64), P(C.c_int32),
+                                     P(C.c_int32)]),
+    "hadros_plan_launch": (C.c_int32, [C.c_void_p, P(HadrosImageOut), C.c_void_p]),
+    "hadros_plan_counters": (C.c_int32, [C.c_void_p, C.c_void_p, P(C.c_int64), P(C.c_int64),
+                                         P(C.c_int32)]),
+    "hadros_plan_destroy": (None, [C.c_void_p]),
     "hadros_trace_paths": (C.c_int32, [C.c_void_p, P(HadrosParams), C.c_void_p, C.c_int32, C.c_int32,
                                        C.c_void_p, C.c_void_p, C.c_void_p]),
     "hadros_transfer_paths": (C.c_int32, [C.c_void_p, P(HadrosParams), C.c_void_p, C.c_int32,

@@ -5,6 +5,7 @@
 // returns a status code and leaves a message for hadros_last_error().
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -137,6 +138,9 @@ int32_t upload_sigma(hadros_ctx* ctx, const hadros_sigma* s, uint64_t serial)
     d.E_min = h.E.front();
     d.E_max = h.E.back();
     d.sigma_scale = h.sigma_scale;
+    d.uniform = h.uniform;
+    d.lx0 = h.lx0;
+    d.inv_dlx = h.inv_dlx;
     d.E = reinterpret_cast<const double*>(base + oE);
     d.S = reinterpret_cast<const double*>(base + oS);
     d.lnE = reinterpret_cast<const double*>(base + olnE);
@@ -1003,6 +1007,7 @@ int32_t hadros_transfer_paths(hadros_ctx* ctx, const hadros_params* p, const had
         A.path_offsets = reinterpret_cast<const int64_t*>(base + o_off);
         A.path_points = reinterpret_cast<const double*>(base + o_pts);
         A.path_fates = fate ? reinterpret_cast<const int8_t*>(base + o_fin) : nullptr;
+        A.fast_geodesic = p->fast_geodesic;
         if (P > 0) {
             cudaEventRecord(ctx->ev0, st);
             rc = launch_path_transfer(A, p->precision, ctx->n_sm, st, err);
@@ -1046,6 +1051,279 @@ int32_t hadros_ctx_synchronize(hadros_ctx* ctx)
     ctx->stats.aborted_rays = static_cast<int32_t>(c[3]);
     if (c[3] > 0) return fail(HADROS_E_TIMEOUT, std::to_string(c[3]) + " rays exceeded the attempt budget");
     return ok();
+}
+
+}  // extern "C"
+
+// ---- plans: uploaded scans, capturable launches ---------------------------
+
+struct hadros_plan {
+    int device = 0;
+    int precision = 0, fast = 0;
+    int64_t P = 0, PB = 0;
+    void* d_tabs = nullptr;          // cams | bins | order | sigma
+    unsigned long long* d_counters = nullptr;
+    TraceArgs A{};
+    LaunchCfg cfg{};
+    hadros_schedule sched{};
+};
+
+namespace {
+
+// Per-pixel cost estimate of a camera from a coarse pre-pass (accepted
+// steps on every `stride`-th pixel; nearest coarse sample elsewhere), and the
+// pixel order by descending cost (ties: pixel order).
+int32_t cost_order(hadros_ctx* ctx, const hadros_params& p, const hadros_sigma* s, int stride,
+                   std::vector<int32_t>& order, double& total_cost)
+{
+    const int nx = p.nx, ny = p.ny;
+    const int cx = (nx + stride - 1) / stride, cy = (ny + stride - 1) / stride;
+    std::vector<int32_t> ids;
+    ids.reserve(static_cast<size_t>(cx) * cy);
+    for (int j = 0; j < ny; j += stride)
+        for (int i = 0; i < nx; i += stride) ids.push_back(j * nx + i);
+    std::vector<int32_t> steps(ids.size());
+    hadros_image_out o{};
+    o.steps = steps.data();
+    hadros_params q = p;
+    q.spectral_kind = HADROS_SPECTRAL_MONOCHROMATIC;   // geometry only
+    int32_t rc = hadros_image_pixels(ctx, &q, s, ids.data(), static_cast<int32_t>(ids.size()), &o);
+    if (rc) return rc;
+    std::vector<float> cost(static_cast<size_t>(nx) * ny);
+    total_cost = 0.0;
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const int ci = std::min((i + stride / 2) / stride, cx - 1), cj = std::min((j + stride / 2) / stride, cy - 1);
+            cost[static_cast<size_t>(j) * nx + i] = static_cast<float>(steps[static_cast<size_t>(cj) * cx + ci]);
+            total_cost += steps[static_cast<size_t>(cj) * cx + ci];
+        }
+    order.resize(cost.size());
+    for (size_t k = 0; k < order.size(); ++k) order[k] = static_cast<int32_t>(k);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return cost[x] > cost[y]; });
+    return HADROS_OK;
+}
+
+// Pixel order walking 8x4 tiles, so a warp's 32 rays are a compact patch.
+void tile_order(const hadros_params& p, std::vector<int32_t>& order)
+{
+    order.clear();
+    order.reserve(static_cast<size_t>(p.nx) * p.ny);
+    for (int tj = 0; tj < p.ny; tj += 4)
+        for (int ti = 0; ti < p.nx; ti += 8)
+            for (int j = tj; j < std::min(tj + 4, p.ny); ++j)
+                for (int i = ti; i < std::min(ti + 8, p.nx); ++i) order.push_back(j * p.nx + i);
+}
+
+}  // namespace
+
+extern "C" {
+
+void hadros_schedule_default(hadros_schedule* s)
+{
+    if (!s) return;
+    s->blocks_per_sm = 0;
+    s->order = HADROS_ORDER_ROWS;
+    s->coarse_stride = 16;
+    s->camera_order = 1;
+}
+
+int32_t hadros_plan_create(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, const hadros_sigma* s,
+                           const hadros_schedule* sched, hadros_plan** out)
+{
+    if (!ctx) return fail(HADROS_E_STATE, "context is NULL");
+    if (!out || !cams || n_cams <= 0 || !s) return fail(HADROS_E_ARG, "NULL argument or empty camera list");
+    *out = nullptr;
+    hadros_schedule sc;
+    hadros_schedule_default(&sc);
+    if (sched) sc = *sched;
+    if (sc.order < 0 || sc.order > 2 || sc.blocks_per_sm < 0 || sc.coarse_stride <= 0)
+        return fail(HADROS_E_ARG, "bad schedule");
+    try {
+        for (int32_t c = 0; c < n_cams; ++c) {
+            int32_t rc = hadros_params_validate(&cams[c]);
+            if (rc) return fail(rc, "camera " + std::to_string(c) + ": " + g_last_error);
+            if (cams[c].precision != cams[0].precision || cams[c].fast_geodesic != cams[0].fast_geodesic)
+                return fail(HADROS_E_ARG, "all cameras of a batch need the same precision and fast_geodesic");
+        }
+        // per-camera pixel orders and costs
+        std::vector<std::vector<int32_t>> orders(static_cast<size_t>(n_cams));
+        std::vector<double> cost(static_cast<size_t>(n_cams), 0.0);
+        for (int32_t c = 0; c < n_cams; ++c) {
+            cost[c] = static_cast<double>(cams[c].nx) * cams[c].ny;
+            if (sc.order == HADROS_ORDER_COST) {
+                int32_t rc = cost_order(ctx, cams[c], s, sc.coarse_stride, orders[c], cost[c]);
+                if (rc) return rc;
+            } else if (sc.order == HADROS_ORDER_TILES) {
+                tile_order(cams[c], orders[c]);
+            }
+        }
+        // queue order of cameras: most expensive first (outputs stay in caller order)
+        std::vector<int32_t> qorder(static_cast<size_t>(n_cams));
+        for (int32_t c = 0; c < n_cams; ++c) qorder[c] = c;
+        if (sc.camera_order)
+            std::stable_sort(qorder.begin(), qorder.end(), [&](int32_t x, int32_t y) { return cost[x] > cost[y]; });
+        std::vector<DevCam> dc(static_cast<size_t>(n_cams));
+        std::vector<DevBin> bins;
+        std::string err;
+        std::vector<int64_t> out_off(static_cast<size_t>(n_cams)), bin_off(static_cast<size_t>(n_cams));
+        int64_t P = 0, PB = 0;
+        for (int32_t c = 0; c < n_cams; ++c) {   // output layout: caller order
+            const int64_t Pc = static_cast<int64_t>(cams[c].nx) * cams[c].ny;
+            const int64_t Bc = cams[c].spectral_kind == HADROS_SPECTRAL_MONOCHROMATIC ? 1 : std::max(cams[c].n_bins, 1);
+            out_off[c] = P;
+            bin_off[c] = PB;
+            P += Pc;
+            PB += Pc * Bc;
+        }
+        std::vector<int32_t> order_all;
+        const bool use_order = sc.order != HADROS_ORDER_ROWS;
+        if (use_order) order_all.reserve(static_cast<size_t>(P));
+        int64_t item = 0;
+        int32_t max_bins = 1, max_cap = 0;
+        for (int32_t k = 0; k < n_cams; ++k) {   // queue layout: cost order
+            const int32_t c = qorder[k];
+            DevCam& d = dc[k];
+            int32_t rc = build_cam(cams[c], s->h, d, bins, err);
+            if (rc) return fail(rc, "camera " + std::to_string(c) + ": " + err);
+            const int64_t Pc = static_cast<int64_t>(cams[c].nx) * cams[c].ny;
+            d.item_begin = item;
+            d.item_end = item + Pc;
+            d.out_offset = out_off[c];
+            d.binout_offset = bin_off[c];
+            item += Pc;
+            max_bins = std::max(max_bins, d.n_bins);
+            max_cap = std::max(max_cap, cams[c].max_steps);
+            if (use_order) order_all.insert(order_all.end(), orders[c].begin(), orders[c].end());
+        }
+        hadros_plan* pl = new hadros_plan();
+        pl->device = ctx->device;
+        pl->precision = cams[0].precision;
+        pl->fast = cams[0].fast_geodesic;
+        pl->P = P;
+        pl->PB = PB;
+        pl->sched = sc;
+        const SigmaHost& h = s->h;
+        const size_t n = h.E.size();
+        auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+        size_t o = 0;
+        const size_t o_cam = o; o = al(o + sizeof(DevCam) * dc.size());
+        const size_t o_bin = o; o = al(o + sizeof(DevBin) * bins.size());
+        const size_t o_ord = o; o = al(o + sizeof(int32_t) * order_all.size());
+        const size_t oE = o; o = al(o + 8 * n);
+        const size_t oS = o; o = al(o + 8 * n);
+        const size_t olnE = o; o = al(o + 8 * n);
+        const size_t olnS = o; o = al(o + 8 * n);
+        const size_t olx = o; o = al(o + 4 * n);
+        const size_t oseg = o; o = al(o + 16 * n);
+        std::vector<unsigned char> blob(o, 0);
+        std::memcpy(blob.data() + o_cam, dc.data(), sizeof(DevCam) * dc.size());
+        std::memcpy(blob.data() + o_bin, bins.data(), sizeof(DevBin) * bins.size());
+        if (use_order) std::memcpy(blob.data() + o_ord, order_all.data(), sizeof(int32_t) * order_all.size());
+        std::memcpy(blob.data() + oE, h.E.data(), 8 * n);
+        std::memcpy(blob.data() + oS, h.s_cm2.data(), 8 * n);
+        std::memcpy(blob.data() + olnE, h.lnE.data(), 8 * n);
+        std::memcpy(blob.data() + olnS, h.lnS.data(), 8 * n);
+        std::memcpy(blob.data() + olx, h.lx.data(), 4 * n);
+        std::memcpy(blob.data() + oseg, h.seg.data(), 16 * n);
+        cudaError_t e = cudaSetDevice(ctx->device);
+        if (e == cudaSuccess) e = cudaMalloc(&pl->d_tabs, o);
+        if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&pl->d_counters), 4 * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMemcpy(pl->d_tabs, blob.data(), o, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            hadros_plan_destroy(pl);
+            return cuda_fail(nullptr, e, "plan upload");
+        }
+        unsigned char* base = static_cast<unsigned char*>(pl->d_tabs);
+        TraceArgs& A = pl->A;
+        A.cams = reinterpret_cast<const DevCam*>(base + o_cam);
+        A.n_cams = n_cams;
+        A.max_bins = max_bins;
+        A.total_items = P;
+        A.bins = reinterpret_cast<const DevBin*>(base + o_bin);
+        A.order = use_order ? reinterpret_cast<const int32_t*>(base + o_ord) : nullptr;
+        A.blocks_per_sm = sc.blocks_per_sm;
+        A.sig.n = static_cast<int32_t>(n);
+        A.sig.uniform = h.uniform;
+        A.sig.lx0 = h.lx0;
+        A.sig.inv_dlx = h.inv_dlx;
+        A.sig.E_min = h.E.front();
+        A.sig.E_max = h.E.back();
+        A.sig.sigma_scale = h.sigma_scale;
+        A.sig.E = reinterpret_cast<const double*>(base + oE);
+        A.sig.S = reinterpret_cast<const double*>(base + oS);
+        A.sig.lnE = reinterpret_cast<const double*>(base + olnE);
+        A.sig.lnS = reinterpret_cast<const double*>(base + olnS);
+        A.sig.lx = reinterpret_cast<const float*>(base + olx);
+        A.sig.seg = reinterpret_cast<const float*>(base + oseg);
+        A.counters = pl->d_counters;
+        A.attempt_budget = ctx->attempt_budget > 0 ? ctx->attempt_budget : static_cast<int64_t>(max_cap) * 51 + 1;
+        A.fast_geodesic = pl->fast;
+        int32_t rc = prepare_trace(A, pl->precision, pl->fast, ctx->n_sm, sc.blocks_per_sm, pl->cfg, err);
+        if (rc) {
+            hadros_plan_destroy(pl);
+            return fail(rc, err);
+        }
+        *out = pl;
+        return ok();
+    } catch (const std::exception& ex) {
+        return fail(HADROS_E_NOMEM, ex.what());
+    }
+}
+
+int32_t hadros_plan_info(const hadros_plan* pl, int64_t* n_pixels, int64_t* n_pixel_bins, int32_t* grid,
+                         int32_t* blocks_per_sm)
+{
+    if (!pl) return fail(HADROS_E_STATE, "plan is NULL");
+    if (n_pixels) *n_pixels = pl->P;
+    if (n_pixel_bins) *n_pixel_bins = pl->PB;
+    if (grid) *grid = static_cast<int32_t>(pl->cfg.grid);
+    if (blocks_per_sm) *blocks_per_sm = pl->cfg.per_sm;
+    return ok();
+}
+
+int32_t hadros_plan_launch(hadros_plan* pl, const hadros_image_out* dev_out, void* stream)
+{
+    if (!pl) return fail(HADROS_E_STATE, "plan is NULL");
+    if (!dev_out) return fail(HADROS_E_ARG, "output struct is NULL");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    TraceArgs A = pl->A;
+    A.tau = dev_out->tau;
+    A.P_surv = dev_out->P_surv;
+    A.I_obs = dev_out->I_obs;
+    A.fate = dev_out->fate;
+    A.steps = dev_out->steps;
+    A.attempts = dev_out->attempts;
+    A.tau_E = dev_out->tau_E;
+    A.I_E = static_cast<double*>(dev_out->I_E);
+    cudaError_t e = cudaMemsetAsync(pl->d_counters, 0, 4 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return fail(HADROS_E_CUDA, std::string("plan counter reset: ") + cudaGetErrorString(e));
+    if (pl->P == 0) return ok();
+    std::string err;
+    const int32_t rc = launch_trace_prepared(A, pl->precision, pl->fast, pl->cfg, st, err);
+    return rc ? fail(rc, err) : ok();
+}
+
+int32_t hadros_plan_counters(hadros_plan* pl, void* stream, int64_t* steps, int64_t* attempts, int32_t* aborted)
+{
+    if (!pl) return fail(HADROS_E_STATE, "plan is NULL");
+    unsigned long long c[4] = {0, 0, 0, 0};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(c, pl->d_counters, sizeof(c), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(HADROS_E_CUDA, std::string("plan counters: ") + cudaGetErrorString(e));
+    if (steps) *steps = static_cast<int64_t>(c[1]);
+    if (attempts) *attempts = static_cast<int64_t>(c[2]);
+    if (aborted) *aborted = static_cast<int32_t>(c[3]);
+    return c[3] > 0 ? fail(HADROS_E_TIMEOUT, "rays exceeded the attempt budget") : ok();
+}
+
+void hadros_plan_destroy(hadros_plan* pl)
+{
+    if (!pl) return;
+    cudaSetDevice(pl->device);
+    cudaFree(pl->d_tabs);
+    cudaFree(pl->d_counters);
+    delete pl;
 }
 
 }  // extern "C"

@@ -8,6 +8,7 @@
 
 #include "../../include/hadros_b200.h"
 #include "hadros_physics.cuh"
+#include "hadros_physics_f32.cuh"
 
 namespace hadros {
 
@@ -32,6 +33,9 @@ struct DevCam {
     double rg_cm;
     Torus torus;
     Source src;
+    TorusF torus_f;                   // FP32 constants for the mixed transfer
+    SourceF src_f;
+    double k_nb;                      // sigma_scale / m_u (mixed transfer)
     int32_t nx, ny, max_steps, n_bins;
     int32_t mono;
     int32_t bin_offset;               // first row in the bin tables
@@ -59,6 +63,8 @@ struct DevBin {
 // mixed-precision lookup sigma = sigma_scale * s1[k] * exp(t * dly[k]).
 struct SigmaDev {
     int32_t n;
+    int32_t uniform;     // ln E nearly evenly spaced: direct segment index
+    float lx0, inv_dlx;
     double E_min, E_max, sigma_scale;
     const double* E;     // [n]
     const double* S;     // [n]  sigma_cm2
@@ -96,6 +102,16 @@ struct TraceArgs {
     const int64_t* path_offsets;
     const double* path_points;
     const int8_t* path_fates;
+    // schedule: optional item -> pixel order (outputs stay in pixel order)
+    // and a cap on resident blocks per SM (0 = occupancy)
+    const int32_t* order;
+    int32_t blocks_per_sm;
+};
+
+struct LaunchCfg {
+    unsigned grid;
+    size_t smem;
+    int per_sm;
 };
 
 // Host-side handle of an uploaded sigma table.
@@ -104,7 +120,18 @@ struct SigmaHost {
     std::vector<double> lnE, lnS;
     std::vector<float> lx, seg;
     double sigma_scale = 1.0;
+    int32_t uniform = 0;
+    float lx0 = 0.0f, inv_dlx = 0.0f;
 };
+
+// FP32 constants of the mixed transfer (torus_f, src_f, k_nb) from a camera's
+// torus and source; called by every camera builder.
+inline void fill_mixed_constants(DevCam& cam, double sigma_scale)
+{
+    cam.torus_f = make_torus_f(cam.torus);
+    cam.src_f = make_source_f(cam.src);
+    cam.k_nb = sigma_scale / kMuG;
+}
 
 // Camera plan building (host, hadros_trace.cu).
 int build_cam(const hadros_params& p, const SigmaHost& sig, DevCam& cam,
@@ -118,6 +145,17 @@ int launch_trace_fast(const TraceArgs& args, int precision, int n_sm, void* stre
                       std::string& err);
 int launch_path_transfer(const TraceArgs& args, int precision, int n_sm, void* stream,
                          std::string& err);
+int launch_path_transfer_fast(const TraceArgs& args, int precision, int n_sm, void* stream,
+                              std::string& err);
+// Prepared launches (plans): the setup once, then only the kernel enqueue.
+int prepare_trace(const TraceArgs& args, int precision, int fast, int n_sm, int blocks_per_sm,
+                  LaunchCfg& cfg, std::string& err);
+int launch_trace_prepared(const TraceArgs& args, int precision, int fast, const LaunchCfg& cfg,
+                          void* stream, std::string& err);
+int prepare_trace_fast(const TraceArgs& args, int precision, int n_sm, int blocks_per_sm,
+                       LaunchCfg& cfg, std::string& err);
+int launch_trace_prepared_fast(const TraceArgs& args, int precision, const LaunchCfg& cfg,
+                               void* stream, std::string& err);
 size_t trace_smem_bytes(int precision, int sig_n, int max_bins);
 
 // Record the calling thread's hadros_last_error() message; returns `code`.

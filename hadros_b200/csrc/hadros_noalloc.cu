@@ -190,6 +190,7 @@ int na_build_cam(const hadros_params& p, const SigmaHost& sig, DevCam& cam, DevB
         else
             s.rho_norm = smax(torus_rho(cam.torus, p.src_r_center_rg, 0.5 * kPi), 1.0e-300);
     }
+    fill_mixed_constants(cam, sig.sigma_scale);
     cam.nx = p.nx;
     cam.ny = p.ny;
     cam.max_steps = p.max_steps;
@@ -331,6 +332,9 @@ extern "C" int32_t hadros_image_device_noalloc(const hadros_params* p, const had
     A.sig.E_min = h.E.front();
     A.sig.E_max = h.E.back();
     A.sig.sigma_scale = h.sigma_scale;
+    A.sig.uniform = h.uniform;
+    A.sig.lx0 = h.lx0;
+    A.sig.inv_dlx = h.inv_dlx;
     A.sig.E = reinterpret_cast<const double*>(base + kOffE);
     A.sig.S = reinterpret_cast<const double*>(base + kOffS);
     A.sig.lnE = reinterpret_cast<const double*>(base + kOffLnE);

@@ -93,6 +93,17 @@ void prepare_sigma(SigmaHost& s)
         smax_v = std::max(smax_v, s.s_cm2[k]);
     }
     s.sigma_scale = smax_v > 0.0 ? smax_v : 1.0;
+    // nearly even spacing in ln E (within 1e-3 of a step): the kernel indexes
+    // the segment directly and corrects it by at most one knot
+    if (n >= 2) {
+        const double step = (s.lnE[n - 1] - s.lnE[0]) / static_cast<double>(n - 1);
+        bool even = step > 0.0;
+        for (size_t k = 1; k < n && even; ++k)
+            even = std::fabs((s.lnE[k] - s.lnE[k - 1]) - step) <= 1.0e-3 * step;
+        s.uniform = even ? 1 : 0;
+        s.lx0 = static_cast<float>(s.lnE[0]);
+        s.inv_dlx = static_cast<float>(1.0 / step);
+    }
     for (size_t k = 1; k < n; ++k) {
         s.seg[4 * k + 0] = static_cast<float>(s.lnE[k - 1]);
         s.seg[4 * k + 1] = static_cast<float>(1.0 / (s.lnE[k] - s.lnE[k - 1]));
@@ -174,6 +185,7 @@ int build_cam(const hadros_params& p, const SigmaHost& sig, DevCam& cam,
         else
             s.rho_norm = smax(torus_rho(cam.torus, p.src_r_center_rg, 0.5 * kPi), 1.0e-300);
     }
+    fill_mixed_constants(cam, sig.sigma_scale);
     cam.nx = p.nx;
     cam.ny = p.ny;
     cam.max_steps = p.max_steps;
@@ -259,36 +271,25 @@ int launch_trace(const TraceArgs& args, int precision, int n_sm, void* stream, s
     return launch_variant<0>(args, precision, n_sm, st, err);
 }
 
-namespace {
-
-int launch_paths(const TraceArgs& args, int precision, int n_sm, cudaStream_t st, std::string& err)
+int prepare_trace(const TraceArgs& args, int precision, int fast, int n_sm, int blocks_per_sm, LaunchCfg& cfg,
+                  std::string& err)
 {
-    const size_t smem = smem_layout(precision, args.sig.n, args.max_bins).total;
-    auto kern = (precision == HADROS_PRECISION_MIXED) ? path_transfer_kernel<1> : path_transfer_kernel<0>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per_sm = 0;
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTPB, smem);
-    if (e != cudaSuccess || per_sm < 1) {
-        err = std::string("path transfer kernel setup: ") + cudaGetErrorString(e);
-        return HADROS_E_CUDA;
-    }
-    long long grid = static_cast<long long>(n_sm) * per_sm;
-    const long long needed = (args.total_items + kTPB - 1) / kTPB;
-    if (grid > needed) grid = needed > 0 ? needed : 1;
-    kern<<<static_cast<unsigned>(grid), kTPB, smem, st>>>(args);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) {
-        err = std::string("path transfer kernel launch: ") + cudaGetErrorString(e);
-        return HADROS_E_CUDA;
-    }
-    return HADROS_OK;
+    if (fast) return prepare_trace_fast(args, precision, n_sm, blocks_per_sm, cfg, err);
+    return prepare_variant<0>(args, precision, n_sm, blocks_per_sm, cfg, err);
 }
 
-}  // namespace
+int launch_trace_prepared(const TraceArgs& args, int precision, int fast, const LaunchCfg& cfg, void* stream,
+                          std::string& err)
+{
+    if (fast) return launch_trace_prepared_fast(args, precision, cfg, stream, err);
+    return launch_prepared_variant<0>(args, precision, cfg, static_cast<cudaStream_t>(stream), err);
+}
 
 int launch_path_transfer(const TraceArgs& args, int precision, int n_sm, void* stream, std::string& err)
 {
-    return launch_paths(args, precision, n_sm, static_cast<cudaStream_t>(stream), err);
+    // the same translation unit (FMA or not) as the matching trace kernel
+    if (args.fast_geodesic) return launch_path_transfer_fast(args, precision, n_sm, stream, err);
+    return launch_paths<0>(args, precision, n_sm, static_cast<cudaStream_t>(stream), err);
 }
 
 }  // namespace hadros

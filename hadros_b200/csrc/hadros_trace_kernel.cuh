@@ -268,6 +268,8 @@ struct SmemTables {
     const float4* seg;
     int n;
     double Emin, Emax, scale;
+    int uniform;
+    float lx0, inv_dlx;
 };
 
 // This thread's column of per-bin accumulators (stride kTPB).
@@ -294,24 +296,24 @@ __device__ __forceinline__ void transfer_point(const DevCam* cam, const DevBin* 
     const double g = 1.0 / smax(z, 1.0e-300);
     const double gg = smax(g, 1.0e-300);
     const double dl_cm = dl * cam->rg_cm;
-    const double rho = torus_rho(cam->torus, r, th);
-    const double C = emissivity_factor(cam->src, cam->torus, r, th, rho);
-    const double g3 = pow(g, 3.0);
     if (MIXED) {
-        // FP32 transfer.  Each bin's intensity is kept as a Kahan sum
-        // I_s scaled by exp(S): every contribution K w(E_loc)/w(E_mid)
+        // FP32 transfer.  Density and ln(emissivity) in FP32
+        // (hadros_physics_f32.cuh).  Each bin's intensity is kept as a Kahan
+        // sum I_s scaled by exp(S): every contribution K w(E_loc)/w(E_mid)
         // exp(-tau) enters as exp(e) with e = ln(...) - tau + S, and S is
-        // re-anchored when the sum is empty or a term would exceed e^40,
-        // so intensities behind optically thick gas (exp(-tau) far below
-        // FP32's range) keep their relative precision.
+        // re-anchored when the sum is empty or a term would exceed e^40, so
+        // intensities behind optically thick gas (exp(-tau) far below FP32's
+        // range) keep their relative precision.
+        const float rho = torus_rho_f(cam->torus, cam->torus_f, r, th);
+        const float lnC = ln_emission_f(cam->src, cam->src_f, cam->torus, cam->torus_f, r, th, rho);
         const double zp = 1.0 / gg;   // E_local / E_mid
         const float lnzp = static_cast<float>(log(zp));
         const float zm1 = static_cast<float>(zp - 1.0);
-        const double Kd = g3 * C * dl_cm;
-        const bool emit = Kd > 0.0;
-        const float lnK = emit ? static_cast<float>(log(Kd)) : 0.0f;
-        const bool have_tau = !(rho <= 0.0);
-        const float nbdl = static_cast<float>((rho / kMuG) * dl_cm * tb.scale);
+        const bool emit = (lnC > -INFINITY) && dl_cm > 0.0;
+        // ln(g^3 C dl_cm) with g = 1 / zp
+        const float lnK = emit ? lnC + __logf(static_cast<float>(dl_cm)) - 3.0f * lnzp : 0.0f;
+        const bool have_tau = rho > 0.0f;
+        const float nbdl = rho * static_cast<float>(dl_cm * cam->k_nb);
         for (int b = 0; b < B; ++b) {
             const DevBin& bn = bins[b];
             float T = acc.T[b * kTPB], Tc = acc.Tc[b * kTPB];
@@ -337,13 +339,21 @@ __device__ __forceinline__ void transfer_point(const DevCam* cam, const DevBin* 
             }
             if (have_tau && gg >= bn.gg_lo && gg <= bn.gg_hi) {
                 const float lnE = bn.lnE + lnzp;
-                int lo = 0, cnt = tb.n;   // lower_bound over lx
-                while (cnt > 0) {
-                    const int st = cnt >> 1;
-                    if (tb.lx[lo + st] < lnE) { lo += st + 1; cnt -= st + 1; }
-                    else cnt = st;
+                int k;
+                if (tb.uniform) {   // evenly spaced ln E: direct index, corrected by one knot
+                    k = static_cast<int>((lnE - tb.lx0) * tb.inv_dlx) + 1;
+                    k = k < 1 ? 1 : (k > tb.n - 1 ? tb.n - 1 : k);
+                    if (k > 1 && lnE < tb.lx[k - 1]) --k;
+                    else if (k < tb.n - 1 && lnE > tb.lx[k]) ++k;
+                } else {
+                    int lo = 0, cnt = tb.n;   // lower_bound over lx
+                    while (cnt > 0) {
+                        const int st = cnt >> 1;
+                        if (tb.lx[lo + st] < lnE) { lo += st + 1; cnt -= st + 1; }
+                        else cnt = st;
+                    }
+                    k = lo < 1 ? 1 : (lo > tb.n - 1 ? tb.n - 1 : lo);
                 }
-                const int k = lo < 1 ? 1 : (lo > tb.n - 1 ? tb.n - 1 : lo);
                 const float4 sg = tb.seg[k];
                 const float t = (lnE - sg.x) * sg.y;
                 kahan_add(T, Tc, nbdl * (sg.z * __expf(t * sg.w)));
@@ -351,6 +361,9 @@ __device__ __forceinline__ void transfer_point(const DevCam* cam, const DevBin* 
             }
         }
     } else {
+        const double rho = torus_rho(cam->torus, r, th);
+        const double C = emissivity_factor(cam->src, cam->torus, r, th, rho);
+        const double g3 = pow(g, 3.0);
         for (int b = 0; b < B; ++b) {
             const double E_loc = bins[b].E_mid / gg;
             double jj = 0.0;
@@ -485,14 +498,14 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
     float* accI = accTc + size_t(kTPB) * A.max_bins;
     float* accIc = accI + size_t(kTPB) * A.max_bins;
     float* accS = accIc + size_t(kTPB) * A.max_bins;
-    const SmemTables tb{sE, sS, slnE, slnS, slx, sseg, n_sig, sigEmin, sigEmax, sig_scale};
+    const SmemTables tb{sE, sS, slnE, slnS, slx, sseg, n_sig, sigEmin, sigEmax, sig_scale, A.sig.uniform, A.sig.lx0, A.sig.inv_dlx};
     const BinAcc acc{accT64, accI64, accT, accTc, accI, accIc, accS};
 
     int phase = kNeedRay;
     // ray state
     const DevCam* cam = nullptr;
     const DevBin* bins = nullptr;
-    long long item = 0, local = 0;
+    long long item = 0, local = 0, row = 0;
     int B = 1, step = 0, att_in_step = 0;
     long long att_total = 0;
     double a = 0.0, r = 0.0, th = 0.0, ph = 0.0, pr = 0.0, pth = 0.0, pt = 0.0, pph = 0.0;
@@ -522,7 +535,9 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                 bins = A.bins + cam->bin_offset;
                 B = cam->n_bins;
                 local = item - cam->item_begin;
-                const long long pid = A.pixel_ids ? static_cast<long long>(A.pixel_ids[local]) : local;
+                const long long pid = A.pixel_ids ? static_cast<long long>(A.pixel_ids[local])
+                                      : (A.order ? static_cast<long long>(A.order[item]) : local);
+                row = A.order ? pid : local;   // output row within the camera
                 const int nx = cam->nx;
                 const int pi = static_cast<int>(pid % nx), pj = static_cast<int>(pid / nx);
                 // KerrCamera::initial_state (kerr_camera.cpp:110-186)
@@ -566,7 +581,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                 stop = true;
             }
             if (stop) {
-                finish_pixel<MIXED>(A, cam, bins, B, acc, local, step, fate, att_total);
+                finish_pixel<MIXED>(A, cam, bins, B, acc, row, step, fate, att_total);
                 atomicAdd(&A.counters[1], static_cast<unsigned long long>(step));
                 atomicAdd(&A.counters[2], static_cast<unsigned long long>(att_total));
                 phase = kNeedRay;
@@ -577,26 +592,59 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
             sincos(th, &s, &c);
             // PathPoint (kerr_camera.cpp:245-273): ZAMO interval and redshift
             double dl = 0.0;
-            if (step != 0) {
-                const double r_mid = 0.5 * (r + r_prev);
-                const double th_mid = 0.5 * (th + th_prev);
-                double sm, cm;
-                sincos(th_mid, &sm, &cm);
-                M5 gmid;
-                bl_metric(a, r_mid, sm, cm, gmid);
-                const double dr = r - r_prev;
-                const double dth = th - th_prev;
-                const double dph = wrapped_dphi(ph, ph_prev);
-                const double dl2 = gmid.rr * dr * dr + gmid.thth * dth * dth + gmid.phph * dph * dph;
-                dl = sqrt(smax(dl2, 0.0));
+            double z;
+            if (FAST) {
+                // the same interval and redshift with reciprocals instead of
+                // IEEE divisions and sin/cos of the midpoint by angle shift
+                const double a2 = a * a;
+                if (step != 0) {
+                    const double r_mid = 0.5 * (r + r_prev);
+                    const double th_mid = 0.5 * (th + th_prev);
+                    double sm, cm;
+                    const double dmid = th_mid - th;
+                    if (fabs(dmid) < 0.05) sincos_shift(s, c, dmid, &sm, &cm);
+                    else sincos(th_mid, &sm, &cm);
+                    const double r2 = r_mid * r_mid, s2 = sm * sm;
+                    const double sig = r2 + a2 * cm * cm;
+                    const double del = r2 - 2.0 * r_mid + a2;
+                    const double grr = sig * rcp_nr(del);
+                    const double gpp = (r2 + a2 + 2.0 * a2 * r_mid * s2 * rcp_nr(sig)) * s2;
+                    const double dr = r - r_prev;
+                    const double dth = th - th_prev;
+                    const double dph = wrapped_dphi(ph, ph_prev);
+                    const double dl2 = grr * dr * dr + sig * dth * dth + gpp * dph * dph;
+                    dl = sqrt(smax(dl2, 0.0));
+                }
+                const double r2 = r * r;
+                const double sig = r2 + a2 * c * c;
+                const double del = r2 - 2.0 * r + a2;
+                const double rpa = r2 + a2;
+                const double inv_A = rcp_nr(rpa * rpa - a2 * del * s * s);
+                const double alpha = sqrt(sig * del * inv_A);
+                const double omega = 2.0 * a * r * inv_A;
+                z = -(pt + omega * pph) * rcp_nr(alpha) * rcp_nr(smax(E_obs, 1.0e-300));
+            } else {
+                if (step != 0) {
+                    const double r_mid = 0.5 * (r + r_prev);
+                    const double th_mid = 0.5 * (th + th_prev);
+                    double sm, cm;
+                    sincos(th_mid, &sm, &cm);
+                    M5 gmid;
+                    bl_metric(a, r_mid, sm, cm, gmid);
+                    const double dr = r - r_prev;
+                    const double dth = th - th_prev;
+                    const double dph = wrapped_dphi(ph, ph_prev);
+                    const double dl2 = gmid.rr * dr * dr + gmid.thth * dth * dth + gmid.phph * dph * dph;
+                    dl = sqrt(smax(dl2, 0.0));
+                }
+                const double alpha = bl_lapse(a, r, s, c);
+                const double omega = bl_omega(a, r, s);
+                z = (-(pt + omega * pph) / alpha) / smax(E_obs, 1.0e-300);
             }
-            const double alpha = bl_lapse(a, r, s, c);
-            const double omega = bl_omega(a, r, s);
-            const double z = (-(pt + omega * pph) / alpha) / smax(E_obs, 1.0e-300);
             if (A.paths && step < A.path_cap) {   // PathPoint record (kerr_camera.cpp:235-273)
                 double sph, cph;
                 sincos(ph, &sph, &cph);
-                double* q = A.paths + ((cam->out_offset + local) * static_cast<long long>(A.path_cap) + step) * 7;
+                double* q = A.paths + ((cam->out_offset + row) * static_cast<long long>(A.path_cap) + step) * 7;
                 q[0] = r;
                 q[1] = th;
                 q[2] = r * s * cph;
@@ -743,7 +791,7 @@ __global__ void __launch_bounds__(kTPB) path_transfer_kernel(const TraceArgs A)
     float* accI = accTc + size_t(kTPB) * A.max_bins;
     float* accIc = accI + size_t(kTPB) * A.max_bins;
     float* accS = accIc + size_t(kTPB) * A.max_bins;
-    const SmemTables tb{sE, sS, slnE, slnS, slx, sseg, n_sig, A.sig.E_min, A.sig.E_max, A.sig.sigma_scale};
+    const SmemTables tb{sE, sS, slnE, slnS, slx, sseg, n_sig, A.sig.E_min, A.sig.E_max, A.sig.sigma_scale, A.sig.uniform, A.sig.lx0, A.sig.inv_dlx};
     const BinAcc acc{accT64, accI64, accT, accTc, accI, accIc, accS};
     const DevCam* cam = A.cams;
     const DevBin* bins = A.bins + cam->bin_offset;
@@ -761,15 +809,43 @@ __global__ void __launch_bounds__(kTPB) path_transfer_kernel(const TraceArgs A)
     }
 }
 
-// Occupancy-sized persistent launch of one kernel variant.
+// Grid-stride launch of the cached-path kernel; FAST only selects the
+// translation unit (FMA contraction or not), like the trace kernel's.
 template <int FAST>
-int launch_variant(const TraceArgs& args, int precision, int n_sm, cudaStream_t st, std::string& err)
+int launch_paths(const TraceArgs& args, int precision, int n_sm, cudaStream_t st, std::string& err)
 {
     const size_t smem = smem_layout(precision, args.sig.n, args.max_bins).total;
-    auto kern = (precision == HADROS_PRECISION_MIXED) ? trace_kernel<1, FAST> : trace_kernel<0, FAST>;
+    auto kern = (precision == HADROS_PRECISION_MIXED) ? path_transfer_kernel<1> : path_transfer_kernel<0>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTPB, smem);
+    if (e != cudaSuccess || per_sm < 1) {
+        err = std::string("path transfer kernel setup: ") + cudaGetErrorString(e);
+        return HADROS_E_CUDA;
+    }
+    long long grid = static_cast<long long>(n_sm) * per_sm;
+    const long long needed = (args.total_items + kTPB - 1) / kTPB;
+    if (grid > needed) grid = needed > 0 ? needed : 1;
+    kern<<<static_cast<unsigned>(grid), kTPB, smem, st>>>(args);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        err = std::string("path transfer kernel launch: ") + cudaGetErrorString(e);
+        return HADROS_E_CUDA;
+    }
+    return HADROS_OK;
+}
+
+// Grid of a persistent launch: SMs x resident blocks (capped at
+// blocks_per_sm when > 0), no more blocks than the work needs.
+template <int FAST>
+int prepare_variant(const TraceArgs& args, int precision, int n_sm, int blocks_per_sm, LaunchCfg& cfg,
+                    std::string& err)
+{
+    cfg.smem = smem_layout(precision, args.sig.n, args.max_bins).total;
+    auto kern = (precision == HADROS_PRECISION_MIXED) ? trace_kernel<1, FAST> : trace_kernel<0, FAST>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
+    int per_sm = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTPB, cfg.smem);
     if (e != cudaSuccess) {
         err = std::string("trace kernel setup: ") + cudaGetErrorString(e);
         return HADROS_E_CUDA;
@@ -778,16 +854,38 @@ int launch_variant(const TraceArgs& args, int precision, int n_sm, cudaStream_t 
         err = "trace kernel does not fit on an SM (shared memory for sigma table and bins)";
         return HADROS_E_ARG;
     }
+    if (blocks_per_sm > 0 && blocks_per_sm < per_sm) per_sm = blocks_per_sm;
     long long grid = static_cast<long long>(n_sm) * per_sm;
     const long long needed = (args.total_items + kTPB - 1) / kTPB;
     if (grid > needed) grid = needed > 0 ? needed : 1;
-    kern<<<static_cast<unsigned>(grid), kTPB, smem, st>>>(args);
-    e = cudaGetLastError();
+    cfg.grid = static_cast<unsigned>(grid);
+    cfg.per_sm = per_sm;
+    return HADROS_OK;
+}
+
+// Enqueue only the kernel (no host work): capturable in a CUDA graph.
+template <int FAST>
+int launch_prepared_variant(const TraceArgs& args, int precision, const LaunchCfg& cfg, cudaStream_t st,
+                            std::string& err)
+{
+    auto kern = (precision == HADROS_PRECISION_MIXED) ? trace_kernel<1, FAST> : trace_kernel<0, FAST>;
+    kern<<<cfg.grid, kTPB, cfg.smem, st>>>(args);
+    const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         err = std::string("trace kernel launch: ") + cudaGetErrorString(e);
         return HADROS_E_CUDA;
     }
     return HADROS_OK;
+}
+
+// Occupancy-sized persistent launch of one kernel variant.
+template <int FAST>
+int launch_variant(const TraceArgs& args, int precision, int n_sm, cudaStream_t st, std::string& err)
+{
+    LaunchCfg cfg{};
+    const int rc = prepare_variant<FAST>(args, precision, n_sm, args.blocks_per_sm, cfg, err);
+    if (rc) return rc;
+    return launch_prepared_variant<FAST>(args, precision, cfg, st, err);
 }
 
 }  // namespace

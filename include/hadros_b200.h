@@ -298,6 +298,42 @@ int32_t hadros_batch_device(hadros_ctx* ctx, const hadros_params* cams, int32_t 
                             const hadros_sigma* s, const hadros_image_out* dev_out,
                             void* stream);
 
+/* ---- plans: scans uploaded once, launches capturable in CUDA graphs -------- */
+
+/* Work schedule of a plan (what the autotuner searches). */
+enum hadros_order {
+    HADROS_ORDER_ROWS = 0,   /* pixels in row order j*nx+i                          */
+    HADROS_ORDER_TILES = 1,  /* 8x4 pixel tiles: a warp traces a compact patch      */
+    HADROS_ORDER_COST = 2    /* by descending cost from a coarse pre-pass           */
+};
+typedef struct hadros_schedule {
+    int32_t blocks_per_sm;   /* resident blocks per SM, 0 = occupancy limit         */
+    int32_t order;           /* enum hadros_order                                   */
+    int32_t coarse_stride;   /* pre-pass stride for HADROS_ORDER_COST (default 16)  */
+    int32_t camera_order;    /* 1: queue costly cameras first (outputs keep order)  */
+} hadros_schedule;
+
+typedef struct hadros_plan hadros_plan;
+void hadros_schedule_default(hadros_schedule* s);
+/* Upload cameras, bins and the sigma table once (and, for
+ * HADROS_ORDER_COST, run the pre-pass).  Replaces the reference's per-tile
+ * host loop with its per-launch synchronization and 4-byte readback
+ * (apps/compute_kerr_image_cuda.cu:2418-2483) for repeated scans. */
+int32_t hadros_plan_create(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams,
+                           const hadros_sigma* s, const hadros_schedule* sched,
+                           hadros_plan** out);
+int32_t hadros_plan_info(const hadros_plan* plan, int64_t* n_pixels, int64_t* n_pixel_bins,
+                         int32_t* grid, int32_t* blocks_per_sm);
+/* Enqueue the plan on `stream` into DEVICE buffers (concatenated outputs as
+ * hadros_batch): a 32-byte counter reset and one kernel launch, nothing on
+ * the host, so the call can be captured in a CUDA graph and replayed.  One
+ * launch of a plan in flight at a time. */
+int32_t hadros_plan_launch(hadros_plan* plan, const hadros_image_out* dev_out, void* stream);
+/* Wait for `stream` and read the last launch's step/attempt totals. */
+int32_t hadros_plan_counters(hadros_plan* plan, void* stream, int64_t* steps, int64_t* attempts,
+                             int32_t* aborted);
+void hadros_plan_destroy(hadros_plan* plan);
+
 /* ---- geodesic cache (compute_kerr_geodesics / --image-from-cache) ---------- */
 
 /* Trace pixels (all: pixel_ids NULL; or a list) and record every path point
