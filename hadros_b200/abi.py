@@ -120,6 +120,21 @@ class HadrosStats(C.Structure):
 
 # Every function the header declares: name -> (restype, argtypes).
 P = C.POINTER
+class HadrosMlpNorm(C.Structure):
+    _fields_ = [("feat_mu", C.c_float * 16), ("feat_inv_sd", C.c_float * 16),
+                ("out_mu", C.c_float * 2), ("out_sd", C.c_float * 2), ("out_floor", C.c_float * 2)]
+
+
+class HadrosAdam(C.Structure):
+    _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float)]
+
+
+class HadrosSurrogateOut(C.Structure):
+    _fields_ = [("ln_tau_E", C.c_void_p), ("ln_I_E", C.c_void_p), ("tau", C.c_void_p),
+                ("P_surv", C.c_void_p), ("I_obs", C.c_void_p), ("spread", C.c_void_p),
+                ("fallback_ids", C.c_void_p), ("counters", C.c_void_p)]
+
+
 SIGNATURES = {
     "hadros_abi_version": (C.c_int32, []),
     "hadros_status_string": (C.c_char_p, [C.c_int32]),
@@ -180,4 +195,30 @@ SIGNATURES = {
                                      C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hadros_write_kimg": (C.c_int32, [C.c_char_p, P(HadrosParams), C.c_double, C.c_double,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hadros_mlp_param_count": (C.c_int64, []),
+    "hadros_mlp_packed_count": (C.c_int64, []),
+    "hadros_mlp_workspace_bytes": (C.c_int64, [C.c_int64]),
+    "hadros_mlp_layout": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "hadros_mlp_pack": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hadros_mlp_featurize": (C.c_int32, [C.c_void_p, C.c_int64, P(HadrosMlpNorm), C.c_void_p,
+                                         C.c_void_p]),
+    "hadros_mlp_raw_features": (C.c_int32, [P(HadrosParams), C.c_void_p, C.c_void_p, C.c_int64,
+                                            C.c_void_p, C.c_void_p]),
+    "hadros_mlp_forward": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                       C.c_void_p, C.c_void_p]),
+    "hadros_mlp_backward": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p]),
+    "hadros_mlp_loss": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                    C.c_void_p, C.c_void_p]),
+    "hadros_mlp_adam": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, P(HadrosAdam),
+                                    C.c_int64, C.c_void_p]),
+    "hadros_mlp_train_step": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_int64, P(HadrosAdam), C.c_int64,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p]),
+    "hadros_mlp_image_bytes": (C.c_int64, []),
+    "hadros_mlp_pack_image": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hadros_surrogate_image": (C.c_int32, [P(HadrosParams), C.c_void_p, C.c_int32, C.c_void_p,
+                                           C.c_void_p, P(HadrosMlpNorm), C.c_int64, C.c_int64,
+                                           C.c_float, P(HadrosSurrogateOut), C.c_void_p]),
 }

@@ -33,9 +33,10 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra"]
 # (source, extra nvcc flags): the reference-arithmetic kernel must not contract
 # a*b+c into FMAs; the fast-geodesic kernel does.
 CU_SOURCES = [("hadros_trace.cu", ["--fmad=false"]), ("hadros_trace_fast.cu", ["--fmad=true"]),
-              ("hadros_noalloc.cu", ["--fmad=false"])]
+              ("hadros_noalloc.cu", ["--fmad=false"]), ("hadros_mlp.cu", []), ("hadros_mlp_umma.cu", [])]
 CXX_SOURCES = ["hadros_host.cpp", "hadros_formats.cpp"]
-HEADERS = ["hadros_internal.h", "hadros_physics.cuh", "hadros_trace_kernel.cuh"]
+HEADERS = ["hadros_internal.h", "hadros_physics.cuh", "hadros_physics_f32.cuh", "hadros_trace_kernel.cuh",
+           "hadros_mlp.cuh"]
 
 
 def _nvcc() -> str:

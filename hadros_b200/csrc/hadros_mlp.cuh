@@ -1,0 +1,126 @@
+// hadros_mlp.cuh — the surrogate network's fixed shape, parameter layouts and
+// the device helpers its training kernels (mma.sync, hadros_mlp.cu) and its
+// fused inference kernel (tcgen05, hadros_mlp_umma.cu) share.
+//
+// The surrogate has no counterpart in the reference: it predicts
+// ln tau_E and ln I_E of one (pixel, bin) sample from 16 raw features
+//   0 alpha, 1 beta (screen coordinates u*r_obs, v*r_obs, in M; the camera of
+//     src/kerr_camera.cpp:110-116), 2 a, 3 cos(theta_obs), 4 log10 rho0,
+//   5..12 one-hot torus profile kind, 13 r0 (M), 14 H/R, 15 log10 E_mid (GeV).
+// Each normalized feature x enters as two BF16 columns, hi = bf16(x) and
+// lo = bf16(x - hi), with tied first-layer weights, so the network sees x to
+// ~16 bits (a pixel of a 4096-wide image) although its operands are BF16.
+// Network: 32 -> 256 -> 256 -> 256 -> 256 (SiLU) -> 2, BF16 weights and
+// activations, FP32 accumulation, FP32 biases, plus an FP32 linear skip from
+// the 16 normalized features (x = hi + lo) to the 2 outputs.
+#pragma once
+
+#include <cstdint>
+
+#ifdef __CUDACC__
+#include <cuda_bf16.h>
+#endif
+
+namespace hadros {
+namespace mlp {
+
+constexpr int kF = 16;      // raw features
+constexpr int kIn = 32;     // BF16 input columns (hi, lo)
+constexpr int kW = 256;     // hidden width
+constexpr int kDepth = 4;   // hidden layers
+constexpr int kOut = 2;     // ln tau_E, ln I_E (standardized)
+constexpr int kOutPad = 16; // rows of the packed last-layer matrix
+
+// FP32 master parameters (what Adam updates), one network:
+//   W1 [256][16] (tied hi/lo weights), b1 [256],
+//   W_l [256][256], b_l [256] for l = 2..4,
+//   W5 [2][256], b5 [2], Ws [2][16] (linear skip).
+constexpr long kOffW1 = 0;
+constexpr long kOffB1 = kOffW1 + long(kW) * kF;
+constexpr long kOffW2 = kOffB1 + kW;
+constexpr long kHidStride = long(kW) * kW + kW;   // W_l then b_l
+constexpr long kOffW5 = kOffW2 + 3 * kHidStride;
+constexpr long kOffB5 = kOffW5 + long(kOut) * kW;
+constexpr long kOffWs = kOffB5 + kOut;
+constexpr long kParamsUsed = kOffWs + long(kOut) * kF;
+constexpr long kParams = (kParamsUsed + 7) / 8 * 8;   // padded for vector access
+
+__host__ __device__ constexpr long off_w(int layer)   // layer 1..4 weights
+{
+    return layer == 1 ? kOffW1 : kOffW2 + (layer - 2) * kHidStride;
+}
+__host__ __device__ constexpr long off_b(int layer)   // layer 1..4 bias
+{
+    return layer == 1 ? kOffB1 : off_w(layer) + long(kW) * kW;
+}
+
+// Row-major BF16 working copy (training kernels and tests):
+//   W1 [256][32] (the 16 master columns twice), W2..W4 [256][256],
+//   W5 [16][256] (rows 0..1 from the master, rows 2..15 zero).
+constexpr long kPW1 = 0;
+constexpr long kPW2 = kPW1 + long(kW) * kIn;
+constexpr long kPW5 = kPW2 + 3L * kW * kW;
+constexpr long kPacked = kPW5 + long(kOutPad) * kW;   // elements
+
+__host__ __device__ constexpr long pw(int layer)       // layer 1..5
+{
+    return layer == 1 ? kPW1 : (layer == 5 ? kPW5 : kPW2 + (layer - 2) * long(kW) * kW);
+}
+
+// Training workspace (bytes) for a batch of n samples: Z1..Z4, H1..H4,
+// two dZ buffers (BF16 [n][256] each) and the [256][32] FP32 layer-1 weight
+// gradient before the hi/lo columns are folded.
+constexpr long kWsAlign = 256;
+__host__ __device__ constexpr long ws_act_bytes(long n) { return n * kW * 2; }
+__host__ __device__ constexpr long ws_bytes(long n) { return 10 * ws_act_bytes(n) + long(kW) * kIn * 4 + kWsAlign; }
+
+// Normalization of one model (FP32): features x = (raw - mu) * inv_sd;
+// targets t = (y - out_mu) / out_sd with y = ln(value + floor).
+struct Norm {
+    float feat_mu[kF];
+    float feat_inv_sd[kF];
+    float out_mu[kOut];
+    float out_sd[kOut];
+    float out_floor[kOut];
+};
+
+#ifdef __CUDACC__
+
+__device__ __forceinline__ float tanh_approx(float x)
+{
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+// sigma(z) = (1 + tanh(z/2)) / 2; the same formula in every kernel, so the
+// trained function and the inferred one agree.
+__device__ __forceinline__ float sigmoid_f(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
+__device__ __forceinline__ float silu_f(float z) { return z * sigmoid_f(z); }
+__device__ __forceinline__ float silu_grad_f(float z)
+{
+    const float s = sigmoid_f(z);
+    return fmaf(z * s, 1.0f - s, s);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+__device__ __forceinline__ float2 unpack_bf16x2(uint32_t u)
+{
+    const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162*>(&u);
+    return __bfloat1622float2(v);
+}
+
+// Normalized feature x split into (hi, lo) BF16 parts.
+__device__ __forceinline__ void split_hi_lo(float x, __nv_bfloat16& hi, __nv_bfloat16& lo)
+{
+    hi = __float2bfloat16_rn(x);
+    lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+
+#endif  // __CUDACC__
+
+}  // namespace mlp
+}  // namespace hadros

@@ -1,0 +1,665 @@
+// hadros_mlp_umma.cu — surrogate inference on the 5th-generation tensor cores
+// (tcgen05), plus the sample features shared with training (no counterpart
+// in the reference).
+//
+// One persistent CTA per SM evaluates every ensemble member on 256 samples
+// (pixel, bin) at a time, the whole network chain without leaving the SM:
+//   - the epilogue warps build each sample's features in the kernel (the same
+//     device function as hadros_mlp_raw_features, which feeds training), and
+//     write them, then each layer's SiLU activations, as BF16 into shared
+//     memory in the UMMA K-major 128-byte-swizzled layout;
+//   - one thread issues tcgen05.mma (M=128, N=256, K=16, BF16 in, FP32 out)
+//     for the two 128-row halves into two TMEM accumulators (512 columns);
+//   - one thread streams the weights (pre-swizzled "images", 32 KB stages)
+//     with cp.async.bulk into a two-slot ring; both halves use each stage;
+//   - the epilogue reads TMEM with tcgen05.ld, adds bias, applies SiLU and
+//     stores the next layer's operand; after the last layer it de-standardizes
+//     ln tau_E and ln I_E, and reduces each pixel's bins (log-sum-exp of
+//     ln I_E + ln dE) per member, giving the ensemble spread of ln I_obs.
+// Pixels whose spread exceeds the threshold are appended to a fallback list
+// for the exact tracer.  Every wait is bounded: on timeout the kernel sets an
+// abort flag that the host reports as HADROS_E_TIMEOUT.
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "hadros_b200.h"
+#include "hadros_internal.h"
+#include "hadros_mlp.cuh"
+
+namespace hadros {
+namespace mlp {
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int kMaxBinsS = 128;   // bins of a surrogate camera
+constexpr int kTileRows = 128;   // rows of one TMEM accumulator
+constexpr int kPair = 2;         // accumulators per CTA pass (256 samples)
+constexpr int kStageBytes = 32768;           // [256 rows x 64 K] BF16, 128B-swizzled
+constexpr int kStages = 2;                   // weight ring slots
+constexpr int kStagesPerMember = 14;         // L1: 1, L2..L4: 4 each, L5: 1
+constexpr int kLastStageBytes = 8192;        // L5: 4 chunks of [16 x 64]
+constexpr long kImageBytes = long(kStagesPerMember - 1) * kStageBytes + kLastStageBytes;
+constexpr int kActBytes = 4 * 16384;         // [128 rows x 256 K] as 4 swizzled chunks
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = (kEpiWarps + 2) * 32;   // + MMA warp + producer warp
+constexpr int kMaxMembers = 8;
+constexpr long kWaitLimit = 1L << 22;        // try_wait rounds before giving up
+
+// Camera and bins of one surrogate image (kernel parameter).
+struct SurCam {
+    int32_t nx, ny, n_bins, profile;
+    float inv_nx, inv_ny, c_alpha, c_beta;
+    float a, cos_i, log_rho0, r0, h_over_r;
+    float log10E[kMaxBinsS];
+    float ln_dE[kMaxBinsS];   // -inf for bins outside the aggregates
+    float w[kMaxBinsS];       // aggregation weight (0 outside)
+};
+
+// The 16 raw features of sample (pixel, bin): the single definition used for
+// training rows and inference rows.
+__device__ __forceinline__ void raw_features(const SurCam& c, long pixel, int bin, float f[kF])
+{
+    const int i = int(pixel % c.nx), j = int(pixel / c.nx);
+    f[0] = (float(2 * i + 1) * c.inv_nx - 1.0f) * c.c_alpha;
+    f[1] = (float(2 * j + 1) * c.inv_ny - 1.0f) * c.c_beta;
+    f[2] = c.a;
+    f[3] = c.cos_i;
+    f[4] = c.log_rho0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) f[5 + q] = (q == c.profile) ? 1.0f : 0.0f;
+    f[13] = c.r0;
+    f[14] = c.h_over_r;
+    f[15] = c.log10E[bin];
+}
+
+__global__ void k_raw_features(SurCam c, const int32_t* __restrict__ pixel_ids, long n_pixels,
+                               float* __restrict__ raw)
+{
+    const long idx = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    const long n = n_pixels * c.n_bins;
+    if (idx >= n) return;
+    const long p = idx / c.n_bins;
+    const int b = int(idx % c.n_bins);
+    float f[kF];
+    raw_features(c, pixel_ids ? long(pixel_ids[p]) : p, b, f);
+#pragma unroll
+    for (int q = 0; q < kF; ++q) raw[idx * kF + q] = f[q];
+}
+
+// ---- weight images ------------------------------------------------------------
+// A K-major 128B-swizzled block has rows of 64 BF16 (128 B); the 16-byte unit
+// u of row r is stored at unit u ^ (r % 8).
+// One thread per 16-byte unit of the image of one network.
+__global__ void k_pack_image(const bf16* __restrict__ packed, uint8_t* __restrict__ image)
+{
+    const long u = long(blockIdx.x) * blockDim.x + threadIdx.x;   // 16-byte unit
+    if (u >= kImageBytes / 16) return;
+    const long byte = u * 16;
+    const int q = int(byte / kStageBytes);
+    const int in = int(byte % kStageBytes);
+    uint4 v = make_uint4(0, 0, 0, 0);
+    bf16 e[8];
+    int row, unit, c, l;
+    if (q < kStagesPerMember - 1) {
+        row = in / 128;                       // 0..255 = output unit n
+        unit = (in % 128) / 16;               // physical unit
+        const int kunit = unit ^ (row & 7);   // logical 16-byte unit
+        if (q == 0) {                         // W1 [256][32], K columns 32..63 zero
+            if (kunit < 4)
+                for (int t = 0; t < 8; ++t) e[t] = packed[pw(1) + long(row) * kIn + kunit * 8 + t];
+            else
+                for (int t = 0; t < 8; ++t) e[t] = __float2bfloat16_rn(0.0f);
+        } else {
+            l = 2 + (q - 1) / 4;
+            c = (q - 1) % 4;
+            for (int t = 0; t < 8; ++t) e[t] = packed[pw(l) + long(row) * kW + c * 64 + kunit * 8 + t];
+        }
+    } else {                                  // W5 [16][256]: chunk c at c * 2048
+        c = in / 2048;
+        const int r = in % 2048;
+        row = r / 128;
+        unit = (r % 128) / 16;
+        const int kunit = unit ^ (row & 7);
+        for (int t = 0; t < 8; ++t) e[t] = packed[pw(5) + long(row) * kW + c * 64 + kunit * 8 + t];
+    }
+    v = *reinterpret_cast<const uint4*>(e);
+    *reinterpret_cast<uint4*>(image + byte) = v;
+}
+
+// ---- PTX wrappers -------------------------------------------------------------
+__device__ __forceinline__ uint32_t saddr(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait; false (and the abort flag set) when the limit ran out or
+// another thread already aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag)
+{
+    for (long it = 0; it < kWaitLimit; ++it) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 255) == 255 && *abort_flag) return false;
+    }
+    *abort_flag = 1;
+    return false;
+}
+// mbar_wait by every lane of a warp, which leaves it converged and agreeing
+// (the tcgen05.ld that follows is warp-collective).
+__device__ __forceinline__ bool warp_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag)
+{
+    const bool ok = mbar_wait(bar, parity, abort_flag);
+    return __all_sync(0xffffffffu, ok) != 0;
+}
+// Bounded wait that ignores the abort flag (draining on the abort path).
+__device__ __forceinline__ bool mbar_wait_plain(uint32_t bar, uint32_t parity)
+{
+    for (long it = 0; it < kWaitLimit; ++it)
+        if (mbar_try(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+                 : "memory");
+}
+// D[tmem] (+)= A[smem] * B[smem]^T, both K-major.
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+          "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+          "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+          "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tc_ld2(uint32_t taddr, uint32_t& r0, uint32_t& r1)
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];\n" : "=r"(r0), "=r"(r1) : "r"(taddr));
+}
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), descriptor version 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr)
+{
+    return uint64_t((addr & 0x3FFFFu) >> 4) | (uint64_t(1) << 16) | (uint64_t(1024 >> 4) << 32) |
+           (uint64_t(1) << 46) | (uint64_t(2) << 61);
+}
+// Instruction descriptor of kind::f16: D FP32, A and B BF16, both K-major.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+struct InferArgs {
+    SurCam cam;
+    Norm norm;
+    const float* masters;     // [members][kParams]
+    const uint8_t* images;    // [members][kImageBytes]
+    int32_t members;
+    int64_t pixel_begin, n_pixels;
+    float spread_threshold;
+    float* ln_tau_E;          // [n_pixels][B] (may be NULL)
+    float* ln_I_E;            // [n_pixels][B] (may be NULL)
+    double* tau;
+    double* P_surv;
+    double* I_obs;
+    float* spread;
+    int32_t* fallback_ids;
+    int32_t* counters;        // [0] fallback count, [1] abort flag
+};
+
+constexpr int kSmemBytes = kPair * kActBytes + kStages * kStageBytes + 2 * 256 * 4 + 256 + 1024;
+static_assert(kSmemBytes <= 232448, "shared memory above the sm_100 per-block limit");
+
+__global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* act = smem;                                      // [2][64 KB]
+    uint8_t* stage = smem + kPair * kActBytes;                // [2][32 KB]
+    float* red_a = reinterpret_cast<float*>(stage + kStages * kStageBytes);   // [256]
+    float* red_b = red_a + 256;                                               // [256]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(red_b + 256);
+    uint64_t* full = bars;                 // [kStages]
+    uint64_t* empty = bars + kStages;      // [kStages]
+    uint64_t* acc_full = bars + 2 * kStages;
+    uint64_t* act_ready = bars + 2 * kStages + 1;
+    uint64_t* epi_bar = bars + 2 * kStages + 2;   // barrier of the 256 epilogue threads
+    uint64_t* drain = bars + 2 * kStages + 3;     // abort path: MMAs in flight
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 4);
+    volatile int* abort_flag = A.counters + 1;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int B = A.cam.n_bins;
+    const long n_samples = A.n_pixels * B;
+    const long n_tiles = (n_samples + kPair * kTileRows - 1) / (kPair * kTileRows);
+    const int K = A.members;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(saddr(&full[s]), 1);
+            mbar_init(saddr(&empty[s]), 1);
+        }
+        mbar_init(saddr(acc_full), 1);
+        mbar_init(saddr(act_ready), kEpiWarps);
+        mbar_init(saddr(epi_bar), kEpiWarps * 32);
+        mbar_init(saddr(drain), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        fence_async_smem();
+    }
+    if (warp == 0) {   // 512 TMEM columns: two 128 x 256 FP32 accumulators
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(saddr(tmem_slot)),
+                     "r"(512)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    long issued = 0;          // producer: stages issued
+    bool mma_issued = false;  // MMA thread: any tcgen05.mma issued
+    uint32_t epi_phase = 0;   // epilogue barrier phase
+    auto epi_sync = [&]() -> bool {
+        mbar_arrive(saddr(epi_bar));
+        const bool ok = warp_wait(saddr(epi_bar), epi_phase, abort_flag);
+        epi_phase ^= 1u;
+        return ok;
+    };
+
+    if (warp == kEpiWarps + 1) {
+        // ---- producer: the same 14-stage stream per member, per tile ----------
+        if (lane == 0) {
+            for (long tile = blockIdx.x; tile < n_tiles && !*abort_flag; tile += gridDim.x)
+                for (int k = 0; k < K; ++k)
+                    for (int q = 0; q < kStagesPerMember; ++q, ++issued) {
+                        const long i = issued;
+                        const int slot = int(i % kStages);
+                        const uint32_t ph = uint32_t((i / kStages) & 1);
+                        if (!mbar_wait(saddr(&empty[slot]), ph ^ 1u, abort_flag)) goto done;
+                        const uint32_t bytes = q == kStagesPerMember - 1 ? kLastStageBytes : kStageBytes;
+                        mbar_expect_tx(saddr(&full[slot]), bytes);
+                        bulk_g2s(saddr(stage + slot * kStageBytes), A.images + k * kImageBytes + long(q) * kStageBytes,
+                                 bytes, saddr(&full[slot]));
+                    }
+        }
+    } else if (warp == kEpiWarps) {
+        // ---- MMA issuer ---------------------------------------------------------
+        if (lane == 0) {
+            long i = 0, layer_count = 0;
+            const uint32_t id256 = idesc_bf16(128, 256), id16 = idesc_bf16(128, 16);
+            for (long tile = blockIdx.x; tile < n_tiles && !*abort_flag; tile += gridDim.x)
+                for (int k = 0; k < K; ++k)
+                    for (int L = 1; L <= 5; ++L, ++layer_count) {
+                        if (!mbar_wait(saddr(act_ready), uint32_t(layer_count & 1), abort_flag)) goto done;
+                        tc_fence_after();
+                        const int nst = (L == 1 || L == 5) ? 1 : 4;
+                        for (int c = 0; c < nst; ++c, ++i) {
+                            const int slot = int(i % kStages);
+                            if (!mbar_wait(saddr(&full[slot]), uint32_t((i / kStages) & 1), abort_flag)) goto done;
+                            tc_fence_after();
+                            const uint32_t sb = saddr(stage + slot * kStageBytes);
+                            mma_issued = true;
+                            for (int t = 0; t < kPair; ++t) {
+                                const uint32_t ab = saddr(act + t * kActBytes);
+                                const uint32_t d = tmem + uint32_t(t * 256);
+                                if (L == 1) {          // K = 32 from chunk 0
+                                    for (int kk = 0; kk < 2; ++kk)
+                                        tc_mma(d, sdesc(ab + kk * 32), sdesc(sb + kk * 32), id256, kk > 0);
+                                } else if (L == 5) {   // N = 16, K = 256 over 4 chunks of the stage
+                                    for (int cc = 0; cc < 4; ++cc)
+                                        for (int kk = 0; kk < 4; ++kk)
+                                            tc_mma(d, sdesc(ab + cc * 16384 + kk * 32), sdesc(sb + cc * 2048 + kk * 32),
+                                                   id16, (cc | kk) != 0);
+                                } else {               // K chunk c of 64
+                                    for (int kk = 0; kk < 4; ++kk)
+                                        tc_mma(d, sdesc(ab + c * 16384 + kk * 32), sdesc(sb + kk * 32), id256,
+                                               (c | kk) != 0);
+                                }
+                            }
+                            tc_commit(saddr(&empty[slot]));   // slot free once these MMAs finish
+                        }
+                        tc_commit(saddr(acc_full));            // layer done
+                    }
+        }
+    } else {
+        // ---- epilogue warps: rows of accumulator t = warp / 4 ---------------------
+        const int t = warp >> 2, qw = warp & 3;
+        const int r = qw * 32 + lane;                 // row in the 128-row half
+        const int trow = t * kTileRows + r;           // row in the 256-sample tile
+        uint8_t* my_act = act + t * kActBytes;
+        const uint32_t lane_base = tmem + (uint32_t(qw * 32) << 16) + uint32_t(t * 256);
+        long layer_count = 0;
+        const bool leader_possible = (trow % B) == 0;
+        for (long tile = blockIdx.x; tile < n_tiles && __all_sync(0xffffffffu, *abort_flag == 0);
+             tile += gridDim.x) {
+            const long s = tile * (kPair * kTileRows) + trow;
+            const bool valid = s < n_samples;
+            const long lp = valid ? s / B : 0;
+            const int b = valid ? int(s % B) : 0;
+            float x[kF];
+            uint32_t feat[16];
+            {
+                float f[kF];
+                raw_features(A.cam, A.pixel_begin + lp, b, f);
+                bf16 hi[kF], lo[kF];
+#pragma unroll
+                for (int q = 0; q < kF; ++q) {
+                    const float xn = valid ? (f[q] - A.norm.feat_mu[q]) * A.norm.feat_inv_sd[q] : 0.0f;
+                    split_hi_lo(xn, hi[q], lo[q]);
+                    x[q] = __bfloat162float(hi[q]) + __bfloat162float(lo[q]);
+                }
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    feat[q] = pack_bf16x2(__bfloat162float(hi[2 * q]), __bfloat162float(hi[2 * q + 1]));
+                    feat[8 + q] = pack_bf16x2(__bfloat162float(lo[2 * q]), __bfloat162float(lo[2 * q + 1]));
+                }
+            }
+            float sum_tau = 0.0f, sum_lnI = 0.0f;
+            float w_ref = 0.0f, w_s1 = 0.0f, w_s2 = 0.0f;   // pixel leader: shifted sums of ln I_k
+            for (int k = 0; k < K; ++k) {
+                const float* P = A.masters + long(k) * kParams;
+                // features -> chunk 0, 16-byte units 0..3 of row r
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    *reinterpret_cast<uint4*>(my_act + r * 128 + ((u ^ (r & 7)) << 4)) =
+                        make_uint4(feat[4 * u], feat[4 * u + 1], feat[4 * u + 2], feat[4 * u + 3]);
+                fence_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(saddr(act_ready));
+                for (int L = 1; L <= 4; ++L, ++layer_count) {
+                    if (!warp_wait(saddr(acc_full), uint32_t(layer_count & 1), abort_flag)) goto done;
+                    tc_fence_after();
+                    const float* bias = P + off_b(L);
+#pragma unroll 1
+                    for (int cb = 0; cb < kW; cb += 32) {
+                        uint32_t v[32];
+                        tc_ld32(lane_base + uint32_t(cb), v);
+                        tc_wait_ld();
+                        uint32_t h[16];
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) {
+                            const float z0 = __uint_as_float(v[2 * q]) + __ldg(bias + cb + 2 * q);
+                            const float z1 = __uint_as_float(v[2 * q + 1]) + __ldg(bias + cb + 2 * q + 1);
+                            h[q] = pack_bf16x2(silu_f(z0), silu_f(z1));
+                        }
+                        uint8_t* chunk = my_act + (cb >> 6) * 16384 + r * 128;
+                        const int u0 = (cb & 63) >> 3;   // logical unit of column cb
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            *reinterpret_cast<uint4*>(chunk + (((u0 + u) ^ (r & 7)) << 4)) =
+                                make_uint4(h[4 * u], h[4 * u + 1], h[4 * u + 2], h[4 * u + 3]);
+                    }
+                    tc_fence_before();
+                    fence_async_smem();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(saddr(act_ready));
+                }
+                // last layer: 2 outputs (+ bias + FP32 skip), de-standardized
+                if (!warp_wait(saddr(acc_full), uint32_t(layer_count & 1), abort_flag)) goto done;
+                ++layer_count;
+                tc_fence_after();
+                uint32_t o0, o1;
+                tc_ld2(lane_base, o0, o1);
+                tc_wait_ld();
+                tc_fence_before();
+                float a0 = __uint_as_float(o0) + P[kOffB5], a1 = __uint_as_float(o1) + P[kOffB5 + 1];
+#pragma unroll
+                for (int q = 0; q < kF; ++q) {
+                    a0 = fmaf(P[kOffWs + q], x[q], a0);
+                    a1 = fmaf(P[kOffWs + kF + q], x[q], a1);
+                }
+                const float ltau = fmaf(a0, A.norm.out_sd[0], A.norm.out_mu[0]);
+                const float lnI = fmaf(a1, A.norm.out_sd[1], A.norm.out_mu[1]);
+                sum_tau += ltau;
+                sum_lnI += lnI;
+                // this member's ln I_obs per pixel: log-sum-exp over the pixel's bins
+                red_a[trow] = valid ? lnI + A.cam.ln_dE[b] : -INFINITY;
+                if (!epi_sync()) goto done;
+                if (leader_possible && valid) {
+                    float m = -INFINITY;
+                    for (int q = 0; q < B; ++q) m = fmaxf(m, red_a[trow + q]);
+                    float sacc = 0.0f;
+                    for (int q = 0; q < B; ++q) sacc += __expf(red_a[trow + q] - m);
+                    const float Lk = m + __logf(sacc);
+                    if (k == 0) w_ref = Lk;
+                    const float d = Lk - w_ref;
+                    w_s1 += d;
+                    w_s2 += d * d;
+                }
+                if (!epi_sync()) goto done;
+            }
+            // ensemble means -> per-sample outputs and per-pixel aggregates
+            const float inv_k = 1.0f / float(K);
+            const float ltau = sum_tau * inv_k, lnI = sum_lnI * inv_k;
+            if (valid) {
+                if (A.ln_tau_E) A.ln_tau_E[s] = ltau;
+                if (A.ln_I_E) A.ln_I_E[s] = lnI;
+            }
+            red_a[trow] = valid ? lnI + A.cam.ln_dE[b] : -INFINITY;
+            red_b[trow] = valid ? fmaxf(__expf(ltau) - A.norm.out_floor[0], 0.0f) : 0.0f;
+            if (!epi_sync()) goto done;
+            if (leader_possible && valid) {
+                float m = -INFINITY;
+                for (int q = 0; q < B; ++q) m = fmaxf(m, red_a[trow + q]);
+                double sacc = 0.0, wsum = 0.0, tsum = 0.0, psum = 0.0;
+                for (int q = 0; q < B; ++q) {
+                    if (m > -INFINITY) sacc += exp(double(red_a[trow + q] - m));
+                    const double w = A.cam.w[q];
+                    wsum += w;
+                    tsum += w * red_b[trow + q];
+                    psum += w * exp(-double(red_b[trow + q]));
+                }
+                const double I = m > -INFINITY ? exp(double(m)) * sacc : 0.0;
+                const float mean = w_s1 * inv_k;
+                const float sd = sqrtf(fmaxf(w_s2 * inv_k - mean * mean, 0.0f));
+                A.tau[lp] = wsum > 0.0 ? tsum / wsum : 0.0;
+                A.P_surv[lp] = wsum > 0.0 ? psum / wsum : 1.0;
+                A.I_obs[lp] = I;
+                A.spread[lp] = sd;
+                if (sd > A.spread_threshold) {
+                    const int slot = atomicAdd(A.counters, 1);
+                    A.fallback_ids[slot] = int32_t(A.pixel_begin + lp);
+                }
+            }
+            if (!epi_sync()) goto done;
+        }
+    }
+done:
+    if (*abort_flag) {
+        // Abort path: let the MMAs and bulk copies this CTA issued finish
+        // before its shared memory and TMEM are released.
+        if (warp == kEpiWarps && lane == 0 && mma_issued) {
+            tc_commit(saddr(drain));
+            mbar_wait_plain(saddr(drain), 0);
+        }
+        if (warp == kEpiWarps + 1 && lane == 0)
+            for (long j = issued - 1; j >= 0 && j >= issued - kStages; --j)
+                mbar_wait_plain(saddr(&full[j % kStages]), uint32_t((j / kStages) & 1));
+    }
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512) : "memory");
+}
+
+int32_t cuda_status(const char* what)
+{
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(HADROS_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return HADROS_OK;
+}
+
+// Camera constants and bins of a surrogate image from the tracer's params.
+int32_t make_surcam(const hadros_params* p, const hadros_sigma* s, SurCam* c)
+{
+    if (int32_t rc = hadros_params_validate(p)) return rc;
+    const int B = p->spectral_kind == HADROS_SPECTRAL_MONOCHROMATIC ? 1 : p->n_bins;
+    if (B < 1 || B > kMaxBinsS)
+        return set_error(HADROS_E_ARG, "the surrogate handles 1.." + std::to_string(kMaxBinsS) + " bins");
+    std::vector<double> E(B), dE(B), w(B);
+    std::vector<int8_t> valid(B);
+    int32_t nb = 0;
+    if (int32_t rc = hadros_spectral_bins(p, s, E.data(), dE.data(), w.data(), valid.data(), &nb)) return rc;
+    *c = SurCam{};
+    c->nx = p->nx;
+    c->ny = p->ny;
+    c->n_bins = nb;
+    c->profile = p->profile_kind;
+    c->inv_nx = 1.0f / float(p->nx);
+    c->inv_ny = 1.0f / float(p->ny);
+    const double th = std::tan(0.5 * p->fov_deg * M_PI / 180.0) * p->r_obs_rg;
+    c->c_alpha = float(th);
+    c->c_beta = float(th);
+    c->a = float(p->a_spin);
+    c->cos_i = float(std::cos(p->theta_obs_rad));
+    c->log_rho0 = float(std::log10(p->rho0_gcm3));
+    c->r0 = float(p->r0_rg);
+    c->h_over_r = float(p->H_over_R);
+    for (int b = 0; b < nb; ++b) {
+        c->log10E[b] = E[b] > 0.0 ? float(std::log10(E[b])) : 0.0f;
+        const bool in = valid[b] != 0 && dE[b] > 0.0;
+        c->ln_dE[b] = in ? float(std::log(dE[b])) : -INFINITY;
+        c->w[b] = in ? float(w[b]) : 0.0f;
+    }
+    return HADROS_OK;
+}
+
+}  // namespace
+}  // namespace mlp
+}  // namespace hadros
+
+using namespace hadros;
+using namespace hadros::mlp;
+
+extern "C" {
+
+int64_t hadros_mlp_image_bytes(void) { return kImageBytes; }
+
+int32_t hadros_mlp_pack_image(const void* packed, void* image, void* stream)
+{
+    if (!packed || !image) return set_error(HADROS_E_ARG, "NULL argument");
+    if (reinterpret_cast<uintptr_t>(image) % 16 != 0) return set_error(HADROS_E_ARG, "image must be 16-byte aligned");
+    const long units = kImageBytes / 16;
+    k_pack_image<<<int((units + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const bf16*>(packed), static_cast<uint8_t*>(image));
+    return cuda_status("hadros_mlp_pack_image");
+}
+
+int32_t hadros_mlp_raw_features(const hadros_params* p, const hadros_sigma* s, const int32_t* pixel_ids,
+                                int64_t n_pixels, float* raw, void* stream)
+{
+    if (!p || !s || !raw || n_pixels < 0) return set_error(HADROS_E_ARG, "bad argument");
+    SurCam c;
+    if (int32_t rc = make_surcam(p, s, &c)) return rc;
+    const long n = n_pixels * c.n_bins;
+    if (n == 0) return HADROS_OK;
+    k_raw_features<<<int((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(c, pixel_ids, n_pixels, raw);
+    return cuda_status("hadros_mlp_raw_features");
+}
+
+int32_t hadros_surrogate_image(const hadros_params* p, const hadros_sigma* s, int32_t n_members,
+                               const float* masters, const void* images, const hadros_mlp_norm* norm,
+                               int64_t pixel_begin, int64_t pixel_end, float spread_threshold,
+                               const hadros_surrogate_out* out, void* stream)
+{
+    if (!p || !s || !masters || !images || !norm || !out || !out->tau || !out->P_surv || !out->I_obs ||
+        !out->spread || !out->fallback_ids || !out->counters)
+        return set_error(HADROS_E_ARG, "NULL argument");
+    if (n_members < 1 || n_members > kMaxMembers)
+        return set_error(HADROS_E_ARG, "n_members must be in 1.." + std::to_string(kMaxMembers));
+    if (reinterpret_cast<uintptr_t>(images) % 16 != 0) return set_error(HADROS_E_ARG, "images must be 16-byte aligned");
+    InferArgs a{};
+    if (int32_t rc = make_surcam(p, s, &a.cam)) return rc;
+    const long P = long(p->nx) * p->ny;
+    if (pixel_begin < 0 || pixel_end > P || pixel_end < pixel_begin)
+        return set_error(HADROS_E_ARG, "pixel range outside the image");
+    if ((kPair * kTileRows) % a.cam.n_bins != 0)
+        return set_error(HADROS_E_ARG, "surrogate inference needs a bin count that divides 256");
+    int dev = 0, n_sm = 0, max_smem = 0, major = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (major != 10) return set_error(HADROS_E_CUDA, "surrogate inference needs an sm_100 GPU");
+    if (max_smem < kSmemBytes) return set_error(HADROS_E_CUDA, "not enough shared memory per block");
+    auto st = static_cast<cudaStream_t>(stream);
+    cudaMemsetAsync(out->counters, 0, 2 * sizeof(int32_t), st);
+    const long n_px = pixel_end - pixel_begin;
+    if (n_px == 0) return cuda_status("hadros_surrogate_image");
+    static_assert(sizeof(hadros_mlp_norm) == sizeof(Norm), "hadros_mlp_norm must mirror mlp::Norm");
+    std::memcpy(&a.norm, norm, sizeof(Norm));
+    a.masters = masters;
+    a.images = static_cast<const uint8_t*>(images);
+    a.members = n_members;
+    a.pixel_begin = pixel_begin;
+    a.n_pixels = n_px;
+    a.spread_threshold = spread_threshold;
+    a.ln_tau_E = out->ln_tau_E;
+    a.ln_I_E = out->ln_I_E;
+    a.tau = out->tau;
+    a.P_surv = out->P_surv;
+    a.I_obs = out->I_obs;
+    a.spread = out->spread;
+    a.fallback_ids = out->fallback_ids;
+    a.counters = out->counters;
+    cudaFuncSetAttribute(k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    const long tiles = (n_px * a.cam.n_bins + kPair * kTileRows - 1) / (kPair * kTileRows);
+    const int grid = int(std::min<long>(tiles, n_sm));
+    k_infer<<<grid, kThreads, kSmemBytes, st>>>(a);
+    return cuda_status("hadros_surrogate_image");
+}
+
+}  // extern "C"

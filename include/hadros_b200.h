@@ -418,6 +418,95 @@ int32_t hadros_kgeo_info(const char* path, int32_t* nx, int32_t* ny, double* a_s
 int32_t hadros_read_kgeo(const char* path, int32_t* pixel_ids, int8_t* captured,
                          int32_t* npoints, double* alpha, double* beta, double* points);
 
+/* ---- surrogate network (no counterpart in the reference) -------------------
+ * A BF16 tensor-core MLP trained on (pixel, bin) samples that this library
+ * traces; it predicts ln tau_E and ln I_E for parameter scans, and an
+ * ensemble of such networks marks, through its spread, the pixels the exact
+ * tracer must redo.  Inputs: 16 raw features per sample (alpha, beta, a,
+ * cos theta_obs, log10 rho0, one-hot profile kind x8, r0, H/R, log10 E_mid);
+ * network 32 -> 4 x 256 (SiLU) -> 2 with the normalized features split into
+ * hi/lo BF16 pairs and an FP32 linear skip.  Pointers are DEVICE pointers
+ * unless stated; calls are asynchronous on `stream` (a cudaStream_t; NULL =
+ * the legacy default stream) and allocate nothing. */
+typedef struct hadros_mlp_norm {   /* host struct, passed by pointer          */
+    float feat_mu[16];             /* x = (raw - mu) * inv_sd                 */
+    float feat_inv_sd[16];
+    float out_mu[2];               /* ln value = mu + sd * network output     */
+    float out_sd[2];
+    float out_floor[2];            /* targets are ln(value + floor)           */
+} hadros_mlp_norm;
+
+typedef struct hadros_adam {
+    float lr, beta1, beta2, eps;
+} hadros_adam;
+
+/* FP32 master parameters of one network, BF16 elements of its row-major
+ * working copy, and training workspace bytes for a batch. */
+int64_t hadros_mlp_param_count(void);
+int64_t hadros_mlp_packed_count(void);
+int64_t hadros_mlp_workspace_bytes(int64_t batch);
+/* Offsets (in floats) of W1, b1, W2, b2, W3, b3, W4, b4, W5, b5, Ws and the
+ * end of the used parameters in the master array (12 slots). */
+int32_t hadros_mlp_layout(int64_t* offsets, int32_t n);
+/* master FP32 -> BF16 working copy (W1 twice for the hi/lo columns). */
+int32_t hadros_mlp_pack(const float* master, void* packed, void* stream);
+/* raw [n][16] FP32 -> X [n][32] BF16 (normalized, hi/lo split). */
+int32_t hadros_mlp_featurize(const float* raw, int64_t n, const hadros_mlp_norm* norm, void* X,
+                             void* stream);
+/* Raw features of the samples (pixel_ids[k], bin b) of a camera, rows
+ * k * n_bins + b; pixel_ids NULL = pixels 0..n_pixels-1.  The same function
+ * the inference kernel evaluates. */
+int32_t hadros_mlp_raw_features(const hadros_params* p, const hadros_sigma* s,
+                                const int32_t* pixel_ids, int64_t n_pixels, float* raw,
+                                void* stream);
+/* Forward pass of a batch (stores activations in `workspace` for backward);
+ * out [n][2] standardized predictions. */
+int32_t hadros_mlp_forward(const float* master, const void* packed, const void* X, int64_t n,
+                           void* workspace, float* out, void* stream);
+/* Backward pass after hadros_mlp_forward on the same workspace: adds the
+ * gradient of sum(dout * out) to grad (master layout; zero it first). */
+int32_t hadros_mlp_backward(const void* packed, const void* X, int64_t n, const float* dout,
+                            void* workspace, float* grad, void* stream);
+/* loss += sum w (out - target)^2 / (2n); dout its gradient; weight may be NULL. */
+int32_t hadros_mlp_loss(const float* out, const float* target, const float* weight, int64_t n,
+                        float* dout, float* loss, void* stream);
+/* One Adam update of the master parameters (step counts from 1). */
+int32_t hadros_mlp_adam(float* master, float* m, float* v, const float* grad,
+                        const hadros_adam* opt, int64_t step, void* stream);
+/* forward + loss + backward + Adam + repack, for one batch. */
+int32_t hadros_mlp_train_step(float* master, void* packed, float* m, float* v, const void* X,
+                              const float* target, const float* weight, int64_t n,
+                              const hadros_adam* opt, int64_t step, void* workspace, float* grad,
+                              float* out, float* dout, float* loss, void* stream);
+
+/* Bytes of one network's inference image (weights pre-swizzled for the
+ * tensor-core kernel) and its construction from the BF16 working copy. */
+int64_t hadros_mlp_image_bytes(void);
+int32_t hadros_mlp_pack_image(const void* packed, void* image, void* stream);
+
+typedef struct hadros_surrogate_out {   /* DEVICE buffers                        */
+    float* ln_tau_E;       /* [P][B] ensemble mean of ln tau_E (may be NULL)   */
+    float* ln_I_E;         /* [P][B] ensemble mean of ln I_E (may be NULL)     */
+    double* tau;           /* [P] spectral aggregates as integrate_kerr_ray_   */
+    double* P_surv;        /*     spectral forms them from the mean prediction */
+    double* I_obs;
+    float* spread;         /* [P] ensemble standard deviation of ln I_obs      */
+    int32_t* fallback_ids; /* [P] pixel ids with spread > threshold, unordered */
+    int32_t* counters;     /* [2]: fallback count, abort flag (set by the call) */
+} hadros_surrogate_out;
+
+/* Surrogate image of pixels [pixel_begin, pixel_end) of camera p with an
+ * ensemble of n_members (1..8) networks: masters [n][param_count] FP32,
+ * images [n][image_bytes] (16-byte aligned).  P = pixel_end - pixel_begin,
+ * outputs indexed from pixel_begin; B = bins of p, which must divide 256.
+ * Asynchronous; after the stream completes, counters[1] != 0 means a wait in
+ * the kernel timed out and the outputs are not valid. */
+int32_t hadros_surrogate_image(const hadros_params* p, const hadros_sigma* s, int32_t n_members,
+                               const float* masters, const void* images,
+                               const hadros_mlp_norm* norm, int64_t pixel_begin,
+                               int64_t pixel_end, float spread_threshold,
+                               const hadros_surrogate_out* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
