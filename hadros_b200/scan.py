@@ -1,0 +1,214 @@
+"""Surrogate-accelerated parameter scans, timed against the plain tracer.
+
+    python -m hadros_b200.scan production --points 256 --side 4096 --bins 64
+    python -m hadros_b200.scan inference            # 2048^2 x 32 with fallback
+
+production: the surrogate is trained on rays the tracer traces at other
+parameter points of the same box (collapsar_ndaf_like, density_weighted
+source, a = 0.95, rho0 log-uniform in [1e9, 1e12], inclination in [10, 80]
+deg); each scan point is then evaluated by the ensemble, the pixels whose
+spread of ln I_obs exceeds the threshold are traced exactly, and the exact
+tracer judges a seeded random 1% of the pixels.  The plain tracer's time per
+point is measured on a few points of the same scan.
+
+inference: the surrogate is trained on cameras with randomized spin,
+inclination, profile, rho0 and two shape parameters, and evaluates the
+mixed_512 camera at 2048 x 2048 x 32 bins with exact fallback.
+
+Prints one JSON object.  Everything runs on CUDA device 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+
+from . import Context, SigmaTable, params
+from . import surrogate as S
+from . import workloads as W
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def plain_image(ctx, p, sigma) -> tuple[dict, float]:
+    """The exact tracer's per-pixel outputs in device memory, and its time (s)."""
+    torch = _torch()
+    P = int(p.nx) * int(p.ny)
+    dev = torch.device("cuda", 0)
+    out = {"tau": torch.empty(P, dtype=torch.float64, device=dev),
+           "P_surv": torch.empty(P, dtype=torch.float64, device=dev),
+           "I_obs": torch.empty(P, dtype=torch.float64, device=dev),
+           "fate": torch.empty(P, dtype=torch.int8, device=dev),
+           "steps": torch.empty(P, dtype=torch.int32, device=dev)}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.image_device(p, sigma, out, stream=torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    return out, time.perf_counter() - t0
+
+
+def errors(I_ex: np.ndarray, I_sur: np.ndarray, floor_rel: float = 1e-6) -> dict:
+    """Relative intensity errors over the pixels whose exact intensity is at
+    least floor_rel of the brightest judged pixel."""
+    I_ex = np.asarray(I_ex, dtype=np.float64)
+    I_sur = np.asarray(I_sur, dtype=np.float64)
+    top = float(I_ex.max()) if I_ex.size else 0.0
+    m = I_ex >= floor_rel * top if top > 0 else np.zeros(I_ex.shape, bool)
+    if not m.any():
+        return {"n": 0, "worst": 0.0, "p99": 0.0, "median": 0.0}
+    rel = np.abs(I_sur[m] - I_ex[m]) / I_ex[m]
+    return {"n": int(m.sum()), "worst": float(rel.max()), "p99": float(np.quantile(rel, 0.99)),
+            "median": float(np.median(rel))}
+
+
+def surrogate_point(ctx, sigma, sur, p, threshold: float, judge_frac: float, rng, buf=None) -> dict:
+    """One scan point: surrogate image, exact fallback, exact judge subset."""
+    torch = _torch()
+    P = int(p.nx) * int(p.ny)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = sur.image(p, sigma, threshold=threshold, per_bin=False, out=buf)
+    cnt = res["counters"].cpu().numpy()
+    if cnt[1]:
+        raise RuntimeError("surrogate inference kernel timed out")
+    t_inf = time.perf_counter() - t0
+    ids = np.sort(res["fallback_ids"][:int(cnt[0])].cpu().numpy()).astype(np.int32)
+    if ids.size:
+        ex = ctx.image(p, sigma, pixel_ids=ids, outputs=("tau", "P_surv", "I_obs"))
+        idx = torch.from_numpy(ids.astype(np.int64)).cuda()
+        for k in ("tau", "P_surv", "I_obs"):
+            res[k].index_copy_(0, idx, torch.from_numpy(ex[k]).cuda())
+    t_fb = time.perf_counter() - t0 - t_inf
+    jn = max(1, int(round(judge_frac * P)))
+    jids = np.sort(rng.choice(P, size=jn, replace=False)).astype(np.int32)
+    jex = ctx.image(p, sigma, pixel_ids=jids, outputs=("tau", "P_surv", "I_obs"))
+    torch.cuda.synchronize()
+    t_total = time.perf_counter() - t0
+    I_sur = res["I_obs"][torch.from_numpy(jids.astype(np.int64)).cuda()].cpu().numpy()
+    fb_mask = np.isin(jids, ids)
+    e_all = errors(jex["I_obs"], I_sur)
+    e_sur = errors(jex["I_obs"][~fb_mask], I_sur[~fb_mask])
+    return {"seconds": t_total, "inference_s": t_inf, "fallback_s": t_fb, "judge_s": t_total - t_inf - t_fb,
+            "fallback_pixels": int(ids.size), "fallback_frac": ids.size / P, "judged": int(jn),
+            "error": e_all, "error_surrogate_pixels": e_sur}
+
+
+def production_cam(rho0: float, theta_deg: float, side: int, n_bins: int):
+    return params(**W.production_point(nx=side, ny=side, rho0_gcm3=rho0, theta_obs_deg=theta_deg,
+                                       n_bins=n_bins))
+
+
+def train(ctx, sigma, cams, pixels_per_cam: int, members: int, epochs: int, seed: int, batch: int,
+          lr: float, val_frac: float = 0.1) -> tuple[object, dict]:
+    """Trace training samples on `cams`, hold out the last val_frac of the
+    cameras, train the ensemble; returns it with timing and validation RMS."""
+    torch = _torch()
+    n_val = max(1, int(round(val_frac * len(cams))))
+    raw, y, info = S.trace_samples(ctx, sigma, cams[:-n_val], pixels_per_cam, seed=seed)
+    vraw, vy, _ = S.trace_samples(ctx, sigma, cams[-n_val:], pixels_per_cam, seed=seed + 1,
+                                  i_floor=info["i_floor"])
+    sur = S.Surrogate(members=members, seed=seed)
+    t0 = time.perf_counter()
+    sur.fit(raw, y, epochs=epochs, batch=batch, lr=lr, floors=(S.TAU_FLOOR, info["i_floor"]))
+    torch.cuda.synchronize()
+    t_fit = time.perf_counter() - t0
+    pred = sur.forward(vraw).mean(0)
+    d = (pred - vy).double()
+    rms = torch.sqrt((d ** 2).mean(0)).cpu().numpy()
+    info.update(fit_s=t_fit, samples=int(raw.shape[0]), val_samples=int(vraw.shape[0]),
+                val_rms_ln_tau=float(rms[0]), val_rms_ln_I=float(rms[1]),
+                final_loss=[h[-1] for h in sur.history])
+    return sur, info
+
+
+def run_production(a) -> dict:
+    torch = _torch()
+    E, g2, s = W.synthetic_sigma_arrays()
+    sigma = SigmaTable.from_arrays(E, s, g2)
+    with Context(0) as ctx:
+        tpts = W.scan_points(a.train_points, seed=W.SEED + 17)
+        cams = [production_cam(r, t, a.train_side, a.bins) for r, t in tpts]
+        sur, info = train(ctx, sigma, cams, a.pixels_per_cam, a.members, a.epochs, W.SEED, a.batch, a.lr)
+        pts = W.scan_points(a.points, seed=W.SEED)
+        rng = np.random.default_rng(W.SEED + 5)
+        buf = S.alloc_image(a.side * a.side, a.bins, sur.device, per_bin=False)
+        rows = []
+        for r, t in pts:
+            rows.append(surrogate_point(ctx, sigma, sur, production_cam(r, t, a.side, a.bins), a.threshold,
+                                        a.judge, rng, buf))
+        del buf
+        plain = []
+        for r, t in pts[:a.plain_points]:
+            _, sec = plain_image(ctx, production_cam(r, t, a.side, a.bins), sigma)
+            plain.append(sec)
+            torch.cuda.empty_cache()
+    sur_total = sum(x["seconds"] for x in rows)
+    plain_per_point = float(np.mean(plain)) if plain else float("nan")
+    setup = info["trace_s"] + info["fit_s"]
+    return {
+        "workload": "production_scan", "points": a.points, "side": a.side, "bins": a.bins,
+        "members": a.members, "threshold": a.threshold, "judge_frac": a.judge,
+        "train": info,
+        "surrogate_s_per_point": sur_total / len(rows),
+        "plain_s_per_point": plain_per_point,
+        "speedup_scan": plain_per_point * len(rows) / (sur_total + setup),
+        "speedup_per_point": plain_per_point * len(rows) / sur_total,
+        "fallback_frac_mean": float(np.mean([x["fallback_frac"] for x in rows])),
+        "worst_pixel_error": max(x["error"]["worst"] for x in rows),
+        "p99_error_max": max(x["error"]["p99"] for x in rows),
+        "median_error_mean": float(np.mean([x["error"]["median"] for x in rows])),
+        "per_point": rows,
+    }
+
+
+def run_inference(a) -> dict:
+    torch = _torch()
+    E, g2, s = W.synthetic_sigma_arrays()
+    sigma = SigmaTable.from_arrays(E, s, g2)
+    with Context(0) as ctx:
+        cams = [params(**c) for c in W.surrogate_training_cams(a.train_points, side=a.train_side, n_bins=a.bins)]
+        sur, info = train(ctx, sigma, cams, a.pixels_per_cam, a.members, a.epochs, W.SEED, a.batch, a.lr)
+        p = params(**W.surrogate_inference_image(nx=a.side, ny=a.side, n_bins=a.bins))
+        row = surrogate_point(ctx, sigma, sur, p, a.threshold, a.judge, np.random.default_rng(W.SEED + 9))
+        _, sec = plain_image(ctx, p, sigma)
+        del torch
+    return {"workload": "surrogate_inference", "side": a.side, "bins": a.bins, "members": a.members,
+            "train": info, "surrogate": row, "plain_s": sec, "speedup": sec / row["seconds"]}
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("workload", choices=("production", "inference"))
+    ap.add_argument("--points", type=int, default=256)
+    ap.add_argument("--plain-points", type=int, default=2)
+    ap.add_argument("--side", type=int, default=None)
+    ap.add_argument("--bins", type=int, default=None)
+    ap.add_argument("--train-points", type=int, default=128)
+    ap.add_argument("--train-side", type=int, default=4096)
+    ap.add_argument("--pixels-per-cam", type=int, default=1024)
+    ap.add_argument("--members", type=int, default=4)
+    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--threshold", type=float, default=0.01)
+    ap.add_argument("--judge", type=float, default=0.01)
+    a = ap.parse_args(argv)
+    if a.workload == "production":
+        a.side = a.side or 4096
+        a.bins = a.bins or 64
+        out = run_production(a)
+    else:
+        a.side = a.side or 2048
+        a.bins = a.bins or 32
+        out = run_inference(a)
+    print(json.dumps(out, default=float))
+
+
+if __name__ == "__main__":
+    main()

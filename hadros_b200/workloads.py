@@ -114,3 +114,37 @@ def strided_pixels(nx: int, ny: int, k: int) -> np.ndarray:
     ii = np.arange(0, nx, k)
     jj = np.arange(0, ny, k)
     return (jj[:, None] * nx + ii[None, :]).ravel().astype(np.int32)
+
+
+def surrogate_training_cams(n_cams: int = 128, seed: int = SEED, side: int = 2048,
+                            n_bins: int = 32) -> list[dict]:
+    """Surrogate training cameras in the style of mixed_512 (funnel_wall source,
+    powerlaw_cutoff 1e5-1e12 GeV, mixed precision) on a side x side pixel grid,
+    with a ~ U[0, 0.998], cos(inclination) ~ U[cos 85, cos 5], profile ~ U over
+    all eight, rho0 log-uniform in [1e8, 1e12] (envelope 0.01 rho0), and the two
+    shape parameters r0 ~ U[6, 14] M and H/R ~ U[0.15, 0.45]."""
+    rng = np.random.default_rng(seed)
+    lo, hi = math.cos(math.radians(85.0)), math.cos(math.radians(5.0))
+    cams = []
+    for _ in range(n_cams):
+        rho0 = float(10.0 ** rng.uniform(8.0, 12.0))
+        cams.append(mixed_512(nx=side, ny=side, n_bins=n_bins, a_spin=float(rng.uniform(0.0, 0.998)),
+                              theta_obs_deg=math.degrees(math.acos(rng.uniform(lo, hi))),
+                              profile=int(rng.integers(0, 8)), rho0_gcm3=rho0, envelope_rho0_gcm3=0.01 * rho0,
+                              r0_rg=float(rng.uniform(6.0, 14.0)), H_over_R=float(rng.uniform(0.15, 0.45))))
+    return cams
+
+
+def surrogate_inference_image(**over) -> dict:
+    """The surrogate's inference image: mixed_512's camera and medium at
+    2048 x 2048 pixels and 32 bins."""
+    d = mixed_512(nx=2048, ny=2048, n_bins=32)
+    d.update(over)
+    return d
+
+
+def scan_points(n: int = 256, seed: int = SEED) -> list[tuple[float, float]]:
+    """Production-scan parameter points: (rho0 log-uniform in [1e9, 1e12],
+    inclination ~ U[10, 80] deg)."""
+    rng = np.random.default_rng(seed)
+    return [(float(10.0 ** rng.uniform(9.0, 12.0)), float(rng.uniform(10.0, 80.0))) for _ in range(n)]
