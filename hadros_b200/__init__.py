@@ -301,6 +301,40 @@ class Context:
             ob += Pc * Bc
         return per
 
+    def batch_pixels(self, cams: list, sigma: SigmaTable, pixel_lists: list, outputs=OUTPUTS) -> list[dict]:
+        """Pixel subsets of many cameras in one launch (hadros_batch_pixels):
+        camera c traces pixel_lists[c]; returns one dict per camera, rows in
+        list order."""
+        n = len(cams)
+        if len(pixel_lists) != n:
+            raise ValueError("one pixel list per camera")
+        arr = (HadrosParams * n)(*cams)
+        lists = [np.ascontiguousarray(ids, dtype=np.int32) for ids in pixel_lists]
+        counts = np.array([ids.size for ids in lists], dtype=np.int32)
+        ids = np.concatenate(lists) if lists else np.zeros(0, np.int32)
+        Bs = [n_bins_of(c) for c in cams]
+        P, PB = int(counts.sum()), int(sum(int(c) * b for c, b in zip(counts, Bs)))
+        fdt = np.float32 if cams[0].precision == PRECISION_MIXED else np.float64
+        shapes = {"tau": (P, np.float64), "P_surv": (P, np.float64), "I_obs": (P, np.float64),
+                  "fate": (P, np.int8), "steps": (P, np.int32), "attempts": (P, np.int32),
+                  "tau_E": (PB, fdt), "I_E": (PB, np.float64)}
+        res = {k: np.zeros(shapes[k][0], dtype=shapes[k][1]) for k in outputs}
+        out = HadrosImageOut()
+        for k, a in res.items():
+            setattr(out, k, a.ctypes.data)
+        _check(lib().hadros_batch_pixels(self.handle, C.addressof(arr), n, sigma.handle, ids.ctypes.data,
+                                         counts.ctypes.data, C.byref(out)))
+        per, o, ob = [], 0, 0
+        for Pc, Bc in zip(counts, Bs):
+            Pc = int(Pc)
+            d = {}
+            for k, a in res.items():
+                d[k] = a[ob:ob + Pc * Bc].reshape(Pc, Bc) if k in ("tau_E", "I_E") else a[o:o + Pc]
+            per.append(d)
+            o += Pc
+            ob += Pc * Bc
+        return per
+
     def trace_paths(self, p: HadrosParams, pixel_ids=None, max_points: int = 50000) -> dict:
         """Record every pixel's path points (r, theta, x, y, z, dl, redshift).
 

@@ -168,6 +168,8 @@ SIGNATURES = {
     "hadros_batch": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, P(HadrosImageOut)]),
     "hadros_batch_device": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
                                         P(HadrosImageOut), C.c_void_p]),
+    "hadros_batch_pixels": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, P(HadrosImageOut)]),
     "hadros_image_device_noalloc": (C.c_int32, [P(HadrosParams), C.c_void_p, P(HadrosImageOut),
                                                 C.c_void_p]),
     "hadros_schedule_default": (None, [P(HadrosSchedule)]),
@@ -220,5 +222,5 @@ SIGNATURES = {
     "hadros_mlp_pack_image": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "hadros_surrogate_image": (C.c_int32, [P(HadrosParams), C.c_void_p, C.c_int32, C.c_void_p,
                                            C.c_void_p, P(HadrosMlpNorm), C.c_int64, C.c_int64,
-                                           C.c_float, P(HadrosSurrogateOut), C.c_void_p]),
+                                           C.c_float, C.c_int32, P(HadrosSurrogateOut), C.c_void_p]),
 }

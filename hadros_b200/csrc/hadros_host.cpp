@@ -608,9 +608,11 @@ int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s
 
 // Many cameras in one persistent launch.  dev_out holds DEVICE pointers to
 // the concatenated outputs (camera order).
+// With `counts`, camera c traces counts[c] pixels whose ids (j*nx+i) follow
+// one another in the host array `pix` (outputs in list order).
 int32_t run_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, const hadros_sigma* s,
                   const hadros_image_out& dev_out, cudaStream_t st, bool time_kernel, int64_t* P_total,
-                  int64_t* PB_total)
+                  int64_t* PB_total, const int32_t* pix = nullptr, const int32_t* counts = nullptr)
 {
     if (!ctx) return fail(HADROS_E_STATE, "context is NULL");
     if (ctx->failed) return fail(HADROS_E_STATE, "context is in a failed state: " + ctx->err);
@@ -632,7 +634,14 @@ int32_t run_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, co
     for (int32_t c = 0; c < n_cams; ++c) {
         int32_t rc = build_cam(cams[c], s->h, dc[c], bins, err);
         if (rc) return fail(rc, "camera " + std::to_string(c) + ": " + err);
-        const int64_t P = static_cast<int64_t>(cams[c].nx) * cams[c].ny;
+        const int64_t full = static_cast<int64_t>(cams[c].nx) * cams[c].ny;
+        const int64_t P = counts ? counts[c] : full;
+        if (counts) {
+            if (P < 0) return fail(HADROS_E_ARG, "camera " + std::to_string(c) + ": negative pixel count");
+            for (int64_t k = 0; k < P; ++k)
+                if (pix[items + k] < 0 || pix[items + k] >= full)
+                    return fail(HADROS_E_ARG, "camera " + std::to_string(c) + ": pixel id outside the image");
+        }
         dc[c].item_begin = items;
         dc[c].item_end = items + P;
         dc[c].out_offset = items;
@@ -653,6 +662,14 @@ int32_t run_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, co
         (e = cudaMemcpyAsync(ctx->d_bins, bins.data(), sizeof(DevBin) * bins.size(), cudaMemcpyHostToDevice, st)) !=
             cudaSuccess)
         return cuda_fail(ctx, e, "camera upload");
+    const int32_t* d_pix = nullptr;
+    if (counts && items > 0) {
+        if ((rc = grow(ctx, &ctx->d_pix, &ctx->pix_cap, sizeof(int32_t) * items, "pixel list"))) return rc;
+        if ((e = cudaMemcpyAsync(ctx->d_pix, pix, sizeof(int32_t) * items, cudaMemcpyHostToDevice, st)) !=
+            cudaSuccess)
+            return cuda_fail(ctx, e, "pixel list upload");
+        d_pix = static_cast<const int32_t*>(ctx->d_pix);
+    }
     if ((e = cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(unsigned long long), st)) != cudaSuccess)
         return cuda_fail(ctx, e, "counter reset");
     TraceArgs A{};
@@ -660,7 +677,7 @@ int32_t run_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, co
     A.n_cams = n_cams;
     A.max_bins = max_bins;
     A.total_items = items;
-    A.pixel_ids = nullptr;
+    A.pixel_ids = d_pix;
     A.bins = static_cast<const DevBin*>(ctx->d_bins);
     A.sig = ctx->sig_dev;
     A.tau = dev_out.tau;
@@ -688,7 +705,8 @@ int32_t run_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, co
     ctx->stats.rays = items;
     ctx->stats.launches = items > 0 ? 1 : 0;
     ctx->stats.h2d_bytes = static_cast<int64_t>(sizeof(DevCam) * dc.size() + sizeof(DevBin) * bins.size()) +
-                           (sigma_new ? static_cast<int64_t>(ctx->sig_cap) : 0);
+                           (sigma_new ? static_cast<int64_t>(ctx->sig_cap) : 0) +
+                           (counts ? static_cast<int64_t>(sizeof(int32_t)) * items : 0);
     ctx->stats.d2h_bytes = 0;
     return HADROS_OK;
 }
@@ -817,8 +835,9 @@ int32_t hadros_batch_device(hadros_ctx* ctx, const hadros_params* cams, int32_t 
     }
 }
 
-int32_t hadros_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, const hadros_sigma* s,
-                     const hadros_image_out* out)
+namespace {
+int32_t batch_host(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, const hadros_sigma* s,
+                   const hadros_image_out* out, const int32_t* pix, const int32_t* counts)
 {
     if (!ctx) return fail(HADROS_E_STATE, "context is NULL");
     if (!out || !cams || n_cams <= 0) return fail(HADROS_E_ARG, "NULL argument or empty camera list");
@@ -827,7 +846,7 @@ int32_t hadros_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams,
         int64_t P = 0, PB = 0;
         for (int32_t c = 0; c < n_cams; ++c) {
             if (hadros_params_validate(&cams[c])) return fail(HADROS_E_ARG, "camera " + std::to_string(c) + ": " + g_last_error);
-            const int64_t pc = static_cast<int64_t>(cams[c].nx) * cams[c].ny;
+            const int64_t pc = counts ? std::max<int64_t>(counts[c], 0) : static_cast<int64_t>(cams[c].nx) * cams[c].ny;
             P += pc;
             PB += pc * (cams[c].spectral_kind == HADROS_SPECTRAL_MONOCHROMATIC ? 1 : std::max(cams[c].n_bins, 1));
         }
@@ -855,7 +874,7 @@ int32_t hadros_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams,
         d.tau_E = out->tau_E ? static_cast<void*>(base + o_tE) : nullptr;
         d.I_E = out->I_E ? static_cast<void*>(base + o_IE) : nullptr;
         int64_t P2 = 0, PB2 = 0;
-        rc = run_batch(ctx, cams, n_cams, s, d, ctx->stream, true, &P2, &PB2);
+        rc = run_batch(ctx, cams, n_cams, s, d, ctx->stream, true, &P2, &PB2, pix, counts);
         if (rc) return rc;
         struct Cp { void* h; const void* d; size_t n; } cps[8] = {
             {out->tau, d.tau, 8 * size_t(P)}, {out->P_surv, d.P_surv, 8 * size_t(P)},
@@ -876,6 +895,20 @@ int32_t hadros_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams,
     } catch (const std::exception& ex) {
         return fail(HADROS_E_NOMEM, ex.what());
     }
+}
+}  // namespace
+
+int32_t hadros_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, const hadros_sigma* s,
+                     const hadros_image_out* out)
+{
+    return batch_host(ctx, cams, n_cams, s, out, nullptr, nullptr);
+}
+
+int32_t hadros_batch_pixels(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, const hadros_sigma* s,
+                            const int32_t* pixel_ids, const int32_t* counts, const hadros_image_out* out)
+{
+    if (!pixel_ids || !counts) return fail(HADROS_E_ARG, "pixel list or counts is NULL");
+    return batch_host(ctx, cams, n_cams, s, out, pixel_ids, counts);
 }
 
 int32_t hadros_trace_paths(hadros_ctx* ctx, const hadros_params* p, const int32_t* pixel_ids, int32_t n_pixels,

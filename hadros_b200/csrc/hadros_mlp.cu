@@ -233,9 +233,10 @@ __global__ void k_pack(const float* __restrict__ master, bf16* __restrict__ pack
     const long idx = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= kPacked) return;
     float v;
-    if (idx < kPW2) {
+    if (idx < kPW2) {   // [hi 16 | lo 16 | Fourier 32] <- master [16 | 32]
         const long o = idx / kIn, c = idx % kIn;
-        v = master[kOffW1 + o * kF + (c % kF)];
+        const long j = c < 2 * kF ? c % kF : c - kF;
+        v = master[kOffW1 + o * kW1In + j];
     } else if (idx < kPW5) {
         const long r = idx - kPW2;
         const int l = 2 + int(r / (long(kW) * kW));
@@ -249,15 +250,16 @@ __global__ void k_pack(const float* __restrict__ master, bf16* __restrict__ pack
 
 __global__ void k_featurize(const float* __restrict__ raw, long n, Norm nm, bf16* __restrict__ X)
 {
-    const long idx = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (idx >= n * kF) return;
-    const long s = idx / kF;
-    const int j = int(idx % kF);
-    const float x = (raw[idx] - nm.feat_mu[j]) * nm.feat_inv_sd[j];
-    bf16 hi, lo;
-    split_hi_lo(x, hi, lo);
-    X[s * kIn + j] = hi;
-    X[s * kIn + kF + j] = lo;
+    const long s = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    float xn[kF];
+#pragma unroll
+    for (int j = 0; j < kF; ++j) xn[j] = (raw[s * kF + j] - nm.feat_mu[j]) * nm.feat_inv_sd[j];
+    bf16 row[kIn];
+    input_row(xn, row);
+#pragma unroll
+    for (int q = 0; q < kIn / 8; ++q)
+        reinterpret_cast<uint4*>(X + s * kIn)[q] = reinterpret_cast<const uint4*>(row)[q];
 }
 
 // out[s][o] = W5[o] . H4[s] + b5[o] + Ws[o] . x[s]   (one warp per sample)
@@ -361,13 +363,14 @@ __global__ void __launch_bounds__(kW) k_bias_grad(const bf16* __restrict__ dZ, l
     atomicAdd(Gb + i, g);
 }
 
-// Tied hi/lo first-layer weights: G_W1[o][j] += dW[o][j] + dW[o][j+16].
+// Tied hi/lo first-layer weights: G_W1[o][j] += dW[o][j] + dW[o][j+16] for
+// the features, G_W1[o][16+q] += dW[o][32+q] for the Fourier columns.
 __global__ void k_fold_w1(const float* __restrict__ dW1, float* __restrict__ G)
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= kW * kF) return;
-    const int o = idx / kF, j = idx % kF;
-    G[kOffW1 + idx] += dW1[o * kIn + j] + dW1[o * kIn + kF + j];
+    if (idx >= kW * kW1In) return;
+    const int o = idx / kW1In, j = idx % kW1In;
+    G[kOffW1 + idx] += j < kF ? dW1[o * kIn + j] + dW1[o * kIn + kF + j] : dW1[o * kIn + kF + j];
 }
 
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
@@ -447,7 +450,7 @@ void backward_impl(const bf16* packed, const bf16* X, long n, const float* dout,
     cudaMemsetAsync(w.dW1, 0, sizeof(float) * kW * kIn, st);
     gemm<false, false>(dZ, kW, X, kIn, kW, kIn, M, wsplits, EpiWgrad{w.dW1, kIn}, st);
     k_bias_grad<<<blocks_for(n, chunk), kW, 0, st>>>(dZ, n, chunk, G + off_b(1));
-    k_fold_w1<<<blocks_for(kW * kF, 256), 256, 0, st>>>(w.dW1, G);
+    k_fold_w1<<<blocks_for(kW * kW1In, 256), 256, 0, st>>>(w.dW1, G);
 }
 
 Norm to_norm(const hadros_mlp_norm& a)
@@ -502,7 +505,7 @@ int32_t hadros_mlp_featurize(const float* raw, int64_t n, const hadros_mlp_norm*
     if (!raw || !norm || !X || n < 0) return set_error(HADROS_E_ARG, "bad argument");
     if (n == 0) return HADROS_OK;
     auto st = static_cast<cudaStream_t>(stream);
-    k_featurize<<<blocks_for(n * kF, 256), 256, 0, st>>>(raw, n, to_norm(*norm), static_cast<bf16*>(X));
+    k_featurize<<<blocks_for(n, 256), 256, 0, st>>>(raw, n, to_norm(*norm), static_cast<bf16*>(X));
     return cuda_status("hadros_mlp_featurize");
 }
 

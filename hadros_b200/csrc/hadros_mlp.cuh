@@ -10,7 +10,10 @@
 // Each normalized feature x enters as two BF16 columns, hi = bf16(x) and
 // lo = bf16(x - hi), with tied first-layer weights, so the network sees x to
 // ~16 bits (a pixel of a 4096-wide image) although its operands are BF16.
-// Network: 32 -> 256 -> 256 -> 256 -> 256 (SiLU) -> 2, BF16 weights and
+// The normalized screen coordinates also enter as Fourier features
+// sin(pi 2^(k-1) x), cos(pi 2^(k-1) x), k = 0..7, so the first layer can
+// resolve image structure down to ~1/100 of the field of view.
+// Network: 64 -> 256 -> 256 -> 256 -> 256 (SiLU) -> 2, BF16 weights and
 // activations, FP32 accumulation, FP32 biases, plus an FP32 linear skip from
 // the 16 normalized features (x = hi + lo) to the 2 outputs.
 #pragma once
@@ -25,18 +28,21 @@ namespace hadros {
 namespace mlp {
 
 constexpr int kF = 16;      // raw features
-constexpr int kIn = 32;     // BF16 input columns (hi, lo)
+constexpr int kFreq = 8;    // Fourier frequencies per screen coordinate
+constexpr int kFour = 4 * kFreq;   // sin and cos of alpha and beta
+constexpr int kW1In = kF + kFour;  // master first-layer inputs (hi/lo tied)
+constexpr int kIn = 2 * kF + kFour;   // BF16 input columns: hi, lo, Fourier
 constexpr int kW = 256;     // hidden width
 constexpr int kDepth = 4;   // hidden layers
 constexpr int kOut = 2;     // ln tau_E, ln I_E (standardized)
 constexpr int kOutPad = 16; // rows of the packed last-layer matrix
 
 // FP32 master parameters (what Adam updates), one network:
-//   W1 [256][16] (tied hi/lo weights), b1 [256],
+//   W1 [256][48] (16 tied hi/lo columns, 32 Fourier columns), b1 [256],
 //   W_l [256][256], b_l [256] for l = 2..4,
 //   W5 [2][256], b5 [2], Ws [2][16] (linear skip).
 constexpr long kOffW1 = 0;
-constexpr long kOffB1 = kOffW1 + long(kW) * kF;
+constexpr long kOffB1 = kOffW1 + long(kW) * kW1In;
 constexpr long kOffW2 = kOffB1 + kW;
 constexpr long kHidStride = long(kW) * kW + kW;   // W_l then b_l
 constexpr long kOffW5 = kOffW2 + 3 * kHidStride;
@@ -55,7 +61,8 @@ __host__ __device__ constexpr long off_b(int layer)   // layer 1..4 bias
 }
 
 // Row-major BF16 working copy (training kernels and tests):
-//   W1 [256][32] (the 16 master columns twice), W2..W4 [256][256],
+//   W1 [256][64] (the 16 feature columns twice, then the 32 Fourier
+//   columns), W2..W4 [256][256],
 //   W5 [16][256] (rows 0..1 from the master, rows 2..15 zero).
 constexpr long kPW1 = 0;
 constexpr long kPW2 = kPW1 + long(kW) * kIn;
@@ -68,8 +75,10 @@ __host__ __device__ constexpr long pw(int layer)       // layer 1..5
 }
 
 // Training workspace (bytes) for a batch of n samples: Z1..Z4, H1..H4,
-// two dZ buffers (BF16 [n][256] each) and the [256][32] FP32 layer-1 weight
+// two dZ buffers (BF16 [n][256] each) and the [256][kIn] FP32 layer-1 weight
 // gradient before the hi/lo columns are folded.
+// The input row X [kIn] = hi[16], lo[16], then for each screen coordinate
+// (alpha, beta) sin and cos of its kFreq frequencies.
 constexpr long kWsAlign = 256;
 __host__ __device__ constexpr long ws_act_bytes(long n) { return n * kW * 2; }
 __host__ __device__ constexpr long ws_bytes(long n) { return 10 * ws_act_bytes(n) + long(kW) * kIn * 4 + kWsAlign; }
@@ -111,6 +120,39 @@ __device__ __forceinline__ float2 unpack_bf16x2(uint32_t u)
 {
     const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162*>(&u);
     return __bfloat1622float2(v);
+}
+
+// Fourier features of a normalized screen coordinate x: out[2k] =
+// sin(pi t), out[2k+1] = cos(pi t), t = 2^(k-1) x reduced to [-1, 1].
+__device__ __forceinline__ void fourier(float x, float* out)
+{
+#pragma unroll
+    for (int k = 0; k < kFreq; ++k) {
+        const float t = x * float(1 << k) * 0.5f;
+        const float r = t - 2.0f * rintf(0.5f * t);
+        float sn, cs;
+        __sincosf(3.14159265358979f * r, &sn, &cs);
+        out[2 * k] = sn;
+        out[2 * k + 1] = cs;
+    }
+}
+
+// One input row of kIn BF16 values from the 16 normalized features.
+__device__ __forceinline__ void input_row(const float* xn, __nv_bfloat16* row)
+{
+#pragma unroll
+    for (int j = 0; j < kF; ++j) {
+        const __nv_bfloat16 hi = __float2bfloat16_rn(xn[j]);
+        row[j] = hi;
+        row[kF + j] = __float2bfloat16_rn(xn[j] - __bfloat162float(hi));
+    }
+    float f[2 * kFreq];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        fourier(xn[c], f);
+#pragma unroll
+        for (int q = 0; q < 2 * kFreq; ++q) row[2 * kF + c * 2 * kFreq + q] = __float2bfloat16_rn(f[q]);
+    }
 }
 
 // Normalized feature x split into (hi, lo) BF16 parts.

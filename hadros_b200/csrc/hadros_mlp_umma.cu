@@ -60,6 +60,8 @@ struct SurCam {
     float log10E[kMaxBinsS];
     float ln_dE[kMaxBinsS];   // -inf for bins outside the aggregates
     float w[kMaxBinsS];       // aggregation weight (0 outside)
+    float ln_sw[kMaxBinsS];   // spread: log-sum-exp over bins of out + ln_sw
+    int32_t spread_out;       // 0: ln I_E (ln_sw = ln dE), 1: ln tau_E (ln w / sum w)
 };
 
 // The 16 raw features of sample (pixel, bin): the single definition used for
@@ -111,11 +113,8 @@ __global__ void k_pack_image(const bf16* __restrict__ packed, uint8_t* __restric
         row = in / 128;                       // 0..255 = output unit n
         unit = (in % 128) / 16;               // physical unit
         const int kunit = unit ^ (row & 7);   // logical 16-byte unit
-        if (q == 0) {                         // W1 [256][32], K columns 32..63 zero
-            if (kunit < 4)
-                for (int t = 0; t < 8; ++t) e[t] = packed[pw(1) + long(row) * kIn + kunit * 8 + t];
-            else
-                for (int t = 0; t < 8; ++t) e[t] = __float2bfloat16_rn(0.0f);
+        if (q == 0) {                         // W1 [256][64]
+            for (int t = 0; t < 8; ++t) e[t] = packed[pw(1) + long(row) * kIn + kunit * 8 + t];
         } else {
             l = 2 + (q - 1) / 4;
             c = (q - 1) % 4;
@@ -353,8 +352,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                             for (int t = 0; t < kPair; ++t) {
                                 const uint32_t ab = saddr(act + t * kActBytes);
                                 const uint32_t d = tmem + uint32_t(t * 256);
-                                if (L == 1) {          // K = 32 from chunk 0
-                                    for (int kk = 0; kk < 2; ++kk)
+                                if (L == 1) {          // K = 64 from chunk 0
+                                    for (int kk = 0; kk < 4; ++kk)
                                         tc_mma(d, sdesc(ab + kk * 32), sdesc(sb + kk * 32), id256, kk > 0);
                                 } else if (L == 5) {   // N = 16, K = 256 over 4 chunks of the stage
                                     for (int cc = 0; cc < 4; ++cc)
@@ -388,30 +387,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
             const long lp = valid ? s / B : 0;
             const int b = valid ? int(s % B) : 0;
             float x[kF];
-            uint32_t feat[16];
+            uint32_t feat[kIn / 2];
             {
-                float f[kF];
+                float f[kF], xn[kF];
                 raw_features(A.cam, A.pixel_begin + lp, b, f);
-                bf16 hi[kF], lo[kF];
 #pragma unroll
-                for (int q = 0; q < kF; ++q) {
-                    const float xn = valid ? (f[q] - A.norm.feat_mu[q]) * A.norm.feat_inv_sd[q] : 0.0f;
-                    split_hi_lo(xn, hi[q], lo[q]);
-                    x[q] = __bfloat162float(hi[q]) + __bfloat162float(lo[q]);
-                }
+                for (int q = 0; q < kF; ++q) xn[q] = valid ? (f[q] - A.norm.feat_mu[q]) * A.norm.feat_inv_sd[q] : 0.0f;
+                __align__(16) bf16 row[kIn];
+                input_row(xn, row);
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    feat[q] = pack_bf16x2(__bfloat162float(hi[2 * q]), __bfloat162float(hi[2 * q + 1]));
-                    feat[8 + q] = pack_bf16x2(__bfloat162float(lo[2 * q]), __bfloat162float(lo[2 * q + 1]));
-                }
+                for (int q = 0; q < kF; ++q) x[q] = __bfloat162float(row[q]) + __bfloat162float(row[kF + q]);
+#pragma unroll
+                for (int q = 0; q < kIn / 2; ++q) feat[q] = reinterpret_cast<const uint32_t*>(row)[q];
             }
             float sum_tau = 0.0f, sum_lnI = 0.0f;
             float w_ref = 0.0f, w_s1 = 0.0f, w_s2 = 0.0f;   // pixel leader: shifted sums of ln I_k
             for (int k = 0; k < K; ++k) {
                 const float* P = A.masters + long(k) * kParams;
-                // features -> chunk 0, 16-byte units 0..3 of row r
+                // features -> chunk 0, the 8 16-byte units of row r
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
+                for (int u = 0; u < kIn / 8; ++u)
                     *reinterpret_cast<uint4*>(my_act + r * 128 + ((u ^ (r & 7)) << 4)) =
                         make_uint4(feat[4 * u], feat[4 * u + 1], feat[4 * u + 2], feat[4 * u + 3]);
                 fence_async_smem();
@@ -463,8 +458,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                 const float lnI = fmaf(a1, A.norm.out_sd[1], A.norm.out_mu[1]);
                 sum_tau += ltau;
                 sum_lnI += lnI;
-                // this member's ln I_obs per pixel: log-sum-exp over the pixel's bins
-                red_a[trow] = valid ? lnI + A.cam.ln_dE[b] : -INFINITY;
+                // this member's ln I_obs (or ln tau) per pixel: log-sum-exp over the bins
+                red_a[trow] = valid ? (A.cam.spread_out ? ltau : lnI) + A.cam.ln_sw[b] : -INFINITY;
                 if (!epi_sync()) goto done;
                 if (leader_possible && valid) {
                     float m = -INFINITY;
@@ -543,7 +538,7 @@ int32_t cuda_status(const char* what)
 }
 
 // Camera constants and bins of a surrogate image from the tracer's params.
-int32_t make_surcam(const hadros_params* p, const hadros_sigma* s, SurCam* c)
+int32_t make_surcam(const hadros_params* p, const hadros_sigma* s, SurCam* c, int32_t spread_out = 0)
 {
     if (int32_t rc = hadros_params_validate(p)) return rc;
     const int B = p->spectral_kind == HADROS_SPECTRAL_MONOCHROMATIC ? 1 : p->n_bins;
@@ -568,11 +563,19 @@ int32_t make_surcam(const hadros_params* p, const hadros_sigma* s, SurCam* c)
     c->log_rho0 = float(std::log10(p->rho0_gcm3));
     c->r0 = float(p->r0_rg);
     c->h_over_r = float(p->H_over_R);
+    double wsum = 0.0;
     for (int b = 0; b < nb; ++b) {
         c->log10E[b] = E[b] > 0.0 ? float(std::log10(E[b])) : 0.0f;
         const bool in = valid[b] != 0 && dE[b] > 0.0;
         c->ln_dE[b] = in ? float(std::log(dE[b])) : -INFINITY;
         c->w[b] = in ? float(w[b]) : 0.0f;
+        if (in && w[b] > 0.0) wsum += w[b];
+    }
+    c->spread_out = spread_out;
+    for (int b = 0; b < nb; ++b) {
+        const bool in = valid[b] != 0 && dE[b] > 0.0;
+        if (spread_out == 0) c->ln_sw[b] = c->ln_dE[b];
+        else c->ln_sw[b] = (in && w[b] > 0.0 && wsum > 0.0) ? float(std::log(w[b] / wsum)) : -INFINITY;
     }
     return HADROS_OK;
 }
@@ -613,7 +616,7 @@ int32_t hadros_mlp_raw_features(const hadros_params* p, const hadros_sigma* s, c
 int32_t hadros_surrogate_image(const hadros_params* p, const hadros_sigma* s, int32_t n_members,
                                const float* masters, const void* images, const hadros_mlp_norm* norm,
                                int64_t pixel_begin, int64_t pixel_end, float spread_threshold,
-                               const hadros_surrogate_out* out, void* stream)
+                               int32_t spread_of, const hadros_surrogate_out* out, void* stream)
 {
     if (!p || !s || !masters || !images || !norm || !out || !out->tau || !out->P_surv || !out->I_obs ||
         !out->spread || !out->fallback_ids || !out->counters)
@@ -621,8 +624,9 @@ int32_t hadros_surrogate_image(const hadros_params* p, const hadros_sigma* s, in
     if (n_members < 1 || n_members > kMaxMembers)
         return set_error(HADROS_E_ARG, "n_members must be in 1.." + std::to_string(kMaxMembers));
     if (reinterpret_cast<uintptr_t>(images) % 16 != 0) return set_error(HADROS_E_ARG, "images must be 16-byte aligned");
+    if (spread_of != 0 && spread_of != 1) return set_error(HADROS_E_ARG, "spread_of must be 0 (ln I_obs) or 1 (ln tau)");
     InferArgs a{};
-    if (int32_t rc = make_surcam(p, s, &a.cam)) return rc;
+    if (int32_t rc = make_surcam(p, s, &a.cam, spread_of)) return rc;
     const long P = long(p->nx) * p->ny;
     if (pixel_begin < 0 || pixel_end > P || pixel_end < pixel_begin)
         return set_error(HADROS_E_ARG, "pixel range outside the image");

@@ -535,7 +535,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                 bins = A.bins + cam->bin_offset;
                 B = cam->n_bins;
                 local = item - cam->item_begin;
-                const long long pid = A.pixel_ids ? static_cast<long long>(A.pixel_ids[local])
+                const long long pid = A.pixel_ids ? static_cast<long long>(A.pixel_ids[item])
                                       : (A.order ? static_cast<long long>(A.order[item]) : local);
                 row = A.order ? pid : local;   // output row within the camera
                 const int nx = cam->nx;

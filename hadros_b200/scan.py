@@ -54,8 +54,8 @@ def plain_image(ctx, p, sigma) -> tuple[dict, float]:
 
 
 def errors(I_ex: np.ndarray, I_sur: np.ndarray, floor_rel: float = 1e-6) -> dict:
-    """Relative intensity errors over the pixels whose exact intensity is at
-    least floor_rel of the brightest judged pixel."""
+    """Relative errors over the pixels whose exact value is at least floor_rel
+    of the largest judged value (intensity, or optical depth)."""
     I_ex = np.asarray(I_ex, dtype=np.float64)
     I_sur = np.asarray(I_sur, dtype=np.float64)
     top = float(I_ex.max()) if I_ex.size else 0.0
@@ -67,13 +67,14 @@ def errors(I_ex: np.ndarray, I_sur: np.ndarray, floor_rel: float = 1e-6) -> dict
             "median": float(np.median(rel))}
 
 
-def surrogate_point(ctx, sigma, sur, p, threshold: float, judge_frac: float, rng, buf=None) -> dict:
+def surrogate_point(ctx, sigma, sur, p, threshold: float, judge_frac: float, rng, buf=None,
+                    spread_of: int = 0) -> dict:
     """One scan point: surrogate image, exact fallback, exact judge subset."""
     torch = _torch()
     P = int(p.nx) * int(p.ny)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    res = sur.image(p, sigma, threshold=threshold, per_bin=False, out=buf)
+    res = sur.image(p, sigma, threshold=threshold, per_bin=False, out=buf, spread_of=spread_of)
     cnt = res["counters"].cpu().numpy()
     if cnt[1]:
         raise RuntimeError("surrogate inference kernel timed out")
@@ -90,13 +91,16 @@ def surrogate_point(ctx, sigma, sur, p, threshold: float, judge_frac: float, rng
     jex = ctx.image(p, sigma, pixel_ids=jids, outputs=("tau", "P_surv", "I_obs"))
     torch.cuda.synchronize()
     t_total = time.perf_counter() - t0
-    I_sur = res["I_obs"][torch.from_numpy(jids.astype(np.int64)).cuda()].cpu().numpy()
+    jt = torch.from_numpy(jids.astype(np.int64)).cuda()
+    sur_v = {k: res[k][jt].cpu().numpy() for k in ("I_obs", "tau", "P_surv")}
     fb_mask = np.isin(jids, ids)
-    e_all = errors(jex["I_obs"], I_sur)
-    e_sur = errors(jex["I_obs"][~fb_mask], I_sur[~fb_mask])
+    key = "I_obs" if spread_of == 0 else "tau"
     return {"seconds": t_total, "inference_s": t_inf, "fallback_s": t_fb, "judge_s": t_total - t_inf - t_fb,
             "fallback_pixels": int(ids.size), "fallback_frac": ids.size / P, "judged": int(jn),
-            "error": e_all, "error_surrogate_pixels": e_sur}
+            "judged_quantity": key,
+            "error": errors(jex[key], sur_v[key]),
+            "error_surrogate_pixels": errors(jex[key][~fb_mask], sur_v[key][~fb_mask]),
+            "P_surv_max_abs_error": float(np.abs(jex["P_surv"] - sur_v["P_surv"]).max())}
 
 
 def production_cam(rho0: float, theta_deg: float, side: int, n_bins: int):
@@ -175,7 +179,8 @@ def run_inference(a) -> dict:
         cams = [params(**c) for c in W.surrogate_training_cams(a.train_points, side=a.train_side, n_bins=a.bins)]
         sur, info = train(ctx, sigma, cams, a.pixels_per_cam, a.members, a.epochs, W.SEED, a.batch, a.lr)
         p = params(**W.surrogate_inference_image(nx=a.side, ny=a.side, n_bins=a.bins))
-        row = surrogate_point(ctx, sigma, sur, p, a.threshold, a.judge, np.random.default_rng(W.SEED + 9))
+        row = surrogate_point(ctx, sigma, sur, p, a.threshold, a.judge, np.random.default_rng(W.SEED + 9),
+                              spread_of=1)
         _, sec = plain_image(ctx, p, sigma)
         del torch
     return {"workload": "surrogate_inference", "side": a.side, "bins": a.bins, "members": a.members,

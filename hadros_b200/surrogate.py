@@ -27,6 +27,7 @@ from . import HadrosError, _check, abi, lib, n_bins_of
 from .abi import HadrosAdam, HadrosMlpNorm, HadrosSurrogateOut
 
 N_FEATURES = 16
+N_INPUT = 64                      # BF16 input columns: hi, lo, Fourier features
 N_OUT = 2
 PROFILE_FEATURES = range(5, 13)   # one-hot torus profile kind
 TAU_FLOOR = 1.0e-6                # ln(tau_E + floor): tau below it is transparent
@@ -56,7 +57,7 @@ def init_master(seed: int) -> np.ndarray:
     off = layout()
     rng = np.random.default_rng(seed)
     m = np.zeros(n, dtype=np.float32)
-    for name, fan_in in (("W1", 2 * N_FEATURES), ("W2", 256), ("W3", 256), ("W4", 256), ("W5", 256)):
+    for name, fan_in in (("W1", N_INPUT), ("W2", 256), ("W3", 256), ("W4", 256), ("W5", 256)):
         a, b = off[name]
         lim = math.sqrt(6.0 / fan_in) * (0.1 if name == "W5" else 1.0)
         m[a:b] = rng.uniform(-lim, lim, b - a)
@@ -138,7 +139,7 @@ class Surrogate:
     # ---- features -----------------------------------------------------------
     def featurize(self, raw, stream=None):
         torch = _torch()
-        X = torch.empty((raw.shape[0], 2 * N_FEATURES), dtype=torch.bfloat16, device=self.device)
+        X = torch.empty((raw.shape[0], N_INPUT), dtype=torch.bfloat16, device=self.device)
         _check(lib().hadros_mlp_featurize(_vp(raw), int(raw.shape[0]), C.byref(self.norm), _vp(X),
                                           _stream_ptr(stream)))
         return X
@@ -232,10 +233,11 @@ class Surrogate:
         return self._masters, self._images
 
     def image(self, p, sigma, pixel_begin: int = 0, pixel_end: int | None = None, threshold: float = 0.01,
-              per_bin: bool = True, stream=None, out: dict | None = None) -> dict:
+              per_bin: bool = True, stream=None, out: dict | None = None, spread_of: int = 0) -> dict:
         """Surrogate image of pixels [pixel_begin, pixel_end) on the GPU.  Returns
         device tensors (ln_tau_E, ln_I_E per bin when per_bin; tau, P_surv, I_obs,
-        spread per pixel; fallback_ids, counters) without synchronizing."""
+        spread per pixel; fallback_ids, counters) without synchronizing.  The
+        spread is over ln I_obs (spread_of 0) or ln tau (spread_of 1)."""
         torch = _torch()
         P = int(p.nx) * int(p.ny)
         pe = P if pixel_end is None else int(pixel_end)
@@ -249,14 +251,14 @@ class Surrogate:
             setattr(o, key, None if t is None else t.data_ptr())
         _check(lib().hadros_surrogate_image(C.byref(p), sigma.handle, len(self.nets), _vp(masters), _vp(images),
                                             C.byref(self.norm), int(pixel_begin), pe, float(threshold),
-                                            C.byref(o), _stream_ptr(stream)))
+                                            int(spread_of), C.byref(o), _stream_ptr(stream)))
         return out
 
-    def image_with_fallback(self, ctx, p, sigma, threshold: float = 0.01, per_bin: bool = False) -> dict:
+    def image_with_fallback(self, ctx, p, sigma, threshold: float = 0.01, spread_of: int = 0) -> dict:
         """Surrogate image whose flagged pixels are replaced by the exact tracer.
         Host numpy arrays; 'fallback' holds the traced pixel ids."""
         torch = _torch()
-        res = self.image(p, sigma, threshold=threshold, per_bin=per_bin)
+        res = self.image(p, sigma, threshold=threshold, per_bin=False, spread_of=spread_of)
         torch.cuda.synchronize(self.device)
         cnt = res["counters"].cpu().numpy()
         if cnt[1]:
@@ -327,21 +329,26 @@ def targets_of(tau_E, I_E, i_floor: float):
 
 
 def trace_samples(ctx, sigma, cams, pixels_per_cam: int, seed: int = 20261203, device=0,
-                  i_floor: float | None = None):
+                  i_floor: float | None = None, chunk: int = 64):
     """Training samples traced by the exact tracer: for each camera a seeded
-    random pixel subset, all of its bins.  Returns (raw [n][16], ln targets
-    [n][2]) as device tensors and a dict with the floor and tracing time."""
+    random pixel subset, all of its bins, `chunk` cameras per launch
+    (hadros_batch_pixels).  Returns (raw [n][16], ln targets [n][2]) as device
+    tensors and a dict with the floor and tracing time."""
     torch = _torch()
     rng = np.random.default_rng(seed)
     raws, taus, Is = [], [], []
     t0 = time.perf_counter()
-    for p in cams:
-        P = int(p.nx) * int(p.ny)
-        ids = np.sort(rng.choice(P, size=min(pixels_per_cam, P), replace=False)).astype(np.int32)
-        r = ctx.image(p, sigma, pixel_ids=ids, outputs=("tau_E", "I_E"))
-        taus.append(r["tau_E"].reshape(-1))
-        Is.append(r["I_E"].reshape(-1))
-        raws.append(raw_features(p, sigma, ids, device))
+    for a in range(0, len(cams), chunk):
+        part = cams[a:a + chunk]
+        lists = []
+        for p in part:
+            P = int(p.nx) * int(p.ny)
+            lists.append(np.sort(rng.choice(P, size=min(pixels_per_cam, P), replace=False)).astype(np.int32))
+        res = ctx.batch_pixels(part, sigma, lists, outputs=("tau_E", "I_E"))
+        for p, ids, r in zip(part, lists, res):
+            taus.append(r["tau_E"].reshape(-1))
+            Is.append(r["I_E"].reshape(-1))
+            raws.append(raw_features(p, sigma, ids, device))
     torch.cuda.synchronize(device)
     t_trace = time.perf_counter() - t0
     tau = np.concatenate(taus)

@@ -294,6 +294,13 @@ int32_t hadros_image_device(hadros_ctx* ctx, const hadros_params* p,
  * parameter point by the scan drivers (scripts/run_robustness_scans.py:81-145). */
 int32_t hadros_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams,
                      const hadros_sigma* s, const hadros_image_out* out);
+/* Pixel subsets of many cameras in one launch: camera c traces counts[c]
+ * pixels whose ids (j*nx+i) follow one another in pixel_ids (host arrays);
+ * outputs in list order, concatenated as hadros_batch's.  The random pixel
+ * subsets the surrogate is trained on, and strided subsets of many cameras. */
+int32_t hadros_batch_pixels(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams,
+                            const hadros_sigma* s, const int32_t* pixel_ids,
+                            const int32_t* counts, const hadros_image_out* out);
 int32_t hadros_batch_device(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams,
                             const hadros_sigma* s, const hadros_image_out* dev_out,
                             void* stream);
@@ -424,8 +431,9 @@ int32_t hadros_read_kgeo(const char* path, int32_t* pixel_ids, int8_t* captured,
  * ensemble of such networks marks, through its spread, the pixels the exact
  * tracer must redo.  Inputs: 16 raw features per sample (alpha, beta, a,
  * cos theta_obs, log10 rho0, one-hot profile kind x8, r0, H/R, log10 E_mid);
- * network 32 -> 4 x 256 (SiLU) -> 2 with the normalized features split into
- * hi/lo BF16 pairs and an FP32 linear skip.  Pointers are DEVICE pointers
+ * network 64 -> 4 x 256 (SiLU) -> 2 whose inputs are the normalized features
+ * split into hi/lo BF16 pairs plus Fourier features of alpha and beta, with
+ * an FP32 linear skip.  Pointers are DEVICE pointers
  * unless stated; calls are asynchronous on `stream` (a cudaStream_t; NULL =
  * the legacy default stream) and allocate nothing. */
 typedef struct hadros_mlp_norm {   /* host struct, passed by pointer          */
@@ -450,7 +458,8 @@ int64_t hadros_mlp_workspace_bytes(int64_t batch);
 int32_t hadros_mlp_layout(int64_t* offsets, int32_t n);
 /* master FP32 -> BF16 working copy (W1 twice for the hi/lo columns). */
 int32_t hadros_mlp_pack(const float* master, void* packed, void* stream);
-/* raw [n][16] FP32 -> X [n][32] BF16 (normalized, hi/lo split). */
+/* raw [n][16] FP32 -> X [n][64] BF16 (normalized: hi[16], lo[16], then
+ * sin/cos of 8 frequencies of alpha and of beta). */
 int32_t hadros_mlp_featurize(const float* raw, int64_t n, const hadros_mlp_norm* norm, void* X,
                              void* stream);
 /* Raw features of the samples (pixel_ids[k], bin b) of a camera, rows
@@ -490,7 +499,7 @@ typedef struct hadros_surrogate_out {   /* DEVICE buffers                       
     double* tau;           /* [P] spectral aggregates as integrate_kerr_ray_   */
     double* P_surv;        /*     spectral forms them from the mean prediction */
     double* I_obs;
-    float* spread;         /* [P] ensemble standard deviation of ln I_obs      */
+    float* spread;         /* [P] ensemble standard deviation (see spread_of)  */
     int32_t* fallback_ids; /* [P] pixel ids with spread > threshold, unordered */
     int32_t* counters;     /* [2]: fallback count, abort flag (set by the call) */
 } hadros_surrogate_out;
@@ -499,12 +508,15 @@ typedef struct hadros_surrogate_out {   /* DEVICE buffers                       
  * ensemble of n_members (1..8) networks: masters [n][param_count] FP32,
  * images [n][image_bytes] (16-byte aligned).  P = pixel_end - pixel_begin,
  * outputs indexed from pixel_begin; B = bins of p, which must divide 256.
- * Asynchronous; after the stream completes, counters[1] != 0 means a wait in
- * the kernel timed out and the outputs are not valid. */
+ * The spread is the ensemble standard deviation of ln I_obs (spread_of 0)
+ * or of ln tau (spread_of 1, for media whose intensity vanishes); pixels
+ * above spread_threshold go to fallback_ids.  Asynchronous; after the stream
+ * completes, counters[1] != 0 means a wait in the kernel timed out and the
+ * outputs are not valid. */
 int32_t hadros_surrogate_image(const hadros_params* p, const hadros_sigma* s, int32_t n_members,
                                const float* masters, const void* images,
                                const hadros_mlp_norm* norm, int64_t pixel_begin,
-                               int64_t pixel_end, float spread_threshold,
+                               int64_t pixel_end, float spread_threshold, int32_t spread_of,
                                const hadros_surrogate_out* out, void* stream);
 
 #ifdef __cplusplus

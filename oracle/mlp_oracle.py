@@ -6,8 +6,10 @@ surrogate has no counterpart in the reference; this oracle restates the
 network defined in hadros_b200/csrc/hadros_mlp.cuh so that the tests can
 check the GPU gradients:
 
-  x_hi, x_lo   BF16 input columns (X [n][32]); x = x_hi + x_lo
-  Z1 = X W1d^T + b1          W1d = [W1, W1] (tied hi/lo weights)
+  X [n][64]    BF16 input columns: x_hi[16], x_lo[16], Fourier[32]
+               (sin, cos of pi 2^(k-1) x for the normalized alpha and beta,
+               k = 0..7); x = x_hi + x_lo
+  Z1 = X W1d^T + b1          W1d = [W1f, W1f, W1four] (hi/lo weights tied)
   H_l = SiLU(Z_l), Z_{l+1} = H_l W_{l+1}^T + b_{l+1}   (l = 1..3)
   out = H4 W5^T + b5 + x Ws^T
 
@@ -21,19 +23,21 @@ from __future__ import annotations
 
 import numpy as np
 
-F, IN, W, DEPTH, OUT = 16, 32, 256, 4, 2
+F, FREQ, W, DEPTH, OUT = 16, 8, 256, 4, 2
+FOUR = 4 * FREQ
+IN = 2 * F + FOUR
 
-# FP32 master layout (hadros_mlp.cuh): W1 [256][16], b1, W2, b2, W3, b3, W4, b4,
+# FP32 master layout (hadros_mlp.cuh): W1 [256][48], b1, W2, b2, W3, b3, W4, b4,
 # W5 [2][256], b5 [2], Ws [2][16].
 OFF = {}
 _o = 0
-for _name, _size in (("W1", W * F), ("b1", W), ("W2", W * W), ("b2", W), ("W3", W * W), ("b3", W),
+for _name, _size in (("W1", W * (F + FOUR)), ("b1", W), ("W2", W * W), ("b2", W), ("W3", W * W), ("b3", W),
                      ("W4", W * W), ("b4", W), ("W5", OUT * W), ("b5", OUT), ("Ws", OUT * F)):
     OFF[_name] = (_o, _size)
     _o += _size
 PARAMS_USED = _o
 PARAMS = (PARAMS_USED + 7) // 8 * 8
-SHAPES = {"W1": (W, F), "W2": (W, W), "W3": (W, W), "W4": (W, W), "W5": (OUT, W), "Ws": (OUT, F)}
+SHAPES = {"W1": (W, F + FOUR), "W2": (W, W), "W3": (W, W), "W4": (W, W), "W5": (OUT, W), "Ws": (OUT, F)}
 
 
 def bf16(x) -> np.ndarray:
@@ -61,13 +65,26 @@ def pack_grad(g: dict) -> np.ndarray:
     return out
 
 
+def fourier(x: np.ndarray) -> np.ndarray:
+    """[n] -> [n][16]: sin, cos of pi t, t = 2^(k-1) x reduced to [-1, 1]."""
+    x = np.asarray(x, np.float32)
+    out = []
+    for k in range(FREQ):
+        t = (x * np.float32(1 << k) * np.float32(0.5)).astype(np.float32)
+        r = (t - np.float32(2.0) * np.rint(np.float32(0.5) * t)).astype(np.float32)
+        a = np.pi * r.astype(np.float64)
+        out += [np.sin(a), np.cos(a)]
+    return np.stack(out, axis=1)
+
+
 def split_features(raw: np.ndarray, mu: np.ndarray, inv_sd: np.ndarray) -> np.ndarray:
-    """X [n][32] (hi, lo) of k_featurize, as float64 BF16 values."""
+    """X [n][64] of k_featurize, as float64 BF16 values."""
     x = ((np.asarray(raw, np.float32) - np.asarray(mu, np.float32)) * np.asarray(inv_sd, np.float32))
     x = x.astype(np.float32)
     hi = bf16(x)
     lo = bf16(x.astype(np.float64) - hi)
-    return np.concatenate([hi, lo], axis=1)
+    four = bf16(np.concatenate([fourier(x[:, 0]), fourier(x[:, 1])], axis=1))
+    return np.concatenate([hi, lo, four], axis=1)
 
 
 def _sig(z):
@@ -88,8 +105,8 @@ def forward(master, X, rounded: bool = True):
     r = bf16 if rounded else (lambda a: np.asarray(a, dtype=np.float64))
     P = unpack(master)
     X = np.asarray(X, dtype=np.float64)
-    x = X[:, :F] + X[:, F:]
-    Wd = {1: r(np.concatenate([P["W1"], P["W1"]], axis=1))}
+    x = X[:, :F] + X[:, F:2 * F]
+    Wd = {1: r(np.concatenate([P["W1"][:, :F], P["W1"][:, :F], P["W1"][:, F:]], axis=1))}
     for l in (2, 3, 4):
         Wd[l] = r(P[f"W{l}"])
     W5 = r(P["W5"])
@@ -114,6 +131,6 @@ def backward(cache, dout) -> dict:
         g[f"b{l}"] = dZ.sum(0)
         dZ = r((dZ @ Wd[l]) * silu_grad(Z[l - 1]))
     gW1 = dZ.T @ H[0]
-    g["W1"] = gW1[:, :F] + gW1[:, F:]
+    g["W1"] = np.concatenate([gW1[:, :F] + gW1[:, F:2 * F], gW1[:, 2 * F:]], axis=1)
     g["b1"] = dZ.sum(0)
     return g

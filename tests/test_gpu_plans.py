@@ -82,3 +82,23 @@ def test_autotuner_picks_and_caches(hb, gpu_ctx, sigma_table, tmp_path, monkeypa
     assert not rep["cached"] and len(rep["timings"]) == len(autotune.CANDIDATES)
     best2, rep2 = autotune.autotune(gpu_ctx, cams, sigma_table, torch, scale=1, repeats=1)
     assert rep2["cached"] and bytes(best2) == bytes(best)
+
+
+def test_batch_pixels_equals_per_camera_pixel_lists(hb, gpu_ctx, sigma_table):
+    """hadros_batch_pixels (pixel subsets of several cameras in one launch)
+    gives, per camera, exactly what hadros_image_pixels gives for its list."""
+    from hadros_b200 import workloads as W
+    rng = np.random.default_rng(11)
+    cams = [hb.params(**W.mixed_512(nx=48, ny=40, h=0.05, theta_obs_deg=t, rho0_gcm3=r))
+            for t, r in ((17.0, 1e11), (45.0, 1e9), (70.0, 3e10))]
+    lists = [np.sort(rng.choice(48 * 40, size=n, replace=False)).astype(np.int32) for n in (37, 0, 150)]
+    got = gpu_ctx.batch_pixels(cams, sigma_table, lists)
+    for p, ids, g in zip(cams, lists, got):
+        if ids.size == 0:
+            assert all(v.size == 0 for v in g.values())
+            continue
+        ref = gpu_ctx.image(p, sigma_table, pixel_ids=ids)
+        for k in ref:
+            np.testing.assert_array_equal(g[k], ref[k], err_msg=k)
+    with pytest.raises(hb.HadrosError):
+        gpu_ctx.batch_pixels(cams[:1], sigma_table, [np.array([48 * 40], dtype=np.int32)])

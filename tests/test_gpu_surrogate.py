@@ -50,7 +50,7 @@ def _features(torch, hb, n, seed):
     for j in range(16):
         norm.feat_inv_sd[j] = 1.0
     raw_t = torch.from_numpy(raw).cuda()
-    X = torch.empty((n, 32), dtype=torch.bfloat16, device="cuda")
+    X = torch.empty((n, 64), dtype=torch.bfloat16, device="cuda")
     assert hb.lib().hadros_mlp_featurize(_vp(raw_t), n, C.byref(norm), _vp(X), None) == 0
     return raw, X
 
@@ -71,7 +71,10 @@ def test_featurize_matches_oracle_split(hb, torch):
     raw, X = _features(torch, hb, 777, 1)
     ref = M.split_features(raw, np.zeros(16), np.ones(16))
     got = X.float().cpu().numpy().astype(np.float64)
-    np.testing.assert_array_equal(got, ref)
+    np.testing.assert_array_equal(got[:, :32], ref[:, :32])
+    # Fourier columns: the GPU's sin/cos may round to the neighbouring BF16 value
+    assert np.abs(got[:, 32:] - ref[:, 32:]).max() <= 2.0 ** -8
+    assert np.mean(got[:, 32:] != ref[:, 32:]) < 0.02
 
 
 @pytest.mark.parametrize("n", [200, 1024, 4100])
@@ -170,13 +173,15 @@ def _random_surrogate(hb, torch, members, seed):
     return sur
 
 
-@pytest.mark.parametrize("members,n_bins,nx,ny,begin,end", [
-    (1, 8, 24, 24, 0, None),
-    (2, 16, 33, 17, 0, None),
-    (3, 64, 20, 20, 37, 333),
-    (4, 1, 50, 30, 0, None),
+@pytest.mark.parametrize("members,n_bins,nx,ny,begin,end,spread_of", [
+    (1, 8, 24, 24, 0, None, 0),
+    (2, 16, 33, 17, 0, None, 0),
+    (3, 64, 20, 20, 37, 333, 0),
+    (4, 1, 50, 30, 0, None, 0),
+    (3, 32, 16, 16, 0, None, 1),
 ])
-def test_umma_inference_matches_training_forward(hb, torch, sigma_table, members, n_bins, nx, ny, begin, end):
+def test_umma_inference_matches_training_forward(hb, torch, sigma_table, members, n_bins, nx, ny, begin, end,
+                                                 spread_of):
     """The fused tcgen05 kernel and the mma.sync training forward pass compute
     the same network: per-sample ensemble means within BF16 rounding, and the
     per-pixel aggregates and spread as the host forms them from the forward
@@ -191,7 +196,7 @@ def test_umma_inference_matches_training_forward(hb, torch, sigma_table, members
     p = hb.params(**kw)
     P = nx * ny
     end = P if end is None else end
-    res = sur.image(p, sigma_table, pixel_begin=begin, pixel_end=end, threshold=0.05)
+    res = sur.image(p, sigma_table, pixel_begin=begin, pixel_end=end, threshold=0.05, spread_of=spread_of)
     torch.cuda.synchronize()
     cnt = res["counters"].cpu().numpy()
     assert cnt[1] == 0, "inference kernel aborted"
@@ -207,10 +212,13 @@ def test_umma_inference_matches_training_forward(hb, torch, sigma_table, members
         assert np.sqrt(np.mean(err ** 2)) < 0.02 * scale, np.sqrt(np.mean(err ** 2))
         assert err.max() < 0.2 * scale, err.max()
     bins = hb.spectral_bins(p, sigma_table)
-    lnI_k = fw[:, :, 1].reshape(members, -1, B)
     valid = (bins["valid"] != 0) & (bins["dE"] > 0)
     lnde = np.where(valid, np.log(np.where(valid, bins["dE"], 1.0)), -np.inf)
-    L_k = np.log(np.sum(np.exp(lnI_k + lnde), axis=2))                # [K][n]
+    if spread_of == 0:
+        L_k = np.log(np.sum(np.exp(fw[:, :, 1].reshape(members, -1, B) + lnde), axis=2))   # [K][n]
+    else:
+        wv = np.where(valid, bins["weight"], 0.0)
+        L_k = np.log(np.sum(np.exp(fw[:, :, 0].reshape(members, -1, B)) * wv, axis=2) / wv.sum())
     spread_ref = L_k.std(0)
     spread = res["spread"].cpu().numpy()
     if members == 1:

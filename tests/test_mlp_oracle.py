@@ -17,7 +17,7 @@ def _master(seed):
     rng = np.random.default_rng(seed)
     m = np.zeros(M.PARAMS)
     for name, (o, n) in M.OFF.items():
-        fan = {"W1": 32, "W5": 256, "Ws": 16}.get(name, 256)
+        fan = {"W1": 64, "W5": 256, "Ws": 16}.get(name, 256)
         m[o:o + n] = rng.uniform(-1, 1, n) * np.sqrt(3.0 / fan)
     return m
 
@@ -34,14 +34,15 @@ def test_split_features_reconstructs_to_16_bits():
     rng = np.random.default_rng(1)
     raw = rng.normal(size=(1000, 16)).astype(np.float32) * 7
     X = M.split_features(raw, np.zeros(16), np.ones(16))
-    rel = np.abs(X[:, :16] + X[:, 16:] - raw) / np.maximum(np.abs(raw), 1e-30)
+    assert X.shape == (1000, 64)
+    rel = np.abs(X[:, :16] + X[:, 16:32] - raw) / np.maximum(np.abs(raw), 1e-30)
     assert rel.max() < 2.0 ** -15
 
 
 def test_exact_gradient_matches_finite_differences():
     rng = np.random.default_rng(2)
     m = _master(3)
-    X = rng.normal(size=(6, 32)) * 0.5
+    X = rng.normal(size=(6, 64)) * 0.5
     dout = rng.normal(size=(6, 2))
     out, cache = M.forward(m, X, rounded=False)
     g = M.pack_grad(M.backward(cache, dout))
@@ -58,3 +59,11 @@ def test_exact_gradient_matches_finite_differences():
             mn[k] -= h
             fd = (f(mp) - f(mn)) / (2 * h)
             assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(fd)), (name, idx, fd, g[k])
+
+
+def test_fourier_features_follow_their_definition():
+    x = np.linspace(-1.9, 1.9, 301).astype(np.float32)
+    f = M.fourier(x)
+    for k in range(M.FREQ):
+        np.testing.assert_allclose(f[:, 2 * k], np.sin(np.pi * 2.0 ** (k - 1) * x.astype(np.float64)), atol=1e-5)
+        np.testing.assert_allclose(f[:, 2 * k + 1], np.cos(np.pi * 2.0 ** (k - 1) * x.astype(np.float64)), atol=1e-5)
