@@ -190,7 +190,8 @@ struct EpiHidden {   // Z = acc + b (BF16, for the backward pass), H = SiLU(acc 
         const float z0 = v0 + bias[n], z1 = v1 + bias[n + 1];
         const long o = long(m) * kW + n;
         if (Z) *reinterpret_cast<uint32_t*>(Z + o) = pack_bf16x2(z0, z1);
-        *reinterpret_cast<uint32_t*>(H + o) = pack_bf16x2(silu_f(z0), silu_f(z1));
+        const float2 h = silu2(z0, z1);
+        *reinterpret_cast<uint32_t*>(H + o) = pack_bf16x2(h.x, h.y);
     }
 };
 
@@ -201,7 +202,8 @@ struct EpiBwdData {   // dZ_prev = acc * SiLU'(Z_prev)
     {
         const long o = long(m) * kW + n;
         const float2 z = unpack_bf16x2(*reinterpret_cast<const uint32_t*>(Zp + o));
-        *reinterpret_cast<uint32_t*>(dZp + o) = pack_bf16x2(v0 * silu_grad_f(z.x), v1 * silu_grad_f(z.y));
+        const float2 g = silu_grad2(z.x, z.y);
+        *reinterpret_cast<uint32_t*>(dZp + o) = pack_bf16x2(v0 * g.x, v1 * g.y);
     }
 };
 

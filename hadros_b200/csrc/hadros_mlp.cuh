@@ -22,6 +22,7 @@
 
 #ifdef __CUDACC__
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #endif
 
 namespace hadros {
@@ -95,21 +96,30 @@ struct Norm {
 
 #ifdef __CUDACC__
 
-__device__ __forceinline__ float tanh_approx(float x)
+// sigma(z) = (1 + tanh(z/2)) / 2 for a pair of values, with tanh on the
+// paired FP16 unit (tanh.approx.f16x2: one MUFU operation for two values).
+// The same function in every kernel, so the trained network and the
+// inferred one agree.
+__device__ __forceinline__ float2 sigmoid2(float z0, float z1)
 {
-    float y;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
+    uint32_t hz, ht;
+    asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(hz) : "f"(0.5f * z1), "f"(0.5f * z0));
+    asm("tanh.approx.f16x2 %0, %1;" : "=r"(ht) : "r"(hz));
+    const __half2 t = *reinterpret_cast<const __half2*>(&ht);
+    const float2 tf = __half22float2(t);
+    return make_float2(fmaf(0.5f, tf.x, 0.5f), fmaf(0.5f, tf.y, 0.5f));
 }
-// sigma(z) = (1 + tanh(z/2)) / 2; the same formula in every kernel, so the
-// trained function and the inferred one agree.
-__device__ __forceinline__ float sigmoid_f(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
-__device__ __forceinline__ float silu_f(float z) { return z * sigmoid_f(z); }
-__device__ __forceinline__ float silu_grad_f(float z)
+__device__ __forceinline__ float2 silu2(float z0, float z1)
 {
-    const float s = sigmoid_f(z);
-    return fmaf(z * s, 1.0f - s, s);
+    const float2 s = sigmoid2(z0, z1);
+    return make_float2(z0 * s.x, z1 * s.y);
 }
+__device__ __forceinline__ float2 silu_grad2(float z0, float z1)
+{
+    const float2 s = sigmoid2(z0, z1);
+    return make_float2(fmaf(z0 * s.x, 1.0f - s.x, s.x), fmaf(z1 * s.y, 1.0f - s.y, s.y));
+}
+__device__ __forceinline__ float silu_grad_f(float z) { return silu_grad2(z, 0.0f).x; }
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
 {

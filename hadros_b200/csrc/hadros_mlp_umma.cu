@@ -224,7 +224,42 @@ __device__ __forceinline__ void tc_ld2(uint32_t taddr, uint32_t& r0, uint32_t& r
 {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];\n" : "=r"(r0), "=r"(r1) : "r"(taddr));
 }
-__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+// The wait, with the loaded registers as operands so that no use of them is
+// scheduled before it.
+__device__ __forceinline__ void tc_wait_ld(uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.wait::ld.sync.aligned;\n"
+        : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+          "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+          "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]),
+          "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]),
+          "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+        :
+        : "memory");
+}
+__device__ __forceinline__ void tc_wait_ld(uint32_t& r0, uint32_t& r1)
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" : "+r"(r0), "+r"(r1) : : "memory");
+}
+
+// Bias, SiLU and BF16 store of 32 accumulator columns [cb, cb+32) of row r.
+__device__ __forceinline__ void epi_chunk(const uint32_t (&v)[32], const float* sb, int cb, uint8_t* act, int r)
+{
+    uint32_t h[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const float2 bb = *reinterpret_cast<const float2*>(sb + cb + 2 * q);
+        const float2 y = silu2(__uint_as_float(v[2 * q]) + bb.x, __uint_as_float(v[2 * q + 1]) + bb.y);
+        h[q] = pack_bf16x2(y.x, y.y);
+    }
+    uint8_t* chunk = act + (cb >> 6) * 16384 + r * 128;
+    const int u0 = (cb & 63) >> 3;   // logical 16-byte unit of column cb
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        *reinterpret_cast<uint4*>(chunk + (((u0 + u) ^ (r & 7)) << 4)) =
+            make_uint4(h[4 * u], h[4 * u + 1], h[4 * u + 2], h[4 * u + 3]);
+}
 
 // Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
 // 1024 bytes apart (SBO), descriptor version 1.
@@ -257,7 +292,8 @@ struct InferArgs {
     int32_t* counters;        // [0] fallback count, [1] abort flag
 };
 
-constexpr int kSmemBytes = kPair * kActBytes + kStages * kStageBytes + 2 * 256 * 4 + 256 + 1024;
+constexpr int kBiasFloats = 4 * kW + kOut + kOut * kF + 6;   // + padding to 8 bytes
+constexpr int kSmemBytes = kPair * kActBytes + kStages * kStageBytes + 2 * 256 * 4 + kBiasFloats * 4 + 256 + 1024;
 static_assert(kSmemBytes <= 232448, "shared memory above the sm_100 per-block limit");
 
 __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
@@ -268,7 +304,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
     uint8_t* stage = smem + kPair * kActBytes;                // [2][32 KB]
     float* red_a = reinterpret_cast<float*>(stage + kStages * kStageBytes);   // [256]
     float* red_b = red_a + 256;                                               // [256]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(red_b + 256);
+    float* sbias = red_b + 256;        // this member's b1..b4 [4][256], b5 [2], Ws [2][16]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sbias + kBiasFloats);
     uint64_t* full = bars;                 // [kStages]
     uint64_t* empty = bars + kStages;      // [kStages]
     uint64_t* acc_full = bars + 2 * kStages;
@@ -404,6 +441,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
             float w_ref = 0.0f, w_s1 = 0.0f, w_s2 = 0.0f;   // pixel leader: shifted sums of ln I_k
             for (int k = 0; k < K; ++k) {
                 const float* P = A.masters + long(k) * kParams;
+                // this member's biases and skip weights -> shared memory (the
+                // previous member's were last read before its closing barrier)
+                {
+                    const int t = trow;   // 0..255
+#pragma unroll
+                    for (int L = 1; L <= 4; ++L) sbias[(L - 1) * kW + t] = P[off_b(L)];
+                    if (t < kOut) sbias[4 * kW + t] = P[kOffB5 + t];
+                    if (t < kOut * kF) sbias[4 * kW + kOut + t] = P[kOffWs + t];
+                }
                 // features -> chunk 0, the 8 16-byte units of row r
 #pragma unroll
                 for (int u = 0; u < kIn / 8; ++u)
@@ -412,28 +458,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                 fence_async_smem();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(saddr(act_ready));
+                if (!epi_sync()) goto done;   // biases visible to every epilogue thread
                 for (int L = 1; L <= 4; ++L, ++layer_count) {
                     if (!warp_wait(saddr(acc_full), uint32_t(layer_count & 1), abort_flag)) goto done;
                     tc_fence_after();
-                    const float* bias = P + off_b(L);
+                    const float* sb = sbias + (L - 1) * kW;
+                    // two register sets: the next 32 columns load from TMEM while
+                    // the current 32 are processed
+                    uint32_t va[32], vb[32];
+                    tc_ld32(lane_base, va);
+                    tc_wait_ld(va);
 #pragma unroll 1
-                    for (int cb = 0; cb < kW; cb += 32) {
-                        uint32_t v[32];
-                        tc_ld32(lane_base + uint32_t(cb), v);
-                        tc_wait_ld();
-                        uint32_t h[16];
-#pragma unroll
-                        for (int q = 0; q < 16; ++q) {
-                            const float z0 = __uint_as_float(v[2 * q]) + __ldg(bias + cb + 2 * q);
-                            const float z1 = __uint_as_float(v[2 * q + 1]) + __ldg(bias + cb + 2 * q + 1);
-                            h[q] = pack_bf16x2(silu_f(z0), silu_f(z1));
-                        }
-                        uint8_t* chunk = my_act + (cb >> 6) * 16384 + r * 128;
-                        const int u0 = (cb & 63) >> 3;   // logical unit of column cb
-#pragma unroll
-                        for (int u = 0; u < 4; ++u)
-                            *reinterpret_cast<uint4*>(chunk + (((u0 + u) ^ (r & 7)) << 4)) =
-                                make_uint4(h[4 * u], h[4 * u + 1], h[4 * u + 2], h[4 * u + 3]);
+                    for (int cb = 0; cb < kW; cb += 64) {
+                        tc_ld32(lane_base + uint32_t(cb + 32), vb);
+                        epi_chunk(va, sb, cb, my_act, r);
+                        tc_wait_ld(vb);
+                        if (cb + 64 < kW) tc_ld32(lane_base + uint32_t(cb + 64), va);
+                        epi_chunk(vb, sb, cb + 32, my_act, r);
+                        if (cb + 64 < kW) tc_wait_ld(va);
                     }
                     tc_fence_before();
                     fence_async_smem();
@@ -446,13 +488,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                 tc_fence_after();
                 uint32_t o0, o1;
                 tc_ld2(lane_base, o0, o1);
-                tc_wait_ld();
+                tc_wait_ld(o0, o1);
                 tc_fence_before();
-                float a0 = __uint_as_float(o0) + P[kOffB5], a1 = __uint_as_float(o1) + P[kOffB5 + 1];
+                const float* st = sbias + 4 * kW;
+                float a0 = __uint_as_float(o0) + st[0], a1 = __uint_as_float(o1) + st[1];
 #pragma unroll
                 for (int q = 0; q < kF; ++q) {
-                    a0 = fmaf(P[kOffWs + q], x[q], a0);
-                    a1 = fmaf(P[kOffWs + kF + q], x[q], a1);
+                    a0 = fmaf(st[kOut + q], x[q], a0);
+                    a1 = fmaf(st[kOut + kF + q], x[q], a1);
                 }
                 const float ltau = fmaf(a0, A.norm.out_sd[0], A.norm.out_mu[0]);
                 const float lnI = fmaf(a1, A.norm.out_sd[1], A.norm.out_mu[1]);
