@@ -219,6 +219,7 @@ SIGNATURES = {
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p]),
     "hadros_mlp_image_bytes": (C.c_int64, []),
+    "hadros_surrogate_schedule": (C.c_int32, [C.c_int32]),
     "hadros_mlp_pack_image": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "hadros_surrogate_image": (C.c_int32, [P(HadrosParams), C.c_void_p, C.c_int32, C.c_void_p,
                                            C.c_void_p, P(HadrosMlpNorm), C.c_int64, C.c_int64,

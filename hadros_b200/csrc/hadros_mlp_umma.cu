@@ -23,6 +23,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -293,9 +294,19 @@ struct InferArgs {
 };
 
 constexpr int kBiasFloats = 4 * kW + kOut + kOut * kF + 6;   // + padding to 8 bytes
-constexpr int kSmemBytes = kPair * kActBytes + kStages * kStageBytes + 2 * 256 * 4 + kBiasFloats * 4 + 256 + 1024;
+constexpr int kSmemBytes = kPair * kActBytes + kStages * kStageBytes + 2 * 256 * 4 + 2 * kBiasFloats * 4 + 256 + 1024;
+
+// First stage (in a member's weight image) of layer L and its stage count.
+__host__ __device__ constexpr int stage_of(int L) { return L == 1 ? 0 : (L == 5 ? kStagesPerMember - 1 : 1 + (L - 2) * 4); }
+__host__ __device__ constexpr int stages_in(int L) { return (L == 1 || L == 5) ? 1 : 4; }
 static_assert(kSmemBytes <= 232448, "shared memory above the sm_100 per-block limit");
 
+// PP = false: the two 128-row halves go through each layer together, each
+// weight stage feeding both (half the weight traffic, but the tensor cores
+// idle during the epilogue).  PP = true ("ping-pong"): the halves take turns,
+// so one half's epilogue overlaps the other half's MMAs; every weight stage
+// is streamed once per half.
+template <bool PP>
 __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
 {
     extern __shared__ uint8_t smem_raw[];
@@ -304,15 +315,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
     uint8_t* stage = smem + kPair * kActBytes;                // [2][32 KB]
     float* red_a = reinterpret_cast<float*>(stage + kStages * kStageBytes);   // [256]
     float* red_b = red_a + 256;                                               // [256]
-    float* sbias = red_b + 256;        // this member's b1..b4 [4][256], b5 [2], Ws [2][16]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sbias + kBiasFloats);
+    float* sbias = red_b + 256;        // per epilogue group: b1..b4 [4][256], b5 [2], Ws [2][16]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sbias + 2 * kBiasFloats);
     uint64_t* full = bars;                 // [kStages]
     uint64_t* empty = bars + kStages;      // [kStages]
-    uint64_t* acc_full = bars + 2 * kStages;
-    uint64_t* act_ready = bars + 2 * kStages + 1;
-    uint64_t* epi_bar = bars + 2 * kStages + 2;   // barrier of the 256 epilogue threads
-    uint64_t* drain = bars + 2 * kStages + 3;     // abort path: MMAs in flight
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 4);
+    uint64_t* acc_full = bars + 2 * kStages;        // [2] (PP: one per half)
+    uint64_t* act_ready = bars + 2 * kStages + 2;   // [2]
+    uint64_t* epi_bar = bars + 2 * kStages + 4;     // [2] barrier of an epilogue group
+    uint64_t* drain = bars + 2 * kStages + 6;       // abort path: MMAs in flight
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 7);
+    constexpr int kGroups = PP ? 2 : 1;             // epilogue groups (and MMA turns per layer)
+    constexpr int kGroupWarps = kEpiWarps / kGroups;
     volatile int* abort_flag = A.counters + 1;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -326,9 +339,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
             mbar_init(saddr(&full[s]), 1);
             mbar_init(saddr(&empty[s]), 1);
         }
-        mbar_init(saddr(acc_full), 1);
-        mbar_init(saddr(act_ready), kEpiWarps);
-        mbar_init(saddr(epi_bar), kEpiWarps * 32);
+        for (int g = 0; g < 2; ++g) {
+            mbar_init(saddr(&acc_full[g]), 1);
+            mbar_init(saddr(&act_ready[g]), kGroupWarps);
+            mbar_init(saddr(&epi_bar[g]), kGroupWarps * 32);
+        }
         mbar_init(saddr(drain), 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         fence_async_smem();
@@ -346,19 +361,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
     long issued = 0;          // producer: stages issued
     bool mma_issued = false;  // MMA thread: any tcgen05.mma issued
     uint32_t epi_phase = 0;   // epilogue barrier phase
+    const int grp = PP ? (warp >> 2) & 1 : 0;
     auto epi_sync = [&]() -> bool {
-        mbar_arrive(saddr(epi_bar));
-        const bool ok = warp_wait(saddr(epi_bar), epi_phase, abort_flag);
+        mbar_arrive(saddr(&epi_bar[grp]));
+        const bool ok = warp_wait(saddr(&epi_bar[grp]), epi_phase, abort_flag);
         epi_phase ^= 1u;
         return ok;
     };
 
     if (warp == kEpiWarps + 1) {
-        // ---- producer: the same 14-stage stream per member, per tile ----------
+        // ---- producer: per member, each layer's stages (once per MMA turn) ---
         if (lane == 0) {
             for (long tile = blockIdx.x; tile < n_tiles && !*abort_flag; tile += gridDim.x)
                 for (int k = 0; k < K; ++k)
-                    for (int q = 0; q < kStagesPerMember; ++q, ++issued) {
+                    for (int L = 1; L <= 5; ++L)
+                        for (int tt = 0; tt < kGroups; ++tt)
+                            for (int c = 0; c < stages_in(L); ++c, ++issued) {
+                        const int q = stage_of(L) + c;
                         const long i = issued;
                         const int slot = int(i % kStages);
                         const uint32_t ph = uint32_t((i / kStages) & 1);
@@ -376,17 +395,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
             const uint32_t id256 = idesc_bf16(128, 256), id16 = idesc_bf16(128, 16);
             for (long tile = blockIdx.x; tile < n_tiles && !*abort_flag; tile += gridDim.x)
                 for (int k = 0; k < K; ++k)
-                    for (int L = 1; L <= 5; ++L, ++layer_count) {
-                        if (!mbar_wait(saddr(act_ready), uint32_t(layer_count & 1), abort_flag)) goto done;
+                    for (int L = 1; L <= 5; ++L, ++layer_count)
+                      for (int tt = 0; tt < kGroups; ++tt) {
+                        if (!mbar_wait(saddr(&act_ready[tt]), uint32_t(layer_count & 1), abort_flag)) goto done;
                         tc_fence_after();
-                        const int nst = (L == 1 || L == 5) ? 1 : 4;
+                        const int nst = stages_in(L);
                         for (int c = 0; c < nst; ++c, ++i) {
                             const int slot = int(i % kStages);
                             if (!mbar_wait(saddr(&full[slot]), uint32_t((i / kStages) & 1), abort_flag)) goto done;
                             tc_fence_after();
                             const uint32_t sb = saddr(stage + slot * kStageBytes);
                             mma_issued = true;
-                            for (int t = 0; t < kPair; ++t) {
+                            for (int t = PP ? tt : 0; t < (PP ? tt + 1 : kPair); ++t) {
                                 const uint32_t ab = saddr(act + t * kActBytes);
                                 const uint32_t d = tmem + uint32_t(t * 256);
                                 if (L == 1) {          // K = 64 from chunk 0
@@ -405,8 +425,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                             }
                             tc_commit(saddr(&empty[slot]));   // slot free once these MMAs finish
                         }
-                        tc_commit(saddr(acc_full));            // layer done
-                    }
+                        tc_commit(saddr(&acc_full[tt]));       // layer done (for this turn)
+                      }
         }
     } else {
         // ---- epilogue warps: rows of accumulator t = warp / 4 ---------------------
@@ -414,6 +434,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
         const int r = qw * 32 + lane;                 // row in the 128-row half
         const int trow = t * kTileRows + r;           // row in the 256-sample tile
         uint8_t* my_act = act + t * kActBytes;
+        float* my_bias = sbias + grp * kBiasFloats;
         const uint32_t lane_base = tmem + (uint32_t(qw * 32) << 16) + uint32_t(t * 256);
         long layer_count = 0;
         const bool leader_possible = (trow % B) == 0;
@@ -444,11 +465,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                 // this member's biases and skip weights -> shared memory (the
                 // previous member's were last read before its closing barrier)
                 {
-                    const int t = trow;   // 0..255
-#pragma unroll
-                    for (int L = 1; L <= 4; ++L) sbias[(L - 1) * kW + t] = P[off_b(L)];
-                    if (t < kOut) sbias[4 * kW + t] = P[kOffB5 + t];
-                    if (t < kOut * kF) sbias[4 * kW + kOut + t] = P[kOffWs + t];
+                    const int gt = PP ? r : trow;      // thread within the group
+                    for (int e = gt; e < 4 * kW; e += kGroupWarps * 32)
+                        my_bias[e] = P[off_b(1 + e / kW) + e % kW];
+                    if (gt < kOut) my_bias[4 * kW + gt] = P[kOffB5 + gt];
+                    if (gt < kOut * kF) my_bias[4 * kW + kOut + gt] = P[kOffWs + gt];
                 }
                 // features -> chunk 0, the 8 16-byte units of row r
 #pragma unroll
@@ -457,12 +478,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                         make_uint4(feat[4 * u], feat[4 * u + 1], feat[4 * u + 2], feat[4 * u + 3]);
                 fence_async_smem();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(saddr(act_ready));
+                if (lane == 0) mbar_arrive(saddr(&act_ready[grp]));
                 if (!epi_sync()) goto done;   // biases visible to every epilogue thread
                 for (int L = 1; L <= 4; ++L, ++layer_count) {
-                    if (!warp_wait(saddr(acc_full), uint32_t(layer_count & 1), abort_flag)) goto done;
+                    if (!warp_wait(saddr(&acc_full[grp]), uint32_t(layer_count & 1), abort_flag)) goto done;
                     tc_fence_after();
-                    const float* sb = sbias + (L - 1) * kW;
+                    const float* sb = my_bias + (L - 1) * kW;
                     // two register sets: the next 32 columns load from TMEM while
                     // the current 32 are processed
                     uint32_t va[32], vb[32];
@@ -480,17 +501,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                     tc_fence_before();
                     fence_async_smem();
                     __syncwarp();
-                    if (lane == 0) mbar_arrive(saddr(act_ready));
+                    if (lane == 0) mbar_arrive(saddr(&act_ready[grp]));
                 }
                 // last layer: 2 outputs (+ bias + FP32 skip), de-standardized
-                if (!warp_wait(saddr(acc_full), uint32_t(layer_count & 1), abort_flag)) goto done;
+                if (!warp_wait(saddr(&acc_full[grp]), uint32_t(layer_count & 1), abort_flag)) goto done;
                 ++layer_count;
                 tc_fence_after();
                 uint32_t o0, o1;
                 tc_ld2(lane_base, o0, o1);
                 tc_wait_ld(o0, o1);
                 tc_fence_before();
-                const float* st = sbias + 4 * kW;
+                const float* st = my_bias + 4 * kW;
                 float a0 = __uint_as_float(o0) + st[0], a1 = __uint_as_float(o1) + st[1];
 #pragma unroll
                 for (int q = 0; q < kF; ++q) {
@@ -573,6 +594,8 @@ done:
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512) : "memory");
 }
 
+std::atomic<int32_t> g_schedule{HADROS_SURROGATE_PINGPONG};
+
 int32_t cuda_status(const char* what)
 {
     const cudaError_t e = cudaGetLastError();
@@ -633,6 +656,15 @@ using namespace hadros::mlp;
 extern "C" {
 
 int64_t hadros_mlp_image_bytes(void) { return kImageBytes; }
+
+int32_t hadros_surrogate_schedule(int32_t schedule)
+{
+    if (schedule == -1) return g_schedule.load();
+    if (schedule != HADROS_SURROGATE_LOCKSTEP && schedule != HADROS_SURROGATE_PINGPONG)
+        return set_error(HADROS_E_ARG, "unknown surrogate schedule");
+    g_schedule.store(schedule);
+    return HADROS_OK;
+}
 
 int32_t hadros_mlp_pack_image(const void* packed, void* image, void* stream)
 {
@@ -702,10 +734,15 @@ int32_t hadros_surrogate_image(const hadros_params* p, const hadros_sigma* s, in
     a.spread = out->spread;
     a.fallback_ids = out->fallback_ids;
     a.counters = out->counters;
-    cudaFuncSetAttribute(k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
     const long tiles = (n_px * a.cam.n_bins + kPair * kTileRows - 1) / (kPair * kTileRows);
     const int grid = int(std::min<long>(tiles, n_sm));
-    k_infer<<<grid, kThreads, kSmemBytes, st>>>(a);
+    if (g_schedule.load() == HADROS_SURROGATE_PINGPONG) {
+        cudaFuncSetAttribute(k_infer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        k_infer<true><<<grid, kThreads, kSmemBytes, st>>>(a);
+    } else {
+        cudaFuncSetAttribute(k_infer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        k_infer<false><<<grid, kThreads, kSmemBytes, st>>>(a);
+    }
     return cuda_status("hadros_surrogate_image");
 }
 

@@ -493,6 +493,14 @@ int32_t hadros_mlp_train_step(float* master, void* packed, float* m, float* v, c
 int64_t hadros_mlp_image_bytes(void);
 int32_t hadros_mlp_pack_image(const void* packed, void* image, void* stream);
 
+/* Schedule of the inference kernel's two 128-sample halves: LOCKSTEP (each
+ * streamed weight stage feeds both halves; tensor cores idle during the
+ * epilogue) or PINGPONG (the halves alternate on the tensor cores, one half's
+ * epilogue overlapping the other's products; default).  Process-wide;
+ * hadros_surrogate_schedule(-1) returns the current one. */
+enum hadros_surrogate_schedule_kind { HADROS_SURROGATE_LOCKSTEP = 0, HADROS_SURROGATE_PINGPONG = 1 };
+int32_t hadros_surrogate_schedule(int32_t schedule);
+
 typedef struct hadros_surrogate_out {   /* DEVICE buffers                        */
     float* ln_tau_E;       /* [P][B] ensemble mean of ln tau_E (may be NULL)   */
     float* ln_I_E;         /* [P][B] ensemble mean of ln I_E (may be NULL)     */

@@ -173,6 +173,7 @@ def _random_surrogate(hb, torch, members, seed):
     return sur
 
 
+@pytest.mark.parametrize("schedule", [0, 1])
 @pytest.mark.parametrize("members,n_bins,nx,ny,begin,end,spread_of", [
     (1, 8, 24, 24, 0, None, 0),
     (2, 16, 33, 17, 0, None, 0),
@@ -181,7 +182,7 @@ def _random_surrogate(hb, torch, members, seed):
     (3, 32, 16, 16, 0, None, 1),
 ])
 def test_umma_inference_matches_training_forward(hb, torch, sigma_table, members, n_bins, nx, ny, begin, end,
-                                                 spread_of):
+                                                 spread_of, schedule):
     """The fused tcgen05 kernel and the mma.sync training forward pass compute
     the same network: per-sample ensemble means within BF16 rounding, and the
     per-pixel aggregates and spread as the host forms them from the forward
@@ -196,7 +197,13 @@ def test_umma_inference_matches_training_forward(hb, torch, sigma_table, members
     p = hb.params(**kw)
     P = nx * ny
     end = P if end is None else end
-    res = sur.image(p, sigma_table, pixel_begin=begin, pixel_end=end, threshold=0.05, spread_of=spread_of)
+    old = hb.lib().hadros_surrogate_schedule(-1)
+    assert hb.lib().hadros_surrogate_schedule(schedule) == 0
+    try:
+        res = sur.image(p, sigma_table, pixel_begin=begin, pixel_end=end, threshold=0.05, spread_of=spread_of)
+        torch.cuda.synchronize()
+    finally:
+        hb.lib().hadros_surrogate_schedule(old)
     torch.cuda.synchronize()
     cnt = res["counters"].cpu().numpy()
     assert cnt[1] == 0, "inference kernel aborted"
