@@ -6,7 +6,8 @@
 // buffering, ldmatrix with or without transposition for the three operand
 // layouts of a forward and backward pass) whose epilogue is fused with the
 // surrounding elementwise work:
-//   forward      Z_l = H_{l-1} W_l^T + b_l,  H_l = SiLU(Z_l)     (both BF16)
+//   forward      Z_l = H_{l-1} W_l^T + b_l,  H_l = SiLU(Z_l)     (both BF16;
+//                SiLU in packed BF16 from h = Z_l / 2, hadros_mlp.cuh)
 //   data grad    dZ_{l-1} = (dZ_l W_l) * SiLU'(Z_{l-1})          (BF16)
 //   weight grad  G_Wl += dZ_l^T H_{l-1}   (split over the batch, FP32 atomics)
 // The 2-output last layer, the loss, bias gradients and Adam are small
@@ -190,8 +191,7 @@ struct EpiHidden {   // Z = acc + b (BF16, for the backward pass), H = SiLU(acc 
         const float z0 = v0 + bias[n], z1 = v1 + bias[n + 1];
         const long o = long(m) * kW + n;
         if (Z) *reinterpret_cast<uint32_t*>(Z + o) = pack_bf16x2(z0, z1);
-        const float2 h = silu2(z0, z1);
-        *reinterpret_cast<uint32_t*>(H + o) = pack_bf16x2(h.x, h.y);
+        *reinterpret_cast<uint32_t*>(H + o) = silu_half_bf16x2(0.5f * z0, 0.5f * z1);
     }
 };
 
@@ -202,8 +202,7 @@ struct EpiBwdData {   // dZ_prev = acc * SiLU'(Z_prev)
     {
         const long o = long(m) * kW + n;
         const float2 z = unpack_bf16x2(*reinterpret_cast<const uint32_t*>(Zp + o));
-        const float2 g = silu_grad2(z.x, z.y);
-        *reinterpret_cast<uint32_t*>(dZp + o) = pack_bf16x2(v0 * g.x, v1 * g.y);
+        *reinterpret_cast<uint32_t*>(dZp + o) = pack_bf16x2(v0 * silu_grad_f(z.x), v1 * silu_grad_f(z.y));
     }
 };
 

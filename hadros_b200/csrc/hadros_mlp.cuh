@@ -22,7 +22,6 @@
 
 #ifdef __CUDACC__
 #include <cuda_bf16.h>
-#include <cuda_fp16.h>
 #endif
 
 namespace hadros {
@@ -96,30 +95,28 @@ struct Norm {
 
 #ifdef __CUDACC__
 
-// sigma(z) = (1 + tanh(z/2)) / 2 for a pair of values, with tanh on the
-// paired FP16 unit (tanh.approx.f16x2: one MUFU operation for two values).
-// The same function in every kernel, so the trained network and the
-// inferred one agree.
-__device__ __forceinline__ float2 sigmoid2(float z0, float z1)
+// SiLU(z) = z sigma(z) = h + h tanh(h) with h = z / 2, evaluated on a pair of
+// values in packed BF16: h is rounded to BF16, tanh runs on the paired unit
+// (tanh.approx.bf16x2) and the result is one fused multiply-add rounded to
+// BF16, the activation's storage type.  Takes h (FP32) and returns the packed
+// BF16 pair.  The same function in every kernel, so the trained network and
+// the inferred one agree; the inference kernel folds the 1/2 into its weights.
+__device__ __forceinline__ uint32_t silu_half_bf16x2(float h0, float h1)
 {
-    uint32_t hz, ht;
-    asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(hz) : "f"(0.5f * z1), "f"(0.5f * z0));
-    asm("tanh.approx.f16x2 %0, %1;" : "=r"(ht) : "r"(hz));
-    const __half2 t = *reinterpret_cast<const __half2*>(&ht);
-    const float2 tf = __half22float2(t);
-    return make_float2(fmaf(0.5f, tf.x, 0.5f), fmaf(0.5f, tf.y, 0.5f));
+    uint32_t hb, t, y;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(hb) : "f"(h1), "f"(h0));
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(hb));
+    asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(y) : "r"(hb), "r"(t));
+    return y;
 }
-__device__ __forceinline__ float2 silu2(float z0, float z1)
+// d SiLU / dz at z (FP32 tanh): (1 + tanh(h) + h (1 - tanh(h)^2)) / 2.
+__device__ __forceinline__ float silu_grad_f(float z)
 {
-    const float2 s = sigmoid2(z0, z1);
-    return make_float2(z0 * s.x, z1 * s.y);
+    const float h = 0.5f * z;
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(h));
+    return 0.5f * (1.0f + t + h * fmaf(-t, t, 1.0f));
 }
-__device__ __forceinline__ float2 silu_grad2(float z0, float z1)
-{
-    const float2 s = sigmoid2(z0, z1);
-    return make_float2(fmaf(z0 * s.x, 1.0f - s.x, s.x), fmaf(z1 * s.y, 1.0f - s.y, s.y));
-}
-__device__ __forceinline__ float silu_grad_f(float z) { return silu_grad2(z, 0.0f).x; }
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
 {

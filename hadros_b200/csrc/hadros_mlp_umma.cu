@@ -129,6 +129,8 @@ __global__ void k_pack_image(const bf16* __restrict__ packed, uint8_t* __restric
         const int kunit = unit ^ (row & 7);
         for (int t = 0; t < 8; ++t) e[t] = packed[pw(5) + long(row) * kW + c * 64 + kunit * 8 + t];
     }
+    if (q < kStagesPerMember - 1)   // hidden layers: weights / 2 (exact), see epi_chunk
+        for (int t = 0; t < 8; ++t) e[t] = __float2bfloat16_rn(0.5f * __bfloat162float(e[t]));
     v = *reinterpret_cast<const uint4*>(e);
     *reinterpret_cast<uint4*>(image + byte) = v;
 }
@@ -244,15 +246,25 @@ __device__ __forceinline__ void tc_wait_ld(uint32_t& r0, uint32_t& r1)
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" : "+r"(r0), "+r"(r1) : : "memory");
 }
 
+// (a0, a1) + (b0, b1) with one packed FP32x2 addition.
+__device__ __forceinline__ void add_f32x2(uint32_t& a0, uint32_t& a1, float2 b)
+{
+    asm("{\n.reg .b64 x, y;\nmov.b64 x, {%0, %1};\nmov.b64 y, {%2, %3};\n"
+        "add.rn.f32x2 x, x, y;\nmov.b64 {%0, %1}, x;\n}\n"
+        : "+r"(a0), "+r"(a1)
+        : "f"(b.x), "f"(b.y));
+}
+
 // Bias, SiLU and BF16 store of 32 accumulator columns [cb, cb+32) of row r.
-__device__ __forceinline__ void epi_chunk(const uint32_t (&v)[32], const float* sb, int cb, uint8_t* act, int r)
+// The weights and biases of the hidden layers are pre-scaled by 1/2, so the
+// accumulator plus bias is h = z / 2.
+__device__ __forceinline__ void epi_chunk(uint32_t (&v)[32], const float* sb, int cb, uint8_t* act, int r)
 {
     uint32_t h[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
-        const float2 bb = *reinterpret_cast<const float2*>(sb + cb + 2 * q);
-        const float2 y = silu2(__uint_as_float(v[2 * q]) + bb.x, __uint_as_float(v[2 * q + 1]) + bb.y);
-        h[q] = pack_bf16x2(y.x, y.y);
+        add_f32x2(v[2 * q], v[2 * q + 1], *reinterpret_cast<const float2*>(sb + cb + 2 * q));
+        h[q] = silu_half_bf16x2(__uint_as_float(v[2 * q]), __uint_as_float(v[2 * q + 1]));
     }
     uint8_t* chunk = act + (cb >> 6) * 16384 + r * 128;
     const int u0 = (cb & 63) >> 3;   // logical 16-byte unit of column cb
@@ -307,7 +319,7 @@ static_assert(kSmemBytes <= 232448, "shared memory above the sm_100 per-block li
 // so one half's epilogue overlaps the other half's MMAs; every weight stage
 // is streamed once per half.
 template <bool PP>
-__global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
+__global__ void __maxnreg__(200) k_infer(const InferArgs A)   // 10 warps x 32 x 200 <= 65536
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -466,8 +478,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                 // previous member's were last read before its closing barrier)
                 {
                     const int gt = PP ? r : trow;      // thread within the group
-                    for (int e = gt; e < 4 * kW; e += kGroupWarps * 32)
-                        my_bias[e] = P[off_b(1 + e / kW) + e % kW];
+                    for (int e = gt; e < 4 * kW; e += kGroupWarps * 32)   // hidden biases / 2
+                        my_bias[e] = 0.5f * P[off_b(1 + e / kW) + e % kW];
                     if (gt < kOut) my_bias[4 * kW + gt] = P[kOffB5 + gt];
                     if (gt < kOut * kF) my_bias[4 * kW + kOut + gt] = P[kOffWs + gt];
                 }

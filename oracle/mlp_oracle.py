@@ -14,8 +14,9 @@ check the GPU gradients:
   out = H4 W5^T + b5 + x Ws^T
 
 With ``rounded=True`` the values are rounded to BF16 where the kernels store
-BF16 (weights, Z_l, H_l, dZ_l), so the GPU and the oracle differ only by FP32
-accumulation order and by the hardware tanh approximation inside SiLU.  With
+BF16 (weights, Z_l, H_l, dZ_l) and SiLU is evaluated as the kernels do (from
+h = bf16(Z_l) / 2 in BF16 arithmetic), so the GPU and the oracle differ only
+by FP32 accumulation order and by the hardware tanh approximation.  With
 ``rounded=False`` it is the exact float64 network, whose gradient the tests
 check against finite differences.
 """
@@ -87,17 +88,22 @@ def split_features(raw: np.ndarray, mu: np.ndarray, inv_sd: np.ndarray) -> np.nd
     return np.concatenate([hi, lo, four], axis=1)
 
 
-def _sig(z):
-    return 0.5 * np.tanh(0.5 * z) + 0.5
-
-
 def silu(z):
-    return z * _sig(z)
+    """z sigma(z) = h + h tanh(h), h = z / 2."""
+    h = 0.5 * z
+    return h + h * np.tanh(h)
+
+
+def silu_bf16(z):
+    """The kernels' SiLU: h = bf16(z) / 2, y = bf16(h + h * bf16(tanh h))."""
+    h = 0.5 * bf16(z)
+    return bf16(h + h * bf16(np.tanh(h)))
 
 
 def silu_grad(z):
-    s = _sig(z)
-    return s + z * s * (1.0 - s)
+    h = 0.5 * z
+    t = np.tanh(h)
+    return 0.5 * (1.0 + t + h * (1.0 - t * t))
 
 
 def forward(master, X, rounded: bool = True):
@@ -114,7 +120,7 @@ def forward(master, X, rounded: bool = True):
     for l in range(1, DEPTH + 1):
         z = Hs[l - 1] @ Wd[l].T + P[f"b{l}"]
         Zs[l] = r(z)
-        Hs[l] = r(silu(z))
+        Hs[l] = silu_bf16(z) if rounded else silu(z)
     out = Hs[DEPTH] @ W5.T + P["b5"] + x @ P["Ws"].T
     return out, {"Z": Zs, "H": Hs, "W": Wd, "W5": W5, "x": x, "r": r}
 
