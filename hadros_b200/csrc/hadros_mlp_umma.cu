@@ -319,7 +319,7 @@ static_assert(kSmemBytes <= 232448, "shared memory above the sm_100 per-block li
 // so one half's epilogue overlaps the other half's MMAs; every weight stage
 // is streamed once per half.
 template <bool PP>
-__global__ void __maxnreg__(200) k_infer(const InferArgs A)   // 10 warps x 32 x 200 <= 65536
+__global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -456,7 +456,6 @@ __global__ void __maxnreg__(200) k_infer(const InferArgs A)   // 10 warps x 32 x
             const bool valid = s < n_samples;
             const long lp = valid ? s / B : 0;
             const int b = valid ? int(s % B) : 0;
-            float x[kF];
             uint32_t feat[kIn / 2];
             {
                 float f[kF], xn[kF];
@@ -465,8 +464,6 @@ __global__ void __maxnreg__(200) k_infer(const InferArgs A)   // 10 warps x 32 x
                 for (int q = 0; q < kF; ++q) xn[q] = valid ? (f[q] - A.norm.feat_mu[q]) * A.norm.feat_inv_sd[q] : 0.0f;
                 __align__(16) bf16 row[kIn];
                 input_row(xn, row);
-#pragma unroll
-                for (int q = 0; q < kF; ++q) x[q] = __bfloat162float(row[q]) + __bfloat162float(row[kF + q]);
 #pragma unroll
                 for (int q = 0; q < kIn / 2; ++q) feat[q] = reinterpret_cast<const uint32_t*>(row)[q];
             }
@@ -526,9 +523,11 @@ __global__ void __maxnreg__(200) k_infer(const InferArgs A)   // 10 warps x 32 x
                 const float* st = my_bias + 4 * kW;
                 float a0 = __uint_as_float(o0) + st[0], a1 = __uint_as_float(o1) + st[1];
 #pragma unroll
-                for (int q = 0; q < kF; ++q) {
-                    a0 = fmaf(st[kOut + q], x[q], a0);
-                    a1 = fmaf(st[kOut + kF + q], x[q], a1);
+                for (int q = 0; q < kF / 2; ++q) {   // skip input x = hi + lo, from the feature registers
+                    const float2 hi = unpack_bf16x2(feat[q]), lo = unpack_bf16x2(feat[kF / 2 + q]);
+                    const float x0 = hi.x + lo.x, x1 = hi.y + lo.y;
+                    a0 = fmaf(st[kOut + 2 * q], x0, fmaf(st[kOut + 2 * q + 1], x1, a0));
+                    a1 = fmaf(st[kOut + kF + 2 * q], x0, fmaf(st[kOut + kF + 2 * q + 1], x1, a1));
                 }
                 const float ltau = fmaf(a0, A.norm.out_sd[0], A.norm.out_mu[0]);
                 const float lnI = fmaf(a1, A.norm.out_sd[1], A.norm.out_mu[1]);
