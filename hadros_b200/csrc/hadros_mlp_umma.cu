@@ -61,6 +61,7 @@ struct SurCam {
     float log10E[kMaxBinsS];
     float ln_dE[kMaxBinsS];   // -inf for bins outside the aggregates
     float w[kMaxBinsS];       // aggregation weight (0 outside)
+    float wsum;               // sum of w
     float ln_sw[kMaxBinsS];   // spread: log-sum-exp over bins of out + ln_sw
     int32_t spread_out;       // 0: ln I_E (ln_sw = ln dE), 1: ln tau_E (ln w / sum w)
 };
@@ -306,7 +307,7 @@ struct InferArgs {
 };
 
 constexpr int kBiasFloats = 4 * kW + kOut + kOut * kF + 6;   // + padding to 8 bytes
-constexpr int kSmemBytes = kPair * kActBytes + kStages * kStageBytes + 2 * 256 * 4 + 2 * kBiasFloats * 4 + 256 + 1024;
+constexpr int kSmemBytes = kPair * kActBytes + kStages * kStageBytes + 2 * 256 * 4 + 4 * kBiasFloats * 4 + 256 + 1024;
 
 // First stage (in a member's weight image) of layer L and its stage count.
 __host__ __device__ constexpr int stage_of(int L) { return L == 1 ? 0 : (L == 5 ? kStagesPerMember - 1 : 1 + (L - 2) * 4); }
@@ -327,8 +328,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
     uint8_t* stage = smem + kPair * kActBytes;                // [2][32 KB]
     float* red_a = reinterpret_cast<float*>(stage + kStages * kStageBytes);   // [256]
     float* red_b = red_a + 256;                                               // [256]
-    float* sbias = red_b + 256;        // per epilogue group: b1..b4 [4][256], b5 [2], Ws [2][16]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sbias + 2 * kBiasFloats);
+    float* sbias = red_b + 256;        // per epilogue group and member parity: b1..b4 [4][256], b5 [2], Ws [2][16]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sbias + 4 * kBiasFloats);
     uint64_t* full = bars;                 // [kStages]
     uint64_t* empty = bars + kStages;      // [kStages]
     uint64_t* acc_full = bars + 2 * kStages;        // [2] (PP: one per half)
@@ -446,7 +447,49 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
         const int r = qw * 32 + lane;                 // row in the 128-row half
         const int trow = t * kTileRows + r;           // row in the 256-sample tile
         uint8_t* my_act = act + t * kActBytes;
-        float* my_bias = sbias + grp * kBiasFloats;
+        long member_count = 0;   // biases are double-buffered by member parity
+        // Segmented reduction over the B consecutive rows (threads) of a pixel:
+        // on entry m = this row's log-sum-exp term, x1, x2 this row's plain
+        // terms; on exit m = the pixel's maximum, se = sum exp(term - m), x1, x2
+        // the pixel's sums.  Pixels of <= 32 bins reduce within a warp; larger
+        // ones combine their warps through shared memory.
+        auto pixel_reduce = [&](float& m, float& se, float& x1, float& x2) -> bool {
+            const int width = B < 32 ? B : 32;
+            const float v = m;
+            for (int off = 1; off < width; off <<= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+            se = (m == -INFINITY) ? 0.0f : __expf(v - m);
+            for (int off = 1; off < width; off <<= 1) {
+                se += __shfl_xor_sync(0xffffffffu, se, off);
+                x1 += __shfl_xor_sync(0xffffffffu, x1, off);
+                x2 += __shfl_xor_sync(0xffffffffu, x2, off);
+            }
+            if (B > 32) {
+                float* wr = red_a + (t * 4 + qw) * 4;
+                if (lane == 0) {
+                    wr[0] = m;
+                    wr[1] = se;
+                    wr[2] = x1;
+                    wr[3] = x2;
+                }
+                if (!epi_sync()) return false;
+                const int nw = B / 32, w0 = t * 4 + (qw / nw) * nw;
+                float M = -INFINITY;
+                for (int j = 0; j < nw; ++j) M = fmaxf(M, red_a[(w0 + j) * 4]);
+                float S = 0.0f, X1 = 0.0f, X2 = 0.0f;
+                for (int j = 0; j < nw; ++j) {
+                    const float* q = red_a + (w0 + j) * 4;
+                    S += (q[0] == -INFINITY) ? 0.0f : q[1] * __expf(q[0] - M);
+                    X1 += q[2];
+                    X2 += q[3];
+                }
+                m = M;
+                se = S;
+                x1 = X1;
+                x2 = X2;
+                if (!epi_sync()) return false;   // slots free for the next reduction
+            }
+            return true;
+        };
         const uint32_t lane_base = tmem + (uint32_t(qw * 32) << 16) + uint32_t(t * 256);
         long layer_count = 0;
         const bool leader_possible = (trow % B) == 0;
@@ -469,10 +512,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
             }
             float sum_tau = 0.0f, sum_lnI = 0.0f;
             float w_ref = 0.0f, w_s1 = 0.0f, w_s2 = 0.0f;   // pixel leader: shifted sums of ln I_k
-            for (int k = 0; k < K; ++k) {
+            for (int k = 0; k < K; ++k, ++member_count) {
                 const float* P = A.masters + long(k) * kParams;
-                // this member's biases and skip weights -> shared memory (the
-                // previous member's were last read before its closing barrier)
+                float* my_bias = sbias + (grp * 2 + int(member_count & 1)) * kBiasFloats;
+                // this member's biases and skip weights -> shared memory (this
+                // buffer was last read two members ago, before the barrier below
+                // of the previous member)
                 {
                     const int gt = PP ? r : trow;      // thread within the group
                     for (int e = gt; e < 4 * kW; e += kGroupWarps * 32)   // hidden biases / 2
@@ -534,20 +579,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                 sum_tau += ltau;
                 sum_lnI += lnI;
                 // this member's ln I_obs (or ln tau) per pixel: log-sum-exp over the bins
-                red_a[trow] = valid ? (A.cam.spread_out ? ltau : lnI) + A.cam.ln_sw[b] : -INFINITY;
-                if (!epi_sync()) goto done;
-                if (leader_possible && valid) {
-                    float m = -INFINITY;
-                    for (int q = 0; q < B; ++q) m = fmaxf(m, red_a[trow + q]);
-                    float sacc = 0.0f;
-                    for (int q = 0; q < B; ++q) sacc += __expf(red_a[trow + q] - m);
-                    const float Lk = m + __logf(sacc);
-                    if (k == 0) w_ref = Lk;
-                    const float d = Lk - w_ref;
-                    w_s1 += d;
-                    w_s2 += d * d;
+                {
+                    float m = valid ? (A.cam.spread_out ? ltau : lnI) + A.cam.ln_sw[b] : -INFINITY;
+                    float se, x1 = 0.0f, x2 = 0.0f;
+                    if (!pixel_reduce(m, se, x1, x2)) goto done;
+                    if (leader_possible && valid) {
+                        const float Lk = m + __logf(se);
+                        if (k == 0) w_ref = Lk;
+                        const float d = Lk - w_ref;
+                        w_s1 += d;
+                        w_s2 += d * d;
+                    }
                 }
-                if (!epi_sync()) goto done;
             }
             // ensemble means -> per-sample outputs and per-pixel aggregates
             const float inv_k = 1.0f / float(K);
@@ -556,33 +599,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                 if (A.ln_tau_E) A.ln_tau_E[s] = ltau;
                 if (A.ln_I_E) A.ln_I_E[s] = lnI;
             }
-            red_a[trow] = valid ? lnI + A.cam.ln_dE[b] : -INFINITY;
-            red_b[trow] = valid ? fmaxf(__expf(ltau) - A.norm.out_floor[0], 0.0f) : 0.0f;
-            if (!epi_sync()) goto done;
-            if (leader_possible && valid) {
-                float m = -INFINITY;
-                for (int q = 0; q < B; ++q) m = fmaxf(m, red_a[trow + q]);
-                double sacc = 0.0, wsum = 0.0, tsum = 0.0, psum = 0.0;
-                for (int q = 0; q < B; ++q) {
-                    if (m > -INFINITY) sacc += exp(double(red_a[trow + q] - m));
-                    const double w = A.cam.w[q];
-                    wsum += w;
-                    tsum += w * red_b[trow + q];
-                    psum += w * exp(-double(red_b[trow + q]));
-                }
-                const double I = m > -INFINITY ? exp(double(m)) * sacc : 0.0;
-                const float mean = w_s1 * inv_k;
-                const float sd = sqrtf(fmaxf(w_s2 * inv_k - mean * mean, 0.0f));
-                A.tau[lp] = wsum > 0.0 ? tsum / wsum : 0.0;
-                A.P_surv[lp] = wsum > 0.0 ? psum / wsum : 1.0;
-                A.I_obs[lp] = I;
-                A.spread[lp] = sd;
-                if (sd > A.spread_threshold) {
-                    const int slot = atomicAdd(A.counters, 1);
-                    A.fallback_ids[slot] = int32_t(A.pixel_begin + lp);
+            {
+                const float tau_b = valid ? fmaxf(__expf(ltau) - A.norm.out_floor[0], 0.0f) : 0.0f;
+                const float wb = valid ? A.cam.w[b] : 0.0f;
+                float m = valid ? lnI + A.cam.ln_dE[b] : -INFINITY;
+                float se, x1 = wb * tau_b, x2 = wb * __expf(-tau_b);
+                if (!pixel_reduce(m, se, x1, x2)) goto done;
+                if (leader_possible && valid) {
+                    const double wsum = A.cam.wsum;
+                    const double I = m > -INFINITY ? exp(double(m)) * double(se) : 0.0;
+                    const float mean = w_s1 * inv_k;
+                    const float sd = sqrtf(fmaxf(w_s2 * inv_k - mean * mean, 0.0f));
+                    A.tau[lp] = wsum > 0.0 ? double(x1) / wsum : 0.0;
+                    A.P_surv[lp] = wsum > 0.0 ? double(x2) / wsum : 1.0;
+                    A.I_obs[lp] = I;
+                    A.spread[lp] = sd;
+                    if (sd > A.spread_threshold) {
+                        const int slot = atomicAdd(A.counters, 1);
+                        A.fallback_ids[slot] = int32_t(A.pixel_begin + lp);
+                    }
                 }
             }
-            if (!epi_sync()) goto done;
         }
     }
 done:
@@ -649,6 +686,7 @@ int32_t make_surcam(const hadros_params* p, const hadros_sigma* s, SurCam* c, in
         if (in && w[b] > 0.0) wsum += w[b];
     }
     c->spread_out = spread_out;
+    c->wsum = float(wsum);
     for (int b = 0; b < nb; ++b) {
         const bool in = valid[b] != 0 && dE[b] > 0.0;
         if (spread_out == 0) c->ln_sw[b] = c->ln_dE[b];

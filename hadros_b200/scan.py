@@ -7,8 +7,9 @@ production: the surrogate is trained on rays the tracer traces at other
 parameter points of the same box (collapsar_ndaf_like, density_weighted
 source, a = 0.95, rho0 log-uniform in [1e9, 1e12], inclination in [10, 80]
 deg); each scan point is then evaluated by the ensemble, the pixels whose
-spread of ln I_obs exceeds the threshold are traced exactly, and the exact
-tracer judges a seeded random 1% of the pixels.  The plain tracer's time per
+predicted error bound (sigmas x the ensemble standard deviation of ln I_obs)
+exceeds --bound are traced exactly, and the exact tracer judges a seeded
+random 1% of the pixels.  The plain tracer's time per
 point is measured on a few points of the same scan.
 
 inference: the surrogate is trained on cameras with randomized spin,
@@ -157,7 +158,8 @@ def run_production(a) -> dict:
     setup = info["trace_s"] + info["fit_s"]
     return {
         "workload": "production_scan", "points": a.points, "side": a.side, "bins": a.bins,
-        "members": a.members, "threshold": a.threshold, "judge_frac": a.judge,
+        "members": a.members, "bound": a.bound, "sigmas": a.sigmas, "threshold": a.threshold,
+        "judge_frac": a.judge,
         "train": info,
         "surrogate_s_per_point": sur_total / len(rows),
         "plain_s_per_point": plain_per_point,
@@ -201,9 +203,13 @@ def main(argv=None) -> None:
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=2e-3)
-    ap.add_argument("--threshold", type=float, default=0.01)
+    ap.add_argument("--bound", type=float, default=0.01,
+                    help="relative error bound above which a pixel is traced exactly")
+    ap.add_argument("--sigmas", type=float, default=3.0,
+                    help="the bound is this many ensemble standard deviations")
     ap.add_argument("--judge", type=float, default=0.01)
     a = ap.parse_args(argv)
+    a.threshold = a.bound / a.sigmas
     if a.workload == "production":
         a.side = a.side or 4096
         a.bins = a.bins or 64
