@@ -68,9 +68,16 @@ def errors(I_ex: np.ndarray, I_sur: np.ndarray, floor_rel: float = 1e-6) -> dict
             "median": float(np.median(rel))}
 
 
+CANDIDATE_THRESHOLDS = (0.002, 0.0025, 0.0033, 0.004, 0.005, 0.0067, 0.01)
+
+
 def surrogate_point(ctx, sigma, sur, p, threshold: float, judge_frac: float, rng, buf=None,
                     spread_of: int = 0) -> dict:
-    """One scan point: surrogate image, exact fallback, exact judge subset."""
+    """One scan point: surrogate image, exact fallback, exact judge subset.
+
+    Besides the errors of the result, reports for other spread thresholds what
+    they would have given: the fraction of pixels above them and the worst
+    judged error among the pixels below them (the surrogate's values there)."""
     torch = _torch()
     P = int(p.nx) * int(p.ny)
     torch.cuda.synchronize()
@@ -84,24 +91,38 @@ def surrogate_point(ctx, sigma, sur, p, threshold: float, judge_frac: float, rng
     # the fallback pixels and the judged pixels are traced exactly in one launch
     jn = max(1, int(round(judge_frac * P)))
     jids = np.sort(rng.choice(P, size=jn, replace=False)).astype(np.int32)
+    jt = torch.from_numpy(jids.astype(np.int64)).cuda()
+    keys = ("I_obs", "tau", "P_surv")
+    raw_j = {k: res[k][jt] for k in keys}                 # surrogate values before the fallback
+    spread_j = res["spread"][jt]
     fb, jex = ctx.batch_pixels([p, p], sigma, [ids, jids], outputs=("tau", "P_surv", "I_obs"))
     if ids.size:
         idx = torch.from_numpy(ids.astype(np.int64)).cuda()
-        for k in ("tau", "P_surv", "I_obs"):
+        for k in keys:
             res[k].index_copy_(0, idx, torch.from_numpy(fb[k]).cuda())
     torch.cuda.synchronize()
     t_total = time.perf_counter() - t0
     t_fb = t_total - t_inf
-    jt = torch.from_numpy(jids.astype(np.int64)).cuda()
-    sur_v = {k: res[k][jt].cpu().numpy() for k in ("I_obs", "tau", "P_surv")}
+    sur_v = {k: res[k][jt].cpu().numpy() for k in keys}
+    raw_v = {k: v.cpu().numpy() for k, v in raw_j.items()}
+    sj = spread_j.cpu().numpy()
     fb_mask = np.isin(jids, ids)
     key = "I_obs" if spread_of == 0 else "tau"
+    what_if = []
+    sp = res["spread"]
+    for thr in CANDIDATE_THRESHOLDS:
+        keep = sj <= thr
+        e = errors(jex[key][keep], raw_v[key][keep]) if keep.any() else {"worst": 0.0, "n": 0}
+        what_if.append({"threshold": thr, "fallback_frac": float((sp > thr).float().mean().item()),
+                        "worst": e["worst"], "n": e["n"]})
     return {"seconds": t_total, "inference_s": t_inf, "exact_s": t_fb,
             "fallback_pixels": int(ids.size), "fallback_frac": ids.size / P, "judged": int(jn),
             "judged_quantity": key,
             "error": errors(jex[key], sur_v[key]),
             "error_surrogate_pixels": errors(jex[key][~fb_mask], sur_v[key][~fb_mask]),
-            "P_surv_max_abs_error": float(np.abs(jex["P_surv"] - sur_v["P_surv"]).max())}
+            "P_surv_max_abs_error": float(np.abs(jex["P_surv"] - sur_v["P_surv"]).max()),
+            "spread_quantiles": [float(q) for q in np.quantile(sj, [0.5, 0.9, 0.99, 0.999])],
+            "what_if": what_if}
 
 
 def production_cam(rho0: float, theta_deg: float, side: int, n_bins: int):
@@ -132,14 +153,34 @@ def train(ctx, sigma, cams, pixels_per_cam: int, members: int, epochs: int, seed
     return sur, info
 
 
+def save_model(path, sur, info: dict) -> None:
+    """The ensemble (npz) and its training record (json beside it)."""
+    sur.save(path)
+    with open(str(path) + ".json", "w") as f:
+        json.dump(info, f, default=float)
+
+
+def load_model(path) -> tuple[object, dict]:
+    sur = S.Surrogate.load(path)
+    with open(str(path) + ".json") as f:
+        info = json.load(f)
+    info["loaded_from"] = str(path)
+    return sur, info
+
+
 def run_production(a) -> dict:
     torch = _torch()
     E, g2, s = W.synthetic_sigma_arrays()
     sigma = SigmaTable.from_arrays(E, s, g2)
     with Context(0) as ctx:
-        tpts = W.scan_points(a.train_points, seed=W.SEED + 17)
-        cams = [production_cam(r, t, a.train_side, a.bins) for r, t in tpts]
-        sur, info = train(ctx, sigma, cams, a.pixels_per_cam, a.members, a.epochs, W.SEED, a.batch, a.lr)
+        if a.load:
+            sur, info = load_model(a.load)
+        else:
+            tpts = W.scan_points(a.train_points, seed=W.SEED + 17)
+            cams = [production_cam(r, t, a.train_side, a.bins) for r, t in tpts]
+            sur, info = train(ctx, sigma, cams, a.pixels_per_cam, a.members, a.epochs, W.SEED, a.batch, a.lr)
+            if a.save:
+                save_model(a.save, sur, info)
         pts = W.scan_points(a.points, seed=W.SEED)
         rng = np.random.default_rng(W.SEED + 5)
         buf = S.alloc_image(a.side * a.side, a.bins, sur.device, per_bin=False)
@@ -208,6 +249,8 @@ def main(argv=None) -> None:
     ap.add_argument("--sigmas", type=float, default=3.0,
                     help="the bound is this many ensemble standard deviations")
     ap.add_argument("--judge", type=float, default=0.01)
+    ap.add_argument("--save", default=None, help="write the trained ensemble here (npz + json)")
+    ap.add_argument("--load", default=None, help="use an ensemble written by --save instead of training")
     a = ap.parse_args(argv)
     a.threshold = a.bound / a.sigmas
     if a.workload == "production":
