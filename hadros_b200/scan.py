@@ -197,6 +197,8 @@ def run_production(a) -> dict:
     sur_total = sum(x["seconds"] for x in rows)
     plain_per_point = float(np.mean(plain)) if plain else float("nan")
     setup = info["trace_s"] + info["fit_s"]
+    n_full = a.scan_total or len(rows)
+    sur_per_point = sur_total / len(rows)
     return {
         "workload": "production_scan", "points": a.points, "side": a.side, "bins": a.bins,
         "members": a.members, "bound": a.bound, "sigmas": a.sigmas, "threshold": a.threshold,
@@ -205,6 +207,8 @@ def run_production(a) -> dict:
         "surrogate_s_per_point": sur_total / len(rows),
         "plain_s_per_point": plain_per_point,
         "speedup_scan": plain_per_point * len(rows) / (sur_total + setup),
+        "scan_total_points": n_full,
+        "speedup_full_scan": plain_per_point * n_full / (setup + n_full * sur_per_point),
         "speedup_per_point": plain_per_point * len(rows) / sur_total,
         "fallback_frac_mean": float(np.mean([x["fallback_frac"] for x in rows])),
         "worst_pixel_error": max(x["error"]["worst"] for x in rows),
@@ -234,6 +238,9 @@ def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("workload", choices=("production", "inference"))
     ap.add_argument("--points", type=int, default=256)
+    ap.add_argument("--scan-total", type=int, default=0,
+                    help="points of the whole scan when --points runs its first ones (for the "
+                         "extrapolated speedup; 0 = --points)")
     ap.add_argument("--plain-points", type=int, default=2)
     ap.add_argument("--side", type=int, default=None)
     ap.add_argument("--bins", type=int, default=None)
