@@ -16,6 +16,7 @@ the trace kernel.  One process per GPU; each GPU traces its own image per step
               over a strided pixel subset of the same image
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py --workload surrogate     # the surrogate's tcgen05 inference kernel
 """
 from __future__ import annotations
 
@@ -371,6 +372,134 @@ def gpu_arm(args) -> None:
         dist.destroy_process_group()
 
 
+# Algorithmic BF16 work of one surrogate network on one (pixel, bin) sample:
+# 64 -> 256, 3 x (256 -> 256), 256 -> 2 (multiply-add = 2 flop).
+F_MLP = 2 * (64 * 256 + 3 * 256 * 256 + 256 * 2)
+
+
+def measured_bf16_peak() -> tuple[float, str]:
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        if d.get("bf16_tflops"):
+            return float(d["bf16_tflops"]), "MEASURED_PEAKS.json bf16_tflops (burst, cuBLAS 8192^3)"
+    return 1590.0, "fallback 1.59 PFLOP/s (no MEASURED_PEAKS.json)"
+
+
+def surrogate_arm(args) -> None:
+    """Surrogate inference: the fused tcgen05 kernel evaluating an ensemble of
+    4 networks on every (pixel, bin) of the config-4 inference image (mixed_512
+    camera at 2048 x 2048, 32 bins).  Random weights: the kernel's work does not
+    depend on their values."""
+    import torch
+
+    import hadros_b200 as hb
+    from hadros_b200 import surrogate as S
+    from hadros_b200 import workloads as W
+
+    rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    side, B, K = args.side or 2048, args.bins or 32, 4
+    E, g2, sg = W.synthetic_sigma_arrays()
+    sig = hb.SigmaTable.from_arrays(E, sg, g2)
+    kw = W.surrogate_inference_image(nx=side, ny=side, n_bins=B)
+    p = hb.params(**kw)
+    P = side * side
+    sur = S.Surrogate(members=K, device=local, seed=1)
+    nm = hb.abi.HadrosMlpNorm()
+    mu = [0.0, 0.0, 0.9, 0.5, 10.5] + [0.0] * 8 + [10.0, 0.3, 8.0]
+    sd = [7.7, 7.7, 0.3, 0.3, 1.0] + [1.0] * 8 + [2.3, 0.1, 2.0]
+    for j in range(16):
+        nm.feat_mu[j], nm.feat_inv_sd[j] = mu[j], 1.0 / sd[j]
+    nm.out_mu[0], nm.out_sd[0], nm.out_mu[1], nm.out_sd[1] = 5.0, 6.0, -60.0, 8.0
+    nm.out_floor[0] = S.TAU_FLOOR
+    sur.norm = nm
+    out = S.alloc_image(P, B, device, per_bin=True)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
+    stream = torch.cuda.Stream(device=device)
+    torch.cuda.set_stream(stream)
+    for _ in range(args.warmup):
+        sur.image(p, sig, threshold=0.005, out=out, stream=stream)
+        flush.zero_()
+    torch.cuda.synchronize()
+    if out["counters"][1].item():
+        raise RuntimeError("surrogate inference kernel aborted")
+    gpu_index = local
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_index) as clocks:
+        t_start.record(stream)
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            sur.image(p, sig, threshold=0.005, out=out, stream=stream)
+            ev[k][1].record(stream)
+            flush.zero_()
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    clk = clocks.summary()
+    per_step = max_over_ranks(t_start.elapsed_time(t_end) / 1e3) / args.steps
+    kern_s = statistics.mean(a.elapsed_time(b) for a, b in ev) / 1e3
+    achieved = P * B * K * F_MLP / kern_s / 1e12
+    peak, peak_src = measured_bf16_peak()
+    # e2e: the same call plus the per-pixel results read back to pinned host memory
+    host = {k: torch.empty(out[k].shape, dtype=out[k].dtype, pin_memory=True)
+            for k in ("tau", "P_surv", "I_obs", "spread")}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    d2h = 0
+    for _ in range(args.steps):
+        sur.image(p, sig, threshold=0.005, out=out, stream=stream, per_bin=False)
+        for k, h in host.items():
+            h.copy_(out[k], non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0) / args.steps
+    d2h = sum(h.numel() * h.element_size() for h in host.values())
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        c = cpu_sample(kw, 160, host_threads())
+        cpu = {"value": c["value"], "unit": "pixel-bins/s", "cores": c["cores"], "kind": c["kind"],
+               "sample": describe_cpu(c, p.nx, p.ny) + " (the exact tracer the surrogate stands in for)"}
+    if rank == 0:
+        line = {
+            "metric": "pixel-bins/sec", "value": world * P * B / per_step, "unit": "pixel-bins/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "data": "synthetic (random network weights; the work does not depend on them)",
+            "config": {"workload": f"surrogate inference: ensemble of {K} networks (64 -> 4x256 -> 2) on "
+                                   f"every pixel and bin of the mixed_512 camera at {side}x{side}, {B} bins",
+                       "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"independent images, {world} GPU(s), no collective"},
+            "samples_per_s": world * P * B * K / per_step,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "peak_source": peak_src,
+                         "flop_per_launch": P * B * K * F_MLP, "kernel_ms": kern_s * 1e3, "traffic": None},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * P * B / e2e_s, "unit": "pixel-bins/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
+            "gpu_launches": args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -378,9 +507,16 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["hadros", "reference"], default="hadros")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["image", "surrogate"], default="image",
+                    help="image: the trace kernel on mixed_512 (default); surrogate: the "
+                         "surrogate inference kernel")
+    ap.add_argument("--side", type=int, default=None, help="surrogate workload: image side")
+    ap.add_argument("--bins", type=int, default=None, help="surrogate workload: bins")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.workload == "surrogate":
+        surrogate_arm(args)
     else:
         gpu_arm(args)
 
