@@ -251,6 +251,12 @@ class Context:
         _check(lib().hadros_ctx_stats(self.handle, C.byref(s)))
         return {name: getattr(s, name) for name, _ in s._fields_}
 
+    def set_transfer(self, mode) -> None:
+        """Mixed-precision transfer placement: "auto", "in_loop" or "deferred"."""
+        m = {"auto": abi.TRANSFER_AUTO, "in_loop": abi.TRANSFER_IN_LOOP,
+             "deferred": abi.TRANSFER_DEFERRED}.get(mode, mode)
+        _check(lib().hadros_ctx_set_transfer(self.handle, int(m)))
+
     def set_attempt_budget(self, attempts_per_ray: int) -> None:
         _check(lib().hadros_ctx_set_attempt_budget(self.handle, int(attempts_per_ray)))
 

@@ -21,6 +21,8 @@ PRECISION_MIXED = 1
 
 FATE_ESCAPED, FATE_CAPTURED, FATE_TRUNCATED = 0, 1, 2
 
+TRANSFER_AUTO, TRANSFER_IN_LOOP, TRANSFER_DEFERRED = 0, 1, 2
+
 
 class HadrosParams(C.Structure):
     _fields_ = [
@@ -158,6 +160,7 @@ SIGNATURES = {
     "hadros_ctx_create": (C.c_int32, [C.c_int32, P(C.c_void_p)]),
     "hadros_ctx_destroy": (None, [C.c_void_p]),
     "hadros_ctx_stats": (C.c_int32, [C.c_void_p, P(HadrosStats)]),
+    "hadros_ctx_set_transfer": (C.c_int32, [C.c_void_p, C.c_int32]),
     "hadros_ctx_set_attempt_budget": (C.c_int32, [C.c_void_p, C.c_int64]),
     "hadros_image": (C.c_int32, [C.c_void_p, P(HadrosParams), C.c_void_p, P(HadrosImageOut)]),
     "hadros_image_pixels": (C.c_int32, [C.c_void_p, P(HadrosParams), C.c_void_p, C.c_void_p,

@@ -69,12 +69,39 @@ struct hadros_ctx {
     void* d_out = nullptr; size_t out_cap = 0;
     unsigned long long* d_counters = nullptr;
     void* d_sig = nullptr; size_t sig_cap = 0;
+    void* d_rec = nullptr; size_t rec_cap = 0;   // deferred-transfer slots
+    int32_t transfer_mode = HADROS_TRANSFER_AUTO;
     const hadros_sigma* sig_key = nullptr;
     uint64_t sig_serial = 0;
     SigmaDev sig_dev{};
 };
 
 namespace {
+
+// Deferred transfer (mixed precision): the trace kernel buffers each ray's
+// path points and replays them warp-wide into the bins every kRecDepth
+// iterations, so the per-bin accumulators leave shared memory and the
+// occupancy no longer falls with the bin count.  Auto picks it from
+// kDeferMinBins bins.
+bool want_defer(int32_t mode, int precision, int max_bins)
+{
+    if (precision != HADROS_PRECISION_MIXED) return false;
+    if (mode == HADROS_TRANSFER_DEFERRED) return true;
+    if (mode == HADROS_TRANSFER_IN_LOOP) return false;
+    return max_bins >= kDeferMinBins;
+}
+
+// Slots for every thread of the largest persistent grid (8 blocks per SM).
+int64_t defer_slots(int n_sm) { return static_cast<int64_t>(n_sm) * 8 * kTPB; }
+
+void set_defer(TraceArgs& A, void* base, int64_t slots, int bmax)
+{
+    A.rec_buf = static_cast<PointRec*>(base);
+    A.rec_state = reinterpret_cast<float*>(static_cast<unsigned char*>(base) +
+                                           static_cast<size_t>(slots) * kRecDepth * sizeof(PointRec));
+    A.rec_bmax = bmax;
+    A.rec_slots = slots;
+}
 
 int32_t cuda_fail(hadros_ctx* ctx, cudaError_t e, const char* what)
 {
@@ -481,10 +508,20 @@ void hadros_ctx_destroy(hadros_ctx* ctx)
     cudaFree(ctx->d_out);
     cudaFree(ctx->d_counters);
     cudaFree(ctx->d_sig);
+    cudaFree(ctx->d_rec);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
+}
+
+int32_t hadros_ctx_set_transfer(hadros_ctx* ctx, int32_t mode)
+{
+    if (!ctx) return fail(HADROS_E_STATE, "context is NULL");
+    if (mode != HADROS_TRANSFER_AUTO && mode != HADROS_TRANSFER_IN_LOOP && mode != HADROS_TRANSFER_DEFERRED)
+        return fail(HADROS_E_ARG, "unknown transfer mode");
+    ctx->transfer_mode = mode;
+    return ok();
 }
 
 int32_t hadros_ctx_stats(const hadros_ctx* ctx, hadros_stats* out)
@@ -588,6 +625,12 @@ int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s
     A.path_cap = g_path_rec.cap;
     A.attempt_budget = ctx->attempt_budget > 0 ? ctx->attempt_budget
                                                : static_cast<int64_t>(p->max_steps) * 51 + 1;
+    if (want_defer(ctx->transfer_mode, p->precision, cam.n_bins)) {
+        const int64_t slots = defer_slots(ctx->n_sm);
+        if ((rc = grow(ctx, &ctx->d_rec, &ctx->rec_cap, rec_bytes(slots, cam.n_bins), "deferred transfer buffers")))
+            return rc;
+        set_defer(A, ctx->d_rec, slots, cam.n_bins);
+    }
 
     if (P > 0) {
         if (time_kernel) cudaEventRecord(ctx->ev0, st);
@@ -693,6 +736,12 @@ int32_t run_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, co
     for (int32_t c = 0; c < n_cams; ++c) max_cap = std::max(max_cap, cams[c].max_steps);
     A.attempt_budget = ctx->attempt_budget > 0 ? ctx->attempt_budget : static_cast<int64_t>(max_cap) * 51 + 1;
     A.fast_geodesic = cams[0].fast_geodesic;
+    if (want_defer(ctx->transfer_mode, cams[0].precision, max_bins)) {
+        const int64_t slots = defer_slots(ctx->n_sm);
+        if ((rc = grow(ctx, &ctx->d_rec, &ctx->rec_cap, rec_bytes(slots, max_bins), "deferred transfer buffers")))
+            return rc;
+        set_defer(A, ctx->d_rec, slots, max_bins);
+    }
     if (items > 0) {
         if (time_kernel) cudaEventRecord(ctx->ev0, st);
         rc = launch_trace(A, cams[0].precision, ctx->n_sm, st, err);
@@ -1096,6 +1145,7 @@ struct hadros_plan {
     int64_t P = 0, PB = 0;
     void* d_tabs = nullptr;          // cams | bins | order | sigma
     unsigned long long* d_counters = nullptr;
+    void* d_rec = nullptr;           // deferred-transfer slots (owned by the plan)
     TraceArgs A{};
     LaunchCfg cfg{};
     hadros_schedule sched{};
@@ -1291,6 +1341,15 @@ int32_t hadros_plan_create(hadros_ctx* ctx, const hadros_params* cams, int32_t n
         A.counters = pl->d_counters;
         A.attempt_budget = ctx->attempt_budget > 0 ? ctx->attempt_budget : static_cast<int64_t>(max_cap) * 51 + 1;
         A.fast_geodesic = pl->fast;
+        if (want_defer(ctx->transfer_mode, pl->precision, max_bins)) {
+            const int64_t slots = defer_slots(ctx->n_sm);
+            cudaError_t e2 = cudaMalloc(&pl->d_rec, rec_bytes(slots, max_bins));
+            if (e2 != cudaSuccess) {
+                hadros_plan_destroy(pl);
+                return fail(HADROS_E_NOMEM, std::string("plan deferred transfer buffers: ") + cudaGetErrorString(e2));
+            }
+            set_defer(A, pl->d_rec, slots, max_bins);
+        }
         int32_t rc = prepare_trace(A, pl->precision, pl->fast, ctx->n_sm, sc.blocks_per_sm, pl->cfg, err);
         if (rc) {
             hadros_plan_destroy(pl);
@@ -1356,6 +1415,7 @@ void hadros_plan_destroy(hadros_plan* pl)
     cudaSetDevice(pl->device);
     cudaFree(pl->d_tabs);
     cudaFree(pl->d_counters);
+    cudaFree(pl->d_rec);
     delete pl;
 }
 

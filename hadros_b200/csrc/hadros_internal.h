@@ -74,6 +74,18 @@ struct SigmaDev {
     const float* seg;    // [4n] per segment k>=1: lx1, 1/(lx2-lx1), s1, dly
 };
 
+// Deferred transfer (mixed precision): one path point's bin-independent
+// transfer terms, as the trace kernel buffers them (24 bytes).
+struct PointRec {
+    double gg;     // max(1/z, 1e-300): the exact E_local range test per bin
+    float lnzp;    // ln(E_local / E_mid) = ln(1/gg)
+    float zm1;     // E_local / E_mid - 1
+    float lnK;     // ln(g^3 C dl_cm); -inf: no emission at this point
+    float nbdl;    // n_b dl_cm; negative: no density
+};
+constexpr int kRecDepth = 64;       // points a thread buffers between deferred transfers
+constexpr int kDeferMinBins = 16;   // bins from which the host picks deferred transfer
+
 struct TraceArgs {
     const DevCam* cams;
     int32_t n_cams;
@@ -106,7 +118,19 @@ struct TraceArgs {
     // and a cap on resident blocks per SM (0 = occupancy)
     const int32_t* order;
     int32_t blocks_per_sm;
+    // deferred transfer (mixed only; rec_buf null = per-point transfer in the
+    // loop): per thread slot kRecDepth PointRecs and 5 x rec_bmax FP32
+    // accumulators (T, Tc, I, Ic, S); at most rec_slots threads in the grid
+    PointRec* rec_buf;
+    float* rec_state;
+    int32_t rec_bmax;
+    int64_t rec_slots;
 };
+
+inline size_t rec_bytes(int64_t slots, int bmax)
+{
+    return static_cast<size_t>(slots) * (kRecDepth * sizeof(PointRec) + 5 * sizeof(float) * static_cast<size_t>(bmax));
+}
 
 struct LaunchCfg {
     unsigned grid;

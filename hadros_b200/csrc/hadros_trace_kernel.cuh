@@ -281,7 +281,85 @@ struct BinAcc {
     float* I;
     float* Ic;
     float* S;
+    int st;   // stride between bins: kTPB in shared memory, 1 in a deferred slot
 };
+
+// The mixed-precision transfer of one path point, in two parts: the
+// bin-independent terms (point_terms_body) and the update of one bin's FP32
+// accumulators (bin_point).  Density and ln(emissivity) are FP32
+// (hadros_physics_f32.cuh).  Each bin's intensity is kept as a Kahan sum I
+// scaled by exp(S): every contribution K w(E_loc)/w(E_mid) exp(-tau) enters
+// as exp(e) with e = ln(...) - tau + S, and S is re-anchored when the sum is
+// empty or a term would exceed e^40, so intensities behind optically thick gas
+// (exp(-tau) far below FP32's range) keep their relative precision.
+__device__ __forceinline__ void point_terms_body(const DevCam* cam, double r, double th, double gg,
+                                                 double dl_cm, PointRec& p)
+{
+    const float rho = torus_rho_f(cam->torus, cam->torus_f, r, th);
+    const float lnC = ln_emission_f(cam->src, cam->src_f, cam->torus, cam->torus_f, r, th, rho);
+    const double zp = 1.0 / gg;   // E_local / E_mid
+    p.gg = gg;
+    p.lnzp = static_cast<float>(log(zp));
+    p.zm1 = static_cast<float>(zp - 1.0);
+    const bool emit = (lnC > -INFINITY) && dl_cm > 0.0;
+    // ln(g^3 C dl_cm) with g = 1 / zp
+    p.lnK = emit ? lnC + __logf(static_cast<float>(dl_cm)) - 3.0f * p.lnzp : -INFINITY;
+    p.nbdl = rho > 0.0f ? rho * static_cast<float>(dl_cm * cam->k_nb) : -1.0f;
+}
+
+// false for a point the transfer skips (radiative_transfer.cpp:501-505)
+__device__ __forceinline__ bool point_terms(const DevCam* cam, double r, double th, double dl, double z,
+                                            PointRec& p)
+{
+    if (r < cam->rt_skip) return false;
+    const double g = 1.0 / smax(z, 1.0e-300);
+    const double gg = smax(g, 1.0e-300);
+    point_terms_body(cam, r, th, gg, dl * cam->rg_cm, p);
+    return true;
+}
+
+__device__ __forceinline__ void bin_point(const PointRec& p, const DevBin& bn, const SmemTables& tb, float& T,
+                                          float& Tc, float& I, float& Ic, float& S)
+{
+    if (p.lnK != -INFINITY && bn.E_mid > 0.0) {
+        const float arg = p.lnK - bn.gamma * p.lnzp - bn.kcut * p.zm1;
+        // ln of this contribution; below -800 it is under FP64's range (the
+        // reference adds an exact or subnormal zero)
+        const double x = static_cast<double>(arg) - (static_cast<double>(T) - static_cast<double>(Tc));
+        if (x >= -800.0) {
+            double e = x + static_cast<double>(S);
+            if (I == 0.0f || e > 40.0) {
+                const float shrink = (I == 0.0f) ? 0.0f : __expf(static_cast<float>(-e));
+                I *= shrink;
+                Ic *= shrink;
+                S = static_cast<float>(-x);   // |S| < ~900: exact to 1e-4
+                e = x + static_cast<double>(S);
+            }
+            kahan_add(I, Ic, __expf(static_cast<float>(e)));
+        }
+    }
+    if (!(p.nbdl < 0.0f) && p.gg >= bn.gg_lo && p.gg <= bn.gg_hi) {
+        const float lnE = bn.lnE + p.lnzp;
+        int k;
+        if (tb.uniform) {   // evenly spaced ln E: direct index, corrected by one knot
+            k = static_cast<int>((lnE - tb.lx0) * tb.inv_dlx) + 1;
+            k = k < 1 ? 1 : (k > tb.n - 1 ? tb.n - 1 : k);
+            if (k > 1 && lnE < tb.lx[k - 1]) --k;
+            else if (k < tb.n - 1 && lnE > tb.lx[k]) ++k;
+        } else {
+            int lo = 0, cnt = tb.n;   // lower_bound over lx
+            while (cnt > 0) {
+                const int st = cnt >> 1;
+                if (tb.lx[lo + st] < lnE) { lo += st + 1; cnt -= st + 1; }
+                else cnt = st;
+            }
+            k = lo < 1 ? 1 : (lo > tb.n - 1 ? tb.n - 1 : lo);
+        }
+        const float4 sg = tb.seg[k];
+        const float t = (lnE - sg.x) * sg.y;
+        kahan_add(T, Tc, p.nbdl * (sg.z * __expf(t * sg.w)));
+    }
+}
 
 // One path point (r, theta, dl, redshift) into every bin: the body of
 // integrate_kerr_ray's point loop (radiative_transfer.cpp:501-672, UHE terms)
@@ -297,68 +375,14 @@ __device__ __forceinline__ void transfer_point(const DevCam* cam, const DevBin* 
     const double gg = smax(g, 1.0e-300);
     const double dl_cm = dl * cam->rg_cm;
     if (MIXED) {
-        // FP32 transfer.  Density and ln(emissivity) in FP32
-        // (hadros_physics_f32.cuh).  Each bin's intensity is kept as a Kahan
-        // sum I_s scaled by exp(S): every contribution K w(E_loc)/w(E_mid)
-        // exp(-tau) enters as exp(e) with e = ln(...) - tau + S, and S is
-        // re-anchored when the sum is empty or a term would exceed e^40, so
-        // intensities behind optically thick gas (exp(-tau) far below FP32's
-        // range) keep their relative precision.
-        const float rho = torus_rho_f(cam->torus, cam->torus_f, r, th);
-        const float lnC = ln_emission_f(cam->src, cam->src_f, cam->torus, cam->torus_f, r, th, rho);
-        const double zp = 1.0 / gg;   // E_local / E_mid
-        const float lnzp = static_cast<float>(log(zp));
-        const float zm1 = static_cast<float>(zp - 1.0);
-        const bool emit = (lnC > -INFINITY) && dl_cm > 0.0;
-        // ln(g^3 C dl_cm) with g = 1 / zp
-        const float lnK = emit ? lnC + __logf(static_cast<float>(dl_cm)) - 3.0f * lnzp : 0.0f;
-        const bool have_tau = rho > 0.0f;
-        const float nbdl = rho * static_cast<float>(dl_cm * cam->k_nb);
+        PointRec pr;
+        point_terms_body(cam, r, th, gg, dl_cm, pr);
         for (int b = 0; b < B; ++b) {
-            const DevBin& bn = bins[b];
-            float T = acc.T[b * kTPB], Tc = acc.Tc[b * kTPB];
-            if (emit && bn.E_mid > 0.0) {
-                float I = acc.I[b * kTPB], Ic = acc.Ic[b * kTPB], S = acc.S[b * kTPB];
-                const float arg = lnK - bn.gamma * lnzp - bn.kcut * zm1;
-                // ln of this contribution; below -800 it is under FP64's
-                // range (the reference adds an exact or subnormal zero)
-                const double x = static_cast<double>(arg) -
-                                 (static_cast<double>(T) - static_cast<double>(Tc));
-                if (x >= -800.0) {
-                    double e = x + static_cast<double>(S);
-                    if (I == 0.0f || e > 40.0) {
-                        const float shrink = (I == 0.0f) ? 0.0f : __expf(static_cast<float>(-e));
-                        I *= shrink;
-                        Ic *= shrink;
-                        S = static_cast<float>(-x);   // |S| < ~900: exact to 1e-4
-                        e = x + static_cast<double>(S);
-                    }
-                    kahan_add(I, Ic, __expf(static_cast<float>(e)));
-                    acc.I[b * kTPB] = I; acc.Ic[b * kTPB] = Ic; acc.S[b * kTPB] = S;
-                }
-            }
-            if (have_tau && gg >= bn.gg_lo && gg <= bn.gg_hi) {
-                const float lnE = bn.lnE + lnzp;
-                int k;
-                if (tb.uniform) {   // evenly spaced ln E: direct index, corrected by one knot
-                    k = static_cast<int>((lnE - tb.lx0) * tb.inv_dlx) + 1;
-                    k = k < 1 ? 1 : (k > tb.n - 1 ? tb.n - 1 : k);
-                    if (k > 1 && lnE < tb.lx[k - 1]) --k;
-                    else if (k < tb.n - 1 && lnE > tb.lx[k]) ++k;
-                } else {
-                    int lo = 0, cnt = tb.n;   // lower_bound over lx
-                    while (cnt > 0) {
-                        const int st = cnt >> 1;
-                        if (tb.lx[lo + st] < lnE) { lo += st + 1; cnt -= st + 1; }
-                        else cnt = st;
-                    }
-                    k = lo < 1 ? 1 : (lo > tb.n - 1 ? tb.n - 1 : lo);
-                }
-                const float4 sg = tb.seg[k];
-                const float t = (lnE - sg.x) * sg.y;
-                kahan_add(T, Tc, nbdl * (sg.z * __expf(t * sg.w)));
-                acc.T[b * kTPB] = T; acc.Tc[b * kTPB] = Tc;
-            }
+            float T = acc.T[b * acc.st], Tc = acc.Tc[b * acc.st];
+            float I = acc.I[b * acc.st], Ic = acc.Ic[b * acc.st], S = acc.S[b * acc.st];
+            bin_point(pr, bins[b], tb, T, Tc, I, Ic, S);
+            acc.T[b * acc.st] = T; acc.Tc[b * acc.st] = Tc;
+            acc.I[b * acc.st] = I; acc.Ic[b * acc.st] = Ic; acc.S[b * acc.st] = S;
         }
     } else {
         const double rho = torus_rho(cam->torus, r, th);
@@ -368,8 +392,8 @@ __device__ __forceinline__ void transfer_point(const DevCam* cam, const DevBin* 
             const double E_loc = bins[b].E_mid / gg;
             double jj = 0.0;
             if (!(E_loc <= 0.0)) jj = C * spectral_weight(cam->src, E_loc);
-            double T = acc.T64[b * kTPB];
-            acc.I64[b * kTPB] += g3 * jj * exp(-T) * dl_cm;
+            double T = acc.T64[b * acc.st];
+            acc.I64[b * acc.st] += g3 * jj * exp(-T) * dl_cm;
             if (rho <= 0.0 || E_loc < tb.Emin || E_loc > tb.Emax) continue;
             // SigmaTable::log_interp (sigma_table.cpp:81-124)
             int lo = 0, cnt = tb.n;
@@ -390,7 +414,7 @@ __device__ __forceinline__ void transfer_point(const DevCam* cam, const DevBin* 
             }
             const double nb = rho / kMuG;
             T += nb * sigma_cm2 * dl_cm;
-            acc.T64[b * kTPB] = T;
+            acc.T64[b * acc.st] = T;
         }
     }
 }
@@ -409,13 +433,13 @@ __device__ __forceinline__ void finish_pixel(const TraceArgs& A, const DevCam* c
     for (int b = 0; b < B; ++b) {
         double tb, ib;
         if (MIXED) {
-            tb = static_cast<double>(acc.T[b * kTPB]);
+            tb = static_cast<double>(acc.T[b * acc.st]);
             // I = (I_s - c) * exp(-S) * w(E_mid)
-            ib = (static_cast<double>(acc.I[b * kTPB]) - static_cast<double>(acc.Ic[b * kTPB])) *
-                 exp(-static_cast<double>(acc.S[b * kTPB])) * bins[b].w0;
+            ib = (static_cast<double>(acc.I[b * acc.st]) - static_cast<double>(acc.Ic[b * acc.st])) *
+                 exp(-static_cast<double>(acc.S[b * acc.st])) * bins[b].w0;
         } else {
-            tb = acc.T64[b * kTPB];
-            ib = acc.I64[b * kTPB];
+            tb = acc.T64[b * acc.st];
+            ib = acc.I64[b * acc.st];
         }
         const long long e = cam->binout_offset + local * B + b;
         if (MIXED) {
@@ -454,23 +478,88 @@ __device__ __forceinline__ void reset_bins(const BinAcc& acc, int B)
 {
     for (int b = 0; b < B; ++b) {
         if (MIXED) {
-            acc.T[b * kTPB] = 0.0f; acc.Tc[b * kTPB] = 0.0f;
-            acc.I[b * kTPB] = 0.0f; acc.Ic[b * kTPB] = 0.0f;
-            acc.S[b * kTPB] = 0.0f;
+            acc.T[b * acc.st] = 0.0f; acc.Tc[b * acc.st] = 0.0f;
+            acc.I[b * acc.st] = 0.0f; acc.Ic[b * acc.st] = 0.0f;
+            acc.S[b * acc.st] = 0.0f;
         } else {
-            acc.T64[b * kTPB] = 0.0; acc.I64[b * kTPB] = 0.0;
+            acc.T64[b * acc.st] = 0.0; acc.I64[b * acc.st] = 0.0;
         }
     }
 }
 
-enum Phase : int { kNeedRay = 0, kStepStart = 1, kAttempt = 2, kDone = 3 };
+enum Phase : int { kNeedRay = 0, kStepStart = 1, kAttempt = 2, kDone = 3, kWaitTransfer = 4 };
+
+// The warp's deferred transfer: every lane's buffered points (fill each, in
+// order) go into that lane's ray's bins, the warp's 32 threads sharing the
+// bins: for up to 32 bins a group of P = next power of two >= rec_bmax
+// threads takes one lane's ray (32 / P rays at a time), thread b of the group
+// bin b; above 32 bins one lane's ray at a time, thread t bins t, t+32, ...
+// The per-bin arithmetic and the point order are those of transfer_point,
+// so the results are the same bits.  warp_slot0 is the slot of lane 0.
+__device__ __forceinline__ void deferred_transfer(const TraceArgs& A, const SmemTables& tb, long long warp_slot0,
+                                               int fill, int B, const DevCam* cam)
+{
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int bmax = A.rec_bmax;
+    if (bmax <= 32) {
+        int P = 1;
+        while (P < bmax) P <<= 1;
+        const int G = 32 / P;
+        for (int base = 0; base < 32; base += G) {
+            const int src = base + lane / P, b = lane % P;
+            const int n = __shfl_sync(full, fill, src);
+            const int Bs = __shfl_sync(full, B, src);
+            const DevCam* cs = reinterpret_cast<const DevCam*>(
+                __shfl_sync(full, reinterpret_cast<unsigned long long>(cam), src));
+            const bool act = n > 0 && b < Bs;
+            int nmax = act ? n : 0;
+            for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(full, nmax, o));
+            if (nmax == 0) continue;
+            const long long sl = warp_slot0 + src;
+            float* st = A.rec_state + sl * 5 * bmax;
+            float T = 0.0f, Tc = 0.0f, I = 0.0f, Ic = 0.0f, S = 0.0f;
+            const DevBin* bn = nullptr;
+            if (act) {
+                T = st[b]; Tc = st[bmax + b]; I = st[2 * bmax + b]; Ic = st[3 * bmax + b]; S = st[4 * bmax + b];
+                bn = A.bins + cs->bin_offset + b;
+            }
+            const PointRec* rb = A.rec_buf + sl * kRecDepth;
+            for (int q = 0; q < nmax; ++q)
+                if (act && q < n) bin_point(rb[q], *bn, tb, T, Tc, I, Ic, S);
+            if (act) {
+                st[b] = T; st[bmax + b] = Tc; st[2 * bmax + b] = I; st[3 * bmax + b] = Ic; st[4 * bmax + b] = S;
+            }
+        }
+    } else {
+        for (int src = 0; src < 32; ++src) {
+            const int n = __shfl_sync(full, fill, src);
+            if (n == 0) continue;
+            const int Bs = __shfl_sync(full, B, src);
+            const DevCam* cs = reinterpret_cast<const DevCam*>(
+                __shfl_sync(full, reinterpret_cast<unsigned long long>(cam), src));
+            const long long sl = warp_slot0 + src;
+            float* st = A.rec_state + sl * 5 * bmax;
+            const PointRec* rb = A.rec_buf + sl * kRecDepth;
+            for (int b = lane; b < Bs; b += 32) {   // at most 4 passes (bins <= 128)
+                float T = st[b], Tc = st[bmax + b], I = st[2 * bmax + b], Ic = st[3 * bmax + b],
+                      S = st[4 * bmax + b];
+                const DevBin& bn = A.bins[cs->bin_offset + b];
+                for (int q = 0; q < n; ++q) bin_point(rb[q], bn, tb, T, Tc, I, Ic, S);
+                st[b] = T; st[bmax + b] = Tc; st[2 * bmax + b] = I; st[3 * bmax + b] = Ic; st[4 * bmax + b] = S;
+            }
+        }
+    }
+}
 
 template <int MIXED, int FAST>
 __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const TraceArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int n_sig = A.sig.n;
-    const SmemLayout L = smem_layout(MIXED ? 1 : 0, n_sig, A.max_bins);
+    // deferred transfer keeps no per-bin accumulators in shared memory
+    const bool defer = MIXED && A.rec_buf != nullptr;
+    const SmemLayout L = smem_layout(MIXED ? 1 : 0, n_sig, defer ? 0 : A.max_bins);
     double* sE = reinterpret_cast<double*>(smem + L.off_E);
     double* sS = reinterpret_cast<double*>(smem + L.off_S);
     double* slnE = reinterpret_cast<double*>(smem + L.off_lnE);
@@ -499,7 +588,14 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
     float* accIc = accI + size_t(kTPB) * A.max_bins;
     float* accS = accIc + size_t(kTPB) * A.max_bins;
     const SmemTables tb{sE, sS, slnE, slnS, slx, sseg, n_sig, sigEmin, sigEmax, sig_scale, A.sig.uniform, A.sig.lx0, A.sig.inv_dlx};
-    const BinAcc acc{accT64, accI64, accT, accTc, accI, accIc, accS};
+    const long long slot = static_cast<long long>(blockIdx.x) * kTPB + tid;   // deferred-transfer slot
+    float* dstate = defer ? A.rec_state + slot * 5 * A.rec_bmax : nullptr;
+    const BinAcc acc = defer ? BinAcc{nullptr, nullptr, dstate, dstate + A.rec_bmax, dstate + 2 * A.rec_bmax,
+                                      dstate + 3 * A.rec_bmax, dstate + 4 * A.rec_bmax, 1}
+                             : BinAcc{accT64, accI64, accT, accTc, accI, accIc, accS, kTPB};
+    PointRec* my_rec = defer ? A.rec_buf + slot * kRecDepth : nullptr;
+    int fill = 0;          // points buffered in my_rec
+    unsigned iter = 0;     // loop iterations (warp-uniform)
 
     int phase = kNeedRay;
     // ray state
@@ -581,9 +677,13 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                 stop = true;
             }
             if (stop) {
-                finish_pixel<MIXED>(A, cam, bins, B, acc, row, step, fate, att_total);
                 atomicAdd(&A.counters[1], static_cast<unsigned long long>(step));
                 atomicAdd(&A.counters[2], static_cast<unsigned long long>(att_total));
+                if (defer) {   // finished at the warp's next transfer
+                    phase = kWaitTransfer;
+                    continue;
+                }
+                finish_pixel<MIXED>(A, cam, bins, B, acc, row, step, fate, att_total);
                 phase = kNeedRay;
                 continue;
             }
@@ -655,7 +755,12 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
             }
 
             // ---- transfer of this point into every bin ------------------
-            transfer_point<MIXED>(cam, bins, B, tb, acc, r, th, dl, z);
+            if (defer) {
+                PointRec pr;
+                if (point_terms(cam, r, th, dl, z, pr)) my_rec[fill++] = pr;
+            } else {
+                transfer_point<MIXED>(cam, bins, B, tb, acc, r, th, dl, z);
+            }
 
             // ---- k1 of the coming step_adaptive (shares sin/cos) ------------
             if (FAST) geo_rhs_fast(a, r, th, s, c, pr, pth, pt, pph, k1);
@@ -670,6 +775,21 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
             phase = kAttempt;
         }
 
+        if (defer) {
+            // Every kRecDepth iterations (each adds at most one point per lane),
+            // or when no lane has a ray in flight, the warp replays every lane's
+            // buffered points into its bins, then finishes the waiting rays.
+            ++iter;
+            const bool idle = __all_sync(0xffffffffu, phase == kDone || phase == kWaitTransfer);
+            if (iter % kRecDepth == 0 || idle) {
+                deferred_transfer(A, tb, slot - (tid & 31), fill, B, cam);
+                if (phase == kWaitTransfer) {
+                    finish_pixel<MIXED>(A, cam, bins, B, acc, row, step, fate, att_total);
+                    phase = kNeedRay;
+                }
+                fill = 0;
+            }
+        }
         if (__all_sync(0xffffffffu, phase == kDone)) break;
         if (phase != kAttempt) continue;
 
@@ -792,7 +912,7 @@ __global__ void __launch_bounds__(kTPB) path_transfer_kernel(const TraceArgs A)
     float* accIc = accI + size_t(kTPB) * A.max_bins;
     float* accS = accIc + size_t(kTPB) * A.max_bins;
     const SmemTables tb{sE, sS, slnE, slnS, slx, sseg, n_sig, A.sig.E_min, A.sig.E_max, A.sig.sigma_scale, A.sig.uniform, A.sig.lx0, A.sig.inv_dlx};
-    const BinAcc acc{accT64, accI64, accT, accTc, accI, accIc, accS};
+    const BinAcc acc{accT64, accI64, accT, accTc, accI, accIc, accS, kTPB};
     const DevCam* cam = A.cams;
     const DevBin* bins = A.bins + cam->bin_offset;
     const int B = cam->n_bins;
@@ -826,6 +946,7 @@ int launch_paths(const TraceArgs& args, int precision, int n_sm, cudaStream_t st
     long long grid = static_cast<long long>(n_sm) * per_sm;
     const long long needed = (args.total_items + kTPB - 1) / kTPB;
     if (grid > needed) grid = needed > 0 ? needed : 1;
+    if (args.rec_buf && grid * kTPB > args.rec_slots) grid = args.rec_slots / kTPB;   // one slot per thread
     kern<<<static_cast<unsigned>(grid), kTPB, smem, st>>>(args);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
@@ -841,7 +962,7 @@ template <int FAST>
 int prepare_variant(const TraceArgs& args, int precision, int n_sm, int blocks_per_sm, LaunchCfg& cfg,
                     std::string& err)
 {
-    cfg.smem = smem_layout(precision, args.sig.n, args.max_bins).total;
+    cfg.smem = smem_layout(precision, args.sig.n, args.rec_buf ? 0 : args.max_bins).total;
     auto kern = (precision == HADROS_PRECISION_MIXED) ? trace_kernel<1, FAST> : trace_kernel<0, FAST>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
     int per_sm = 0;
@@ -858,6 +979,7 @@ int prepare_variant(const TraceArgs& args, int precision, int n_sm, int blocks_p
     long long grid = static_cast<long long>(n_sm) * per_sm;
     const long long needed = (args.total_items + kTPB - 1) / kTPB;
     if (grid > needed) grid = needed > 0 ? needed : 1;
+    if (args.rec_buf && grid * kTPB > args.rec_slots) grid = args.rec_slots / kTPB;   // one slot per thread
     cfg.grid = static_cast<unsigned>(grid);
     cfg.per_sm = per_sm;
     return HADROS_OK;

@@ -264,6 +264,17 @@ int32_t hadros_ctx_stats(const hadros_ctx* ctx, hadros_stats* out);
  * HADROS_E_TIMEOUT (0 = max_steps * 51, the most step_adaptive can take). */
 int32_t hadros_ctx_set_attempt_budget(hadros_ctx* ctx, int64_t attempts_per_ray);
 
+/* Where the mixed-precision transfer runs.  IN_LOOP: each thread adds every
+ * path point to its ray's bins as the point is reached (accumulators in shared
+ * memory, so resident rays per SM fall as bins grow).  DEFERRED: each thread
+ * buffers 64 points (24 bytes each) and the warp replays them into the bins
+ * together, 32 threads sharing the bins (accumulators in a device slot per
+ * thread); same results bit for bit.  AUTO (default): deferred from 16 bins.
+ * FP64 mode always transfers in the loop.  Applies to later calls and plans. */
+enum hadros_transfer_mode { HADROS_TRANSFER_AUTO = 0, HADROS_TRANSFER_IN_LOOP = 1,
+                            HADROS_TRANSFER_DEFERRED = 2 };
+int32_t hadros_ctx_set_transfer(hadros_ctx* ctx, int32_t mode);
+
 /* Whole image.  Replaces compute_kerr_geodesics + compute_kerr_image_from_
  * cache (apps/compute_kerr_geodesics.cpp:24-146, apps/compute_kerr_image_
  * from_cache.cpp:31-722) and compute_kerr_image_cuda's in-line mode
