@@ -35,11 +35,13 @@ def cmd_image(a) -> int:
         E, g2, s = W.synthetic_sigma_arrays()
         sig = SigmaTable.from_arrays(E, s, g2)
     with Context(a.device) as ctx:
+        ctx.set_transfer(a.transfer)
         for r in range(a.repeat):
             img = ctx.image(p, sig, outputs=("tau", "I_obs", "fate", "steps", "attempts"))
             st = ctx.stats()
             fates = np.bincount(img["fate"].astype(np.int64), minlength=3)
-            print(json.dumps({"workload": a.workload, "nx": p.nx, "ny": p.ny,
+            print(json.dumps({"workload": a.workload, "nx": p.nx, "ny": p.ny, "bins": int(p.n_bins),
+                              "transfer": a.transfer,
                               "precision": int(p.precision), "repeat": r,
                               "kernel_ms": st["kernel_ms"], "total_ms": st["total_ms"],
                               "rays": st["rays"], "accepted_steps": st["accepted_steps"],
@@ -63,6 +65,8 @@ def main(argv=None) -> int:
     im.add_argument("--max-steps", dest="max_steps", type=int)
     im.add_argument("--precision", choices=["fp64", "mixed"])
     im.add_argument("--repeat", type=int, default=1)
+    im.add_argument("--transfer", choices=["auto", "in_loop", "deferred"], default="auto",
+                    help="mixed precision: per-point transfer in the loop, or deferred (warp replays)")
     im.add_argument("--device", type=int, default=0)
     im.add_argument("--sigma", help="sigma table file (reference 3-column format)")
     a = ap.parse_args(argv)
