@@ -490,75 +490,90 @@ __device__ __forceinline__ void reset_bins(const BinAcc& acc, int B)
 enum Phase : int { kNeedRay = 0, kStepStart = 1, kAttempt = 2, kDone = 3, kWaitTransfer = 4 };
 
 // The warp's deferred transfer: every lane's buffered points (fill each, in
-// order) go into that lane's ray's bins, the warp's 32 threads sharing the
-// bins: for up to 32 bins a group of P = next power of two >= rec_bmax
-// threads takes one lane's ray (32 / P rays at a time), thread b of the group
-// bin b; above 32 bins one lane's ray at a time, thread t bins t, t+32, ...
-// The per-bin arithmetic and the point order are those of transfer_point,
-// so the results are the same bits.  warp_slot0 is the slot of lane 0.
+// order) go into that lane's ray's bins.  The warp's (lane, bin) pairs are
+// numbered through a prefix sum of the lanes' bin counts and dealt to its 32
+// threads, kDeferChains independent pairs per thread at a time so that their
+// accumulation chains interleave.  The per-bin arithmetic and the point
+// order are those of transfer_point, so the results are the same bits.
+// warp_slot0 is the slot of lane 0.
+constexpr int kDeferChains = 4;
+
 __device__ __forceinline__ void deferred_transfer(const TraceArgs& A, const SmemTables& tb, long long warp_slot0,
-                                               int fill, int B, const DevCam* cam)
+                                                  int fill, int B, const DevCam* cam)
 {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int bmax = A.rec_bmax;
-    if (bmax <= 32) {
-        int P = 1;
-        while (P < bmax) P <<= 1;
-        const int G = 32 / P;
-        for (int base = 0; base < 32; base += G) {
-            const int src = base + lane / P, b = lane % P;
-            const int n = __shfl_sync(full, fill, src);
-            const int Bs = __shfl_sync(full, B, src);
+    const int nb = fill > 0 ? B : 0;
+    int pre = nb;   // inclusive prefix sum of the lanes' bin counts
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(full, pre, o);
+        if (lane >= o) pre += v;
+    }
+    const int total = __shfl_sync(full, pre, 31);
+    pre -= nb;      // exclusive
+    for (int k0 = 0; k0 < total; k0 += 32 * kDeferChains) {
+        float T[kDeferChains], Tc[kDeferChains], I[kDeferChains], Ic[kDeferChains], S[kDeferChains];
+        int n[kDeferChains], bb[kDeferChains];
+        const PointRec* rb[kDeferChains];
+        const DevBin* bn[kDeferChains];
+        float* st[kDeferChains];
+        int nmax = 0;
+#pragma unroll
+        for (int u = 0; u < kDeferChains; ++u) {
+            const int k = k0 + 32 * u + lane;
+            // source lane: the last lane whose exclusive prefix is <= k
+            int src = 0;
+#pragma unroll
+            for (int bit = 16; bit > 0; bit >>= 1) {
+                const int cand = src + bit;
+                const int pc = __shfl_sync(full, pre, cand & 31);
+                if (cand < 32 && pc <= k) src = cand;
+            }
+            const int ps = __shfl_sync(full, pre, src);
+            const int fs = __shfl_sync(full, fill, src);
             const DevCam* cs = reinterpret_cast<const DevCam*>(
                 __shfl_sync(full, reinterpret_cast<unsigned long long>(cam), src));
-            const bool act = n > 0 && b < Bs;
-            int nmax = act ? n : 0;
-            for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(full, nmax, o));
-            if (nmax == 0) continue;
+            const bool act = k < total;
+            n[u] = act ? fs : 0;
+            bb[u] = k - ps;
+            nmax = max(nmax, n[u]);
             const long long sl = warp_slot0 + src;
-            float* st = A.rec_state + sl * 5 * bmax;
-            float T = 0.0f, Tc = 0.0f, I = 0.0f, Ic = 0.0f, S = 0.0f;
-            const DevBin* bn = nullptr;
+            st[u] = A.rec_state + sl * 5 * bmax;
+            rb[u] = A.rec_buf + sl * kRecDepth;
+            bn[u] = act ? A.bins + cs->bin_offset + bb[u] : A.bins;
+            T[u] = Tc[u] = I[u] = Ic[u] = S[u] = 0.0f;
             if (act) {
-                T = st[b]; Tc = st[bmax + b]; I = st[2 * bmax + b]; Ic = st[3 * bmax + b]; S = st[4 * bmax + b];
-                bn = A.bins + cs->bin_offset + b;
-            }
-            const PointRec* rb = A.rec_buf + sl * kRecDepth;
-            for (int q = 0; q < nmax; ++q)
-                if (act && q < n) bin_point(rb[q], *bn, tb, T, Tc, I, Ic, S);
-            if (act) {
-                st[b] = T; st[bmax + b] = Tc; st[2 * bmax + b] = I; st[3 * bmax + b] = Ic; st[4 * bmax + b] = S;
+                const int b = bb[u];
+                T[u] = st[u][b]; Tc[u] = st[u][bmax + b]; I[u] = st[u][2 * bmax + b];
+                Ic[u] = st[u][3 * bmax + b]; S[u] = st[u][4 * bmax + b];
             }
         }
-    } else {
-        for (int src = 0; src < 32; ++src) {
-            const int n = __shfl_sync(full, fill, src);
-            if (n == 0) continue;
-            const int Bs = __shfl_sync(full, B, src);
-            const DevCam* cs = reinterpret_cast<const DevCam*>(
-                __shfl_sync(full, reinterpret_cast<unsigned long long>(cam), src));
-            const long long sl = warp_slot0 + src;
-            float* st = A.rec_state + sl * 5 * bmax;
-            const PointRec* rb = A.rec_buf + sl * kRecDepth;
-            for (int b = lane; b < Bs; b += 32) {   // at most 4 passes (bins <= 128)
-                float T = st[b], Tc = st[bmax + b], I = st[2 * bmax + b], Ic = st[3 * bmax + b],
-                      S = st[4 * bmax + b];
-                const DevBin& bn = A.bins[cs->bin_offset + b];
-                for (int q = 0; q < n; ++q) bin_point(rb[q], bn, tb, T, Tc, I, Ic, S);
-                st[b] = T; st[bmax + b] = Tc; st[2 * bmax + b] = I; st[3 * bmax + b] = Ic; st[4 * bmax + b] = S;
-            }
+        for (int q = 0; q < nmax; ++q) {
+#pragma unroll
+            for (int u = 0; u < kDeferChains; ++u)
+                if (q < n[u]) bin_point(rb[u][q], *bn[u], tb, T[u], Tc[u], I[u], Ic[u], S[u]);
         }
+#pragma unroll
+        for (int u = 0; u < kDeferChains; ++u)
+            if (k0 + 32 * u + lane < total) {
+                const int b = bb[u];
+                st[u][b] = T[u]; st[u][bmax + b] = Tc[u]; st[u][2 * bmax + b] = I[u];
+                st[u][3 * bmax + b] = Ic[u]; st[u][4 * bmax + b] = S[u];
+            }
     }
 }
 
-template <int MIXED, int FAST>
+// DEFER (mixed only): the deferred transfer; a separate instantiation so the
+// in-loop kernel carries none of its code or registers.
+template <int MIXED, int FAST, int DEFER>
 __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const TraceArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int n_sig = A.sig.n;
     // deferred transfer keeps no per-bin accumulators in shared memory
-    const bool defer = MIXED && A.rec_buf != nullptr;
+    static_assert(!DEFER || MIXED, "the deferred transfer is mixed precision only");
+    constexpr bool defer = DEFER != 0;
     const SmemLayout L = smem_layout(MIXED ? 1 : 0, n_sig, defer ? 0 : A.max_bins);
     double* sE = reinterpret_cast<double*>(smem + L.off_E);
     double* sS = reinterpret_cast<double*>(smem + L.off_S);
@@ -956,6 +971,14 @@ int launch_paths(const TraceArgs& args, int precision, int n_sm, cudaStream_t st
     return HADROS_OK;
 }
 
+// The trace kernel instantiation for a precision and transfer placement.
+template <int FAST>
+auto trace_kernel_for(const TraceArgs& args, int precision) -> void (*)(const TraceArgs)
+{
+    if (precision != HADROS_PRECISION_MIXED) return trace_kernel<0, FAST, 0>;
+    return args.rec_buf ? trace_kernel<1, FAST, 1> : trace_kernel<1, FAST, 0>;
+}
+
 // Grid of a persistent launch: SMs x resident blocks (capped at
 // blocks_per_sm when > 0), no more blocks than the work needs.
 template <int FAST>
@@ -963,7 +986,7 @@ int prepare_variant(const TraceArgs& args, int precision, int n_sm, int blocks_p
                     std::string& err)
 {
     cfg.smem = smem_layout(precision, args.sig.n, args.rec_buf ? 0 : args.max_bins).total;
-    auto kern = (precision == HADROS_PRECISION_MIXED) ? trace_kernel<1, FAST> : trace_kernel<0, FAST>;
+    auto kern = trace_kernel_for<FAST>(args, precision);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
     int per_sm = 0;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTPB, cfg.smem);
@@ -990,7 +1013,7 @@ template <int FAST>
 int launch_prepared_variant(const TraceArgs& args, int precision, const LaunchCfg& cfg, cudaStream_t st,
                             std::string& err)
 {
-    auto kern = (precision == HADROS_PRECISION_MIXED) ? trace_kernel<1, FAST> : trace_kernel<0, FAST>;
+    auto kern = trace_kernel_for<FAST>(args, precision);
     kern<<<cfg.grid, kTPB, cfg.smem, st>>>(args);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
