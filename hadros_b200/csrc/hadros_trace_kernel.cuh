@@ -318,7 +318,15 @@ __device__ __forceinline__ bool point_terms(const DevCam* cam, double r, double 
     return true;
 }
 
-__device__ __forceinline__ void bin_point(const PointRec& p, const DevBin& bn, const SmemTables& tb, float& T,
+// The fields of a DevBin the transfer reads (the deferred replay keeps four
+// of them in registers).
+struct BinK {
+    double E_mid, gg_lo, gg_hi;
+    float lnE, gamma, kcut;
+};
+
+template <class Bin>
+__device__ __forceinline__ void bin_point(const PointRec& p, const Bin& bn, const SmemTables& tb, float& T,
                                           float& Tc, float& I, float& Ic, float& S)
 {
     if (p.lnK != -INFINITY && bn.E_mid > 0.0) {
@@ -490,76 +498,83 @@ __device__ __forceinline__ void reset_bins(const BinAcc& acc, int B)
 enum Phase : int { kNeedRay = 0, kStepStart = 1, kAttempt = 2, kDone = 3, kWaitTransfer = 4 };
 
 // The warp's deferred transfer: every lane's buffered points (fill each, in
-// order) go into that lane's ray's bins.  The warp's (lane, bin) pairs are
-// numbered through a prefix sum of the lanes' bin counts and dealt to its 32
-// threads, kDeferChains independent pairs per thread at a time so that their
-// accumulation chains interleave.  The per-bin arithmetic and the point
-// order are those of transfer_point, so the results are the same bits.
+// order) go into that lane's ray's bins.  Each thread takes one lane's ray
+// and kDeferBins consecutive bins of it (the warp's (lane, bin group) pairs
+// are numbered through a prefix sum of the lanes' group counts), so every
+// buffered point is loaded once for kDeferBins independent accumulation
+// chains whose bin constants sit in registers.  The per-bin arithmetic and the
+// point order are those of transfer_point, so the results are the same bits.
+// Not inlined: called once every kRecDepth loop iterations, its registers are
+// saved around the call instead of crowding the RKF45 attempt's.
 // warp_slot0 is the slot of lane 0.
-constexpr int kDeferChains = 4;
+constexpr int kDeferBins = 4;
 
-__device__ __forceinline__ void deferred_transfer(const TraceArgs& A, const SmemTables& tb, long long warp_slot0,
-                                                  int fill, int B, const DevCam* cam)
+__device__ __noinline__ void deferred_transfer(PointRec* rec_buf, float* rec_state, const DevBin* bins, int bmax,
+                                               const SmemTables tb, long long warp_slot0, int fill, int B,
+                                               const DevCam* cam)
 {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const int bmax = A.rec_bmax;
-    const int nb = fill > 0 ? B : 0;
-    int pre = nb;   // inclusive prefix sum of the lanes' bin counts
+    const int ng = fill > 0 ? (B + kDeferBins - 1) / kDeferBins : 0;
+    int pre = ng;   // inclusive prefix sum of the lanes' bin-group counts
     for (int o = 1; o < 32; o <<= 1) {
         const int v = __shfl_up_sync(full, pre, o);
         if (lane >= o) pre += v;
     }
     const int total = __shfl_sync(full, pre, 31);
-    pre -= nb;      // exclusive
-    for (int k0 = 0; k0 < total; k0 += 32 * kDeferChains) {
-        float T[kDeferChains], Tc[kDeferChains], I[kDeferChains], Ic[kDeferChains], S[kDeferChains];
-        int n[kDeferChains], bb[kDeferChains];
-        const PointRec* rb[kDeferChains];
-        const DevBin* bn[kDeferChains];
-        float* st[kDeferChains];
-        int nmax = 0;
+    pre -= ng;      // exclusive
+    for (int k0 = 0; k0 < total; k0 += 32) {
+        const int k = k0 + lane;
+        int src = 0;   // the last lane whose exclusive prefix is <= k
 #pragma unroll
-        for (int u = 0; u < kDeferChains; ++u) {
-            const int k = k0 + 32 * u + lane;
-            // source lane: the last lane whose exclusive prefix is <= k
-            int src = 0;
+        for (int bit = 16; bit > 0; bit >>= 1) {
+            const int cand = src + bit;
+            const int pc = __shfl_sync(full, pre, cand & 31);
+            if (cand < 32 && pc <= k) src = cand;
+        }
+        const int ps = __shfl_sync(full, pre, src);
+        const int n_src = __shfl_sync(full, fill, src);
+        const int B_src = __shfl_sync(full, B, src);
+        const DevCam* cs = reinterpret_cast<const DevCam*>(
+            __shfl_sync(full, reinterpret_cast<unsigned long long>(cam), src));
+        const bool act = k < total;
+        const int n = act ? n_src : 0;
+        const int b0 = (k - ps) * kDeferBins;
+        const long long sl = warp_slot0 + src;
+        float* st = rec_state + sl * 5 * bmax;
+        const PointRec* rb = rec_buf + sl * kRecDepth;
+        float T[kDeferBins], Tc[kDeferBins], I[kDeferBins], Ic[kDeferBins], S[kDeferBins];
+        BinK bk[kDeferBins];
+        bool on[kDeferBins];
 #pragma unroll
-            for (int bit = 16; bit > 0; bit >>= 1) {
-                const int cand = src + bit;
-                const int pc = __shfl_sync(full, pre, cand & 31);
-                if (cand < 32 && pc <= k) src = cand;
-            }
-            const int ps = __shfl_sync(full, pre, src);
-            const int fs = __shfl_sync(full, fill, src);
-            const DevCam* cs = reinterpret_cast<const DevCam*>(
-                __shfl_sync(full, reinterpret_cast<unsigned long long>(cam), src));
-            const bool act = k < total;
-            n[u] = act ? fs : 0;
-            bb[u] = k - ps;
-            nmax = max(nmax, n[u]);
-            const long long sl = warp_slot0 + src;
-            st[u] = A.rec_state + sl * 5 * bmax;
-            rb[u] = A.rec_buf + sl * kRecDepth;
-            bn[u] = act ? A.bins + cs->bin_offset + bb[u] : A.bins;
-            T[u] = Tc[u] = I[u] = Ic[u] = S[u] = 0.0f;
-            if (act) {
-                const int b = bb[u];
-                T[u] = st[u][b]; Tc[u] = st[u][bmax + b]; I[u] = st[u][2 * bmax + b];
-                Ic[u] = st[u][3 * bmax + b]; S[u] = st[u][4 * bmax + b];
+        for (int j = 0; j < kDeferBins; ++j) {
+            const int b = b0 + j;
+            on[j] = act && b < B_src;
+            T[j] = Tc[j] = I[j] = Ic[j] = S[j] = 0.0f;
+            bk[j] = BinK{0.0, INFINITY, -INFINITY, 0.0f, 0.0f, 0.0f};
+            if (on[j]) {
+                const DevBin& d = bins[cs->bin_offset + b];
+                bk[j] = BinK{d.E_mid, d.gg_lo, d.gg_hi, d.lnE, d.gamma, d.kcut};
+                T[j] = st[b]; Tc[j] = st[bmax + b]; I[j] = st[2 * bmax + b];
+                Ic[j] = st[3 * bmax + b]; S[j] = st[4 * bmax + b];
             }
         }
+        int nmax = n;
+        for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(full, nmax, o));
         for (int q = 0; q < nmax; ++q) {
+            if (q < n) {
+                const PointRec pr = rb[q];
 #pragma unroll
-            for (int u = 0; u < kDeferChains; ++u)
-                if (q < n[u]) bin_point(rb[u][q], *bn[u], tb, T[u], Tc[u], I[u], Ic[u], S[u]);
+                for (int j = 0; j < kDeferBins; ++j)
+                    if (on[j]) bin_point(pr, bk[j], tb, T[j], Tc[j], I[j], Ic[j], S[j]);
+            }
         }
 #pragma unroll
-        for (int u = 0; u < kDeferChains; ++u)
-            if (k0 + 32 * u + lane < total) {
-                const int b = bb[u];
-                st[u][b] = T[u]; st[u][bmax + b] = Tc[u]; st[u][2 * bmax + b] = I[u];
-                st[u][3 * bmax + b] = Ic[u]; st[u][4 * bmax + b] = S[u];
+        for (int j = 0; j < kDeferBins; ++j)
+            if (on[j]) {
+                const int b = b0 + j;
+                st[b] = T[j]; st[bmax + b] = Tc[j]; st[2 * bmax + b] = I[j];
+                st[3 * bmax + b] = Ic[j]; st[4 * bmax + b] = S[j];
             }
     }
 }
@@ -797,7 +812,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
             ++iter;
             const bool idle = __all_sync(0xffffffffu, phase == kDone || phase == kWaitTransfer);
             if (iter % kRecDepth == 0 || idle) {
-                deferred_transfer(A, tb, slot - (tid & 31), fill, B, cam);
+                deferred_transfer(A.rec_buf, A.rec_state, A.bins, A.rec_bmax, tb, slot - (tid & 31), fill, B, cam);
                 if (phase == kWaitTransfer) {
                     finish_pixel<MIXED>(A, cam, bins, B, acc, row, step, fate, att_total);
                     phase = kNeedRay;
