@@ -226,11 +226,14 @@ __device__ __forceinline__ double wrapped_dphi(double phi_new, double phi_old)
     return dphi;
 }
 
+// Kahan step with rounding intrinsics: never fused with the product that
+// makes x, whatever the surrounding code (the in-loop and deferred transfers
+// must round alike).
 __device__ __forceinline__ void kahan_add(float& s, float& c, float x)
 {
-    const float y = x - c;
-    const float t = s + y;
-    c = (t - s) - y;
+    const float y = __fsub_rn(x, c);
+    const float t = __fadd_rn(s, y);
+    c = __fsub_rn(__fsub_rn(t, s), y);
     s = t;
 }
 
@@ -303,7 +306,8 @@ __device__ __forceinline__ void point_terms_body(const DevCam* cam, double r, do
     p.zm1 = static_cast<float>(zp - 1.0);
     const bool emit = (lnC > -INFINITY) && dl_cm > 0.0;
     // ln(g^3 C dl_cm) with g = 1 / zp
-    p.lnK = emit ? lnC + __logf(static_cast<float>(dl_cm)) - 3.0f * p.lnzp : -INFINITY;
+    p.lnK = emit ? __fsub_rn(__fadd_rn(lnC, __logf(static_cast<float>(dl_cm))), __fmul_rn(3.0f, p.lnzp))
+                 : -INFINITY;
     p.nbdl = rho > 0.0f ? rho * static_cast<float>(dl_cm * cam->k_nb) : -1.0f;
 }
 
@@ -329,28 +333,30 @@ template <class Bin>
 __device__ __forceinline__ void bin_point(const PointRec& p, const Bin& bn, const SmemTables& tb, float& T,
                                           float& Tc, float& I, float& Ic, float& S)
 {
+    // Rounding intrinsics throughout: no multiply-add is fused differently in
+    // the in-loop and the deferred transfer.
     if (p.lnK != -INFINITY && bn.E_mid > 0.0) {
-        const float arg = p.lnK - bn.gamma * p.lnzp - bn.kcut * p.zm1;
+        const float arg = __fsub_rn(__fsub_rn(p.lnK, __fmul_rn(bn.gamma, p.lnzp)), __fmul_rn(bn.kcut, p.zm1));
         // ln of this contribution; below -800 it is under FP64's range (the
         // reference adds an exact or subnormal zero)
-        const double x = static_cast<double>(arg) - (static_cast<double>(T) - static_cast<double>(Tc));
+        const double x = __dsub_rn(static_cast<double>(arg), __dsub_rn(static_cast<double>(T), static_cast<double>(Tc)));
         if (x >= -800.0) {
-            double e = x + static_cast<double>(S);
+            double e = __dadd_rn(x, static_cast<double>(S));
             if (I == 0.0f || e > 40.0) {
                 const float shrink = (I == 0.0f) ? 0.0f : __expf(static_cast<float>(-e));
-                I *= shrink;
-                Ic *= shrink;
+                I = __fmul_rn(I, shrink);
+                Ic = __fmul_rn(Ic, shrink);
                 S = static_cast<float>(-x);   // |S| < ~900: exact to 1e-4
-                e = x + static_cast<double>(S);
+                e = __dadd_rn(x, static_cast<double>(S));
             }
             kahan_add(I, Ic, __expf(static_cast<float>(e)));
         }
     }
     if (!(p.nbdl < 0.0f) && p.gg >= bn.gg_lo && p.gg <= bn.gg_hi) {
-        const float lnE = bn.lnE + p.lnzp;
+        const float lnE = __fadd_rn(bn.lnE, p.lnzp);
         int k;
         if (tb.uniform) {   // evenly spaced ln E: direct index, corrected by one knot
-            k = static_cast<int>((lnE - tb.lx0) * tb.inv_dlx) + 1;
+            k = static_cast<int>(__fmul_rn(__fsub_rn(lnE, tb.lx0), tb.inv_dlx)) + 1;
             k = k < 1 ? 1 : (k > tb.n - 1 ? tb.n - 1 : k);
             if (k > 1 && lnE < tb.lx[k - 1]) --k;
             else if (k < tb.n - 1 && lnE > tb.lx[k]) ++k;
@@ -364,8 +370,8 @@ __device__ __forceinline__ void bin_point(const PointRec& p, const Bin& bn, cons
             k = lo < 1 ? 1 : (lo > tb.n - 1 ? tb.n - 1 : lo);
         }
         const float4 sg = tb.seg[k];
-        const float t = (lnE - sg.x) * sg.y;
-        kahan_add(T, Tc, p.nbdl * (sg.z * __expf(t * sg.w)));
+        const float t = __fmul_rn(__fsub_rn(lnE, sg.x), sg.y);
+        kahan_add(T, Tc, __fmul_rn(p.nbdl, __fmul_rn(sg.z, __expf(__fmul_rn(t, sg.w)))));
     }
 }
 
