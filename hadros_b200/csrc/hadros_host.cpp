@@ -82,7 +82,7 @@ namespace {
 // path points and replays them warp-wide into the bins every kRecDepth
 // iterations, so the per-bin accumulators leave shared memory and the
 // occupancy no longer falls with the bin count.  Auto picks it from
-// kDeferMinBins bins.
+// kDeferMinBins bins (measured crossover between 16 and 32 bins).
 bool want_defer(int32_t mode, int precision, int max_bins)
 {
     if (precision != HADROS_PRECISION_MIXED) return false;

@@ -84,7 +84,7 @@ struct PointRec {
     float nbdl;    // n_b dl_cm; negative: no density
 };
 constexpr int kRecDepth = 64;       // points a thread buffers between deferred transfers
-constexpr int kDeferMinBins = 16;   // bins from which the host picks deferred transfer
+constexpr int kDeferMinBins = 24;   // bins from which the host picks deferred transfer
 
 struct TraceArgs {
     const DevCam* cams;

@@ -269,7 +269,10 @@ int32_t hadros_ctx_set_attempt_budget(hadros_ctx* ctx, int64_t attempts_per_ray)
  * memory, so resident rays per SM fall as bins grow).  DEFERRED: each thread
  * buffers 64 points (24 bytes each) and the warp replays them into the bins
  * together, 32 threads sharing the bins (accumulators in a device slot per
- * thread); same results bit for bit.  AUTO (default): deferred from 16 bins.
+ * thread); the same per-bin arithmetic, so with fast_geodesic = 0 the
+ * results are the same bits (the fast arithmetic's FMA contraction may differ
+ * between the two kernels, as between any two builds).  AUTO (default):
+ * deferred from 24 bins.
  * FP64 mode always transfers in the loop.  Applies to later calls and plans. */
 enum hadros_transfer_mode { HADROS_TRANSFER_AUTO = 0, HADROS_TRANSFER_IN_LOOP = 1,
                             HADROS_TRANSFER_DEFERRED = 2 };
