@@ -7,9 +7,9 @@ production: the surrogate is trained on rays the tracer traces at other
 parameter points of the same box (collapsar_ndaf_like, density_weighted
 source, a = 0.95, rho0 log-uniform in [1e9, 1e12], inclination in [10, 80]
 deg); each scan point is then evaluated by the ensemble, the pixels whose
-predicted error bound (sigmas x the ensemble standard deviation of ln I_obs)
-exceeds --bound are traced exactly, and the exact tracer judges a seeded
-random 1% of the pixels.  The plain tracer's time per
+predicted error bound (c x the ensemble standard deviation of ln I_obs, c
+calibrated on held-out cameras, or --sigmas) exceeds --bound are traced
+exactly, and the exact tracer judges a seeded random 1% of the pixels.  The plain tracer's time per
 point is measured on a few points of the same scan.
 
 inference: the surrogate is trained on cameras with randomized spin,
@@ -27,7 +27,7 @@ import time
 
 import numpy as np
 
-from . import Context, SigmaTable, params
+from . import Context, SigmaTable, n_bins_of, params, spectral_bins
 from . import surrogate as S
 from . import workloads as W
 
@@ -130,15 +130,59 @@ def production_cam(rho0: float, theta_deg: float, side: int, n_bins: int):
                                        n_bins=n_bins))
 
 
-def train(ctx, sigma, cams, pixels_per_cam: int, members: int, epochs: int, seed: int, batch: int,
-          lr: float, val_frac: float = 0.1) -> tuple[object, dict]:
-    """Trace training samples on `cams`, hold out the last val_frac of the
-    cameras, train the ensemble; returns it with timing and validation RMS."""
+def n_held_out(n_cams: int, val_frac: float = 0.1) -> int:
+    return max(1, int(round(val_frac * n_cams)))
+
+
+def held_out_samples(ctx, sigma, cams, pixels_per_cam: int, seed: int, i_floor: float):
+    """The held-out cameras' samples (the last n_held_out cameras), as train() traces them."""
+    n_val = n_held_out(len(cams))
+    vraw, vy, _ = S.trace_samples(ctx, sigma, cams[-n_val:], pixels_per_cam, seed=seed + 1, i_floor=i_floor)
+    return cams[-n_val:], vraw, vy
+
+
+def calibrate(sur, sigma, cams, raw, y, i_floor: float, q: float = 0.999, floor_rel: float = 1e-6) -> dict:
+    """How the ensemble's spread relates to its error, on held-out cameras.
+
+    For every held-out pixel (all its bins are in raw/y, camera by camera):
+    the ensemble's I_obs as the inference kernel forms it (log-sum-exp over the
+    bins of the members' mean ln I_E + ln dE), its relative error against the
+    traced I_obs, and the spread (standard deviation over members of each
+    member's ln I_obs).  c is the q-quantile of error / spread over the pixels
+    above floor_rel of the brightest, so c x spread bounds the error of all
+    but a fraction 1 - q of such pixels."""
     torch = _torch()
-    n_val = max(1, int(round(val_frac * len(cams))))
+    B = n_bins_of(cams[0])
+    bins = spectral_bins(cams[0], sigma)
+    valid = (np.asarray(bins["valid"]) != 0) & (np.asarray(bins["dE"]) > 0)
+    dE = torch.tensor(np.where(valid, bins["dE"], 0.0), dtype=torch.float64, device=raw.device)
+    lnde = torch.tensor(np.where(valid, np.log(np.where(valid, bins["dE"], 1.0)), -np.inf),
+                        dtype=torch.float64, device=raw.device)
+    fw = sur.forward(raw).double()                      # [K][n][2]
+    K, n = fw.shape[0], fw.shape[1]
+    P = n // B
+    lnI = fw[:, :, 1].reshape(K, P, B)
+    L_k = torch.logsumexp(lnI + lnde, dim=2)            # [K][P]
+    spread = L_k.std(0, unbiased=False)
+    I_sur = torch.exp(torch.logsumexp(lnI.mean(0) + lnde, dim=1))
+    I_ex = ((torch.exp(y[:, 1].double()) - i_floor).clamp_min(0.0).reshape(P, B) * dE).sum(1)
+    m = I_ex >= floor_rel * I_ex.max()
+    err = ((I_sur - I_ex).abs() / I_ex)[m]
+    ratio = err / spread[m].clamp_min(1e-7)
+    c = float(torch.quantile(ratio, q).item())
+    return {"c": c, "q": q, "pixels": int(m.sum().item()),
+            "error_p99": float(torch.quantile(err, 0.99).item()), "error_max": float(err.max().item()),
+            "spread_median": float(spread[m].median().item())}
+
+
+def train(ctx, sigma, cams, pixels_per_cam: int, members: int, epochs: int, seed: int, batch: int,
+          lr: float) -> tuple[object, dict]:
+    """Trace training samples on `cams`, hold out the last cameras
+    (n_held_out), train the ensemble; returns it with timing and validation RMS."""
+    torch = _torch()
+    n_val = n_held_out(len(cams))
     raw, y, info = S.trace_samples(ctx, sigma, cams[:-n_val], pixels_per_cam, seed=seed)
-    vraw, vy, _ = S.trace_samples(ctx, sigma, cams[-n_val:], pixels_per_cam, seed=seed + 1,
-                                  i_floor=info["i_floor"])
+    _, vraw, vy = held_out_samples(ctx, sigma, cams, pixels_per_cam, seed, info["i_floor"])
     sur = S.Surrogate(members=members, seed=seed)
     t0 = time.perf_counter()
     sur.fit(raw, y, epochs=epochs, batch=batch, lr=lr, floors=(S.TAU_FLOOR, info["i_floor"]))
@@ -173,14 +217,19 @@ def run_production(a) -> dict:
     E, g2, s = W.synthetic_sigma_arrays()
     sigma = SigmaTable.from_arrays(E, s, g2)
     with Context(0) as ctx:
+        tpts = W.scan_points(a.train_points, seed=W.SEED + 17)
+        cams = [production_cam(r, t, a.train_side, a.bins) for r, t in tpts]
         if a.load:
             sur, info = load_model(a.load)
         else:
-            tpts = W.scan_points(a.train_points, seed=W.SEED + 17)
-            cams = [production_cam(r, t, a.train_side, a.bins) for r, t in tpts]
             sur, info = train(ctx, sigma, cams, a.pixels_per_cam, a.members, a.epochs, W.SEED, a.batch, a.lr)
             if a.save:
                 save_model(a.save, sur, info)
+        calib = None
+        if a.sigmas <= 0:   # calibrated bound: c x spread, c from the held-out cameras
+            vcams, vraw, vy = held_out_samples(ctx, sigma, cams, a.pixels_per_cam, W.SEED, info["i_floor"])
+            calib = calibrate(sur, sigma, vcams, vraw, vy, info["i_floor"])
+            a.threshold = a.bound / max(calib["c"], 0.5)
         pts = W.scan_points(a.points, seed=W.SEED)
         rng = np.random.default_rng(W.SEED + 5)
         buf = S.alloc_image(a.side * a.side, a.bins, sur.device, per_bin=False)
@@ -202,7 +251,7 @@ def run_production(a) -> dict:
     return {
         "workload": "production_scan", "points": a.points, "side": a.side, "bins": a.bins,
         "members": a.members, "bound": a.bound, "sigmas": a.sigmas, "threshold": a.threshold,
-        "judge_frac": a.judge,
+        "calibration": calib, "judge_frac": a.judge,
         "train": info,
         "surrogate_s_per_point": sur_total / len(rows),
         "plain_s_per_point": plain_per_point,
@@ -253,13 +302,14 @@ def main(argv=None) -> None:
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--bound", type=float, default=0.01,
                     help="relative error bound above which a pixel is traced exactly")
-    ap.add_argument("--sigmas", type=float, default=3.0,
-                    help="the bound is this many ensemble standard deviations")
+    ap.add_argument("--sigmas", type=float, default=0.0,
+                    help="the predicted error bound is this many ensemble standard deviations; "
+                         "0 (default, production): calibrated on the held-out cameras")
     ap.add_argument("--judge", type=float, default=0.01)
     ap.add_argument("--save", default=None, help="write the trained ensemble here (npz + json)")
     ap.add_argument("--load", default=None, help="use an ensemble written by --save instead of training")
     a = ap.parse_args(argv)
-    a.threshold = a.bound / a.sigmas
+    a.threshold = a.bound / (a.sigmas if a.sigmas > 0 else 3.0)
     if a.workload == "production":
         a.side = a.side or 4096
         a.bins = a.bins or 64

@@ -46,3 +46,34 @@ def test_training_cameras_are_seeded_and_vary_what_config_4_varies():
     cos_i = np.cos(np.radians([c["theta_obs_deg"] for c in cams]))
     assert cos_i.min() >= math.cos(math.radians(85.0)) - 1e-12
     assert all(c["envelope_rho0_gcm3"] == 0.01 * c["rho0_gcm3"] for c in cams)
+
+
+def test_calibration_of_the_spread_against_the_error(hb, sigma_table):
+    """calibrate(): per held-out pixel, the error of the ensemble's I_obs over
+    the spread of the members' ln I_obs.  A stand-in ensemble whose members
+    sit at +-d around a mean that is off by e has spread d and relative error
+    ~e, so c ~ e / d."""
+    import torch
+
+    B, P, K = 4, 300, 4
+    p = hb.params(**W.production_point(nx=64, ny=64, n_bins=B))
+    bins = hb.spectral_bins(p, sigma_table)
+    rng = np.random.default_rng(3)
+    lnI_true = rng.uniform(-70, -50, size=(P, B))
+    floor = 1e-40
+    y = np.stack([np.zeros(P * B), np.log(np.exp(lnI_true).reshape(-1) + floor)], axis=1)
+    e, d = 0.004, 0.002
+    offs = np.array([d, -d, d, -d])[:, None, None]          # members at +-d: spread d
+    lnI_k = lnI_true[None] + np.log1p(e) + offs
+
+    class Ens:
+        def forward(self, raw):
+            out = np.zeros((K, P * B, 2))
+            out[:, :, 1] = lnI_k.reshape(K, -1)
+            return torch.from_numpy(out)
+
+    raw = torch.zeros((P * B, 16))
+    c = scan.calibrate(Ens(), sigma_table, [p], raw, torch.from_numpy(y), floor)
+    assert c["pixels"] > 0.5 * P
+    assert abs(c["spread_median"] - d) < 1e-6
+    assert math.isclose(c["c"], e / d, rel_tol=0.05)
