@@ -48,23 +48,23 @@ def test_training_cameras_are_seeded_and_vary_what_config_4_varies():
     assert all(c["envelope_rho0_gcm3"] == 0.01 * c["rho0_gcm3"] for c in cams)
 
 
-def test_calibration_of_the_spread_against_the_error(hb, sigma_table):
-    """calibrate(): per held-out pixel, the error of the ensemble's I_obs over
-    the spread of the members' ln I_obs.  A stand-in ensemble whose members
-    sit at +-d around a mean that is off by e has spread d and relative error
-    ~e, so c ~ e / d."""
+def test_calibration_picks_the_largest_safe_threshold(hb, sigma_table):
+    """calibrate(): the threshold is the largest spread below which held-out
+    pixels rarely err beyond the bound.  A stand-in ensemble whose pixels have
+    spread d_i and error 0.5% below spread 0.004 but 3% above it must get a
+    threshold just below 0.004."""
     import torch
 
-    B, P, K = 4, 300, 4
+    B, P, K = 4, 2000, 4
     p = hb.params(**W.production_point(nx=64, ny=64, n_bins=B))
-    bins = hb.spectral_bins(p, sigma_table)
     rng = np.random.default_rng(3)
     lnI_true = rng.uniform(-70, -50, size=(P, B))
     floor = 1e-40
     y = np.stack([np.zeros(P * B), np.log(np.exp(lnI_true).reshape(-1) + floor)], axis=1)
-    e, d = 0.004, 0.002
-    offs = np.array([d, -d, d, -d])[:, None, None]          # members at +-d: spread d
-    lnI_k = lnI_true[None] + np.log1p(e) + offs
+    d = np.geomspace(2e-4, 1e-2, P)
+    e = np.where(d < 0.004, 0.005, 0.03)
+    offs = np.array([1.0, -1.0, 1.0, -1.0])[:, None, None] * d[None, :, None]
+    lnI_k = lnI_true[None] + np.log1p(e)[None, :, None] + offs
 
     class Ens:
         def forward(self, raw):
@@ -73,7 +73,7 @@ def test_calibration_of_the_spread_against_the_error(hb, sigma_table):
             return torch.from_numpy(out)
 
     raw = torch.zeros((P * B, 16))
-    c = scan.calibrate(Ens(), sigma_table, [p], raw, torch.from_numpy(y), floor)
+    c = scan.calibrate(Ens(), sigma_table, [p], raw, torch.from_numpy(y), floor, bound=0.01)
     assert c["pixels"] > 0.5 * P
-    assert abs(c["spread_median"] - d) < 1e-6
-    assert math.isclose(c["c"], e / d, rel_tol=0.05)
+    assert 0.0025 < c["threshold"] < 0.004
+    assert abs(c["fallback_frac_held_out"] - (d > c["threshold"]).mean()) < 0.02
