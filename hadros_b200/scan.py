@@ -2,6 +2,7 @@
 
     python -m hadros_b200.scan production --points 256 --side 4096 --bins 64
     python -m hadros_b200.scan inference            # 2048^2 x 32 with fallback
+    python -m hadros_b200.scan batched              # 64 cameras, one graph-captured launch
 
 production: the surrogate is trained on rays the tracer traces at other
 parameter points of the same box (collapsar_ndaf_like, density_weighted
@@ -12,6 +13,11 @@ held-out cameras so that pixels below it err by more than the --bound
 rarely, or --bound / --sigmas) are traced exactly, and the exact tracer
 judges a seeded random 1% of the pixels.  The plain tracer's time per
 point is measured on a few points of the same scan.
+
+batched: 64 cameras of uneven size (64..1024 pixels a side), spin,
+inclination, all eight profiles and rho0, 16 bins, traced in one persistent
+launch from an autotuned plan replayed from a CUDA graph, against the same
+cameras traced one launch each.
 
 inference: the surrogate is trained on cameras with randomized spin,
 inclination, profile, rho0 and two shape parameters, and evaluates the
@@ -297,9 +303,64 @@ def run_inference(a) -> dict:
             "train": info, "surrogate": row, "plain_s": sec, "speedup": sec / row["seconds"]}
 
 
+def run_batched(a) -> dict:
+    """The batched scan: every camera in one persistent launch from a plan
+    whose schedule the autotuner picked, captured in a CUDA graph and
+    replayed; against the same cameras traced one launch after another."""
+    torch = _torch()
+    from . import autotune as AT
+    E, g2, s = W.synthetic_sigma_arrays()
+    sigma = SigmaTable.from_arrays(E, s, g2)
+    cams = [params(**c) for c in W.batched_scan(a.points)]
+    dev = torch.device("cuda", 0)
+    P = sum(int(c.nx) * int(c.ny) for c in cams)
+    B = n_bins_of(cams[0])
+    with Context(0) as ctx:
+        t0 = time.perf_counter()
+        sched, rep = AT.autotune(ctx, cams, sigma, torch, scale=8, repeats=1, use_cache=False)
+        t_tune = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        plan = ctx.plan(cams, sigma, sched)
+        t_plan = time.perf_counter() - t0
+        out = plan.alloc(torch, device=dev, outputs=("tau", "P_surv", "I_obs", "fate", "steps"))
+        st = torch.cuda.Stream()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=st):
+            plan.launch(out, st)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        with torch.cuda.stream(st):
+            g.replay()
+        e1.record(st)
+        torch.cuda.synchronize()
+        t_graph = e0.elapsed_time(e1) / 1e3
+        steps_graph = int(out["steps"].to(torch.int64).sum().item())
+        del g
+        plan.close()
+        # the same cameras, one launch each (the reference's per-camera loop)
+        pmax = max(int(c.nx) * int(c.ny) for c in cams)
+        one = {"tau": torch.empty(pmax, dtype=torch.float64, device=dev),
+               "P_surv": torch.empty(pmax, dtype=torch.float64, device=dev),
+               "I_obs": torch.empty(pmax, dtype=torch.float64, device=dev),
+               "fate": torch.empty(pmax, dtype=torch.int8, device=dev),
+               "steps": torch.empty(pmax, dtype=torch.int32, device=dev)}
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for c in cams:
+            ctx.image_device(c, sigma, one, stream=torch.cuda.current_stream())
+        torch.cuda.synchronize()
+        t_sep = time.perf_counter() - t0
+    return {"workload": "batched_scan", "cameras": len(cams), "pixels": P, "bins": B,
+            "schedule": rep["best"], "autotune_s": t_tune, "plan_s": t_plan,
+            "graph_replay_s": t_graph, "pixel_bins_per_s": P * B / t_graph,
+            "separate_launches_s": t_sep, "speedup_vs_separate": t_sep / t_graph,
+            "accepted_steps": steps_graph, "autotune": rep["timings"]}
+
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("workload", choices=("production", "inference"))
+    ap.add_argument("workload", choices=("production", "inference", "batched"))
     ap.add_argument("--points", type=int, default=256)
     ap.add_argument("--scan-total", type=int, default=0,
                     help="points of the whole scan when --points runs its first ones (for the "
@@ -328,6 +389,9 @@ def main(argv=None) -> None:
         a.side = a.side or 4096
         a.bins = a.bins or 64
         out = run_production(a)
+    elif a.workload == "batched":
+        a.points = a.points if a.points != 256 else 64
+        out = run_batched(a)
     else:
         a.side = a.side or 2048
         a.bins = a.bins or 32
