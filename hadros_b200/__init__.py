@@ -78,13 +78,32 @@ _DEG = {"theta_obs_deg": "theta_obs_rad", "funnel_theta_deg": "funnel_theta_rad"
         "src_gradient_dtheta_deg": "src_gradient_dtheta_rad"}
 
 
+# MeV channel names -> (parser, hadros_params field)
+_MEV_NAMES = {"mev_model": ("hadros_parse_mev_model", "mev_model"),
+              "mev_flavor": ("hadros_parse_mev_flavor", "mev_flavor"),
+              "mev_thermal": ("hadros_parse_mev_thermal", "mev_thermal_profile"),
+              "mev_ye": ("hadros_parse_mev_ye", "mev_ye_profile"),
+              "mev_spectral": ("hadros_parse_mev_spectral", "mev_spectral_mode")}
+
+
+def _mev_kind(fn: str, name: str) -> int:
+    k = C.c_int32()
+    _check(getattr(lib(), fn)(str(name).encode(), C.byref(k)))
+    return k.value
+
+
 def params(**kw) -> HadrosParams:
     """hadros_params_default() with overrides.
 
     Accepts every hadros_params field, the model names ``profile``, ``source``,
     ``spectral`` (reference spellings and aliases), ``precision`` as
     "fp64"/"mixed", and ``*_deg`` forms of the angle fields (converted as the
-    reference apps do: value * M_PI / 180.0).
+    reference apps do: value * M_PI / 180.0).  MeV channel: ``mev_channel``,
+    the names ``mev_model``, ``mev_flavor``, ``mev_thermal``, ``mev_ye``,
+    ``mev_spectral`` and one boolean per switch (``mev_urca``, ``mev_pair``,
+    ``mev_brems``, ``mev_absorption``, ``mev_scattering``,
+    ``mev_degeneracy_correction``, ``mev_abs_n``, ``mev_abs_p``, ``mev_scat_n``,
+    ``mev_scat_p``, ``mev_scat_e``).
     """
     p = HadrosParams()
     lib().hadros_params_default(C.byref(p))
@@ -99,6 +118,12 @@ def params(**kw) -> HadrosParams:
             p.fast_geodesic = 1 if val else 0
         elif key == "precision":
             p.precision = {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}.get(val, val)
+        elif key in _MEV_NAMES:
+            fn, field = _MEV_NAMES[key]
+            setattr(p, field, val if isinstance(val, int) else _mev_kind(fn, val))
+        elif key.startswith("mev_") and key[4:] in abi.MEV_FLAG_BITS:
+            bit = abi.MEV_FLAG_BITS[key[4:]]
+            p.mev_flags = (p.mev_flags | bit) if val else (p.mev_flags & ~bit)
         elif key in _DEG:
             setattr(p, _DEG[key], float(val) * math.pi / 180.0)
         elif hasattr(p, key):
@@ -176,6 +201,14 @@ def spectral_bins(p: HadrosParams, sigma: SigmaTable) -> dict:
 
 
 OUTPUTS = ("tau", "P_surv", "I_obs", "fate", "steps", "attempts", "tau_E", "I_E")
+MEV_OUTPUTS = abi.MEV_OUTPUTS
+
+
+def _with_mev(outputs, cams) -> tuple:
+    """The default outputs gain the MeV channel's when a camera computes it."""
+    if outputs is OUTPUTS and any(int(c.mev_channel) for c in cams):
+        return OUTPUTS + MEV_OUTPUTS
+    return tuple(outputs)
 
 
 def pack_paths(points: np.ndarray, npoints: np.ndarray) -> np.ndarray:
@@ -263,12 +296,14 @@ class Context:
     def image(self, p: HadrosParams, sigma: SigmaTable, pixel_ids=None,
               outputs=OUTPUTS) -> dict:
         """Trace an image (or a pixel list) into host numpy arrays."""
+        outputs = _with_mev(outputs, [p])
         B = n_bins_of(p)
         P = int(p.nx) * int(p.ny) if pixel_ids is None else len(pixel_ids)
         fdt = np.float32 if p.precision == PRECISION_MIXED else np.float64
         shapes = {"tau": (P, np.float64), "P_surv": (P, np.float64), "I_obs": (P, np.float64),
                   "fate": (P, np.int8), "steps": (P, np.int32), "attempts": (P, np.int32),
                   "tau_E": ((P, B), fdt), "I_E": ((P, B), np.float64)}
+        shapes.update({k: (P, np.float64) for k in MEV_OUTPUTS})
         res = {k: np.zeros(shapes[k][0], dtype=shapes[k][1]) for k in outputs}
         out = HadrosImageOut()
         for k, arr in res.items():
@@ -283,6 +318,7 @@ class Context:
 
     def batch(self, cams: list, sigma: SigmaTable, outputs=OUTPUTS) -> list[dict]:
         """Trace many cameras in one launch; returns one dict per camera."""
+        outputs = _with_mev(outputs, cams)
         n = len(cams)
         arr = (HadrosParams * n)(*cams)
         Ps = [int(c.nx) * int(c.ny) for c in cams]
@@ -292,6 +328,7 @@ class Context:
         shapes = {"tau": (P, np.float64), "P_surv": (P, np.float64), "I_obs": (P, np.float64),
                   "fate": (P, np.int8), "steps": (P, np.int32), "attempts": (P, np.int32),
                   "tau_E": (PB, fdt), "I_E": (PB, np.float64)}
+        shapes.update({k: (P, np.float64) for k in MEV_OUTPUTS})
         res = {k: np.zeros(shapes[k][0], dtype=shapes[k][1]) for k in outputs}
         out = HadrosImageOut()
         for k, a in res.items():
@@ -311,6 +348,7 @@ class Context:
         """Pixel subsets of many cameras in one launch (hadros_batch_pixels):
         camera c traces pixel_lists[c]; returns one dict per camera, rows in
         list order."""
+        outputs = _with_mev(outputs, cams)
         n = len(cams)
         if len(pixel_lists) != n:
             raise ValueError("one pixel list per camera")
@@ -324,6 +362,7 @@ class Context:
         shapes = {"tau": (P, np.float64), "P_surv": (P, np.float64), "I_obs": (P, np.float64),
                   "fate": (P, np.int8), "steps": (P, np.int32), "attempts": (P, np.int32),
                   "tau_E": (PB, fdt), "I_E": (PB, np.float64)}
+        shapes.update({k: (P, np.float64) for k in MEV_OUTPUTS})
         res = {k: np.zeros(shapes[k][0], dtype=shapes[k][1]) for k in outputs}
         out = HadrosImageOut()
         for k, a in res.items():
@@ -357,7 +396,10 @@ class Context:
 
     def transfer_paths(self, p: HadrosParams, sigma: SigmaTable, npoints, points, fate=None,
                        outputs=("tau", "P_surv", "I_obs", "fate", "steps", "tau_E", "I_E")) -> dict:
-        """Transfer over cached paths: points packed back to back [sum(npoints), 7]."""
+        """Transfer over cached paths: points packed back to back [sum(npoints), 7]
+        (with the MeV channel's outputs when p computes it)."""
+        if int(p.mev_channel):
+            outputs = tuple(outputs) + tuple(k for k in MEV_OUTPUTS if k not in outputs)
         n = np.ascontiguousarray(npoints, dtype=np.int32)
         pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 7)
         if pts.shape[0] != int(n.sum()):
@@ -368,6 +410,7 @@ class Context:
         shapes = {"tau": (P, np.float64), "P_surv": (P, np.float64), "I_obs": (P, np.float64),
                   "fate": (P, np.int8), "steps": (P, np.int32),
                   "tau_E": ((P, B), fdt), "I_E": ((P, B), np.float64)}
+        shapes.update({k: (P, np.float64) for k in MEV_OUTPUTS})
         res = {k: np.zeros(shapes[k][0], dtype=shapes[k][1]) for k in outputs}
         out = HadrosImageOut()
         for k, a in res.items():
@@ -431,6 +474,8 @@ class Plan:
         spec = {"tau": (P, torch.float64), "P_surv": (P, torch.float64), "I_obs": (P, torch.float64),
                 "fate": (P, torch.int8), "steps": (P, torch.int32), "attempts": (P, torch.int32),
                 "tau_E": (PB, torch.float32 if f32 else torch.float64), "I_E": (PB, torch.float64)}
+        spec.update({k: (P, torch.float64) for k in MEV_OUTPUTS})
+        outputs = _with_mev(outputs, self.cams)
         return {k: torch.empty(spec[k][0], dtype=spec[k][1], device=device) for k in outputs}
 
     def launch(self, out: dict, stream=None) -> None:

@@ -6,7 +6,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK, E_ARG, E_IO, E_CUDA, E_RANGE, E_TIMEOUT, E_NOMEM, E_STATE = range(8)
 
@@ -74,6 +74,29 @@ class HadrosParams(C.Structure):
         ("spec_ecut_GeV", C.c_double),
         ("spec_e_min_GeV", C.c_double),
         ("spec_e_max_GeV", C.c_double),
+        ("mev_channel", C.c_int32),
+        ("mev_model", C.c_int32),
+        ("mev_flavor", C.c_int32),
+        ("mev_thermal_profile", C.c_int32),
+        ("mev_ye_profile", C.c_int32),
+        ("mev_spectral_mode", C.c_int32),
+        ("mev_n_bins", C.c_int32),
+        ("mev_flags", C.c_uint32),
+        ("mev_Enu_obs_MeV", C.c_double),
+        ("mev_norm", C.c_double),
+        ("mev_sigma_abs0_cm2", C.c_double),
+        ("mev_sigma_scat0_cm2", C.c_double),
+        ("mev_neutrinosphere_tau", C.c_double),
+        ("mev_T0_MeV", C.c_double),
+        ("mev_T_floor_MeV", C.c_double),
+        ("mev_T_power", C.c_double),
+        ("mev_Ye_torus", C.c_double),
+        ("mev_Ye_funnel", C.c_double),
+        ("mev_Ye_envelope", C.c_double),
+        ("mev_Ye_floor", C.c_double),
+        ("mev_Ye_ceil", C.c_double),
+        ("mev_E_min_MeV", C.c_double),
+        ("mev_E_max_MeV", C.c_double),
     ]
 
     def copy(self) -> "HadrosParams":
@@ -95,7 +118,23 @@ class HadrosImageOut(C.Structure):
         ("attempts", C.c_void_p),
         ("tau_E", C.c_void_p),
         ("I_E", C.c_void_p),
+        ("tau_mev", C.c_void_p),
+        ("P_surv_mev", C.c_void_p),
+        ("I_obs_mev", C.c_void_p),
+        ("r_nu", C.c_void_p),
+        ("leakage", C.c_void_p),
     ]
+
+
+# MeV thermal channel (enum hadros_mev_* of include/hadros_b200.h)
+MEV_TOY, MEV_PHYSICAL = 0, 1
+MEV_NU_E, MEV_ANTI_NU_E, MEV_NU_X = 0, 1, 2
+MEV_MONOCHROMATIC, MEV_FERMI_DIRAC_BAND = 0, 1
+MEV_FLAG_BITS = {"urca": 1 << 0, "pair": 1 << 1, "brems": 1 << 2, "absorption": 1 << 3, "scattering": 1 << 4,
+                 "degeneracy_correction": 1 << 5, "abs_n": 1 << 6, "abs_p": 1 << 7, "scat_n": 1 << 8,
+                 "scat_p": 1 << 9, "scat_e": 1 << 10}
+MEV_FLAGS_DEFAULT = 0x7DF
+MEV_OUTPUTS = ("tau_mev", "P_surv_mev", "I_obs_mev", "r_nu", "leakage")
 
 
 ORDER_ROWS, ORDER_TILES, ORDER_COST = 0, 1, 2
@@ -149,6 +188,16 @@ SIGNATURES = {
     "hadros_profile_name": (C.c_char_p, [C.c_int32]),
     "hadros_source_name": (C.c_char_p, [C.c_int32]),
     "hadros_spectral_name": (C.c_char_p, [C.c_int32]),
+    "hadros_parse_mev_model": (C.c_int32, [C.c_char_p, P(C.c_int32)]),
+    "hadros_parse_mev_flavor": (C.c_int32, [C.c_char_p, P(C.c_int32)]),
+    "hadros_parse_mev_thermal": (C.c_int32, [C.c_char_p, P(C.c_int32)]),
+    "hadros_parse_mev_ye": (C.c_int32, [C.c_char_p, P(C.c_int32)]),
+    "hadros_parse_mev_spectral": (C.c_int32, [C.c_char_p, P(C.c_int32)]),
+    "hadros_mev_model_name": (C.c_char_p, [C.c_int32]),
+    "hadros_mev_flavor_name": (C.c_char_p, [C.c_int32]),
+    "hadros_mev_thermal_name": (C.c_char_p, [C.c_int32]),
+    "hadros_mev_ye_name": (C.c_char_p, [C.c_int32]),
+    "hadros_mev_spectral_name": (C.c_char_p, [C.c_int32]),
     "hadros_sigma_load": (C.c_int32, [C.c_char_p, P(C.c_void_p)]),
     "hadros_sigma_from_arrays": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                              P(C.c_void_p)]),
@@ -200,6 +249,8 @@ SIGNATURES = {
                                      C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "hadros_write_kimg": (C.c_int32, [C.c_char_p, P(HadrosParams), C.c_double, C.c_double,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hadros_write_dat_mev": (C.c_int32, [C.c_char_p, P(HadrosParams), C.c_char_p, P(HadrosImageOut)]),
+    "hadros_write_kimg_mev": (C.c_int32, [C.c_char_p, P(HadrosParams), P(HadrosImageOut)]),
     "hadros_mlp_param_count": (C.c_int64, []),
     "hadros_mlp_packed_count": (C.c_int64, []),
     "hadros_mlp_workspace_bytes": (C.c_int64, [C.c_int64]),

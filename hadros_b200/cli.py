@@ -1,11 +1,12 @@
 """Command-line entry: trace a named workload image through the C ABI.
 
     python -m hadros_b200.cli image --workload mixed_512 [--nx 256 --ny 256]
-           [--precision mixed|fp64] [--repeat N] [--sigma FILE]
+           [--precision mixed|fp64] [--repeat N] [--sigma FILE] [--mev]
 
 Prints one JSON line with the run statistics (rays, accepted steps, attempts,
-kernel time, fates).  The reference's own command-line drop-in
-(compute_kerr_image, positional argv) lives in hadros_b200.compute_kerr_image.
+kernel time, fates).  --mev also runs the MeV thermal channel.  The
+reference's own command-line drop-in (compute_kerr_image, positional argv) is
+the executable hadros_b200/bin/compute_kerr_image.
 """
 from __future__ import annotations
 
@@ -28,6 +29,8 @@ def cmd_image(a) -> int:
         v = getattr(a, k)
         if v is not None:
             kw[k] = v
+    if a.mev:
+        kw["mev_channel"] = 1
     p = params(**kw)
     if a.sigma:
         sig = SigmaTable.load(a.sigma)
@@ -41,7 +44,7 @@ def cmd_image(a) -> int:
             st = ctx.stats()
             fates = np.bincount(img["fate"].astype(np.int64), minlength=3)
             print(json.dumps({"workload": a.workload, "nx": p.nx, "ny": p.ny, "bins": int(p.n_bins),
-                              "transfer": a.transfer,
+                              "transfer": a.transfer, "mev_channel": int(p.mev_channel),
                               "precision": int(p.precision), "repeat": r,
                               "kernel_ms": st["kernel_ms"], "total_ms": st["total_ms"],
                               "rays": st["rays"], "accepted_steps": st["accepted_steps"],
@@ -69,6 +72,7 @@ def main(argv=None) -> int:
                     help="mixed precision: per-point transfer in the loop, or deferred (warp replays)")
     im.add_argument("--device", type=int, default=0)
     im.add_argument("--sigma", help="sigma table file (reference 3-column format)")
+    im.add_argument("--mev", action="store_true", help="also run the MeV thermal channel")
     a = ap.parse_args(argv)
     if a.cmd == "image":
         return cmd_image(a)

@@ -18,7 +18,17 @@
 // data/sigma/sigma_nuN_CC_GBW.dat, as the reference hard-codes at :2366),
 // --spectral=MODEL --gamma=G --ecut=E --emin=E --emax=E --nbins=N (the CPU
 // app's spectral arguments, apps/compute_kerr_image_from_cache.cpp:271-288),
-// --precision=fp64|mixed, --device=N, --outdir=DIR (default output/images).
+// --precision=fp64|mixed, --device=N, --outdir=DIR (default output/images),
+// and the MeV thermal channel, which the CPU app computes with arguments
+// 45-71 (apps/compute_kerr_image_from_cache.cpp:201-305): --mev=physical|toy|off
+// (default physical), --mev-flavor=, --mev-thermal=, --mev-ye=,
+// --mev-spectral=, --mev-emin=, --mev-emax=, --mev-nbins=, --mev-t0=,
+// --mev-tfloor=, --mev-tpower=, --mev-ye-torus=, --mev-ye-funnel=,
+// --mev-ye-envelope=, --mev-ye-floor=, --mev-ye-ceil=, --mev-sigma-abs=,
+// --mev-sigma-scat=, --mev-nusphere-tau= and the 0/1 switches --mev-urca=,
+// --mev-pair=, --mev-brems=, --mev-absorption=, --mev-scattering=,
+// --mev-degeneracy=, --mev-abs-n=, --mev-abs-p=, --mev-scat-n=, --mev-scat-p=,
+// --mev-scat-e=.  Its five columns go into both output files.
 //
 // Writes DIR/<name>.bin (KIMG) and DIR/<name>.dat with the reference's file
 // name (apps/compute_kerr_image_cuda.cu:2108-2128) and prints the reference's
@@ -29,6 +39,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/hadros_b200.h"
@@ -50,7 +61,13 @@ void usage(const char* argv0)
                  " SOURCE_RADIAL_S SOURCE_GRADIENT_DR SOURCE_GRADIENT_DTHETA_DEG"
                  " SOURCE_RHO_REF SOURCE_CUTOFF_MIN SOURCE_CUTOFF_MAX]\n"
                  "  options: --sigma=FILE --spectral=MODEL --gamma=G --ecut=E --emin=E --emax=E"
-                 " --nbins=N --precision=fp64|mixed --device=N --outdir=DIR\n",
+                 " --nbins=N --precision=fp64|mixed --device=N --outdir=DIR\n"
+                 "  MeV channel: --mev=physical|toy|off --mev-flavor=F --mev-thermal=T --mev-ye=Y"
+                 " --mev-spectral=S --mev-emin=E --mev-emax=E --mev-nbins=N --mev-t0=T --mev-tfloor=T"
+                 " --mev-tpower=P --mev-ye-torus=Y --mev-ye-funnel=Y --mev-ye-envelope=Y"
+                 " --mev-ye-floor=Y --mev-ye-ceil=Y --mev-sigma-abs=S --mev-sigma-scat=S"
+                 " --mev-nusphere-tau=T --mev-{urca,pair,brems,absorption,scattering,degeneracy,"
+                 "abs-n,abs-p,scat-n,scat-p,scat-e}=0|1\n",
                  argv0);
 }
 
@@ -60,11 +77,55 @@ int die(const char* what)
     return 1;
 }
 
+// One --mev-* option into the parameters; false for an unknown key, and
+// *bad for a value the reference's parsers reject.
+bool mev_option(hadros_params& p, const std::string& key, const std::string& val, bool* bad)
+{
+    const double x = std::atof(val.c_str());
+    struct Num { const char* k; double* f; } nums[] = {
+        {"mev-emin", &p.mev_E_min_MeV}, {"mev-emax", &p.mev_E_max_MeV}, {"mev-t0", &p.mev_T0_MeV},
+        {"mev-tfloor", &p.mev_T_floor_MeV}, {"mev-tpower", &p.mev_T_power}, {"mev-ye-torus", &p.mev_Ye_torus},
+        {"mev-ye-funnel", &p.mev_Ye_funnel}, {"mev-ye-envelope", &p.mev_Ye_envelope},
+        {"mev-ye-floor", &p.mev_Ye_floor}, {"mev-ye-ceil", &p.mev_Ye_ceil},
+        {"mev-sigma-abs", &p.mev_sigma_abs0_cm2}, {"mev-sigma-scat", &p.mev_sigma_scat0_cm2},
+        {"mev-nusphere-tau", &p.mev_neutrinosphere_tau}};
+    for (const Num& n : nums)
+        if (key == n.k) { *n.f = x; return true; }
+    struct Bit { const char* k; uint32_t bit; } bits[] = {
+        {"mev-urca", HADROS_MEV_URCA}, {"mev-pair", HADROS_MEV_PAIR}, {"mev-brems", HADROS_MEV_BREMS},
+        {"mev-absorption", HADROS_MEV_ABSORPTION}, {"mev-scattering", HADROS_MEV_SCATTERING},
+        {"mev-degeneracy", HADROS_MEV_DEGENERACY_CORRECTION}, {"mev-abs-n", HADROS_MEV_ABS_N},
+        {"mev-abs-p", HADROS_MEV_ABS_P}, {"mev-scat-n", HADROS_MEV_SCAT_N}, {"mev-scat-p", HADROS_MEV_SCAT_P},
+        {"mev-scat-e", HADROS_MEV_SCAT_E}};
+    for (const Bit& b : bits)
+        if (key == b.k) {   // std::atoi(argv) != 0, as the CPU app reads its switches
+            if (std::atoi(val.c_str()) != 0) p.mev_flags |= b.bit;
+            else p.mev_flags &= ~b.bit;
+            return true;
+        }
+    if (key == "mev-nbins") { p.mev_n_bins = std::atoi(val.c_str()); return true; }
+    if (key == "mev") {
+        if (val == "off") { p.mev_channel = 0; return true; }
+        p.mev_channel = 1;
+        *bad = hadros_parse_mev_model(val.c_str(), &p.mev_model) != 0;
+        return true;
+    }
+    if (key == "mev-flavor") { *bad = hadros_parse_mev_flavor(val.c_str(), &p.mev_flavor) != 0; return true; }
+    if (key == "mev-thermal") { *bad = hadros_parse_mev_thermal(val.c_str(), &p.mev_thermal_profile) != 0; return true; }
+    if (key == "mev-ye") { *bad = hadros_parse_mev_ye(val.c_str(), &p.mev_ye_profile) != 0; return true; }
+    if (key == "mev-spectral") {
+        *bad = hadros_parse_mev_spectral(val.c_str(), &p.mev_spectral_mode) != 0;
+        return true;
+    }
+    return false;
+}
+
 }  // namespace
 
 int main(int argc, char** argv)
 {
     std::vector<std::string> pos;
+    std::vector<std::pair<std::string, std::string>> mev_opts;
     std::string sigma_path = "data/sigma/sigma_nuN_CC_GBW.dat", outdir = "output/images";
     std::string spectral, precision;
     double gamma = NAN, ecut = NAN, emin = NAN, emax = NAN;
@@ -86,6 +147,7 @@ int main(int argc, char** argv)
             else if (key == "nbins") nbins = std::atoi(val.c_str());
             else if (key == "device") device = std::atoi(val.c_str());
             else if (key == "help") { usage(argv[0]); return 0; }
+            else if (key.rfind("mev", 0) == 0) mev_opts.emplace_back(key, val);
             else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); usage(argv[0]); return 1; }
         } else {
             pos.push_back(a);
@@ -110,6 +172,7 @@ int main(int argc, char** argv)
     p.src_cutoff_min = 0.0; p.src_cutoff_max = 1.0e2; p.src_gradient_dr_rg = 0.1;
     p.src_gradient_dtheta_rad = 1.0 * PI / 180.0;
     double mev_E = 10.0, mev_norm = 1.0;
+    p.mev_channel = 1;   // the CPU app always runs its physical MeV block
     p.r_obs_rg = 60.0; p.theta_obs_rad = 80.0 * PI / 180.0; p.fov_deg = 25.0;
     p.nx = 100; p.ny = 100; p.r_max_rg = 120.0; p.h = 0.001; p.tolerance = 1.0e-6;
     p.max_steps = 200000;
@@ -165,6 +228,17 @@ int main(int argc, char** argv)
     if (!std::isnan(emin)) p.spec_e_min_GeV = emin;
     if (!std::isnan(emax)) p.spec_e_max_GeV = emax;
     if (nbins > 0) p.n_bins = nbins;
+    p.mev_Enu_obs_MeV = mev_E;
+    p.mev_norm = mev_norm;
+    for (const auto& kv : mev_opts) {
+        bool bad = false;
+        if (!mev_option(p, kv.first, kv.second, &bad)) {
+            std::fprintf(stderr, "unknown option --%s\n", kv.first.c_str());
+            usage(argv[0]);
+            return 1;
+        }
+        if (bad) return die("MeV channel");
+    }
     if (precision == "mixed") p.precision = HADROS_PRECISION_MIXED;
     else if (!precision.empty() && precision != "fp64") { usage(argv[0]); return 1; }
 
@@ -182,12 +256,21 @@ int main(int argc, char** argv)
     std::vector<double> tau(P), Ps(P), I(P);
     std::vector<int8_t> fate(P);
     std::vector<int32_t> steps(P);
+    std::vector<double> mev[5];
     hadros_image_out out{};
     out.tau = tau.data();
     out.P_surv = Ps.data();
     out.I_obs = I.data();
     out.fate = fate.data();
     out.steps = steps.data();
+    if (p.mev_channel) {
+        for (auto& v : mev) v.resize(P);
+        out.tau_mev = mev[0].data();
+        out.P_surv_mev = mev[1].data();
+        out.I_obs_mev = mev[2].data();
+        out.r_nu = mev[3].data();
+        out.leakage = mev[4].data();
+    }
     std::printf("Grid: %d x %d\n", p.nx, p.ny);
     const auto t0 = std::chrono::steady_clock::now();
     if (hadros_image(ctx, &p, sig, &out)) return die("trace");
@@ -200,10 +283,8 @@ int main(int argc, char** argv)
         hadros_image_filename(&p, 0, nullptr, mev_E, mev_norm, ".dat", name_dat, sizeof(name_dat)))
         return die("file name");
     const std::string bin_path = outdir + "/" + name_bin, dat_path = outdir + "/" + name_dat;
-    if (hadros_write_kimg(bin_path.c_str(), &p, mev_E, mev_norm, tau.data(), Ps.data(), I.data(), fate.data()))
-        return die("write");
-    if (hadros_write_dat(dat_path.c_str(), &p, "GBW", mev_E, mev_norm, tau.data(), Ps.data(), I.data(), fate.data()))
-        return die("write");
+    if (hadros_write_kimg_mev(bin_path.c_str(), &p, &out)) return die("write");
+    if (hadros_write_dat_mev(dat_path.c_str(), &p, "GBW", &out)) return die("write");
     std::printf("Saved: %s\nSaved: %s\n", bin_path.c_str(), dat_path.c_str());
     std::printf("CUDA timing: %g s, %g rays/s, tiles=1, advance launches=%d, accepted steps=%lld\n", elapsed,
                 static_cast<double>(P) / std::max(elapsed, 1.0e-300), st.launches,

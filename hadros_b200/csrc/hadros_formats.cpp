@@ -13,7 +13,8 @@
 //  * output file names (apps/compute_kerr_image_cuda.cu:2108-2128 and
 //    apps/compute_kerr_image_from_cache.cpp:477-500), which the Python drivers
 //    re-derive to find the image.
-// The MeV thermal channel is not computed by this library: its five columns
+// The five MeV columns come from the MeV channel's outputs when the caller
+// passes them (hadros_write_dat_mev / hadros_write_kimg_mev) and otherwise
 // carry RTResult's defaults (tau 0, P 1, I 0, r_nu -1, leakage 1).
 #include <cmath>
 #include <cstdint>
@@ -109,8 +110,12 @@ int32_t hadros_image_filename(const hadros_params* p, int32_t style, const char*
                (p->source_kind == HADROS_SOURCE_INNER_RING ? "" : std::string("_Source_") + kSource[p->source_kind]) +
                (p->spectral_kind == HADROS_SPECTRAL_MONOCHROMATIC ? "" : std::string("_Spectrum_") + kSpectral[p->spectral_kind]) +
                "_Enu_" + make_tag("%.0e", p->Enu_obs_GeV) + "_MeVEnu_" + make_tag("%.0e", mev_E_MeV) +
-               "_MeVNorm_" + make_tag("%.0e", mev_norm) + "_CamTheta_" +
-               make_tag("%.1f", rad2deg(p->theta_obs_rad));
+               "_MeVNorm_" + make_tag("%.0e", mev_norm) +
+               (p->mev_spectral_mode == HADROS_MEV_FERMI_DIRAC_BAND
+                    ? "_MeVSpectrum_fermi_dirac_band_E" + make_tag("%.0e", p->mev_E_min_MeV) + "_" +
+                          make_tag("%.0e", p->mev_E_max_MeV)
+                    : std::string()) +
+               "_CamTheta_" + make_tag("%.1f", rad2deg(p->theta_obs_rad));
     }
     name += ext;
     if (static_cast<int32_t>(name.size()) + 1 > buflen) return ferr(HADROS_E_ARG, "buffer too small");
@@ -118,9 +123,36 @@ int32_t hadros_image_filename(const hadros_params* p, int32_t style, const char*
     return HADROS_OK;
 }
 
-int32_t hadros_write_dat(const char* path, const hadros_params* p, const char* dis_model,
-                         double mev_E_MeV, double mev_norm, const double* tau, const double* P_surv,
-                         const double* I_obs, const int8_t* fate)
+namespace {
+
+// The five MeV columns of pixel k: the arrays given, else RTResult's defaults.
+struct MevCols {
+    const double* a[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    void row(size_t k, double* out) const
+    {
+        static const double def[5] = {0.0, 1.0, 0.0, -1.0, 1.0};
+        for (int c = 0; c < 5; ++c) out[c] = a[c] ? a[c][k] : def[c];
+    }
+};
+
+MevCols mev_cols(const hadros_image_out* h)
+{
+    MevCols m;
+    if (h) {
+        m.a[0] = h->tau_mev;
+        m.a[1] = h->P_surv_mev;
+        m.a[2] = h->I_obs_mev;
+        m.a[3] = h->r_nu;
+        m.a[4] = h->leakage;
+    }
+    return m;
+}
+
+const char* name_or(const char* n) { return n ? n : "?"; }
+
+int32_t write_dat(const char* path, const hadros_params* p, const char* dis_model, double mev_E_MeV,
+                  double mev_norm, const double* tau, const double* P_surv, const double* I_obs,
+                  const int8_t* fate, const MevCols& mev)
 {
     if (!path || !kinds_ok(p) || !tau || !P_surv || !I_obs || !fate)
         return ferr(HADROS_E_ARG, "bad argument");
@@ -160,7 +192,37 @@ int32_t hadros_write_dat(const char* path, const hadros_params* p, const char* d
                  kSpectral[p->spectral_kind], p->spec_gamma, p->spec_ecut_GeV);
     std::fprintf(f, "# spectral_E_min_GeV %g\n# spectral_E_max_GeV %g\n# spectral_N_bins %d\n", p->spec_e_min_GeV,
                  p->spec_e_max_GeV, p->n_bins);
-    std::fprintf(f, "# MEV_ENERGY_MEV %g\n# MEV_NORM %g\n# MEV_CUDA_STATUS not_computed\n", mev_E_MeV, mev_norm);
+    if (p->mev_channel) {   // apps/compute_kerr_image_from_cache.cpp:563-591
+        const uint32_t fl = p->mev_flags;
+        auto on = [&](uint32_t bit) { return (fl & bit) ? 1 : 0; };
+        std::fprintf(f, "# MEV_MODEL %s\n# MEV_CPU_MODEL %s\n# MEV_CUDA_STATUS physical_cpu_equivalent\n",
+                     name_or(hadros_mev_model_name(p->mev_model)), name_or(hadros_mev_model_name(p->mev_model)));
+        std::fprintf(f, "# MEV_FLAVOR %s\n# MEV_ENERGY_MEV %g\n# MEV_NORM %g\n",
+                     name_or(hadros_mev_flavor_name(p->mev_flavor)), mev_E_MeV, mev_norm);
+        std::fprintf(f, "# MEV_INCLUDE_URCA %d\n# MEV_INCLUDE_PAIR %d\n# MEV_INCLUDE_BREMS %d\n",
+                     on(HADROS_MEV_URCA), on(HADROS_MEV_PAIR), on(HADROS_MEV_BREMS));
+        std::fprintf(f, "# MEV_INCLUDE_ABSORPTION %d\n# MEV_INCLUDE_SCATTERING %d\n", on(HADROS_MEV_ABSORPTION),
+                     on(HADROS_MEV_SCATTERING));
+        std::fprintf(f, "# MEV_THERMAL_PROFILE %s\n# MEV_YE_PROFILE %s\n",
+                     name_or(hadros_mev_thermal_name(p->mev_thermal_profile)),
+                     name_or(hadros_mev_ye_name(p->mev_ye_profile)));
+        std::fprintf(f, "# MEV_T0_MEV %g\n# MEV_T_FLOOR_MEV %g\n# MEV_T_POWER %g\n", p->mev_T0_MeV,
+                     p->mev_T_floor_MeV, p->mev_T_power);
+        std::fprintf(f, "# MEV_YE_TORUS %g\n# MEV_YE_FUNNEL %g\n# MEV_YE_ENVELOPE %g\n# MEV_YE_FLOOR %g\n",
+                     p->mev_Ye_torus, p->mev_Ye_funnel, p->mev_Ye_envelope, p->mev_Ye_floor);
+        std::fprintf(f, "# MEV_YE_CEIL %g\n# MEV_SPECTRAL_MODE %s\n# MEV_E_MIN_MEV %g\n# MEV_E_MAX_MEV %g\n",
+                     p->mev_Ye_ceil, name_or(hadros_mev_spectral_name(p->mev_spectral_mode)), p->mev_E_min_MeV,
+                     p->mev_E_max_MeV);
+        std::fprintf(f, "# MEV_N_BINS %d\n# MEV_USE_DEGENERACY_CORRECTION %d\n# MEV_INCLUDE_ABS_N %d\n",
+                     p->mev_n_bins, on(HADROS_MEV_DEGENERACY_CORRECTION), on(HADROS_MEV_ABS_N));
+        std::fprintf(f, "# MEV_INCLUDE_ABS_P %d\n# MEV_INCLUDE_SCAT_N %d\n# MEV_INCLUDE_SCAT_P %d\n",
+                     on(HADROS_MEV_ABS_P), on(HADROS_MEV_SCAT_N), on(HADROS_MEV_SCAT_P));
+        std::fprintf(f, "# MEV_INCLUDE_SCAT_E %d\n# mev_emissivity_units local_spectral_emissivity_proxy_per_MeV\n"
+                        "# mev_opacity_units cm^-1\n",
+                     on(HADROS_MEV_SCAT_E));
+    } else {
+        std::fprintf(f, "# MEV_ENERGY_MEV %g\n# MEV_NORM %g\n# MEV_CUDA_STATUS not_computed\n", mev_E_MeV, mev_norm);
+    }
     std::fprintf(f, "# step_cap %d\n# rkf45_tolerance %g\n# camera_step_rg %g\n# camera_fov_deg %g\n",
                  p->max_steps, p->tolerance, p->h, p->fov_deg);
     std::fprintf(f, "# precision %s\n# backend hadros_b200\n",
@@ -171,9 +233,11 @@ int32_t hadros_write_dat(const char* path, const hadros_params* p, const char* d
         const double v = pixel_v(p, j);
         for (int i = 0; i < p->nx; ++i) {
             const size_t k = static_cast<size_t>(j) * p->nx + i;
+            double m[5];
+            mev.row(k, m);
             std::fprintf(f, "%d %d %.8e %.8e %.8e %.8e %.8e %d %.8e %.8e %.8e %.8e %.8e\n", i, j, pixel_u(p, i), v,
-                         tau[k], P_surv[k], I_obs[k], fate[k] == HADROS_FATE_CAPTURED ? 1 : 0, 0.0, 1.0, 0.0,
-                         -1.0, 1.0);
+                         tau[k], P_surv[k], I_obs[k], fate[k] == HADROS_FATE_CAPTURED ? 1 : 0, m[0], m[1], m[2],
+                         m[3], m[4]);
         }
     }
     const bool ok = std::ferror(f) == 0;
@@ -181,8 +245,8 @@ int32_t hadros_write_dat(const char* path, const hadros_params* p, const char* d
     return ok ? HADROS_OK : ferr(HADROS_E_IO, std::string("write failed: ") + path);
 }
 
-int32_t hadros_write_kimg(const char* path, const hadros_params* p, double mev_E_MeV, double mev_norm,
-                          const double* tau, const double* P_surv, const double* I_obs, const int8_t* fate)
+int32_t write_kimg(const char* path, const hadros_params* p, double mev_E_MeV, double mev_norm, const double* tau,
+                   const double* P_surv, const double* I_obs, const int8_t* fate, const MevCols& mev)
 {
     if (!path || !kinds_ok(p) || !tau || !P_surv || !I_obs || !fate)
         return ferr(HADROS_E_ARG, "bad argument");
@@ -196,15 +260,46 @@ int32_t hadros_write_kimg(const char* path, const hadros_params* p, double mev_E
         const double v = pixel_v(p, j);
         for (int i = 0; i < p->nx; ++i) {
             const size_t k = static_cast<size_t>(j) * p->nx + i;
-            const double row[13] = {static_cast<double>(i), static_cast<double>(j), pixel_u(p, i), v, tau[k],
-                                    P_surv[k], I_obs[k], fate[k] == HADROS_FATE_CAPTURED ? 1.0 : 0.0,
-                                    0.0, 1.0, 0.0, -1.0, 1.0};
+            double row[13] = {static_cast<double>(i), static_cast<double>(j), pixel_u(p, i), v, tau[k],
+                              P_surv[k], I_obs[k], fate[k] == HADROS_FATE_CAPTURED ? 1.0 : 0.0,
+                              0.0, 0.0, 0.0, 0.0, 0.0};
+            mev.row(k, row + 8);
             std::fwrite(row, sizeof(row), 1, f);
         }
     }
     const bool ok = std::ferror(f) == 0;
     std::fclose(f);
     return ok ? HADROS_OK : ferr(HADROS_E_IO, std::string("write failed: ") + path);
+}
+
+}  // namespace
+
+int32_t hadros_write_dat(const char* path, const hadros_params* p, const char* dis_model,
+                         double mev_E_MeV, double mev_norm, const double* tau, const double* P_surv,
+                         const double* I_obs, const int8_t* fate)
+{
+    return write_dat(path, p, dis_model, mev_E_MeV, mev_norm, tau, P_surv, I_obs, fate, MevCols{});
+}
+
+int32_t hadros_write_kimg(const char* path, const hadros_params* p, double mev_E_MeV, double mev_norm,
+                          const double* tau, const double* P_surv, const double* I_obs, const int8_t* fate)
+{
+    return write_kimg(path, p, mev_E_MeV, mev_norm, tau, P_surv, I_obs, fate, MevCols{});
+}
+
+int32_t hadros_write_dat_mev(const char* path, const hadros_params* p, const char* dis_model,
+                             const hadros_image_out* host)
+{
+    if (!host || !p) return ferr(HADROS_E_ARG, "bad argument");
+    return write_dat(path, p, dis_model, p->mev_Enu_obs_MeV, p->mev_norm, host->tau, host->P_surv, host->I_obs,
+                     host->fate, mev_cols(host));
+}
+
+int32_t hadros_write_kimg_mev(const char* path, const hadros_params* p, const hadros_image_out* host)
+{
+    if (!host || !p) return ferr(HADROS_E_ARG, "bad argument");
+    return write_kimg(path, p, p->mev_Enu_obs_MeV, p->mev_norm, host->tau, host->P_surv, host->I_obs, host->fate,
+                      mev_cols(host));
 }
 
 int32_t hadros_write_kgeo(const char* path, const hadros_params* p, int32_t n_rays, const int32_t* pixel_ids,

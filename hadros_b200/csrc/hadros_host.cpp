@@ -15,6 +15,7 @@
 #include <new>
 #include <sstream>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "hadros_internal.h"
@@ -43,6 +44,32 @@ const char* const kProfileNames[8] = {"gaussian", "powerlaw", "gaussian_funnel",
 const char* const kSourceNames[5] = {"inner_ring", "funnel_wall", "jet_base", "shock_layer",
                                      "density_weighted"};
 const char* const kSpectralNames[3] = {"monochromatic", "powerlaw", "powerlaw_cutoff"};
+
+// One MeV name table: the accepted spellings of each kind and the
+// reference's error text (src/mev_neutrino_physics.cpp:37-238).
+int32_t parse_names(const char* name, int32_t* kind, std::initializer_list<std::initializer_list<const char*>> kinds,
+                    const char* what, const char* choices)
+{
+    if (!name || !kind) return fail(HADROS_E_ARG, "NULL argument");
+    const std::string n(name);
+    int32_t k = 0;
+    for (const auto& names : kinds) {
+        for (const char* a : names)
+            if (n == a) {
+                *kind = k;
+                return ok();
+            }
+        ++k;
+    }
+    return fail(HADROS_E_ARG, std::string("Unknown ") + what + " '" + n + "'. Use " + choices + ".");
+}
+const char* const kMevModelNames[2] = {"toy", "physical"};
+const char* const kMevFlavorNames[3] = {"nu_e", "anti_nu_e", "nu_x"};
+const char* const kMevThermalNames[5] = {"constant", "inner_hot_torus", "radial_powerlaw",
+                                         "torus_plus_cool_envelope", "collapsar_inner_hot"};
+const char* const kMevYeNames[5] = {"constant", "neutron_rich_torus", "funnel_proton_rich",
+                                    "torus_envelope_contrast", "collapsar_neutron_rich"};
+const char* const kMevSpectralNames[2] = {"monochromatic", "fermi_dirac_band"};
 
 std::atomic<uint64_t> g_sigma_serial{1};
 
@@ -179,6 +206,101 @@ int32_t upload_sigma(hadros_ctx* ctx, const hadros_sigma* s, uint64_t serial)
     return HADROS_OK;
 }
 
+// Every array of hadros_image_out with its element size and extent: P rows
+// per pixel, or PB per-bin elements (tau_E in the transfer's precision).
+template <class F>
+void each_output(size_t fsz, F&& f)
+{
+    f(&hadros_image_out::tau, size_t(8), false);
+    f(&hadros_image_out::P_surv, size_t(8), false);
+    f(&hadros_image_out::I_obs, size_t(8), false);
+    f(&hadros_image_out::steps, size_t(4), false);
+    f(&hadros_image_out::attempts, size_t(4), false);
+    f(&hadros_image_out::fate, size_t(1), false);
+    f(&hadros_image_out::tau_E, fsz, true);
+    f(&hadros_image_out::I_E, size_t(8), true);
+    f(&hadros_image_out::tau_mev, size_t(8), false);
+    f(&hadros_image_out::P_surv_mev, size_t(8), false);
+    f(&hadros_image_out::I_obs_mev, size_t(8), false);
+    f(&hadros_image_out::r_nu, size_t(8), false);
+    f(&hadros_image_out::leakage, size_t(8), false);
+}
+
+// Device staging of a call with host outputs: one 256-byte aligned slice of
+// ctx->d_out per requested array, after `head` bytes the caller keeps.
+struct Staged {
+    hadros_image_out d{};
+    struct Cp { void* h; const void* d; size_t n; };
+    std::vector<Cp> copies;
+    unsigned char* base = nullptr;
+};
+
+int32_t stage_outputs(hadros_ctx* ctx, const hadros_image_out* out, int64_t P, int64_t PB, size_t fsz, size_t head,
+                      Staged& st)
+{
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    std::vector<size_t> offs;
+    size_t o = al(head);
+    each_output(fsz, [&](auto m, size_t esz, bool per_bin) {
+        offs.push_back(o);
+        if (out->*m) o = al(o + esz * static_cast<size_t>(per_bin ? PB : P));
+    });
+    const int32_t rc = grow(ctx, &ctx->d_out, &ctx->out_cap, o, "output buffers");
+    if (rc) return rc;
+    st.base = static_cast<unsigned char*>(ctx->d_out);
+    st.copies.clear();
+    size_t k = 0;
+    each_output(fsz, [&](auto m, size_t esz, bool per_bin) {
+        using T = std::remove_reference_t<decltype(st.d.*m)>;
+        const size_t off = offs[k++];
+        if (!(out->*m)) {
+            st.d.*m = nullptr;
+            return;
+        }
+        st.d.*m = static_cast<T>(static_cast<void*>(st.base + off));
+        st.copies.push_back({static_cast<void*>(out->*m), static_cast<const void*>(st.d.*m),
+                             esz * static_cast<size_t>(per_bin ? PB : P)});
+    });
+    return HADROS_OK;
+}
+
+// Enqueue the device-to-host copies of a staged call; adds their bytes to *d2h.
+int32_t download_outputs(hadros_ctx* ctx, const Staged& st, cudaStream_t stream, int64_t* d2h)
+{
+    for (const Staged::Cp& c : st.copies) {
+        if (c.n == 0) continue;
+        *d2h += static_cast<int64_t>(c.n);
+        const cudaError_t e = cudaMemcpyAsync(c.h, c.d, c.n, cudaMemcpyDeviceToHost, stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "output download");
+    }
+    return HADROS_OK;
+}
+
+// Output pointers of a launch (DEVICE pointers).
+void set_outputs(TraceArgs& A, const hadros_image_out& d)
+{
+    A.tau = d.tau;
+    A.P_surv = d.P_surv;
+    A.I_obs = d.I_obs;
+    A.fate = d.fate;
+    A.steps = d.steps;
+    A.attempts = d.attempts;
+    A.tau_E = d.tau_E;
+    A.I_E = static_cast<double*>(d.I_E);
+    A.tau_mev = d.tau_mev;
+    A.P_surv_mev = d.P_surv_mev;
+    A.I_obs_mev = d.I_obs_mev;
+    A.r_nu = d.r_nu;
+    A.leakage = d.leakage;
+}
+
+bool any_mev(const hadros_params* cams, int32_t n)
+{
+    for (int32_t c = 0; c < n; ++c)
+        if (cams[c].mev_channel) return true;
+    return false;
+}
+
 }  // namespace
 
 namespace {
@@ -263,6 +385,31 @@ void hadros_params_default(hadros_params* p)
     p->n_bins = 8;
     p->precision = HADROS_PRECISION_FP64;
     p->fast_geodesic = 1;
+    // MeVThermalParams defaults (include/radiative_transfer.hpp:64-101); the
+    // channel itself is off until mev_channel is set
+    p->mev_channel = 0;
+    p->mev_model = HADROS_MEV_PHYSICAL;
+    p->mev_flavor = HADROS_MEV_ANTI_NU_E;
+    p->mev_thermal_profile = HADROS_MEV_T_INNER_HOT_TORUS;
+    p->mev_ye_profile = HADROS_MEV_YE_NEUTRON_RICH_TORUS;
+    p->mev_spectral_mode = HADROS_MEV_MONOCHROMATIC;
+    p->mev_n_bins = 8;
+    p->mev_flags = HADROS_MEV_FLAGS_DEFAULT;
+    p->mev_Enu_obs_MeV = 10.0;
+    p->mev_norm = 1.0;
+    p->mev_sigma_abs0_cm2 = 9.6e-44;
+    p->mev_sigma_scat0_cm2 = 1.7e-44;
+    p->mev_neutrinosphere_tau = 2.0 / 3.0;
+    p->mev_T0_MeV = 6.0;
+    p->mev_T_floor_MeV = 0.1;
+    p->mev_T_power = 0.2;
+    p->mev_Ye_torus = 0.25;
+    p->mev_Ye_funnel = 0.55;
+    p->mev_Ye_envelope = 0.45;
+    p->mev_Ye_floor = 0.01;
+    p->mev_Ye_ceil = 0.60;
+    p->mev_E_min_MeV = 3.0;
+    p->mev_E_max_MeV = 50.0;
 }
 
 int32_t hadros_params_validate(const hadros_params* p)
@@ -290,6 +437,23 @@ int32_t hadros_params_validate(const hadros_params* p)
     if (!finite_all({p->a_spin, p->r_obs_rg, p->theta_obs_rad, p->fov_deg, p->r_max_rg,
                      p->Enu_obs_GeV, p->M_bh_msun}))
         return fail(HADROS_E_ARG, "camera parameters must be finite");
+    if (p->mev_channel != 0 && p->mev_channel != 1) return fail(HADROS_E_ARG, "mev_channel must be 0 or 1");
+    if (p->mev_channel) {
+        if (p->mev_model < 0 || p->mev_model > 1) return fail(HADROS_E_ARG, "mev_model out of range");
+        if (p->mev_flavor < 0 || p->mev_flavor > 2) return fail(HADROS_E_ARG, "mev_flavor out of range");
+        if (p->mev_thermal_profile < 0 || p->mev_thermal_profile > 4)
+            return fail(HADROS_E_ARG, "mev_thermal_profile out of range");
+        if (p->mev_ye_profile < 0 || p->mev_ye_profile > 4) return fail(HADROS_E_ARG, "mev_ye_profile out of range");
+        if (p->mev_spectral_mode < 0 || p->mev_spectral_mode > 1)
+            return fail(HADROS_E_ARG, "mev_spectral_mode out of range");
+        if (p->mev_spectral_mode == HADROS_MEV_FERMI_DIRAC_BAND && p->mev_n_bins > 4096)
+            return fail(HADROS_E_ARG, "mev_n_bins must be <= 4096");
+        if (!finite_all({p->mev_Enu_obs_MeV, p->mev_norm, p->mev_sigma_abs0_cm2, p->mev_sigma_scat0_cm2,
+                         p->mev_neutrinosphere_tau, p->mev_T0_MeV, p->mev_T_floor_MeV, p->mev_T_power,
+                         p->mev_Ye_torus, p->mev_Ye_funnel, p->mev_Ye_envelope, p->mev_Ye_floor, p->mev_Ye_ceil,
+                         p->mev_E_min_MeV, p->mev_E_max_MeV}))
+            return fail(HADROS_E_ARG, "MeV channel parameters must be finite");
+    }
     return ok();
 }
 
@@ -347,6 +511,57 @@ int32_t hadros_parse_spectral(const char* name, int32_t* kind)
     *kind = k;
     return ok();
 }
+
+
+int32_t hadros_parse_mev_model(const char* name, int32_t* kind)
+{   // parse_mev_model, src/mev_neutrino_physics.cpp:37-51
+    return parse_names(name, kind, {{"toy", "TOY"}, {"physical", "PHYSICAL", "phys"}}, "MEV_MODEL",
+                       "toy or physical");
+}
+
+int32_t hadros_parse_mev_flavor(const char* name, int32_t* kind)
+{   // parse_mev_flavor, :65-90
+    return parse_names(name, kind,
+                       {{"nu_e", "nue", "NU_E"}, {"anti_nu_e", "antinue", "anti-nu-e", "ANTI_NU_E"},
+                        {"nu_x", "nux", "NU_X"}},
+                       "MEV_FLAVOR", "nu_e, anti_nu_e, or nu_x");
+}
+
+int32_t hadros_parse_mev_thermal(const char* name, int32_t* kind)
+{   // parse_mev_thermal_profile, :106-130
+    return parse_names(name, kind,
+                       {{"constant", "CONSTANT"}, {"inner_hot_torus", "INNER_HOT_TORUS"},
+                        {"radial_powerlaw", "RADIAL_POWERLAW"},
+                        {"torus_plus_cool_envelope", "TORUS_PLUS_COOL_ENVELOPE"},
+                        {"collapsar_inner_hot", "COLLAPSAR_INNER_HOT"}},
+                       "MEV_THERMAL_PROFILE",
+                       "constant, inner_hot_torus, radial_powerlaw, torus_plus_cool_envelope, or collapsar_inner_hot");
+}
+
+int32_t hadros_parse_mev_ye(const char* name, int32_t* kind)
+{   // parse_mev_ye_profile, :149-173
+    return parse_names(name, kind,
+                       {{"constant", "CONSTANT"}, {"neutron_rich_torus", "NEUTRON_RICH_TORUS"},
+                        {"funnel_proton_rich", "FUNNEL_PROTON_RICH"},
+                        {"torus_envelope_contrast", "TORUS_ENVELOPE_CONTRAST"},
+                        {"collapsar_neutron_rich", "COLLAPSAR_NEUTRON_RICH"}},
+                       "MEV_YE_PROFILE",
+                       "constant, neutron_rich_torus, funnel_proton_rich, torus_envelope_contrast, or "
+                       "collapsar_neutron_rich");
+}
+
+int32_t hadros_parse_mev_spectral(const char* name, int32_t* kind)
+{   // parse_mev_spectral_mode, :192-209
+    return parse_names(name, kind,
+                       {{"monochromatic", "MONOCHROMATIC", "mono"}, {"fermi_dirac_band", "FERMI_DIRAC_BAND", "fd_band"}},
+                       "MEV_SPECTRAL_MODE", "monochromatic or fermi_dirac_band");
+}
+
+const char* hadros_mev_model_name(int32_t k) { return (k >= 0 && k < 2) ? kMevModelNames[k] : nullptr; }
+const char* hadros_mev_flavor_name(int32_t k) { return (k >= 0 && k < 3) ? kMevFlavorNames[k] : nullptr; }
+const char* hadros_mev_thermal_name(int32_t k) { return (k >= 0 && k < 5) ? kMevThermalNames[k] : nullptr; }
+const char* hadros_mev_ye_name(int32_t k) { return (k >= 0 && k < 5) ? kMevYeNames[k] : nullptr; }
+const char* hadros_mev_spectral_name(int32_t k) { return (k >= 0 && k < 2) ? kMevSpectralNames[k] : nullptr; }
 
 const char* hadros_profile_name(int32_t kind) { return (kind >= 0 && kind < 8) ? kProfileNames[kind] : nullptr; }
 const char* hadros_source_name(int32_t kind) { return (kind >= 0 && kind < 5) ? kSourceNames[kind] : nullptr; }
@@ -611,14 +826,8 @@ int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s
     A.pixel_ids = d_pix;
     A.bins = static_cast<const DevBin*>(ctx->d_bins);
     A.sig = ctx->sig_dev;
-    A.tau = dev_out.tau;
-    A.P_surv = dev_out.P_surv;
-    A.I_obs = dev_out.I_obs;
-    A.fate = dev_out.fate;
-    A.steps = dev_out.steps;
-    A.attempts = dev_out.attempts;
-    A.tau_E = dev_out.tau_E;
-    A.I_E = static_cast<double*>(dev_out.I_E);
+    set_outputs(A, dev_out);
+    A.mev = p->mev_channel ? 1 : 0;
     A.counters = ctx->d_counters;
     A.fast_geodesic = p->fast_geodesic;
     A.paths = g_path_rec.buf;
@@ -723,14 +932,8 @@ int32_t run_batch(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, co
     A.pixel_ids = d_pix;
     A.bins = static_cast<const DevBin*>(ctx->d_bins);
     A.sig = ctx->sig_dev;
-    A.tau = dev_out.tau;
-    A.P_surv = dev_out.P_surv;
-    A.I_obs = dev_out.I_obs;
-    A.fate = dev_out.fate;
-    A.steps = dev_out.steps;
-    A.attempts = dev_out.attempts;
-    A.tau_E = dev_out.tau_E;
-    A.I_E = static_cast<double*>(dev_out.I_E);
+    set_outputs(A, dev_out);
+    A.mev = any_mev(cams, n_cams) ? 1 : 0;
     A.counters = ctx->d_counters;
     int32_t max_cap = 0;
     for (int32_t c = 0; c < n_cams; ++c) max_cap = std::max(max_cap, cams[c].max_steps);
@@ -791,42 +994,12 @@ int32_t image_host(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* 
     const int64_t P = pix ? n_pix : static_cast<int64_t>(p->nx) * p->ny;
     const int64_t B = p->spectral_kind == HADROS_SPECTRAL_MONOCHROMATIC ? 1 : std::max(p->n_bins, 1);
     const size_t fsz = p->precision == HADROS_PRECISION_MIXED ? 4 : 8;
-    // device staging: tau, P, I (8B), steps, attempts (4B), fate (1B), tau_E, I_E
-    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-    size_t o = 0;
-    const size_t o_tau = o; o = al(o + (out->tau ? 8 * P : 0));
-    const size_t o_P = o; o = al(o + (out->P_surv ? 8 * P : 0));
-    const size_t o_I = o; o = al(o + (out->I_obs ? 8 * P : 0));
-    const size_t o_st = o; o = al(o + (out->steps ? 4 * P : 0));
-    const size_t o_at = o; o = al(o + (out->attempts ? 4 * P : 0));
-    const size_t o_f = o; o = al(o + (out->fate ? P : 0));
-    const size_t o_tE = o; o = al(o + (out->tau_E ? fsz * P * B : 0));
-    const size_t o_IE = o; o = al(o + (out->I_E ? 8 * P * B : 0));
-    if ((rc = grow(ctx, &ctx->d_out, &ctx->out_cap, o, "output buffers"))) return rc;
-    unsigned char* base = static_cast<unsigned char*>(ctx->d_out);
-    hadros_image_out d{};
-    d.tau = out->tau ? reinterpret_cast<double*>(base + o_tau) : nullptr;
-    d.P_surv = out->P_surv ? reinterpret_cast<double*>(base + o_P) : nullptr;
-    d.I_obs = out->I_obs ? reinterpret_cast<double*>(base + o_I) : nullptr;
-    d.steps = out->steps ? reinterpret_cast<int32_t*>(base + o_st) : nullptr;
-    d.attempts = out->attempts ? reinterpret_cast<int32_t*>(base + o_at) : nullptr;
-    d.fate = out->fate ? reinterpret_cast<int8_t*>(base + o_f) : nullptr;
-    d.tau_E = out->tau_E ? static_cast<void*>(base + o_tE) : nullptr;
-    d.I_E = out->I_E ? static_cast<void*>(base + o_IE) : nullptr;
-    rc = run_image(ctx, p, s, pix, n_pix, d, ctx->stream, true);
+    Staged sg;
+    if ((rc = stage_outputs(ctx, out, P, P * B, fsz, 0, sg))) return rc;
+    rc = run_image(ctx, p, s, pix, n_pix, sg.d, ctx->stream, true);
     if (rc) return rc;
-    struct Cp { void* h; const void* d; size_t n; } cps[8] = {
-        {out->tau, d.tau, 8 * size_t(P)}, {out->P_surv, d.P_surv, 8 * size_t(P)},
-        {out->I_obs, d.I_obs, 8 * size_t(P)}, {out->steps, d.steps, 4 * size_t(P)},
-        {out->attempts, d.attempts, 4 * size_t(P)}, {out->fate, d.fate, size_t(P)},
-        {out->tau_E, d.tau_E, fsz * size_t(P * B)}, {out->I_E, d.I_E, 8 * size_t(P * B)}};
     int64_t d2h = 4 * sizeof(unsigned long long);
-    for (auto& c : cps) {
-        if (!c.h || c.n == 0) continue;
-        d2h += static_cast<int64_t>(c.n);
-        cudaError_t e = cudaMemcpyAsync(c.h, c.d, c.n, cudaMemcpyDeviceToHost, ctx->stream);
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "output download");
-    }
+    if ((rc = download_outputs(ctx, sg, ctx->stream, &d2h))) return rc;
     rc = finish_sync(ctx, true);
     ctx->stats.d2h_bytes = d2h;
     ctx->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -900,43 +1073,14 @@ int32_t batch_host(hadros_ctx* ctx, const hadros_params* cams, int32_t n_cams, c
             PB += pc * (cams[c].spectral_kind == HADROS_SPECTRAL_MONOCHROMATIC ? 1 : std::max(cams[c].n_bins, 1));
         }
         const size_t fsz = cams[0].precision == HADROS_PRECISION_MIXED ? 4 : 8;
-        auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-        size_t o = 0;
-        const size_t o_tau = o; o = al(o + (out->tau ? 8 * P : 0));
-        const size_t o_P = o; o = al(o + (out->P_surv ? 8 * P : 0));
-        const size_t o_I = o; o = al(o + (out->I_obs ? 8 * P : 0));
-        const size_t o_st = o; o = al(o + (out->steps ? 4 * P : 0));
-        const size_t o_at = o; o = al(o + (out->attempts ? 4 * P : 0));
-        const size_t o_f = o; o = al(o + (out->fate ? P : 0));
-        const size_t o_tE = o; o = al(o + (out->tau_E ? fsz * PB : 0));
-        const size_t o_IE = o; o = al(o + (out->I_E ? 8 * PB : 0));
-        int32_t rc = grow(ctx, &ctx->d_out, &ctx->out_cap, o, "output buffers");
+        Staged sg;
+        int32_t rc = stage_outputs(ctx, out, P, PB, fsz, 0, sg);
         if (rc) return rc;
-        unsigned char* base = static_cast<unsigned char*>(ctx->d_out);
-        hadros_image_out d{};
-        d.tau = out->tau ? reinterpret_cast<double*>(base + o_tau) : nullptr;
-        d.P_surv = out->P_surv ? reinterpret_cast<double*>(base + o_P) : nullptr;
-        d.I_obs = out->I_obs ? reinterpret_cast<double*>(base + o_I) : nullptr;
-        d.steps = out->steps ? reinterpret_cast<int32_t*>(base + o_st) : nullptr;
-        d.attempts = out->attempts ? reinterpret_cast<int32_t*>(base + o_at) : nullptr;
-        d.fate = out->fate ? reinterpret_cast<int8_t*>(base + o_f) : nullptr;
-        d.tau_E = out->tau_E ? static_cast<void*>(base + o_tE) : nullptr;
-        d.I_E = out->I_E ? static_cast<void*>(base + o_IE) : nullptr;
         int64_t P2 = 0, PB2 = 0;
-        rc = run_batch(ctx, cams, n_cams, s, d, ctx->stream, true, &P2, &PB2, pix, counts);
+        rc = run_batch(ctx, cams, n_cams, s, sg.d, ctx->stream, true, &P2, &PB2, pix, counts);
         if (rc) return rc;
-        struct Cp { void* h; const void* d; size_t n; } cps[8] = {
-            {out->tau, d.tau, 8 * size_t(P)}, {out->P_surv, d.P_surv, 8 * size_t(P)},
-            {out->I_obs, d.I_obs, 8 * size_t(P)}, {out->steps, d.steps, 4 * size_t(P)},
-            {out->attempts, d.attempts, 4 * size_t(P)}, {out->fate, d.fate, size_t(P)},
-            {out->tau_E, d.tau_E, fsz * size_t(PB)}, {out->I_E, d.I_E, 8 * size_t(PB)}};
         int64_t d2h = 4 * sizeof(unsigned long long);
-        for (auto& c : cps) {
-            if (!c.h || c.n == 0) continue;
-            d2h += static_cast<int64_t>(c.n);
-            cudaError_t e = cudaMemcpyAsync(c.h, c.d, c.n, cudaMemcpyDeviceToHost, ctx->stream);
-            if (e != cudaSuccess) return cuda_fail(ctx, e, "output download");
-        }
+        if ((rc = download_outputs(ctx, sg, ctx->stream, &d2h))) return rc;
         rc = finish_sync(ctx, true);
         ctx->stats.d2h_bytes = d2h;
         ctx->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -974,6 +1118,7 @@ int32_t hadros_trace_paths(hadros_ctx* ctx, const hadros_params* p, const int32_
         // a path-only trace: monochromatic, no per-bin outputs
         hadros_params q = *p;
         q.spectral_kind = HADROS_SPECTRAL_MONOCHROMATIC;
+        q.mev_channel = 0;
         if (!(q.Enu_obs_GeV > 0.0)) q.Enu_obs_GeV = 1.0e9;
         void* d_paths = nullptr;
         cudaError_t e = cudaSetDevice(ctx->device);
@@ -1050,14 +1195,8 @@ int32_t hadros_transfer_paths(hadros_ctx* ctx, const hadros_params* p, const had
         const size_t o_pts = o; o = al(o + 56 * static_cast<size_t>(n_pts));
         const size_t o_off = o; o = al(o + 8 * offs.size());
         const size_t o_fin = o; o = al(o + P);
-        const size_t o_tau = o; o = al(o + (out->tau ? 8 * P : 0));
-        const size_t o_P = o; o = al(o + (out->P_surv ? 8 * P : 0));
-        const size_t o_I = o; o = al(o + (out->I_obs ? 8 * P : 0));
-        const size_t o_st = o; o = al(o + (out->steps ? 4 * P : 0));
-        const size_t o_f = o; o = al(o + (out->fate ? P : 0));
-        const size_t o_tE = o; o = al(o + (out->tau_E ? fsz * P * B : 0));
-        const size_t o_IE = o; o = al(o + (out->I_E ? 8 * P * B : 0));
-        if ((rc = grow(ctx, &ctx->d_out, &ctx->out_cap, o, "path buffers"))) return rc;
+        Staged sg;   // the cached paths, then the outputs
+        if ((rc = stage_outputs(ctx, out, P, P * B, fsz, o, sg))) return rc;
         if ((rc = upload_sigma(ctx, s, sigma_serial(s)))) return rc;
         if ((rc = grow(ctx, &ctx->d_cams, &ctx->cams_cap, sizeof(DevCam), "camera table"))) return rc;
         if ((rc = grow(ctx, &ctx->d_bins, &ctx->bins_cap, sizeof(DevBin) * bins.size(), "bin table"))) return rc;
@@ -1078,13 +1217,8 @@ int32_t hadros_transfer_paths(hadros_ctx* ctx, const hadros_params* p, const had
         A.total_items = P;
         A.bins = static_cast<const DevBin*>(ctx->d_bins);
         A.sig = ctx->sig_dev;
-        A.tau = out->tau ? reinterpret_cast<double*>(base + o_tau) : nullptr;
-        A.P_surv = out->P_surv ? reinterpret_cast<double*>(base + o_P) : nullptr;
-        A.I_obs = out->I_obs ? reinterpret_cast<double*>(base + o_I) : nullptr;
-        A.steps = out->steps ? reinterpret_cast<int32_t*>(base + o_st) : nullptr;
-        A.fate = out->fate ? reinterpret_cast<int8_t*>(base + o_f) : nullptr;
-        A.tau_E = out->tau_E ? static_cast<void*>(base + o_tE) : nullptr;
-        A.I_E = out->I_E ? reinterpret_cast<double*>(base + o_IE) : nullptr;
+        set_outputs(A, sg.d);
+        A.mev = p->mev_channel ? 1 : 0;
         A.counters = ctx->d_counters;
         A.path_offsets = reinterpret_cast<const int64_t*>(base + o_off);
         A.path_points = reinterpret_cast<const double*>(base + o_pts);
@@ -1099,18 +1233,8 @@ int32_t hadros_transfer_paths(hadros_ctx* ctx, const hadros_params* p, const had
         ctx->stats.rays = P;
         ctx->stats.launches = P > 0 ? 1 : 0;
         ctx->stats.h2d_bytes = static_cast<int64_t>(56 * n_pts + 8 * offs.size() + (fate ? P : 0));
-        struct Cp { void* h; const void* d; size_t n; } cps[7] = {
-            {out->tau, A.tau, 8 * size_t(P)}, {out->P_surv, A.P_surv, 8 * size_t(P)},
-            {out->I_obs, A.I_obs, 8 * size_t(P)}, {out->steps, A.steps, 4 * size_t(P)},
-            {out->fate, A.fate, size_t(P)}, {out->tau_E, A.tau_E, fsz * size_t(P * B)},
-            {out->I_E, A.I_E, 8 * size_t(P * B)}};
         int64_t d2h = 0;
-        for (auto& c : cps) {
-            if (!c.h || c.n == 0) continue;
-            d2h += static_cast<int64_t>(c.n);
-            e = cudaMemcpyAsync(c.h, c.d, c.n, cudaMemcpyDeviceToHost, st);
-            if (e != cudaSuccess) return cuda_fail(ctx, e, "output download");
-        }
+        if ((rc = download_outputs(ctx, sg, st, &d2h))) return rc;
         rc = finish_sync(ctx, true);
         ctx->stats.d2h_bytes = d2h;
         ctx->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -1170,6 +1294,7 @@ int32_t cost_order(hadros_ctx* ctx, const hadros_params& p, const hadros_sigma* 
     o.steps = steps.data();
     hadros_params q = p;
     q.spectral_kind = HADROS_SPECTRAL_MONOCHROMATIC;   // geometry only
+    q.mev_channel = 0;
     int32_t rc = hadros_image_pixels(ctx, &q, s, ids.data(), static_cast<int32_t>(ids.size()), &o);
     if (rc) return rc;
     std::vector<float> cost(static_cast<size_t>(nx) * ny);
@@ -1341,6 +1466,7 @@ int32_t hadros_plan_create(hadros_ctx* ctx, const hadros_params* cams, int32_t n
         A.counters = pl->d_counters;
         A.attempt_budget = ctx->attempt_budget > 0 ? ctx->attempt_budget : static_cast<int64_t>(max_cap) * 51 + 1;
         A.fast_geodesic = pl->fast;
+        A.mev = any_mev(cams, n_cams) ? 1 : 0;
         if (want_defer(ctx->transfer_mode, pl->precision, max_bins)) {
             const int64_t slots = defer_slots(ctx->n_sm);
             cudaError_t e2 = cudaMalloc(&pl->d_rec, rec_bytes(slots, max_bins));
@@ -1379,14 +1505,7 @@ int32_t hadros_plan_launch(hadros_plan* pl, const hadros_image_out* dev_out, voi
     if (!dev_out) return fail(HADROS_E_ARG, "output struct is NULL");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     TraceArgs A = pl->A;
-    A.tau = dev_out->tau;
-    A.P_surv = dev_out->P_surv;
-    A.I_obs = dev_out->I_obs;
-    A.fate = dev_out->fate;
-    A.steps = dev_out->steps;
-    A.attempts = dev_out->attempts;
-    A.tau_E = dev_out->tau_E;
-    A.I_E = static_cast<double*>(dev_out->I_E);
+    set_outputs(A, *dev_out);
     cudaError_t e = cudaMemsetAsync(pl->d_counters, 0, 4 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail(HADROS_E_CUDA, std::string("plan counter reset: ") + cudaGetErrorString(e));
     if (pl->P == 0) return ok();

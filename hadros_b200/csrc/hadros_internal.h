@@ -9,6 +9,7 @@
 #include "../../include/hadros_b200.h"
 #include "hadros_physics.cuh"
 #include "hadros_physics_f32.cuh"
+#include "hadros_mev.cuh"
 
 namespace hadros {
 
@@ -36,6 +37,7 @@ struct DevCam {
     TorusF torus_f;                   // FP32 constants for the mixed transfer
     SourceF src_f;
     double k_nb;                      // sigma_scale / m_u (mixed transfer)
+    Mev mev;                          // MeV thermal channel (radiative_transfer.cpp:522-638)
     int32_t nx, ny, max_steps, n_bins;
     int32_t mono;
     int32_t bin_offset;               // first row in the bin tables
@@ -103,6 +105,12 @@ struct TraceArgs {
     int32_t* attempts;
     void* tau_E;        // float (mixed) or double (fp64)
     double* I_E;
+    double* tau_mev;    // MeV channel per pixel
+    double* P_surv_mev;
+    double* I_obs_mev;
+    double* r_nu;
+    double* leakage;
+    int32_t mev;        // some camera has mev_channel set: the kernel variant that computes it
     // scratch
     unsigned long long* counters;   // [0] work cursor, [1] steps, [2] attempts, [3] aborted
     int64_t attempt_budget;

@@ -260,6 +260,9 @@ int na_build_cam(const hadros_params& p, const SigmaHost& sig, DevCam& cam, DevB
         return HADROS_E_ARG;
     }
     cam.n_bins = nb;
+    bool have_ref = false;   // MeV result of the first valid bin (radiative_transfer.cpp:741-774)
+    for (int k = 0; k < nb; ++k) have_ref = have_ref || bins[k].valid != 0;
+    cam.mev = make_mev(p, cam.torus, have_ref);
     cam.bin_offset = 0;
     *n_bins = nb;
     return HADROS_OK;
@@ -349,6 +352,12 @@ extern "C" int32_t hadros_image_device_noalloc(const hadros_params* p, const had
     A.attempts = dev_out->attempts;
     A.tau_E = dev_out->tau_E;
     A.I_E = static_cast<double*>(dev_out->I_E);
+    A.tau_mev = dev_out->tau_mev;
+    A.P_surv_mev = dev_out->P_surv_mev;
+    A.I_obs_mev = dev_out->I_obs_mev;
+    A.r_nu = dev_out->r_nu;
+    A.leakage = dev_out->leakage;
+    A.mev = p->mev_channel ? 1 : 0;
     A.counters = reinterpret_cast<unsigned long long*>(base + kOffCounters);
     A.attempt_budget = static_cast<int64_t>(p->max_steps) * 51 + 1;
     A.fast_geodesic = 0;

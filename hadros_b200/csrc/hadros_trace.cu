@@ -254,6 +254,11 @@ int build_cam(const hadros_params& p, const SigmaHost& sig, DevCam& cam,
         err = "n_bins exceeds 256";
         return HADROS_E_ARG;
     }
+    // MeV channel: the spectral aggregate keeps the first valid bin's MeV
+    // result (radiative_transfer.cpp:741-774), none without a valid bin
+    bool have_ref = false;
+    for (const DevBin& b : bb) have_ref = have_ref || b.valid != 0;
+    cam.mev = make_mev(p, cam.torus, have_ref);
     cam.bin_offset = static_cast<int32_t>(bins.size());
     bins.insert(bins.end(), bb.begin(), bb.end());
     return HADROS_OK;

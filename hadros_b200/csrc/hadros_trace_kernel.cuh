@@ -486,6 +486,28 @@ __device__ __forceinline__ void finish_pixel(const TraceArgs& A, const DevCam* c
     if (A.attempts) A.attempts[orow] = static_cast<int32_t>(att_total > 2147483647LL ? 2147483647LL : att_total);
 }
 
+// The MeV channel's outputs of a finished pixel (kernels built with MEV).
+__device__ __forceinline__ void finish_mev(const TraceArgs& A, const DevCam* cam, const MevAcc& ma, long long local,
+                                           int step)
+{
+    const long long orow = cam->out_offset + local;
+    double t, P, I, rn, lk;
+    mev_finish(cam->mev, ma, step, &t, &P, &I, &rn, &lk);
+    if (A.tau_mev) A.tau_mev[orow] = t;
+    if (A.P_surv_mev) A.P_surv_mev[orow] = P;
+    if (A.I_obs_mev) A.I_obs_mev[orow] = I;
+    if (A.r_nu) A.r_nu[orow] = rn;
+    if (A.leakage) A.leakage[orow] = lk;
+}
+
+// One path point into the MeV sums (points inside r_+ + 1e-3 are skipped as
+// by the UHE transfer, radiative_transfer.cpp:501-505).
+__device__ __forceinline__ void mev_path_point(const DevCam* cam, MevAcc& ma, double r, double th, double dl, double z)
+{
+    if (!cam->mev.on || r < cam->rt_skip) return;
+    mev_point(cam->mev, ma, r, th, torus_rho(cam->torus, r, th), z, dl * cam->rg_cm);
+}
+
 // Zero this thread's per-bin accumulators.
 template <int MIXED>
 __device__ __forceinline__ void reset_bins(const BinAcc& acc, int B)
@@ -586,8 +608,9 @@ __device__ __noinline__ void deferred_transfer(PointRec* rec_buf, float* rec_sta
 }
 
 // DEFER (mixed only): the deferred transfer; a separate instantiation so the
-// in-loop kernel carries none of its code or registers.
-template <int MIXED, int FAST, int DEFER>
+// in-loop kernel carries none of its code or registers.  MEV: the MeV thermal
+// channel (FP64, once per point), likewise only in the kernels that need it.
+template <int MIXED, int FAST, int DEFER, int MEV>
 __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const TraceArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -645,6 +668,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
     K5 k1{};
     double s_base = 0.0, c_base = 1.0;   // sin/cos of theta at the step start
     int fate = HADROS_FATE_TRUNCATED;
+    MevAcc ma{};
 
     while (true) {
         while (phase == kNeedRay || phase == kStepStart) {
@@ -699,6 +723,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                 step = 0;
                 att_total = 0;
                 reset_bins<MIXED>(acc, B);
+                if (MEV) mev_reset(ma);
                 phase = kStepStart;
             }
 
@@ -720,6 +745,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                     continue;
                 }
                 finish_pixel<MIXED>(A, cam, bins, B, acc, row, step, fate, att_total);
+                if (MEV) finish_mev(A, cam, ma, row, step);
                 phase = kNeedRay;
                 continue;
             }
@@ -797,6 +823,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
             } else {
                 transfer_point<MIXED>(cam, bins, B, tb, acc, r, th, dl, z);
             }
+            if (MEV) mev_path_point(cam, ma, r, th, dl, z);
 
             // ---- k1 of the coming step_adaptive (shares sin/cos) ------------
             if (FAST) geo_rhs_fast(a, r, th, s, c, pr, pth, pt, pph, k1);
@@ -821,6 +848,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                 deferred_transfer(A.rec_buf, A.rec_state, A.bins, A.rec_bmax, tb, slot - (tid & 31), fill, B, cam);
                 if (phase == kWaitTransfer) {
                     finish_pixel<MIXED>(A, cam, bins, B, acc, row, step, fate, att_total);
+                    if (MEV) finish_mev(A, cam, ma, row, step);
                     phase = kNeedRay;
                 }
                 fill = 0;
@@ -917,8 +945,8 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
 // Transfer over cached paths (compute_kerr_image_from_cache,
 // apps/compute_kerr_image_from_cache.cpp:599-711): one thread per ray walks
 // its recorded points (r, theta, x, y, z, dl, redshift) through the same
-// transfer_point as the fused kernel.  Grid-stride over rays.
-template <int MIXED>
+// transfer_point (and MeV channel) as the fused kernel.  Grid-stride over rays.
+template <int MIXED, int MEV>
 __global__ void __launch_bounds__(kTPB) path_transfer_kernel(const TraceArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -955,13 +983,17 @@ __global__ void __launch_bounds__(kTPB) path_transfer_kernel(const TraceArgs A)
     for (long long ray = static_cast<long long>(blockIdx.x) * kTPB + tid; ray < A.total_items;
          ray += static_cast<long long>(gridDim.x) * kTPB) {
         reset_bins<MIXED>(acc, B);
+        MevAcc ma;
+        mev_reset(ma);
         const long long k0 = A.path_offsets[ray], k1 = A.path_offsets[ray + 1];
         for (long long kk = k0; kk < k1; ++kk) {
             const double* q = A.path_points + kk * 7;
             transfer_point<MIXED>(cam, bins, B, tb, acc, q[0], q[1], q[5], q[6]);
+            if (MEV) mev_path_point(cam, ma, q[0], q[1], q[5], q[6]);
         }
         const int fate = A.path_fates ? A.path_fates[ray] : HADROS_FATE_ESCAPED;
         finish_pixel<MIXED>(A, cam, bins, B, acc, ray, static_cast<int>(k1 - k0), fate, 0);
+        if (MEV) finish_mev(A, cam, ma, ray, static_cast<int>(k1 - k0));
     }
 }
 
@@ -971,7 +1003,9 @@ template <int FAST>
 int launch_paths(const TraceArgs& args, int precision, int n_sm, cudaStream_t st, std::string& err)
 {
     const size_t smem = smem_layout(precision, args.sig.n, args.max_bins).total;
-    auto kern = (precision == HADROS_PRECISION_MIXED) ? path_transfer_kernel<1> : path_transfer_kernel<0>;
+    const bool mixed = precision == HADROS_PRECISION_MIXED;
+    auto kern = args.mev ? (mixed ? path_transfer_kernel<1, 1> : path_transfer_kernel<0, 1>)
+                         : (mixed ? path_transfer_kernel<1, 0> : path_transfer_kernel<0, 0>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTPB, smem);
@@ -992,12 +1026,19 @@ int launch_paths(const TraceArgs& args, int precision, int n_sm, cudaStream_t st
     return HADROS_OK;
 }
 
-// The trace kernel instantiation for a precision and transfer placement.
+// The trace kernel instantiation for a precision, transfer placement and
+// MeV channel.
+template <int FAST, int MEV>
+auto trace_kernel_mev(const TraceArgs& args, int precision) -> void (*)(const TraceArgs)
+{
+    if (precision != HADROS_PRECISION_MIXED) return trace_kernel<0, FAST, 0, MEV>;
+    return args.rec_buf ? trace_kernel<1, FAST, 1, MEV> : trace_kernel<1, FAST, 0, MEV>;
+}
+
 template <int FAST>
 auto trace_kernel_for(const TraceArgs& args, int precision) -> void (*)(const TraceArgs)
 {
-    if (precision != HADROS_PRECISION_MIXED) return trace_kernel<0, FAST, 0>;
-    return args.rec_buf ? trace_kernel<1, FAST, 1> : trace_kernel<1, FAST, 0>;
+    return args.mev ? trace_kernel_mev<FAST, 1>(args, precision) : trace_kernel_mev<FAST, 0>(args, precision);
 }
 
 // Grid of a persistent launch: SMs x resident blocks (capped at

@@ -39,7 +39,7 @@
 extern "C" {
 #endif
 
-#define HADROS_ABI_VERSION 1
+#define HADROS_ABI_VERSION 2
 
 /* Status codes.  The reference reports errors by throwing std::runtime_error
  * (e.g. src/torus_profile.cpp:85-90, src/sigma_table.cpp:14-16) or by exiting
@@ -100,6 +100,45 @@ enum hadros_fate {
     HADROS_FATE_CAPTURED = 1,  /* r <= r_+ + 1e-3                          */
     HADROS_FATE_TRUNCATED = 2  /* step cap reached first ("neither")      */
 };
+
+/* MeV thermal neutrino channel: the second transfer that integrate_kerr_ray
+ * runs along the same path (src/radiative_transfer.cpp:522-638) with the
+ * microphysics of src/mev_neutrino_physics.cpp.  Enums in the order of
+ * include/mev_neutrino_physics.hpp:8-37. */
+enum hadros_mev_model { HADROS_MEV_TOY = 0, HADROS_MEV_PHYSICAL = 1 };
+enum hadros_mev_flavor { HADROS_MEV_NU_E = 0, HADROS_MEV_ANTI_NU_E = 1, HADROS_MEV_NU_X = 2 };
+enum hadros_mev_thermal {
+    HADROS_MEV_T_CONSTANT = 0,
+    HADROS_MEV_T_INNER_HOT_TORUS = 1,
+    HADROS_MEV_T_RADIAL_POWERLAW = 2,
+    HADROS_MEV_T_TORUS_PLUS_COOL_ENVELOPE = 3,
+    HADROS_MEV_T_COLLAPSAR_INNER_HOT = 4
+};
+enum hadros_mev_ye {
+    HADROS_MEV_YE_CONSTANT = 0,
+    HADROS_MEV_YE_NEUTRON_RICH_TORUS = 1,
+    HADROS_MEV_YE_FUNNEL_PROTON_RICH = 2,
+    HADROS_MEV_YE_TORUS_ENVELOPE_CONTRAST = 3,
+    HADROS_MEV_YE_COLLAPSAR_NEUTRON_RICH = 4
+};
+enum hadros_mev_spectral { HADROS_MEV_MONOCHROMATIC = 0, HADROS_MEV_FERMI_DIRAC_BAND = 1 };
+/* The include_* / use_* switches of MeVThermalParams
+ * (include/radiative_transfer.hpp:71-81) as bits of hadros_params.mev_flags. */
+enum hadros_mev_flag {
+    HADROS_MEV_URCA = 1 << 0,
+    HADROS_MEV_PAIR = 1 << 1,
+    HADROS_MEV_BREMS = 1 << 2,
+    HADROS_MEV_ABSORPTION = 1 << 3,
+    HADROS_MEV_SCATTERING = 1 << 4,
+    HADROS_MEV_DEGENERACY_CORRECTION = 1 << 5,
+    HADROS_MEV_ABS_N = 1 << 6,
+    HADROS_MEV_ABS_P = 1 << 7,
+    HADROS_MEV_SCAT_N = 1 << 8,
+    HADROS_MEV_SCAT_P = 1 << 9,
+    HADROS_MEV_SCAT_E = 1 << 10
+};
+/* every switch of the reference's defaults: all on but the degeneracy correction */
+#define HADROS_MEV_FLAGS_DEFAULT 0x7DF
 
 /* All parameters of one camera/image.  Fill with hadros_params_default()
  * and override fields.  Angles are radians except fov_deg, which KerrCamera
@@ -165,6 +204,34 @@ typedef struct hadros_params {
     double spec_ecut_GeV;
     double spec_e_min_GeV;
     double spec_e_max_GeV;
+
+    /* MeV thermal channel: MeVThermalParams (include/radiative_transfer.hpp:
+     * 64-101), defaults as there.  mev_channel = 0 skips the channel (no cost;
+     * the MeV outputs hold RTResult's defaults tau 0, P 1, I 0, r_nu -1,
+     * leakage 1); 1 computes it.  FP64 in both precisions. */
+    int32_t mev_channel;
+    int32_t mev_model;            /* enum hadros_mev_model                    */
+    int32_t mev_flavor;           /* enum hadros_mev_flavor                   */
+    int32_t mev_thermal_profile;  /* enum hadros_mev_thermal                  */
+    int32_t mev_ye_profile;       /* enum hadros_mev_ye                       */
+    int32_t mev_spectral_mode;    /* enum hadros_mev_spectral                 */
+    int32_t mev_n_bins;           /* Fermi-Dirac band bins                    */
+    uint32_t mev_flags;           /* enum hadros_mev_flag bits                */
+    double mev_Enu_obs_MeV;
+    double mev_norm;
+    double mev_sigma_abs0_cm2;
+    double mev_sigma_scat0_cm2;
+    double mev_neutrinosphere_tau;
+    double mev_T0_MeV;
+    double mev_T_floor_MeV;
+    double mev_T_power;
+    double mev_Ye_torus;
+    double mev_Ye_funnel;
+    double mev_Ye_envelope;
+    double mev_Ye_floor;
+    double mev_Ye_ceil;
+    double mev_E_min_MeV;
+    double mev_E_max_MeV;
 } hadros_params;
 
 /* Caller-owned outputs.  Any pointer may be NULL (that output is skipped).
@@ -184,6 +251,14 @@ typedef struct hadros_image_out {
     int32_t* attempts;  /* RKF45 attempts (>= steps)                       */
     void* tau_E;
     void* I_E;
+    /* MeV channel per pixel (RTResult, include/radiative_transfer.hpp:16-20):
+     * tau_mev, exp(-tau_mev), I_obs_mev, r of the first point whose
+     * tau_mev >= mev_neutrinosphere_tau (-1 if none) and leakage_factor. */
+    double* tau_mev;
+    double* P_surv_mev;
+    double* I_obs_mev;
+    double* r_nu;
+    double* leakage;
 } hadros_image_out;
 
 /* Run statistics of the last image/batch call on a context. */
@@ -223,6 +298,20 @@ int32_t hadros_parse_spectral(const char* name, int32_t* kind);
 const char* hadros_profile_name(int32_t kind);
 const char* hadros_source_name(int32_t kind);
 const char* hadros_spectral_name(int32_t kind);
+/* MeV channel names with the reference's aliases and error text
+ * (src/mev_neutrino_physics.cpp:37-238): parse_mev_model, parse_mev_flavor,
+ * parse_mev_thermal_profile, parse_mev_ye_profile, parse_mev_spectral_mode
+ * and their *_name inverses. */
+int32_t hadros_parse_mev_model(const char* name, int32_t* kind);
+int32_t hadros_parse_mev_flavor(const char* name, int32_t* kind);
+int32_t hadros_parse_mev_thermal(const char* name, int32_t* kind);
+int32_t hadros_parse_mev_ye(const char* name, int32_t* kind);
+int32_t hadros_parse_mev_spectral(const char* name, int32_t* kind);
+const char* hadros_mev_model_name(int32_t kind);
+const char* hadros_mev_flavor_name(int32_t kind);
+const char* hadros_mev_thermal_name(int32_t kind);
+const char* hadros_mev_ye_name(int32_t kind);
+const char* hadros_mev_spectral_name(int32_t kind);
 
 /* ---- sigma_CC(E) table (SigmaTable, src/sigma_table.cpp) ------------------ */
 
@@ -410,16 +499,26 @@ int32_t hadros_image_filename(const hadros_params* p, int32_t style, const char*
                               double mev_E_MeV, double mev_norm, const char* ext, char* buf,
                               int32_t buflen);
 /* 13-column text image with the reference's '#' metadata header
- * (apps/compute_kerr_image_from_cache.cpp:512-653); rows in j*nx+i order;
- * the MeV columns carry RTResult's defaults (the MeV channel is not
- * computed).  Arrays hold nx*ny entries. */
+ * (apps/compute_kerr_image_from_cache.cpp:512-653); rows in j*nx+i order.
+ * The MeV columns carry RTResult's defaults (tau 0, P 1, I 0, r_nu -1,
+ * leakage 1); hadros_write_dat_mev writes computed ones.  Arrays hold nx*ny
+ * entries. */
 int32_t hadros_write_dat(const char* path, const hadros_params* p, const char* dis_model,
                          double mev_E_MeV, double mev_norm, const double* tau,
                          const double* P_surv, const double* I_obs, const int8_t* fate);
-/* KIMG binary image (apps/compute_kerr_image_cuda.cu:279-332). */
+/* KIMG binary image (apps/compute_kerr_image_cuda.cu:279-332), MeV columns
+ * as hadros_write_dat. */
 int32_t hadros_write_kimg(const char* path, const hadros_params* p, double mev_E_MeV,
                           double mev_norm, const double* tau, const double* P_surv,
                           const double* I_obs, const int8_t* fate);
+/* The same files with the MeV columns of a host hadros_image_out (tau_mev,
+ * P_surv_mev, I_obs_mev, r_nu, leakage; a NULL array writes its default) and,
+ * in the text header, the MeV parameters of `p` as the CPU app lists them
+ * (apps/compute_kerr_image_from_cache.cpp:563-591) when p->mev_channel is
+ * set.  The MeV energy and norm of the file name/header are p's. */
+int32_t hadros_write_dat_mev(const char* path, const hadros_params* p, const char* dis_model,
+                             const hadros_image_out* host);
+int32_t hadros_write_kimg_mev(const char* path, const hadros_params* p, const hadros_image_out* host);
 
 /* KGEO geodesic cache files (apps/compute_kerr_geodesics.cpp:14-22, :95-138):
  * header <int32 magic 0x4B47454F, int32 version 1, int32 nx, int32 ny,

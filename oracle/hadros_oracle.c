@@ -21,9 +21,11 @@
  * claim is checked by tests against the reference itself, built from its own
  * sources by oracle/build_ref.sh, and against fixtures made from it.
  *
+ *   MeV thermal channel    src/radiative_transfer.cpp:522-638 with
+ *                          src/mev_neutrino_physics.cpp:240-770
  * Deliberate differences from the reference, none of which changes a result:
- *   - the MeV thermal channel (src/radiative_transfer.cpp:522-638) is not
- *     evaluated: it only feeds the MeV outputs, never tau/P_surv/I_obs;
+ *   - the MeV thermal channel is evaluated only when its outputs are asked
+ *     for: it never feeds tau/P_surv/I_obs;
  *   - the four off-centre inverse metrics of each RHS are evaluated once
  *     instead of once per (mu, nu) pair (same arguments, same values);
  *   - terms that are exactly zero (g^{01}, g^{02}, derivatives of zero
@@ -615,13 +617,246 @@ int hor_spectral_bins(const hadros_params* p, double sig_Emin, double sig_Emax,
     return n_bins;
 }
 
+/* ---------------- MeV thermal channel ------------------------------------
+ * mev_neutrino_physics.cpp with the MeVThermalParams of hadros_params
+ * (mev_* fields; switches as HADROS_MEV_* bits). */
+
+#define HOR_HBAR_C_MEV_CM 1.973269804e-11   /* mev_neutrino_physics.cpp:14 */
+#define HOR_M_E_MEV 0.510998950             /* :15 */
+#define HOR_SIGMA_SCAT_E0 3.4e-45           /* MeVPhysicsParams default (mev_neutrino_physics.hpp:61) */
+
+static int mev_flag(const hadros_params* p, unsigned bit) { return (p->mev_flags & bit) != 0u; }
+static double mev_clamp_ye(double Ye) { return sclamp(Ye, 0.0, 1.0); }          /* :17-20 */
+static double mev_safe_pow(double x, double e) { return pow(smax(x, 0.0), e); }   /* :22-25 */
+static double mev_density_shape(double rho, double rho0)                        /* :27-35 */
+{
+    return sclamp(rho / smax(rho0, 1.0e-300), 0.0, 1.0);
+}
+
+static double mev_temperature(const hadros_params* p, const hor_torus* t, double r, double th, double rho)
+{   /* mev_temperature_profile_MeV, :240-273 */
+    const double T0 = smax(p->mev_T0_MeV, 1.0e-12);
+    const double fl = smax(p->mev_T_floor_MeV, 1.0e-12);
+    const double shape = mev_density_shape(rho, t->rho0);
+    const double radial = pow(smax(r / smax(t->r0, 1.0e-300), 1.0e-300), -p->mev_T_power);
+    const double equatorial = exp(-pow((th - 0.5 * PI) / 0.45, 2.0));
+    const int outside_torus = r > t->r_max || r < t->r_min;
+    double T = T0;
+    switch (p->mev_thermal_profile) {
+    case HADROS_MEV_T_INNER_HOT_TORUS:
+        T = fl + T0 * pow(shape, smax(p->mev_T_power, 0.0));
+        break;
+    case HADROS_MEV_T_RADIAL_POWERLAW:
+        T = fl + T0 * radial * (0.35 + 0.65 * equatorial);
+        break;
+    case HADROS_MEV_T_TORUS_PLUS_COOL_ENVELOPE:
+        T = fl + T0 * pow(shape, smax(p->mev_T_power, 0.0));
+        if (outside_torus || shape < 1.0e-3) T = fl + 0.15 * T0 * radial;
+        break;
+    case HADROS_MEV_T_COLLAPSAR_INNER_HOT: {
+        const double inner_hot = exp(-pow((r - t->r_min) / smax(1.15 * t->r0, 1.0e-6), 2.0));
+        const double radial_cooling = pow(1.0 + smax(r - t->r_min, 0.0) / smax(t->r0, 1.0e-6), -0.75);
+        T = fl + T0 * (0.30 + 0.70 * pow(shape, 0.18)) * (0.45 + 0.55 * equatorial) *
+                 (0.55 + 0.45 * inner_hot) * radial_cooling;
+        break;
+    }
+    default:
+        T = T0;
+    }
+    return smax(T, fl);
+}
+
+static double mev_ye(const hadros_params* p, const hor_torus* t, double r, double th, double rho)
+{   /* mev_ye_profile, :275-318 */
+    const double shape = mev_density_shape(rho, t->rho0);
+    const double polar = exp(-pow(th / 0.35, 2.0)) + exp(-pow((PI - th) / 0.35, 2.0));
+    const int envelope_like = r > t->r0 && (r > t->r_max || shape < 1.0e-2);
+    double Ye = p->mev_Ye_torus;
+    switch (p->mev_ye_profile) {
+    case HADROS_MEV_YE_NEUTRON_RICH_TORUS:
+        Ye = p->mev_Ye_torus + 0.05 * exp(-pow((r - t->r0) / 4.0, 2.0));
+        break;
+    case HADROS_MEV_YE_FUNNEL_PROTON_RICH:
+        Ye = p->mev_Ye_torus * (1.0 - sclamp(polar, 0.0, 1.0)) + p->mev_Ye_funnel * sclamp(polar, 0.0, 1.0);
+        break;
+    case HADROS_MEV_YE_TORUS_ENVELOPE_CONTRAST:
+        Ye = envelope_like ? p->mev_Ye_envelope : p->mev_Ye_torus;
+        if (r < t->r_min && shape < 1.0e-2) Ye = p->mev_Ye_funnel;
+        break;
+    case HADROS_MEV_YE_COLLAPSAR_NEUTRON_RICH: {
+        const double polar_weight = sclamp(polar, 0.0, 1.0);
+        const double dense_weight = pow(shape, 0.25);
+        const double radial_neutronization = exp(-pow((r - t->r0) / smax(1.2 * t->r0, 1.0e-6), 2.0));
+        const double torus_ye = p->mev_Ye_torus - 0.05 * dense_weight * radial_neutronization;
+        Ye = torus_ye * (1.0 - polar_weight) + p->mev_Ye_funnel * polar_weight;
+        break;
+    }
+    default:
+        Ye = p->mev_Ye_torus;
+    }
+    return sclamp(Ye, smax(p->mev_Ye_floor, 1.0e-6), smin(p->mev_Ye_ceil, 1.0 - 1.0e-6));
+}
+
+static double mev_thermal_shape(double E, double T)
+{   /* mev_thermal_spectral_shape, :320-340 */
+    if (E <= 0.0 || T <= 0.0) return 0.0;
+    const double x = E / T;
+    if (x > 120.0) return 0.0;
+    const double T3 = smax(T * T * T, 1.0e-300);
+    return E * E / (exp(x) + 1.0) / T3;
+}
+
+static double mev_fd_weight(double E, double T)
+{   /* mev_fermi_dirac_weight, :342-354 */
+    if (E <= 0.0 || T <= 0.0) return 0.0;
+    const double x = E / T;
+    if (x > 120.0) return 0.0;
+    return E * E / (exp(x) + 1.0);
+}
+
+static double mev_electron_density(double rho, double Ye)
+{   /* electron_number_density_cm3, :356-366 */
+    if (rho <= 0.0) return 0.0;
+    return rho * mev_clamp_ye(Ye) / HOR_M_U_G;
+}
+
+static double mev_degeneracy_correction(double rho, double Ye, double T, int flavor)
+{   /* mev_urca_degeneracy_correction with electron_degeneracy_eta and the
+     * zero-temperature chemical potential, :368-432 */
+    if (flavor == HADROS_MEV_NU_X) return 1.0;
+    double eta = 0.0;
+    if (T > 0.0) {
+        const double ne = mev_electron_density(rho, Ye);
+        const double pF = ne <= 0.0 ? 0.0 : HOR_HBAR_C_MEV_CM * cbrt(3.0 * PI * PI * ne);
+        eta = sqrt(pF * pF + HOR_M_E_MEV * HOR_M_E_MEV) / T;
+    }
+    if (!isfinite(eta)) return 1.0;
+    const double shift = 0.25 * tanh((eta - 1.0) / 4.0);
+    const double factor = flavor == HADROS_MEV_NU_E ? (1.0 + shift) : (1.0 - shift);
+    return sclamp(factor, 0.5, 1.5);
+}
+
+static double mev_emissivity(const hadros_params* p, double rho, double T, double Ye, double E)
+{   /* mev_total_emissivity with the URCA, pair and bremsstrahlung terms, :434-588 */
+    const int flavor = p->mev_flavor;
+    if (p->mev_model == HADROS_MEV_TOY) {
+        if (rho <= 0.0 || T <= 0.0 || E <= 0.0) return 0.0;
+        const double nb = rho / HOR_M_U_G;
+        const double neutron_fraction = sclamp(1.0 - Ye, 0.0, 1.0);
+        const double proton_fraction = sclamp(Ye, 0.0, 1.0);
+        const double charged_current_weight = neutron_fraction + 0.5 * proton_fraction;
+        const double thermal_spectrum = E * E / (exp(smin(E / T, 120.0)) + 1.0);
+        const double capture_like = nb * charged_current_weight * pow(T, 6.0);
+        const double pair_like = 0.05 * nb * pow(T, 9.0);
+        return p->mev_norm * (capture_like + pair_like) * thermal_spectrum;
+    }
+    double total = 0.0;
+    if (mev_flag(p, HADROS_MEV_URCA)) {
+        double urca = 0.0;
+        if (!(rho <= 0.0 || T <= 0.0 || E <= 0.0) && flavor != HADROS_MEV_NU_X) {
+            const double ye = mev_clamp_ye(Ye);
+            const double flavor_factor = flavor == HADROS_MEV_NU_E ? ye : (1.0 - ye);
+            urca = 1.0e30 * mev_safe_pow(rho / 1.0e10, 1.0) * mev_safe_pow(T / 10.0, 6.0) * flavor_factor *
+                   mev_thermal_shape(E, T);
+        }
+        if (mev_flag(p, HADROS_MEV_DEGENERACY_CORRECTION)) urca *= mev_degeneracy_correction(rho, Ye, T, flavor);
+        total += urca;
+    }
+    if (mev_flag(p, HADROS_MEV_PAIR) && !(T <= 0.0 || E <= 0.0)) {
+        const double flavor_factor = flavor == HADROS_MEV_NU_X ? 1.0 : 0.7;
+        total += 3.0e28 * mev_safe_pow(T / 10.0, 9.0) * flavor_factor * mev_thermal_shape(E, T);
+    }
+    if (mev_flag(p, HADROS_MEV_BREMS) && !(rho <= 0.0 || T <= 0.0 || E <= 0.0)) {
+        const double flavor_factor = flavor == HADROS_MEV_NU_X ? 1.0 : 0.8;
+        total += 1.0e27 * mev_safe_pow(rho / 1.0e10, 2.0) * mev_safe_pow(T / 10.0, 5.0) * flavor_factor *
+                 mev_thermal_shape(E, T);
+    }
+    return p->mev_norm * total;
+}
+
+static double mev_opacity(const hadros_params* p, double rho, double Ye, double E)
+{   /* mev_total_opacity_cm_inv = absorption + scattering, :590-770 */
+    const int absorb = mev_flag(p, HADROS_MEV_ABSORPTION), scatter = mev_flag(p, HADROS_MEV_SCATTERING);
+    const double nb = rho / HOR_M_U_G;
+    double ka = 0.0, ks = 0.0;
+    if (p->mev_model == HADROS_MEV_TOY) {
+        if (absorb && !(rho <= 0.0 || E <= 0.0)) {
+            const double target_fraction = sclamp(1.0 - Ye, 0.0, 1.0) + 0.25 * sclamp(Ye, 0.0, 1.0);
+            ka = nb * p->mev_sigma_abs0_cm2 * E * E * target_fraction;
+        }
+        if (scatter && !(rho <= 0.0 || E <= 0.0)) {
+            const double composition_factor = 1.0 + 0.5 * sclamp(Ye, 0.0, 1.0);
+            ks = nb * p->mev_sigma_scat0_cm2 * E * E * composition_factor;
+        }
+        return ka + ks;
+    }
+    const int dense = !(rho <= 0.0 || E <= 0.0);
+    double abs_n = 0.0, abs_p = 0.0, scat_n = 0.0, scat_p = 0.0, scat_e = 0.0;
+    if (dense && absorb && mev_flag(p, HADROS_MEV_ABS_N) && p->mev_flavor == HADROS_MEV_NU_E)
+        abs_n = nb * (1.0 - mev_clamp_ye(Ye)) * p->mev_sigma_abs0_cm2 * E * E;
+    if (dense && absorb && mev_flag(p, HADROS_MEV_ABS_P) && p->mev_flavor == HADROS_MEV_ANTI_NU_E)
+        abs_p = nb * mev_clamp_ye(Ye) * p->mev_sigma_abs0_cm2 * E * E;
+    if (dense && scatter && mev_flag(p, HADROS_MEV_SCAT_N))
+        scat_n = nb * (1.0 - mev_clamp_ye(Ye)) * p->mev_sigma_scat0_cm2 * E * E;
+    if (dense && scatter && mev_flag(p, HADROS_MEV_SCAT_P))
+        scat_p = nb * mev_clamp_ye(Ye) * 0.5 * p->mev_sigma_scat0_cm2 * E * E;
+    if (dense && scatter && mev_flag(p, HADROS_MEV_SCAT_E))
+        scat_e = mev_electron_density(rho, Ye) * HOR_SIGMA_SCAT_E0 * E * E;
+    return (abs_n + abs_p) + (scat_n + scat_p + scat_e);
+}
+
+/* MeV sums of one ray: tau, I, r_nu, leakage sum and weight. */
+typedef struct { double tau, I, r_nu, leak_sum, leak_weight; } hor_mev_acc;
+
+static void mev_point(const hadros_params* p, const hor_torus* t, hor_mev_acc* m, double r, double th,
+                      double rho, double g, double dl_cm)
+{   /* integrate_kerr_ray, radiative_transfer.cpp:507-607 */
+    const double T = mev_temperature(p, t, r, th, rho);
+    const double Ye = mev_ye(p, t, r, th, rho);
+    double kappa = 0.0, j = 0.0;
+    if (p->mev_spectral_mode == HADROS_MEV_FERMI_DIRAC_BAND) {
+        const int n_bins = p->mev_n_bins > 1 ? p->mev_n_bins : 1;
+        const double e_min = smax(p->mev_E_min_MeV, 1.0e-6);
+        const double e_max = smax(p->mev_E_max_MeV, e_min);
+        const double dE = (e_max - e_min) / (double)n_bins;
+        double weight_sum = 0.0, kappa_weighted = 0.0;
+        for (int ib = 0; ib < n_bins; ++ib) {
+            const double E_mid = e_min + ((double)ib + 0.5) * dE;
+            const double E_local = E_mid / smax(g, 1.0e-300);
+            const double w = mev_fd_weight(E_local, T) * dE;
+            if (w <= 0.0 || !isfinite(w)) continue;
+            const double local_kappa = mev_opacity(p, rho, Ye, E_local);
+            j += mev_emissivity(p, rho, T, Ye, E_local) * dE;
+            kappa_weighted += w * local_kappa;
+            weight_sum += w;
+        }
+        kappa = weight_sum > 0.0 ? kappa_weighted / weight_sum : 0.0;
+    } else {
+        const double E_local = p->mev_Enu_obs_MeV / smax(g, 1.0e-300);
+        kappa = mev_opacity(p, rho, Ye, E_local);
+        j = mev_emissivity(p, rho, T, Ye, E_local);
+    }
+    const double dtau = kappa * dl_cm;
+    if (kappa > 0.0 && dtau > 1.0e-12) {
+        const double attenuation = exp(-smin(dtau, 700.0));
+        m->I = m->I * attenuation + pow(g, 3.0) * (j / kappa) * (1.0 - attenuation);
+    } else {
+        m->I += pow(g, 3.0) * j * dl_cm;
+    }
+    m->leak_sum += j * dl_cm;
+    m->leak_weight += j * dl_cm;
+    m->tau += dtau;
+    if (m->r_nu < 0.0 && m->tau >= p->mev_neutrinosphere_tau) m->r_nu = r;
+}
+
 /* ---------------- one pixel, all bins ------------------------------------ */
 
 
 int hor_trace_pixel(const hor_cam* cam, int i, int j,
                     double* tau_b, double* I_b, int32_t* steps_out, int32_t* attempts_out,
-                    hor_point_cb cb, void* cb_user)
+                    double* mev5, hor_point_cb cb, void* cb_user)
 {
+    hor_mev_acc mev = {0.0, 0.0, -1.0, 0.0, 0.0};
     const hadros_params* p = cam->p;
     const double a = p->a_spin;
     hor_state y, y_prev;
@@ -651,6 +886,7 @@ int hor_trace_pixel(const hor_cam* cam, int i, int j,
             const double g = 1.0 / smax(redshift, 1.0e-300);
             const double dl_cm = dl_rg * cam->rg_cm;
             const double rho = hor_rho(&cam->torus, pr_r, pr_th);
+            if (mev5) mev_point(p, &cam->torus, &mev, pr_r, pr_th, rho, g, dl_cm);
             const double C = emissivity_factor(p, &cam->torus, cam->rho_norm, pr_r, pr_th, rho);
             const double g3 = pow(g, 3.0);
             for (int b = 0; b < B; ++b) {
@@ -671,6 +907,13 @@ int hor_trace_pixel(const hor_cam* cam, int i, int j,
     }
     *steps_out = step;
     *attempts_out = (int32_t)(attempts > 2147483647L ? 2147483647L : attempts);
+    if (mev5) {   /* radiative_transfer.cpp:673-679 */
+        mev5[0] = mev.tau;
+        mev5[1] = exp(-mev.tau);
+        mev5[2] = mev.I;
+        mev5[3] = mev.r_nu;
+        mev5[4] = mev.leak_weight > 0.0 ? mev.leak_sum / mev.leak_weight : 1.0;
+    }
     return fate;
 }
 
@@ -702,8 +945,11 @@ int hor_image(const hadros_params* p, const double* sigE, const double* sigS_cm2
               const int32_t* pixel_ids, int32_t n_pixels,
               double* tau, double* P_surv, double* I_obs, int8_t* fate,
               int32_t* steps, int32_t* attempts, double* tau_E, double* I_E,
+              double* tau_mev, double* P_surv_mev, double* I_obs_mev, double* r_nu, double* leakage,
               int n_threads)
 {
+    double* const mev_out[5] = {tau_mev, P_surv_mev, I_obs_mev, r_nu, leakage};
+    const int want_mev = tau_mev || P_surv_mev || I_obs_mev || r_nu || leakage;
     double E_mid[HOR_MAX_BINS], dE[HOR_MAX_BINS], w[HOR_MAX_BINS];
     int8_t valid[HOR_MAX_BINS];
     if (p->n_bins > HOR_MAX_BINS) return -1;
@@ -723,8 +969,18 @@ int hor_image(const hadros_params* p, const double* sigE, const double* sigS_cm2
         const long pid = pixel_ids ? (long)pixel_ids[k] : k;
         const int i = (int)(pid % p->nx), j = (int)(pid / p->nx);
         double tb[HOR_MAX_BINS], ib[HOR_MAX_BINS];
+        double m5[5] = {0.0, 1.0, 0.0, -1.0, 1.0};   /* RTResult defaults */
         int32_t st = 0, at = 0;
-        const int f = hor_trace_pixel(&cam, i, j, tb, ib, &st, &at, NULL, NULL);
+        const int f = hor_trace_pixel(&cam, i, j, tb, ib, &st, &at, want_mev ? m5 : NULL, NULL, NULL);
+        /* the spectral aggregate keeps the first valid bin's MeV fields
+         * (radiative_transfer.cpp:741-774); an empty ray keeps the defaults */
+        int have_ref = mono;
+        for (int b = 0; b < B && !have_ref; ++b) have_ref = valid[b];
+        if (want_mev && (st == 0 || !have_ref)) {
+            m5[0] = 0.0; m5[1] = 1.0; m5[2] = 0.0; m5[3] = -1.0; m5[4] = 1.0;
+        }
+        for (int c = 0; c < 5; ++c)
+            if (mev_out[c]) mev_out[c][k] = m5[c];
         double t_out = 0.0, p_out = 1.0, i_out = 0.0;
         if (st > 0) {   /* compute_kerr_image_from_cache.cpp:617-633: empty rays keep defaults */
             if (mono) {
@@ -815,7 +1071,7 @@ int hor_trace_points(const hadros_params* p, const double* sigE, const double* s
     hor_cam cam;
     hor_cam_init(&cam, &q, sigE, sigS_cm2, sig_n, E_mid, 1);
     hor_pt_sink sink = {out_points5, max_points, 0};
-    *fate = hor_trace_pixel(&cam, i, j, tb, ib, &st, &at, hor_pt_collect, &sink);
+    *fate = hor_trace_pixel(&cam, i, j, tb, ib, &st, &at, NULL, hor_pt_collect, &sink);
     *n_points = st;
     return sink.n;
 }

@@ -71,9 +71,10 @@ int hor_spectral_bins(const hadros_params* p, double sig_Emin, double sig_Emax,
 
 int hor_cam_init(hor_cam* cam, const hadros_params* p, const double* sigE,
                  const double* sigS_cm2, int sig_n, const double* E_mid, int n_bins);
-/* Trace one pixel; fills tau_b/I_b[n_bins]; returns enum hadros_fate. */
+/* Trace one pixel; fills tau_b/I_b[n_bins] and, when mev5 is not NULL, the
+ * MeV channel's tau, P, I, r_nu, leakage; returns enum hadros_fate. */
 int hor_trace_pixel(const hor_cam* cam, int i, int j, double* tau_b, double* I_b,
-                    int32_t* steps_out, int32_t* attempts_out,
+                    int32_t* steps_out, int32_t* attempts_out, double* mev5,
                     hor_point_cb cb, void* cb_user);
 
 /* Whole image (pixel_ids == NULL) or a pixel list, OpenMP over pixels.
@@ -82,7 +83,8 @@ int hor_image(const hadros_params* p, const double* sigE, const double* sigS_cm2
               const int32_t* pixel_ids, int32_t n_pixels,
               double* tau, double* P_surv, double* I_obs, int8_t* fate,
               int32_t* steps, int32_t* attempts, double* tau_E, double* I_E,
-              int n_threads);
+              double* tau_mev, double* P_surv_mev, double* I_obs_mev, double* r_nu,
+              double* leakage, int n_threads);
 
 /* Helpers for tests (ctypes-friendly, no structs by value). */
 void hor_inverse_metric5(double a, double r, double th, double* out5);

@@ -40,7 +40,7 @@ def oracle_lib() -> C.CDLL:
         L = C.CDLL(str(ORACLE_SO))
         vp, i32 = C.c_void_p, C.c_int32
         L.hor_image.restype = C.c_int
-        L.hor_image.argtypes = [vp, vp, vp, C.c_int, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int]
+        L.hor_image.argtypes = [vp, vp, vp, C.c_int, vp, i32] + [vp] * 13 + [C.c_int]
         L.hor_inverse_metric5.argtypes = [C.c_double, C.c_double, C.c_double, vp]
         L.hor_metric5.argtypes = [C.c_double, C.c_double, C.c_double, vp]
         L.hor_lapse.restype = C.c_double
@@ -71,7 +71,7 @@ def ref_lib() -> C.CDLL:
         L = C.CDLL(str(REF_SO))
         vp, i32 = C.c_void_p, C.c_int32
         L.ref_image.restype = C.c_int
-        L.ref_image.argtypes = [vp, C.c_char_p, vp, i32, vp, vp, vp, vp, vp, vp, vp, C.c_int]
+        L.ref_image.argtypes = [vp, C.c_char_p, vp, i32] + [vp] * 12 + [C.c_int]
         _REF = L
     return _REF
 
@@ -80,41 +80,53 @@ def _n_bins(p) -> int:
     return 1 if p.spectral_kind == 0 else max(int(p.n_bins), 1)
 
 
-def _alloc(P: int, B: int) -> dict:
-    return {"tau": np.zeros(P), "P_surv": np.zeros(P), "I_obs": np.zeros(P),
-            "fate": np.zeros(P, np.int8), "steps": np.zeros(P, np.int32),
-            "attempts": np.zeros(P, np.int32), "tau_E": np.zeros((P, B)), "I_E": np.zeros((P, B))}
+MEV_KEYS = ("tau_mev", "P_surv_mev", "I_obs_mev", "r_nu", "leakage")
 
 
-def oracle_image(p, sig_E, sig_cm2, pixel_ids=None, threads: int = 0) -> dict:
-    """The C restatement over a whole image or a pixel list (OpenMP)."""
+def _alloc(P: int, B: int, mev: bool = False) -> dict:
+    out = {"tau": np.zeros(P), "P_surv": np.zeros(P), "I_obs": np.zeros(P),
+           "fate": np.zeros(P, np.int8), "steps": np.zeros(P, np.int32),
+           "attempts": np.zeros(P, np.int32), "tau_E": np.zeros((P, B)), "I_E": np.zeros((P, B))}
+    if mev:
+        out.update({k: np.zeros(P) for k in MEV_KEYS})
+    return out
+
+
+def _mev_ptrs(out: dict) -> list:
+    return [out[k].ctypes.data if k in out else None for k in MEV_KEYS]
+
+
+def oracle_image(p, sig_E, sig_cm2, pixel_ids=None, threads: int = 0, mev: bool = False) -> dict:
+    """The C restatement over a whole image or a pixel list (OpenMP); with
+    mev=True also the MeV channel's five outputs."""
     L = oracle_lib()
     E = np.ascontiguousarray(sig_E, dtype=np.float64)
     S = np.ascontiguousarray(sig_cm2, dtype=np.float64)
     ids = None if pixel_ids is None else np.ascontiguousarray(pixel_ids, dtype=np.int32)
     P = int(p.nx) * int(p.ny) if ids is None else int(ids.size)
     B = _n_bins(p)
-    out = _alloc(P, B)
+    out = _alloc(P, B, mev)
     rc = L.hor_image(C.addressof(p), E.ctypes.data, S.ctypes.data, int(E.size),
                      None if ids is None else ids.ctypes.data, 0 if ids is None else int(ids.size),
                      *(out[k].ctypes.data for k in ("tau", "P_surv", "I_obs", "fate", "steps",
                                                      "attempts", "tau_E", "I_E")),
-                     int(threads))
+                     *_mev_ptrs(out), int(threads))
     if rc < 0:
         raise RuntimeError(f"oracle hor_image failed ({rc})")
     return out
 
 
 def ref_image(p, sig_E, sig_gev2, sig_cm2, pixel_ids=None, threads: int = 0,
-              per_bin: bool = True) -> dict:
+              per_bin: bool = True, mev: bool = False) -> dict:
     """The reference's own code (KerrCamera::trace_pixel + integrate_kerr_ray_spectral).
-    per_bin=False skips the extra per-bin integrate_kerr_ray calls (timing runs)."""
+    per_bin=False skips the extra per-bin integrate_kerr_ray calls (timing runs);
+    mev=True returns the MeV channel's five outputs too."""
     from hadros_b200.workloads import write_sigma_file
     L = ref_lib()
     ids = None if pixel_ids is None else np.ascontiguousarray(pixel_ids, dtype=np.int32)
     P = int(p.nx) * int(p.ny) if ids is None else int(ids.size)
     B = _n_bins(p)
-    out = _alloc(P, B)
+    out = _alloc(P, B, mev)
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "sigma.dat")
         write_sigma_file(path, sig_E, sig_gev2, sig_cm2)
@@ -123,7 +135,7 @@ def ref_image(p, sig_E, sig_gev2, sig_cm2, pixel_ids=None, threads: int = 0,
                          *(out[k].ctypes.data for k in ("tau", "P_surv", "I_obs", "fate", "steps")),
                          out["tau_E"].ctypes.data if per_bin else None,
                          out["I_E"].ctypes.data if per_bin else None,
-                         int(threads))
+                         *_mev_ptrs(out), int(threads))
     if rc < 0:
         raise RuntimeError(f"reference ref_image failed ({rc})")
     del out["attempts"]

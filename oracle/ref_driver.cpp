@@ -44,7 +44,8 @@ const char* profile_name(int k)
 extern "C" int ref_image(const hadros_params* p, const char* sigma_path,
                          const int32_t* pixel_ids, int32_t n_pixels, double* tau,
                          double* P_surv, double* I_obs, int8_t* fate, int32_t* steps,
-                         double* tau_E, double* I_E, int n_threads)
+                         double* tau_E, double* I_E, double* tau_mev, double* P_surv_mev,
+                         double* I_obs_mev, double* r_nu, double* leakage, int n_threads)
 {
     try {
         if (p->max_steps > 200000 || p->tolerance != 1.0e-6) return -2;
@@ -80,7 +81,50 @@ extern "C" int ref_image(const hadros_params* p, const char* sigma_path,
         spectral.e_min_GeV = p->spec_e_min_GeV;
         spectral.e_max_GeV = p->spec_e_max_GeV;
         spectral.n_bins = p->n_bins;
-        MeVThermalParams mev;   // shipped defaults; feeds only the MeV columns
+        // MeV channel: the shipped defaults, or hadros_params' mev_* fields
+        // when mev_channel is set (the argv 14-15 and 45-71 mapping of
+        // apps/compute_kerr_image_from_cache.cpp:97-304)
+        MeVThermalParams mev;
+        if (p->mev_channel) {
+            const uint32_t fl = p->mev_flags;
+            mev.Enu_obs_MeV = p->mev_Enu_obs_MeV;
+            mev.norm = p->mev_norm;
+            mev.sigma_abs0_cm2 = p->mev_sigma_abs0_cm2;
+            mev.sigma_scat0_cm2 = p->mev_sigma_scat0_cm2;
+            mev.neutrinosphere_tau = p->mev_neutrinosphere_tau;
+            mev.model = static_cast<mev_neutrino::MeVModel>(p->mev_model);
+            mev.model_name = mev_neutrino::mev_model_name(mev.model);
+            mev.flavor = static_cast<mev_neutrino::MeVFlavor>(p->mev_flavor);
+            mev.flavor_name = mev_neutrino::mev_flavor_name(mev.flavor);
+            mev.include_urca = (fl & HADROS_MEV_URCA) != 0;
+            mev.include_pair = (fl & HADROS_MEV_PAIR) != 0;
+            mev.include_brems = (fl & HADROS_MEV_BREMS) != 0;
+            mev.include_absorption = (fl & HADROS_MEV_ABSORPTION) != 0;
+            mev.include_scattering = (fl & HADROS_MEV_SCATTERING) != 0;
+            mev.use_degeneracy_correction = (fl & HADROS_MEV_DEGENERACY_CORRECTION) != 0;
+            mev.include_abs_n = (fl & HADROS_MEV_ABS_N) != 0;
+            mev.include_abs_p = (fl & HADROS_MEV_ABS_P) != 0;
+            mev.include_scat_n = (fl & HADROS_MEV_SCAT_N) != 0;
+            mev.include_scat_p = (fl & HADROS_MEV_SCAT_P) != 0;
+            mev.include_scat_e = (fl & HADROS_MEV_SCAT_E) != 0;
+            mev.thermal_profile = static_cast<mev_neutrino::MeVThermalProfile>(p->mev_thermal_profile);
+            mev.thermal_profile_name = mev_neutrino::mev_thermal_profile_name(mev.thermal_profile);
+            mev.ye_profile = static_cast<mev_neutrino::MeVYeProfile>(p->mev_ye_profile);
+            mev.ye_profile_name = mev_neutrino::mev_ye_profile_name(mev.ye_profile);
+            mev.spectral_mode = static_cast<mev_neutrino::MeVSpectralMode>(p->mev_spectral_mode);
+            mev.spectral_mode_name = mev_neutrino::mev_spectral_mode_name(mev.spectral_mode);
+            mev.T0_MeV = p->mev_T0_MeV;
+            mev.T_floor_MeV = p->mev_T_floor_MeV;
+            mev.T_power = p->mev_T_power;
+            mev.Ye_torus = p->mev_Ye_torus;
+            mev.Ye_funnel = p->mev_Ye_funnel;
+            mev.Ye_envelope = p->mev_Ye_envelope;
+            mev.Ye_floor = p->mev_Ye_floor;
+            mev.Ye_ceil = p->mev_Ye_ceil;
+            mev.E_min_MeV = p->mev_E_min_MeV;
+            mev.E_max_MeV = p->mev_E_max_MeV;
+            mev.n_bins = p->mev_n_bins;
+        }
 
         // Per-bin energies exactly as integrate_kerr_ray_spectral forms them.
         std::vector<double> E_mid;
@@ -134,6 +178,11 @@ extern "C" int ref_image(const hadros_params* p, const char* sigma_path,
                 if (I_obs) I_obs[k] = rt.I_obs;
                 if (fate) fate[k] = static_cast<int8_t>(f);
                 if (steps) steps[k] = static_cast<int32_t>(ray.points.size());
+                if (tau_mev) tau_mev[k] = rt.tau_mev;
+                if (P_surv_mev) P_surv_mev[k] = rt.P_surv_mev;
+                if (I_obs_mev) I_obs_mev[k] = rt.I_obs_mev;
+                if (r_nu) r_nu[k] = rt.r_neutrinosphere_rg;
+                if (leakage) leakage[k] = rt.leakage_factor;
                 if (tau_E || I_E) {
                     for (int b = 0; b < B; ++b) {
                         RTResult rb;

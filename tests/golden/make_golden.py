@@ -6,7 +6,7 @@ sources by oracle/build_ref.sh into oracle/_ref/libhadros_ref.so) and stores
 its per-pixel outputs together with the parameters.  Run it where the
 reference sources are available:
 
-    oracle/build_ref.sh && python tests/golden/make_golden.py
+    oracle/build_ref.sh && python tests/golden/make_golden.py [name-prefix]
 
 The fixtures pin the CPU oracle (tests/test_oracle.py) and are what the GPU
 parity tests compare against on machines without the reference.
@@ -62,6 +62,28 @@ def cases() -> dict[str, dict]:
     c["edge_equatorial_wide"] = W.mixed_512(nx=5, ny=5, precision="fp64", theta_obs_deg=89.0,
                                             fov_deg=60.0, h=0.05, a_spin=0.7)
     c["edge_polar"] = W.mixed_512(nx=3, ny=3, precision="fp64", theta_obs_deg=2.0, h=0.05)
+    # MeV thermal channel (mev_* fixtures also store its five outputs)
+    col = dict(nx=5, ny=4, h=0.05, a_spin=0.95, theta_obs_deg=70.0, r_obs_rg=60.0, r_max_rg=120.0,
+               fov_deg=25.0, M_bh_msun=3.0, rho0_gcm3=1.0e11, profile="collapsar_ndaf_like", r0_rg=12.0,
+               sigma_r_rg=8.0, H_over_R=0.45, torus_r_min_rg=3.0, torus_r_max_rg=80.0,
+               rho_floor_gcm3=1.0e-3, source="density_weighted", precision="fp64", mev_channel=1)
+    c["mev_physical_collapsar"] = dict(col)
+    for th, ye in zip(("constant", "inner_hot_torus", "radial_powerlaw", "torus_plus_cool_envelope",
+                       "collapsar_inner_hot"),
+                      ("collapsar_neutron_rich", "constant", "neutron_rich_torus", "funnel_proton_rich",
+                       "torus_envelope_contrast")):
+        c[f"mev_T_{th}"] = dict(col, nx=4, ny=4, mev_thermal=th, mev_ye=ye)
+    c["mev_nu_e_degeneracy"] = dict(col, nx=4, ny=3, mev_flavor="nu_e", mev_degeneracy_correction=True)
+    c["mev_nu_x"] = dict(col, nx=4, ny=3, mev_flavor="nu_x", mev_Enu_obs_MeV=25.0)
+    c["mev_toy"] = dict(col, nx=4, ny=3, mev_model="toy", mev_norm=1.0e-40)
+    c["mev_fd_band_spectral"] = dict(col, nx=4, ny=3, mev_spectral="fermi_dirac_band", mev_n_bins=5,
+                                     spectral="powerlaw_cutoff", n_bins=4)
+    c["mev_empty_band"] = dict(col, nx=3, ny=3, spectral="powerlaw", spec_e_min_GeV=1.0e13,
+                               spec_e_max_GeV=1.0e14)
+    c["mev_switches_off"] = dict(col, nx=4, ny=3, mev_pair=False, mev_scat_e=False, mev_abs_p=False,
+                                 mev_neutrinosphere_tau=5.0)
+    c["mev_gaussian_thin"] = W.mixed_512(nx=4, ny=4, precision="fp64", h=0.05, mev_channel=1,
+                                         rho0_gcm3=1.0e8, mev_thermal="radial_powerlaw")
     return c
 
 
@@ -70,9 +92,12 @@ def main() -> None:
         raise SystemExit("oracle/_ref/libhadros_ref.so missing: run oracle/build_ref.sh first")
     E, g2, s = W.synthetic_sigma_arrays()
     np.savez(HERE / "sigma_synthetic.npz", E=E, sigma_GeV2=g2, sigma_cm2=s)
+    only = sys.argv[1] if len(sys.argv) > 1 else ""   # optional name prefix
     for name, kw in cases().items():
+        if not name.startswith(only):
+            continue
         p = hb.params(**kw)
-        out = O.ref_image(p, E, g2, s)
+        out = O.ref_image(p, E, g2, s, mev=name.startswith("mev_"))
         meta = {k: (v if not isinstance(v, (np.floating, np.integer)) else v.item())
                 for k, v in kw.items()}
         np.savez_compressed(HERE / f"{name}.npz", params=json.dumps(meta), **out)

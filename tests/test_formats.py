@@ -82,6 +82,64 @@ def test_dat_and_kimg_layout(hb, tmp_path):
     np.testing.assert_allclose(rows[:, :4], d[:, :4], rtol=1e-8)
 
 
+def test_mev_columns_and_header(hb, tmp_path):
+    """hadros_write_dat_mev / hadros_write_kimg_mev: the MeV channel's five
+    columns and, with the channel on, the CPU app's MeV metadata lines."""
+    kw, ref = load_golden("mev_fd_band_spectral")
+    p = hb.params(**kw)
+    host = {k: np.ascontiguousarray(ref[k]) for k in ("tau", "P_surv", "I_obs", "fate") + hb.MEV_OUTPUTS}
+    out = hb.HadrosImageOut()
+    for k, a in host.items():
+        setattr(out, k, a.ctypes.data)
+    dat, kimg = tmp_path / "m.dat", tmp_path / "m.bin"
+    L = hb.lib()
+    assert L.hadros_write_dat_mev(str(dat).encode(), C.byref(p), b"GBW", C.byref(out)) == 0
+    assert L.hadros_write_kimg_mev(str(kimg).encode(), C.byref(p), C.byref(out)) == 0
+    text = dat.read_text().splitlines()
+    for line in ("# MEV_MODEL physical", "# MEV_FLAVOR anti_nu_e", "# MEV_THERMAL_PROFILE inner_hot_torus",
+                 "# MEV_YE_PROFILE neutron_rich_torus", "# MEV_SPECTRAL_MODE fermi_dirac_band",
+                 "# MEV_N_BINS 5", "# MEV_INCLUDE_URCA 1", "# MEV_USE_DEGENERACY_CORRECTION 0",
+                 "# mev_opacity_units cm^-1"):
+        assert line in text, line
+    d = np.loadtxt(dat, comments="#")
+    for c, k in enumerate(hb.MEV_OUTPUTS):
+        np.testing.assert_allclose(d[:, 8 + c], ref[k], rtol=1e-8, err_msg=k)
+    rows = np.fromfile(kimg, dtype="<f8", offset=struct.calcsize("<7i4d")).reshape(-1, 13)
+    for c, k in enumerate(hb.MEV_OUTPUTS):
+        np.testing.assert_array_equal(rows[:, 8 + c], ref[k], err_msg=k)
+    # the CPU app's file name carries the MeV band
+    assert "_MeVSpectrum_fermi_dirac_band_E3e_00_5e_01_" in fname(hb, p, 1, ".dat", b"GBW")
+    # a missing array writes its default
+    out.r_nu = None
+    assert L.hadros_write_dat_mev(str(dat).encode(), C.byref(p), b"GBW", C.byref(out)) == 0
+    np.testing.assert_array_equal(np.loadtxt(dat, comments="#")[:, 11], -1.0)
+
+
+def test_mev_names_and_validation(hb):
+    L = hb.lib()
+    k = C.c_int32()
+    for fn, name, want in (("hadros_parse_mev_model", b"phys", 1), ("hadros_parse_mev_flavor", b"anti-nu-e", 1),
+                           ("hadros_parse_mev_thermal", b"COLLAPSAR_INNER_HOT", 4),
+                           ("hadros_parse_mev_ye", b"funnel_proton_rich", 2),
+                           ("hadros_parse_mev_spectral", b"fd_band", 1)):
+        assert getattr(L, fn)(name, C.byref(k)) == 0 and k.value == want
+    assert L.hadros_parse_mev_flavor(b"nu_tau", C.byref(k)) == hb.abi.E_ARG
+    assert L.hadros_last_error().decode() == "Unknown MEV_FLAVOR 'nu_tau'. Use nu_e, anti_nu_e, or nu_x."
+    assert L.hadros_mev_thermal_name(3) == b"torus_plus_cool_envelope"
+    assert L.hadros_mev_ye_name(9) is None
+    p = hb.params(mev_channel=1)
+    assert L.hadros_params_validate(C.byref(p)) == 0
+    p.mev_flavor = 3
+    assert L.hadros_params_validate(C.byref(p)) == hb.abi.E_ARG
+    p.mev_channel = 0   # the channel's fields are ignored while it is off
+    assert L.hadros_params_validate(C.byref(p)) == 0
+    q = hb.params(mev_channel=1, mev_T0_MeV=float("nan"))
+    assert L.hadros_params_validate(C.byref(q)) == hb.abi.E_ARG
+    d = hb.params()
+    assert (d.mev_channel, d.mev_model, d.mev_flavor, d.mev_flags) == (0, 1, 1, 0x7DF)
+    assert d.mev_neutrinosphere_tau == 2.0 / 3.0 and d.mev_sigma_abs0_cm2 == 9.6e-44
+
+
 def test_alpha_beta_are_reference_camera_coordinates(hb, tmp_path):
     import math
     kw, ref = load_golden("edge_ragged_3x5")

@@ -26,6 +26,34 @@ def test_oracle_bit_exact_vs_reference_fixture(hb, sigma_arrays, name):
         np.testing.assert_array_equal(got[k], ref[k], err_msg=f"{name}: {k}")
 
 
+MEV_CASES = [n for n in CPU_CASES if n.startswith("mev_")]
+
+
+@pytest.mark.parametrize("name", MEV_CASES)
+def test_oracle_mev_channel_bit_exact_vs_reference_fixture(hb, sigma_arrays, name):
+    """The MeV thermal channel (radiative_transfer.cpp:522-638 with
+    mev_neutrino_physics.cpp) of the C restatement equals the reference's."""
+    kw, ref = load_golden(name)
+    E, _, s = sigma_arrays
+    got = O.oracle_image(hb.params(**kw), E, s, mev=True)
+    for k in FIELDS + O.MEV_KEYS:
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=f"{name}: {k}")
+
+
+def test_mev_fixtures_exercise_the_channel():
+    """The MeV fixtures are not trivial: optically thick and thin rays,
+    neutrinospheres found and not, defaults for the empty band."""
+    _, thick = load_golden("mev_physical_collapsar")
+    assert thick["tau_mev"].max() > 1.0 and (thick["r_nu"] > 0).any()
+    assert (thick["I_obs_mev"] > 0).all()
+    _, thin = load_golden("mev_gaussian_thin")
+    assert (thin["r_nu"] < 0).any()
+    _, empty = load_golden("mev_empty_band")
+    np.testing.assert_array_equal(empty["tau_mev"], 0.0)
+    np.testing.assert_array_equal(empty["r_nu"], -1.0)
+    np.testing.assert_array_equal(empty["leakage"], 1.0)
+
+
 def test_oracle_bit_exact_plain_tracer_subset(hb, sigma_arrays):
     """Every 5th pixel of the 32x32 plain tracer (the full image is in the GPU tests)."""
     kw, ref = load_golden("plain_tracer_32")
