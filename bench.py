@@ -17,6 +17,7 @@ the trace kernel.  One process per GPU; each GPU traces its own image per step
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
     python bench.py --workload surrogate     # the surrogate's tcgen05 inference kernel
+    python bench.py --mev                    # image workload with the MeV thermal channel
 """
 from __future__ import annotations
 
@@ -44,6 +45,10 @@ import numpy as np  # noqa: E402
 # inputs + y4/y5 + error = 1573 flop; one accepted step's ZAMO interval and
 # redshift = 52 flop.  Per point 44 flop and per point-bin 16 flop of transfer.
 F_ATT, F_GEO, F_PT, F_PB = 1573, 52, 44, 16
+# The MeV thermal channel (physical model, default profiles, monochromatic),
+# FP64 per path point: interval in cm 1, density 30, redshift 1, temperature 3,
+# electron fraction 6, local energy 1, opacity 24, emissivity 31, transfer 12.
+F_MEV = 109
 FP64_PEAK_DATASHEET_TFLOPS = 37.0
 WORKLOAD_DESC = ("512x512 px x 8 powerlaw_cutoff bins (1e5-1e12 GeV), a=0.998, i=17 deg, "
                  "powerlaw_funnel_envelope, funnel_wall source, r_obs 60 M, fov 25 deg, h0 0.01, "
@@ -251,7 +256,7 @@ def gpu_arm(args) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         return float(t.item())
 
-    kw = W.mixed_512()
+    kw = W.mixed_512(**({"mev_channel": 1} if args.mev else {}))
     p = hb.params(**kw)          # library default: fast geodesic arithmetic
     E, g2, s = W.synthetic_sigma_arrays()
     sig = hb.SigmaTable.from_arrays(E, s, g2)
@@ -268,6 +273,8 @@ def gpu_arm(args) -> None:
         "tau_E": torch.empty(P * B, dtype=torch.float32 if f32 else torch.float64, device=device),
         "I_E": torch.empty(P * B, dtype=torch.float64, device=device),
     }
+    if args.mev:
+        out.update({k: torch.empty(P, dtype=torch.float64, device=device) for k in hb.MEV_OUTPUTS})
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)   # > 126 MB L2
     # a non-default stream: the library launches on it, the events bracket it
     stream = torch.cuda.Stream(device=device)
@@ -311,7 +318,7 @@ def gpu_arm(args) -> None:
 
     attempts = float(out["attempts"].to(torch.int64).sum().item())
     steps_sum = float(out["steps"].to(torch.int64).sum().item())
-    flop64 = attempts * F_ATT + steps_sum * F_GEO
+    flop64 = attempts * F_ATT + steps_sum * (F_GEO + (F_MEV if args.mev else 0))
     flop32 = steps_sum * (F_PT + B * F_PB)
     kern_s = statistics.mean(kernel_ms) / 1e3
     peak = fp64_peak_tflops(torch, device)
@@ -344,7 +351,8 @@ def gpu_arm(args) -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64+f32", "data": "synthetic",
-            "config": {"workload": "mixed_512: " + WORKLOAD_DESC,
+            "config": {"workload": "mixed_512: " + WORKLOAD_DESC +
+                                   (" + FP64 MeV thermal channel (physical, defaults)" if args.mev else ""),
                        "per_gpu": "one 512x512x8 image per GPU per step",
                        "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"independent images, {world} GPU(s), no collective"},
@@ -512,6 +520,9 @@ def main() -> None:
                          "surrogate inference kernel")
     ap.add_argument("--side", type=int, default=None, help="surrogate workload: image side")
     ap.add_argument("--bins", type=int, default=None, help="surrogate workload: bins")
+    ap.add_argument("--mev", action="store_true",
+                    help="image workload: also run the MeV thermal channel (the reference arm's CPU "
+                         "code always runs it)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

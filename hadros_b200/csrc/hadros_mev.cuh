@@ -13,7 +13,9 @@
 // trace kernel evaluates it once per point next to the per-bin UHE terms.
 //
 // Expressions keep the reference's operand order; std::pow(x, 2.0) is x * x
-// and std::pow(x, 1.0) is x (both exact), other powers call pow.
+// and std::pow(x, 1.0) is x (both exact), the integer powers 3, 5, 6 and 9
+// are products (a few ulp from pow, far inside the 1e-6 parity bound and
+// without pow's cost), other powers call pow.
 #pragma once
 
 #include <cstdint>
@@ -174,13 +176,15 @@ HD double mev_emissivity(const Mev& m, double rho, double T, double Ye, double E
         const double proton_fraction = sclamp(Ye, 0.0, 1.0);
         const double charged_current_weight = neutron_fraction + 0.5 * proton_fraction;
         const double thermal_spectrum = E * E / (exp(smin(E / T, 120.0)) + 1.0);
-        const double capture_like = nb * charged_current_weight * pow(T, 6.0);
-        const double pair_like = 0.05 * nb * pow(T, 9.0);
+        const double T3 = T * T * T, T6 = T3 * T3;
+        const double capture_like = nb * charged_current_weight * T6;
+        const double pair_like = 0.05 * nb * (T6 * T3);
         return m.norm * (capture_like + pair_like) * thermal_spectrum;
     }
     double shape = 0.0;
     if (T > 0.0 && E > 0.0) shape = mev_fd(E, T) / smax(T * T * T, 1.0e-300);
     const double T10 = T / 10.0;
+    const double t2 = T10 * T10, t3 = t2 * T10, t6 = t3 * t3;
     const double rho10 = rho / 1.0e10;
     double total = 0.0;
     if (mev_has(m, HADROS_MEV_URCA)) {
@@ -188,18 +192,18 @@ HD double mev_emissivity(const Mev& m, double rho, double T, double Ye, double E
         if (!(rho <= 0.0 || T <= 0.0 || E <= 0.0) && m.flavor != HADROS_MEV_NU_X) {
             const double ye = mev_clamp_ye(Ye);
             const double flavor_factor = m.flavor == HADROS_MEV_NU_E ? ye : (1.0 - ye);
-            urca = 1.0e30 * rho10 * pow(T10, 6.0) * flavor_factor * shape;
+            urca = 1.0e30 * rho10 * t6 * flavor_factor * shape;
         }
         if (mev_has(m, HADROS_MEV_DEGENERACY_CORRECTION)) urca *= mev_degeneracy(rho, Ye, T, m.flavor);
         total += urca;
     }
     if (mev_has(m, HADROS_MEV_PAIR) && !(T <= 0.0 || E <= 0.0)) {
         const double flavor_factor = m.flavor == HADROS_MEV_NU_X ? 1.0 : 0.7;
-        total += 3.0e28 * pow(T10, 9.0) * flavor_factor * shape;
+        total += 3.0e28 * (t6 * t3) * flavor_factor * shape;
     }
     if (mev_has(m, HADROS_MEV_BREMS) && !(rho <= 0.0 || T <= 0.0 || E <= 0.0)) {
         const double flavor_factor = m.flavor == HADROS_MEV_NU_X ? 1.0 : 0.8;
-        total += 1.0e27 * (rho10 * rho10) * pow(T10, 5.0) * flavor_factor * shape;
+        total += 1.0e27 * (rho10 * rho10) * (t3 * t2) * flavor_factor * shape;
     }
     return m.norm * total;
 }
@@ -268,7 +272,7 @@ HD void mev_point(const Mev& m, MevAcc& acc, double r, double th, double rho, do
         j = mev_emissivity(m, rho, T, Ye, E_local);
     }
     const double dtau = kappa * dl_cm;
-    const double g3 = pow(g, 3.0);
+    const double g3 = g * g * g;
     if (kappa > 0.0 && dtau > 1.0e-12) {
         const double attenuation = exp(-smin(dtau, 700.0));
         acc.I = acc.I * attenuation + g3 * (j / kappa) * (1.0 - attenuation);

@@ -486,7 +486,9 @@ __device__ __forceinline__ void finish_pixel(const TraceArgs& A, const DevCam* c
     if (A.attempts) A.attempts[orow] = static_cast<int32_t>(att_total > 2147483647LL ? 2147483647LL : att_total);
 }
 
-// The MeV channel's outputs of a finished pixel (kernels built with MEV).
+// The MeV channel's outputs of a finished pixel: its sums, or RTResult's
+// defaults for a camera without the channel (every kernel writes them, so a
+// requested MeV output is never left unwritten).
 __device__ __forceinline__ void finish_mev(const TraceArgs& A, const DevCam* cam, const MevAcc& ma, long long local,
                                            int step)
 {
@@ -668,7 +670,8 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
     K5 k1{};
     double s_base = 0.0, c_base = 1.0;   // sin/cos of theta at the step start
     int fate = HADROS_FATE_TRUNCATED;
-    MevAcc ma{};
+    MevAcc ma;
+    mev_reset(ma);
 
     while (true) {
         while (phase == kNeedRay || phase == kStepStart) {
@@ -745,7 +748,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                     continue;
                 }
                 finish_pixel<MIXED>(A, cam, bins, B, acc, row, step, fate, att_total);
-                if (MEV) finish_mev(A, cam, ma, row, step);
+                finish_mev(A, cam, ma, row, step);
                 phase = kNeedRay;
                 continue;
             }
@@ -848,7 +851,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                 deferred_transfer(A.rec_buf, A.rec_state, A.bins, A.rec_bmax, tb, slot - (tid & 31), fill, B, cam);
                 if (phase == kWaitTransfer) {
                     finish_pixel<MIXED>(A, cam, bins, B, acc, row, step, fate, att_total);
-                    if (MEV) finish_mev(A, cam, ma, row, step);
+                    finish_mev(A, cam, ma, row, step);
                     phase = kNeedRay;
                 }
                 fill = 0;
@@ -993,7 +996,7 @@ __global__ void __launch_bounds__(kTPB) path_transfer_kernel(const TraceArgs A)
         }
         const int fate = A.path_fates ? A.path_fates[ray] : HADROS_FATE_ESCAPED;
         finish_pixel<MIXED>(A, cam, bins, B, acc, ray, static_cast<int>(k1 - k0), fate, 0);
-        if (MEV) finish_mev(A, cam, ma, ray, static_cast<int>(k1 - k0));
+        finish_mev(A, cam, ma, ray, static_cast<int>(k1 - k0));
     }
 }
 
