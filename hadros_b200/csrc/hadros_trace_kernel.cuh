@@ -861,45 +861,67 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
         if (phase != kAttempt) continue;
 
         // ---- one RKF45 attempt (kerr_geodesic.cpp:239-326) -----------------
-        double cf[15];
-        if (att_in_step == 0) {
-#pragma unroll
-            for (int q = 0; q < 15; ++q) cf[q] = cam->c0[q];
-        } else {
-            cf[0] = h * 1.0 / 4.0;
-            cf[1] = h * 3.0 / 32.0; cf[2] = h * 9.0 / 32.0;
-            cf[3] = h * 1932.0 / 2197.0; cf[4] = h * -7200.0 / 2197.0; cf[5] = h * 7296.0 / 2197.0;
-            cf[6] = h * 439.0 / 216.0; cf[7] = h * -8.0; cf[8] = h * 3680.0 / 513.0;
-            cf[9] = h * -845.0 / 4104.0;
-            cf[10] = h * -8.0 / 27.0; cf[11] = h * 2.0; cf[12] = h * -3544.0 / 2565.0;
-            cf[13] = h * 1859.0 / 4104.0; cf[14] = h * -11.0 / 40.0;
-        }
+        // Stage coefficients h * a_ij (:241-308): the camera's values at
+        // h = h0 on a step's first attempt, else formed from h, each where its
+        // stage uses it so that none stays live across the attempt.  The phi
+        // components of k enter only y4 and y5: their weighted sums are
+        // accumulated as the stages produce them, in the reference's order.
+        const bool first = att_in_step == 0;
+        const double* c0 = cam->c0;
+#define HAD_CF(q, num, den) (first ? c0[q] : h * (num) / (den))
+#define HAD_CFM(q, num) (first ? c0[q] : h * (num))
+        double s4p = A1 * k1.ph, s5p = B1 * k1.ph;   // y4, y5 phi sums so far
         K5 k2, k3, k4, k5, k6;
-        geo_rhs_sel<FAST>(a, r + cf[0] * k1.r, th + cf[0] * k1.th, pr + cf[0] * k1.pr,
-                   pth + cf[0] * k1.pth, pt, pph, k2, th, s_base, c_base);
-        geo_rhs_sel<FAST>(a, r + cf[1] * k1.r + cf[2] * k2.r, th + cf[1] * k1.th + cf[2] * k2.th,
-                   pr + cf[1] * k1.pr + cf[2] * k2.pr, pth + cf[1] * k1.pth + cf[2] * k2.pth,
-                   pt, pph, k3, th, s_base, c_base);
-        geo_rhs_sel<FAST>(a, r + cf[3] * k1.r + cf[4] * k2.r + cf[5] * k3.r,
-                   th + cf[3] * k1.th + cf[4] * k2.th + cf[5] * k3.th,
-                   pr + cf[3] * k1.pr + cf[4] * k2.pr + cf[5] * k3.pr,
-                   pth + cf[3] * k1.pth + cf[4] * k2.pth + cf[5] * k3.pth, pt, pph, k4, th, s_base, c_base);
-        geo_rhs_sel<FAST>(a, r + cf[6] * k1.r + cf[7] * k2.r + cf[8] * k3.r + cf[9] * k4.r,
-                   th + cf[6] * k1.th + cf[7] * k2.th + cf[8] * k3.th + cf[9] * k4.th,
-                   pr + cf[6] * k1.pr + cf[7] * k2.pr + cf[8] * k3.pr + cf[9] * k4.pr,
-                   pth + cf[6] * k1.pth + cf[7] * k2.pth + cf[8] * k3.pth + cf[9] * k4.pth,
-                   pt, pph, k5, th, s_base, c_base);
-        geo_rhs_sel<FAST>(a,
-                   r + cf[10] * k1.r + cf[11] * k2.r + cf[12] * k3.r + cf[13] * k4.r + cf[14] * k5.r,
-                   th + cf[10] * k1.th + cf[11] * k2.th + cf[12] * k3.th + cf[13] * k4.th + cf[14] * k5.th,
-                   pr + cf[10] * k1.pr + cf[11] * k2.pr + cf[12] * k3.pr + cf[13] * k4.pr + cf[14] * k5.pr,
-                   pth + cf[10] * k1.pth + cf[11] * k2.pth + cf[12] * k3.pth + cf[13] * k4.pth + cf[14] * k5.pth,
-                   pt, pph, k6, th, s_base, c_base);
+        {
+            const double c = HAD_CF(0, 1.0, 4.0);
+            geo_rhs_sel<FAST>(a, r + c * k1.r, th + c * k1.th, pr + c * k1.pr, pth + c * k1.pth, pt, pph, k2,
+                              th, s_base, c_base);
+        }
+        {
+            const double c1 = HAD_CF(1, 3.0, 32.0), c2 = HAD_CF(2, 9.0, 32.0);
+            geo_rhs_sel<FAST>(a, r + c1 * k1.r + c2 * k2.r, th + c1 * k1.th + c2 * k2.th,
+                              pr + c1 * k1.pr + c2 * k2.pr, pth + c1 * k1.pth + c2 * k2.pth, pt, pph, k3, th,
+                              s_base, c_base);
+        }
+        s4p = s4p + A3 * k3.ph;
+        s5p = s5p + B3 * k3.ph;
+        {
+            const double c3 = HAD_CF(3, 1932.0, 2197.0), c4 = HAD_CF(4, -7200.0, 2197.0),
+                         c5 = HAD_CF(5, 7296.0, 2197.0);
+            geo_rhs_sel<FAST>(a, r + c3 * k1.r + c4 * k2.r + c5 * k3.r, th + c3 * k1.th + c4 * k2.th + c5 * k3.th,
+                              pr + c3 * k1.pr + c4 * k2.pr + c5 * k3.pr,
+                              pth + c3 * k1.pth + c4 * k2.pth + c5 * k3.pth, pt, pph, k4, th, s_base, c_base);
+        }
+        s4p = s4p + A4 * k4.ph;
+        s5p = s5p + B4 * k4.ph;
+        {
+            const double c6 = HAD_CF(6, 439.0, 216.0), c7 = HAD_CFM(7, -8.0), c8 = HAD_CF(8, 3680.0, 513.0),
+                         c9 = HAD_CF(9, -845.0, 4104.0);
+            geo_rhs_sel<FAST>(a, r + c6 * k1.r + c7 * k2.r + c8 * k3.r + c9 * k4.r,
+                              th + c6 * k1.th + c7 * k2.th + c8 * k3.th + c9 * k4.th,
+                              pr + c6 * k1.pr + c7 * k2.pr + c8 * k3.pr + c9 * k4.pr,
+                              pth + c6 * k1.pth + c7 * k2.pth + c8 * k3.pth + c9 * k4.pth, pt, pph, k5, th,
+                              s_base, c_base);
+        }
+        s4p = s4p - A5 * k5.ph;
+        s5p = s5p - B5 * k5.ph;
+        {
+            const double c10 = HAD_CF(10, -8.0, 27.0), c11 = HAD_CFM(11, 2.0), c12 = HAD_CF(12, -3544.0, 2565.0),
+                         c13 = HAD_CF(13, 1859.0, 4104.0), c14 = HAD_CF(14, -11.0, 40.0);
+            geo_rhs_sel<FAST>(a, r + c10 * k1.r + c11 * k2.r + c12 * k3.r + c13 * k4.r + c14 * k5.r,
+                              th + c10 * k1.th + c11 * k2.th + c12 * k3.th + c13 * k4.th + c14 * k5.th,
+                              pr + c10 * k1.pr + c11 * k2.pr + c12 * k3.pr + c13 * k4.pr + c14 * k5.pr,
+                              pth + c10 * k1.pth + c11 * k2.pth + c12 * k3.pth + c13 * k4.pth + c14 * k5.pth, pt,
+                              pph, k6, th, s_base, c_base);
+        }
+        s5p = s5p + B6 * k6.ph;
+#undef HAD_CF
+#undef HAD_CFM
 #define HAD_Y4(f) (A1 * k1.f + A3 * k3.f + A4 * k4.f - A5 * k5.f)
 #define HAD_Y5(f) (B1 * k1.f + B3 * k3.f + B4 * k4.f - B5 * k5.f + B6 * k6.f)
         const double y4r = r + h * HAD_Y4(r), y5r = r + h * HAD_Y5(r);
         const double y4t = th + h * HAD_Y4(th), y5t = th + h * HAD_Y5(th);
-        const double y4p = ph + h * HAD_Y4(ph), y5p = ph + h * HAD_Y5(ph);
+        const double y4p = ph + h * s4p, y5p = ph + h * s5p;
         const double y4pr = pr + h * HAD_Y4(pr), y5pr = pr + h * HAD_Y5(pr);
         const double y4pt = pth + h * HAD_Y4(pth), y5pt = pth + h * HAD_Y5(pth);
 #undef HAD_Y4
