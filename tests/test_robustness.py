@@ -1,0 +1,109 @@
+"""hadros_b200.robustness: the reference's robustness scan
+(scripts/run_robustness_scans.py) through the C ABI.  CPU tests: the case
+table, the argv mapping, and our rows against the reference's own two
+executables run the way the script runs them (where oracle/build_ref.sh built
+them).  The GPU run is in test_gpu_robustness.py."""
+from __future__ import annotations
+
+import collections
+import math
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+REF_DIR = ROOT / "oracle" / "_ref"
+REF_GEO = REF_DIR / "compute_kerr_geodesics"
+REF_IMG = REF_DIR / "compute_kerr_image_from_cache"
+
+
+def test_case_table_is_the_reference_scan():
+    from hadros_b200 import robustness as R
+    t = R.cases()
+    assert len(t) == 47
+    assert collections.Counter(c["scan"] for c in t) == {
+        "source_model": 5, "density_background": 4, "energy": 15, "inclination": 5, "spin": 4,
+        "parameter_stability": 14}
+    assert [c["case"] for c in t[:5]] == ["inner_ring", "jet_base", "funnel_wall", "density_weighted",
+                                          "shock_layer"]
+    assert t[9]["case"] == "inner_ring_E1e4" and t[9]["updates"] == {"source_model": "inner_ring", "enu": "1e4"}
+    caches = {c["cache"] for c in t}
+    assert len(caches) == 10   # the ten geodesic caches the script makes
+
+
+def test_case_params_follow_the_cpu_app_argv(hb):
+    from hadros_b200 import robustness as R
+    t = {(c["scan"], c["case"]): c for c in R.cases()}
+    p, v = R.case_params(t[("density_background", "powerlaw_funnel_envelope")])
+    assert (p.nx, p.ny, p.h, p.r_max_rg, p.r_obs_rg, p.fov_deg) == (16, 16, 0.02, 60.0, 60.0, 25.0)
+    assert p.H_over_R == 0.25 and p.sigma_r_rg == 5.0 and p.r0_rg == 10.0 and p.rho0_gcm3 == 1.0e-2
+    assert p.profile_kind == hb.PROFILES.index("powerlaw_funnel_envelope")
+    assert p.source_kind == hb.SOURCES.index("funnel_wall")
+    assert p.funnel_depletion == 1.0 and p.envelope_rho0_gcm3 == 1.0e-4
+    assert p.theta_obs_rad == 80.0 * math.pi / 180.0 and p.src_theta_width_rad == 15.0 * math.pi / 180.0
+    assert p.a_spin == 0.0001 and p.Enu_obs_GeV == 1.0e5 and p.mev_channel == 1
+    q, _ = R.case_params(t[("spin", "a_0.99")])
+    assert q.a_spin == 0.99
+    w, _ = R.case_params(t[("parameter_stability", "funnel_wall_width25.0")])
+    assert w.src_theta_width_rad == 25.0 * math.pi / 180.0
+
+
+def _ref_image_args(R, case, cache, sigma_path):
+    """scripts/run_robustness_scans.py:101-141 with this machine's sigma file."""
+    v = dict(R.BASE)
+    v.update(case["updates"])
+    v["sigma_path"] = str(sigma_path)
+    keys = ["enu", "aspin", "mbh", "rho0", "r0", "sigma", "h", "source_r", "source_sigma", "source_theta",
+            "source_powerlaw", "source_emax", "source_norm", "mev_enu", "mev_norm", "cam_theta", "sigma_path",
+            "density_profile", "radial_power", "funnel_depletion", "funnel_theta", "envelope_rho0",
+            "envelope_alpha", "r_min", "r_max", "rho_floor", "observer_distance", "use_f3"]
+    tail = ["source_model", "source_funnel_theta", "source_q", "source_s", "source_grad_dr", "source_grad_dtheta",
+            "source_rho_ref", "source_cutoff_min", "source_cutoff_max"]
+    return [str(REF_IMG)] + [v[k] for k in keys] + [str(cache)] + [v[k] for k in tail]
+
+
+@pytest.mark.skipif(not (REF_GEO.exists() and REF_IMG.exists()), reason="reference executables not built here")
+def test_rows_equal_the_reference_executables(hb, tmp_path, sigma_arrays):
+    """Three cases at 4x4 pixels run as the script runs them
+    (compute_kerr_geodesics, then compute_kerr_image_from_cache, then the
+    .dat read back): our rows, built from the oracle's in-memory outputs, give
+    the same five metrics, and the .dat's MeV columns are the oracle's."""
+    from hadros_b200 import robustness as R
+    from hadros_b200 import workloads as W
+    from oracle import pyoracle as O
+    E, g2, s = sigma_arrays
+    sig = tmp_path / "sigma.dat"
+    W.write_sigma_file(sig, E, g2, s)
+    (tmp_path / "output" / "images").mkdir(parents=True)
+    table = {(c["scan"], c["case"]): c for c in R.cases()}
+    picks = [table[("source_model", "funnel_wall")], table[("energy", "jet_base_E1e6")],
+             table[("spin", "a_0.9")]]
+    for case in picks:
+        spin, theta = case["cache"]
+        cache = tmp_path / f"cache_{spin}_{theta}.bin"
+        r = subprocess.run([str(REF_GEO), spin, "60.0", theta, "25.0", "4", "4", "60.0", "0.02", str(cache)],
+                           capture_output=True, text=True, timeout=600, env={"OMP_NUM_THREADS": "4"})
+        assert r.returncode == 0, r.stderr
+        r = subprocess.run(_ref_image_args(R, case, cache, sig), cwd=tmp_path, capture_output=True, text=True,
+                           timeout=600, env={"OMP_NUM_THREADS": "4"})
+        assert r.returncode == 0, r.stderr
+        saved = [ln.split("Saved: ", 1)[1] for ln in r.stdout.splitlines()
+                 if ln.startswith("Saved: ") and ln.endswith(".dat")]
+        data = np.loadtxt(tmp_path / saved[0], comments="#")
+        tau, psurv, inten, captured = data[:, 4], data[:, 5], data[:, 6], data[:, 7]
+        finite = np.isfinite(tau) & np.isfinite(psurv) & np.isfinite(inten)
+        theirs = {"mean_tau": np.mean(tau[finite]), "max_tau": np.max(tau[finite]),
+                  "mean_P_surv": np.mean(psurv[finite]), "total_intensity": np.sum(inten[finite]),
+                  "valid_rays": int(np.count_nonzero(finite & (captured == 0)))}
+        p, _ = R.case_params(case, pixels=4)
+        ref = O.oracle_image(p, E, s, mev=True)
+        row = R.make_rows([case], [ref])[0]
+        for k in ("mean_tau", "max_tau", "mean_P_surv", "total_intensity"):
+            assert row[k] == pytest.approx(theirs[k], rel=1e-12, abs=0.0), (case["case"], k)
+        assert row["valid_rays"] == theirs["valid_rays"]
+        for c, key in enumerate(O.MEV_KEYS):   # .dat rows are in cache order: key them by pixel
+            for line in data:
+                k = int(line[1]) * 4 + int(line[0])
+                assert line[8 + c] == pytest.approx(ref[key][k], rel=1e-8, abs=1e-300), (case["case"], key)
