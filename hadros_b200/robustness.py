@@ -1,4 +1,6 @@
-"""Robustness scans through the C ABI instead of subprocesses.
+"""The reference's scan scripts through the C ABI instead of subprocesses.
+
+robustness (default):
 
 The reference's scripts/run_robustness_scans.py (:19-56 parameters,
 :190-270 cases) traces ten geodesic caches with compute_kerr_geodesics, runs
@@ -13,6 +15,16 @@ reference script are not drawn: matplotlib is not a dependency.
 
     python -m hadros_b200.robustness [--outdir output/scans] [--sigma FILE]
            [--pixels 16] [--precision fp64|mixed] [--write-dat DIR]
+
+spectral: scripts/validate_uhe_spectral_models.py (:21-61 parameters,
+:153-171 metrics, :240-296 outputs) runs compute_kerr_image_from_cache six
+times on the Makefile's small cache (a 0.0001, r_obs 60, theta 80, fov 25,
+32x32, r_max 40, step 0.01; Makefile:224-230, :671): the three UHE spectral
+models at 8 bins and powerlaw_cutoff at 4, 8 and 16 bins.  Here the six
+images are one batch launch; spectral_validation.csv and
+spectral_validation.md are the script's.
+
+    python -m hadros_b200.robustness spectral [--outdir output/spectra] ...
 
 Argument mapping (compute_kerr_image_from_cache argv, apps/
 compute_kerr_image_from_cache.cpp:57-201): the "h" of the parameter table is
@@ -238,12 +250,107 @@ def write_markdown(rows: list[dict], outdir: Path) -> Path:
     return path
 
 
+# scripts/validate_uhe_spectral_models.py:21-61 (the same parameter table)
+SPECTRAL_BASE = {
+    "enu": "1e11", "a": "0.0001", "mbh": "3.0", "rho0": "1.0e0", "r0": "10.0", "sigma": "5.0", "h": "0.25",
+    "source_r": "3.5", "source_sigma": "1.0", "source_theta": "15.0", "source_powerlaw": "2.0",
+    "source_emax": "1.0e12", "source_norm": "1.0", "mev_enu": "10.0", "mev_norm": "1.0", "cam_theta": "80.0",
+    "sigma_path": "data/sigma/sigma_nuN_CC_GBW.dat", "profile": "powerlaw_funnel_envelope",
+    "radial_power": "2.0", "funnel_depletion": "1.0", "funnel_theta": "20.0", "envelope_rho0": "1.0e-2",
+    "envelope_alpha": "2.5", "r_min": "4.0", "r_max": "60.0", "rho_floor": "1.0e-99",
+    "observer_distance": "60.0", "use_f3": "1", "cache": "output/rays/kerr_geodesics_small.bin",
+    "source_model": "funnel_wall", "source_funnel_theta": "20.0", "source_q": "1.0", "source_s": "2.0",
+    "source_grad_dr": "0.1", "source_grad_dtheta": "1.0", "source_rho_ref": "1.0e0",
+    "source_cutoff_min": "0.0", "source_cutoff_max": "1.0e2",
+}
+# the small cache (Makefile:43-51, :224-230, :671)
+SMALL_CACHE = {"a": 0.0001, "r_obs": 60.0, "theta": 80.0, "fov_deg": 25.0, "pixels": 32, "r_max": 40.0,
+               "step": 0.01}
+
+
+def spectral_cases() -> list[tuple[str, int, str]]:
+    """(spectral model, bins, row label) in the script's order (:244-252)."""
+    out = [(m, 8, m) for m in ("monochromatic", "powerlaw", "powerlaw_cutoff")]
+    out += [("powerlaw_cutoff", n, f"powerlaw_cutoff_bins{n}") for n in (4, 8, 16)]
+    return out
+
+
+def spectral_params(model: str, n_bins: int, pixels: int = 32, precision: str = "fp64", **over):
+    """compute() of the script (:98-150): the CPU app's argv 1-44 with the
+    spectral arguments model, gamma 2, E_cut 1e12, 1e5-1e12 GeV, n_bins."""
+    v = SPECTRAL_BASE
+    f = lambda k: float(v[k])   # noqa: E731  (std::atof)
+    kw = dict(
+        a_spin=SMALL_CACHE["a"], r_obs_rg=SMALL_CACHE["r_obs"], theta_obs_deg=SMALL_CACHE["theta"],
+        fov_deg=SMALL_CACHE["fov_deg"], nx=pixels, ny=pixels, r_max_rg=SMALL_CACHE["r_max"],
+        h=SMALL_CACHE["step"],
+        Enu_obs_GeV=f("enu"), M_bh_msun=f("mbh"), rho0_gcm3=f("rho0"), r0_rg=f("r0"), sigma_r_rg=f("sigma"),
+        H_over_R=f("h"), src_r_center_rg=f("source_r"), src_sigma_r_rg=f("source_sigma"),
+        src_theta_width_deg=f("source_theta"), src_powerlaw=f("source_powerlaw"),
+        src_emax_GeV=f("source_emax"), src_norm=f("source_norm"), mev_Enu_obs_MeV=f("mev_enu"),
+        mev_norm=f("mev_norm"), profile=v["profile"], radial_power=f("radial_power"),
+        funnel_depletion=f("funnel_depletion"), funnel_theta_deg=f("funnel_theta"),
+        envelope_rho0_gcm3=f("envelope_rho0"), envelope_alpha=f("envelope_alpha"),
+        torus_r_min_rg=f("r_min"), torus_r_max_rg=f("r_max"), rho_floor_gcm3=f("rho_floor"),
+        source=v["source_model"], src_funnel_theta_deg=f("source_funnel_theta"),
+        src_density_power_q=f("source_q"), src_radial_power_s=f("source_s"),
+        src_gradient_dr_rg=f("source_grad_dr"), src_gradient_dtheta_deg=f("source_grad_dtheta"),
+        src_rho_ref_gcm3=f("source_rho_ref"), src_cutoff_min=f("source_cutoff_min"),
+        src_cutoff_max=f("source_cutoff_max"),
+        spectral=model, spec_gamma=2.0, spec_ecut_GeV=1.0e12, spec_e_min_GeV=1.0e5, spec_e_max_GeV=1.0e12,
+        n_bins=n_bins, mev_channel=1, precision=precision)
+    kw.update(over)
+    return params(**kw)
+
+
+def spectral_metrics(out: dict, label: str, n_bins: int) -> dict:
+    """metrics() of the script (:153-171)."""
+    tau, psurv, inten = dat_round(out["tau"]), dat_round(out["P_surv"]), dat_round(out["I_obs"])
+    finite = np.isfinite(tau) & np.isfinite(psurv) & np.isfinite(inten)
+    return {"spectral_model": label, "n_bins": n_bins, "mean_tau": float(np.mean(tau[finite])),
+            "max_tau": float(np.max(tau[finite])), "mean_Psurv": float(np.mean(psurv[finite])),
+            "integrated_intensity": float(np.sum(inten[finite])), "valid_pixels": int(np.count_nonzero(finite)),
+            "finite_outputs": bool(np.all(finite)), "positive_weights": True}
+
+
+def run_spectral(ctx: Context, sigma: SigmaTable, pixels: int = 32, precision: str = "fp64") -> tuple[list, dict]:
+    """The six images in one hadros_batch launch; returns (rows, launch stats)."""
+    table = spectral_cases()
+    cams = [spectral_params(m, n, pixels, precision) for m, n, _ in table]
+    outs = ctx.batch(cams, sigma, outputs=("tau", "P_surv", "I_obs", "fate", "steps"))
+    return [spectral_metrics(o, label, n) for (m, n, label), o in zip(table, outs)], ctx.stats()
+
+
+def write_spectral(rows: list[dict], outdir: Path) -> tuple[Path, Path]:
+    """spectral_validation.csv and .md as the script writes them (:254-293)."""
+    outdir.mkdir(parents=True, exist_ok=True)
+    csv_path = outdir / "spectral_validation.csv"
+    with csv_path.open("w", newline="") as f:
+        w = csv.DictWriter(f, fieldnames=list(rows[0].keys()))
+        w.writeheader()
+        w.writerows(rows)
+    finite_ok = all(bool(r["finite_outputs"]) for r in rows)
+    positive = all(float(r["integrated_intensity"]) >= 0.0 for r in rows)
+    conv = [float(r["integrated_intensity"]) for r in rows if str(r["spectral_model"]).startswith("powerlaw_cutoff_bins")]
+    rel_8_16 = abs(conv[1] - conv[2]) / max(abs(conv[2]), 1.0e-300)
+    lines = ["# UHE spectral validation", "", f"- finite_outputs: {finite_ok}",
+             f"- nonnegative_integrated_intensity: {positive}",
+             f"- powerlaw_cutoff convergence |I_8-I_16|/I_16: {rel_8_16:.6e}", "", "## Metrics", ""]
+    for r in rows:
+        lines.append(f"- {r['spectral_model']} bins={r['n_bins']}: mean_tau={float(r['mean_tau']):.6e}, "
+                     f"mean_Psurv={float(r['mean_Psurv']):.6e}, I={float(r['integrated_intensity']):.6e}")
+    md_path = outdir / "spectral_validation.md"
+    md_path.write_text("\n".join(lines) + "\n")
+    return csv_path, md_path
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(prog="python -m hadros_b200.robustness", description=__doc__,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--outdir", default="output/scans")
+    ap.add_argument("scan", nargs="?", choices=("robustness", "spectral"), default="robustness")
+    ap.add_argument("--outdir", default=None, help="default output/scans (robustness), output/spectra (spectral)")
     ap.add_argument("--sigma", default=None, help="sigma table (reference format); default: the synthetic table")
-    ap.add_argument("--pixels", type=int, default=16)
+    ap.add_argument("--pixels", type=int, default=None, help="image side (default 16 robustness, 32 spectral)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--write-dat", default=None, help="also write each case's .dat into this directory")
     ap.add_argument("--device", type=int, default=0)
@@ -253,9 +360,16 @@ def main(argv=None) -> int:
     else:
         E, g2, s = W.synthetic_sigma_arrays()
         sig = SigmaTable.from_arrays(E, s, g2)
+    if a.scan == "spectral":
+        with Context(a.device) as ctx:
+            rows, st = run_spectral(ctx, sig, a.pixels or SMALL_CACHE["pixels"], a.precision)
+        csv_path, md_path = write_spectral(rows, Path(a.outdir or "output/spectra"))
+        print(json.dumps({"images_per_launch": len(rows), "launches": st["launches"], "rays": st["rays"],
+                          "kernel_ms": st["kernel_ms"], "csv": str(csv_path), "md": str(md_path)}))
+        return 0
     with Context(a.device) as ctx:
-        rows, st = run(ctx, sig, a.pixels, a.precision, a.write_dat)
-    out = Path(a.outdir)
+        rows, st = run(ctx, sig, a.pixels or 16, a.precision, a.write_dat)
+    out = Path(a.outdir or "output/scans")
     csv_path = write_csv(rows, out)
     md_path = write_markdown(rows, out)
     print(json.dumps({"cases": len(rows), "cameras_per_launch": len(rows), "launches": st["launches"],

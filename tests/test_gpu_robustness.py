@@ -29,3 +29,21 @@ def test_scan_in_one_launch_matches_oracle_rows(hb, gpu_ctx, sigma_table, sigma_
     out = R.write_csv(rows, tmp_path)
     assert out.read_text().splitlines()[0].startswith("anomaly,aspin,cam_theta,case,")
     assert R.write_markdown(rows, tmp_path).read_text().startswith("# Robustness scan summary")
+
+
+def test_spectral_validation_in_one_launch_matches_oracle(hb, gpu_ctx, sigma_table, sigma_arrays, tmp_path):
+    from hadros_b200 import robustness as R
+    from oracle import pyoracle as O
+    E, _, s = sigma_arrays
+    rows, stats = R.run_spectral(gpu_ctx, sigma_table, pixels=8)
+    assert len(rows) == 6 and stats["launches"] == 1
+    for (model, n, label), got in zip(R.spectral_cases(), rows):
+        ref = R.spectral_metrics(O.oracle_image(R.spectral_params(model, n, pixels=8), E, s), label, n)
+        assert got["valid_pixels"] == ref["valid_pixels"] and got["finite_outputs"] == ref["finite_outputs"]
+        for k in ("mean_tau", "max_tau", "mean_Psurv", "integrated_intensity"):
+            assert got[k] == pytest.approx(ref[k], rel=1e-6, abs=1e-300), (label, k)
+    csv_path, md_path = R.write_spectral(rows, tmp_path)
+    assert csv_path.read_text().splitlines()[0] == ("spectral_model,n_bins,mean_tau,max_tau,mean_Psurv,"
+                                                    "integrated_intensity,valid_pixels,finite_outputs,"
+                                                    "positive_weights")
+    assert "powerlaw_cutoff convergence" in md_path.read_text()

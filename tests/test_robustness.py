@@ -1,8 +1,9 @@
 """hadros_b200.robustness: the reference's robustness scan
-(scripts/run_robustness_scans.py) through the C ABI.  CPU tests: the case
-table, the argv mapping, and our rows against the reference's own two
-executables run the way the script runs them (where oracle/build_ref.sh built
-them).  The GPU run is in test_gpu_robustness.py."""
+(scripts/run_robustness_scans.py) and spectral validation
+(scripts/validate_uhe_spectral_models.py) through the C ABI.  CPU tests: the
+case tables, the argv mapping, and our rows against the reference's own two
+executables run the way the scripts run them (where oracle/build_ref.sh built
+them).  The GPU runs are in test_gpu_robustness.py."""
 from __future__ import annotations
 
 import collections
@@ -107,3 +108,53 @@ def test_rows_equal_the_reference_executables(hb, tmp_path, sigma_arrays):
             for line in data:
                 k = int(line[1]) * 4 + int(line[0])
                 assert line[8 + c] == pytest.approx(ref[key][k], rel=1e-8, abs=1e-300), (case["case"], key)
+
+
+def test_spectral_table_and_params(hb):
+    from hadros_b200 import robustness as R
+    t = R.spectral_cases()
+    assert [x[2] for x in t] == ["monochromatic", "powerlaw", "powerlaw_cutoff", "powerlaw_cutoff_bins4",
+                                 "powerlaw_cutoff_bins8", "powerlaw_cutoff_bins16"]
+    p = R.spectral_params("powerlaw_cutoff", 16)
+    assert (p.nx, p.r_max_rg, p.h, p.a_spin, p.fov_deg) == (32, 40.0, 0.01, 0.0001, 25.0)
+    assert p.spectral_kind == 2 and p.n_bins == 16 and p.spec_e_min_GeV == 1.0e5 and p.spec_ecut_GeV == 1.0e12
+    assert p.rho0_gcm3 == 1.0 and p.envelope_rho0_gcm3 == 1.0e-2 and p.src_rho_ref_gcm3 == 1.0
+
+
+@pytest.mark.skipif(not (REF_GEO.exists() and REF_IMG.exists()), reason="reference executables not built here")
+def test_spectral_rows_equal_the_reference_executables(hb, tmp_path, sigma_arrays):
+    """validate_uhe_spectral_models.py's compute() + metrics() for the
+    powerlaw_cutoff case on a 4x4 small cache, against our row from the
+    oracle's outputs."""
+    from hadros_b200 import robustness as R
+    from hadros_b200 import workloads as W
+    from oracle import pyoracle as O
+    E, g2, s = sigma_arrays
+    sig = tmp_path / "sigma.dat"
+    W.write_sigma_file(sig, E, g2, s)
+    (tmp_path / "output" / "images").mkdir(parents=True)
+    cache = tmp_path / "small.bin"
+    r = subprocess.run([str(REF_GEO), "0.0001", "60.0", "80.0", "25.0", "4", "4", "40.0", "0.01", str(cache)],
+                       capture_output=True, text=True, timeout=600, env={"OMP_NUM_THREADS": "4"})
+    assert r.returncode == 0, r.stderr
+    v = dict(R.SPECTRAL_BASE, sigma_path=str(sig), cache=str(cache))
+    keys = ["enu", "a", "mbh", "rho0", "r0", "sigma", "h", "source_r", "source_sigma", "source_theta",
+            "source_powerlaw", "source_emax", "source_norm", "mev_enu", "mev_norm", "cam_theta", "sigma_path",
+            "profile", "radial_power", "funnel_depletion", "funnel_theta", "envelope_rho0", "envelope_alpha",
+            "r_min", "r_max", "rho_floor", "observer_distance", "use_f3", "cache", "source_model",
+            "source_funnel_theta", "source_q", "source_s", "source_grad_dr", "source_grad_dtheta",
+            "source_rho_ref", "source_cutoff_min", "source_cutoff_max"]
+    argv = [str(REF_IMG)] + [v[k] for k in keys] + ["powerlaw_cutoff", "2.0", "1.0e12", "1.0e5", "1.0e12", "4"]
+    r = subprocess.run(argv, cwd=tmp_path, capture_output=True, text=True, timeout=600,
+                       env={"OMP_NUM_THREADS": "4"})
+    assert r.returncode == 0, r.stderr
+    saved = [ln.split("Saved: ", 1)[1] for ln in r.stdout.splitlines() if ln.startswith("Saved: ")]
+    data = np.loadtxt(tmp_path / saved[0])
+    tau, psurv, inten = data[:, 4], data[:, 5], data[:, 6]
+    ours = R.spectral_metrics(O.oracle_image(R.spectral_params("powerlaw_cutoff", 4, pixels=4), E, s),
+                              "powerlaw_cutoff_bins4", 4)
+    assert ours["mean_tau"] == pytest.approx(np.mean(tau), rel=1e-12)
+    assert ours["max_tau"] == pytest.approx(np.max(tau), rel=1e-12)
+    assert ours["mean_Psurv"] == pytest.approx(np.mean(psurv), rel=1e-12)
+    assert ours["integrated_intensity"] == pytest.approx(np.sum(inten), rel=1e-12, abs=0.0)
+    assert ours["valid_pixels"] == 16 and ours["finite_outputs"]
