@@ -132,6 +132,81 @@ def reference_arm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def reference_cuda_arm(args) -> None:
+    """--impl reference-cuda: the reference's own GPU executable
+    (apps/compute_kerr_image_cuda.cu, built from its source by
+    oracle/build_ref.sh into oracle/_ref/compute_kerr_image_cuda) on the bench
+    camera with a monochromatic 1e9 GeV spectrum (the only kind it traces), next
+    to this library on the same image.  The reference runs twice: with its
+    Makefile launch settings (32x32 tiles, 128 steps per launch,
+    Makefile:208-209; at most 64x64 pixels, as that setting leaves all but 8 SMs
+    idle and needs minutes per 256x256 image) and with the whole image as one
+    tile and 1024 steps per launch, its best setting; its RKF45 tolerance is
+    set to the CPU image path's 1e-6, which this library uses.  Its own
+    printed timing is used (host clock around its tile loop and file writes,
+    rays/s).  Rank 0 only."""
+    import torch
+
+    import hadros_b200 as hb
+    from hadros_b200 import workloads as W
+    if env_int("RANK", 0) != 0:
+        return
+    exe = ROOT / "oracle" / "_ref" / "compute_kerr_image_cuda"
+    side = args.side or 256
+    kw = W.mixed_512(nx=side, ny=side, spectral="monochromatic", Enu_obs_GeV=1.0e9)
+    if not exe.exists():
+        print(json.dumps({"impl": "reference-cuda", "unavailable": "oracle/_ref/compute_kerr_image_cuda not built"}))
+        return
+    E, g2, s = W.synthetic_sigma_arrays()
+    f = lambda x: f"{x:.17g}"   # noqa: E731
+    argv = [f(kw["Enu_obs_GeV"]), f(kw["a_spin"]), f(kw["M_bh_msun"]), f(kw["rho0_gcm3"]), f(kw["r0_rg"]),
+            f(kw["sigma_r_rg"]), f(kw["H_over_R"]), f(kw["src_r_center_rg"]), f(kw["src_sigma_r_rg"]),
+            f(kw["src_theta_width_deg"]), f(kw["src_powerlaw"]), f(kw["src_emax_GeV"]), f(kw["src_norm"]),
+            "10", "1", f(kw["theta_obs_deg"]), f(kw["r_obs_rg"]), f(kw["fov_deg"]), str(side), str(side),
+            f(kw["r_max_rg"]), f(kw["h"])]
+    tail = ["200000", "1e-6", "powerlaw_funnel_envelope", f(kw["radial_power"]), f(kw["funnel_depletion"]),
+            f(kw["funnel_theta_deg"]), f(kw["envelope_rho0_gcm3"]), f(kw["envelope_alpha"]),
+            f(kw["torus_r_min_rg"]), f(kw["torus_r_max_rg"]), f(kw["rho_floor_gcm3"]), "funnel_wall",
+            f(kw["src_funnel_theta_deg"]), "1", "2", "0.1", "1", "-1", "0", "100"]
+    runs = {}
+    with tempfile.TemporaryDirectory() as td:
+        Path(td, "data", "sigma").mkdir(parents=True)
+        Path(td, "output", "images").mkdir(parents=True)
+        W.write_sigma_file(Path(td, "data", "sigma", "sigma_nuN_CC_GBW.dat"), E, g2, s)
+        small = min(side, 64)
+        for name, n, tile, spl in ((f"makefile_tiles_32_steps_128_{small}x{small}", small, 32, 128),
+                                   (f"one_tile_steps_1024_{side}x{side}", side, side, 1024)):
+            a = list(argv)
+            a[18] = a[19] = str(n)
+            r = subprocess.run([str(exe), *a, str(tile), str(spl), *tail], cwd=td, capture_output=True,
+                               text=True, timeout=1200)
+            line = next((ln for ln in r.stdout.splitlines() if ln.startswith("CUDA timing:")), "")
+            if r.returncode != 0 or not line:
+                runs[name] = {"failed": (r.stderr or r.stdout)[-300:]}
+                continue
+            parts = line.split()
+            runs[name] = {"seconds": float(parts[2]), "rays_per_s": float(parts[4]),
+                          "accepted_steps": int(line.rsplit("=", 1)[1]),
+                          "advance_launches": int(line.split("advance launches=")[1].split(",")[0])}
+    # this library on the same image (device-timed; default fast arithmetic)
+    sig = hb.SigmaTable.from_arrays(E, s, g2)
+    ours = {}
+    with hb.Context(0) as ctx:
+        for prec in ("fp64", "mixed"):
+            p = hb.params(**dict(kw, precision=prec))
+            ctx.image(p, sig, outputs=("steps",))            # warm-up
+            img = ctx.image(p, sig, outputs=("steps",))
+            st = ctx.stats()
+            ours[prec] = {"seconds": st["kernel_ms"] / 1e3, "rays_per_s": side * side / (st["kernel_ms"] / 1e3),
+                          "e2e_seconds": st["total_ms"] / 1e3, "accepted_steps": int(img["steps"].sum())}
+    line = {"impl": "reference-cuda", "metric": "rays/sec", "unit": "rays/s",
+            "config": {"workload": f"mixed_512 camera at {side}x{side}, monochromatic 1e9 GeV, "
+                                   "powerlaw_funnel_envelope, funnel_wall, RKF45 tol 1e-6"},
+            "reference_cuda": runs, "hadros_b200": ours,
+            "gpu": torch.cuda.get_device_name(0)}
+    print(json.dumps(line), flush=True)
+
+
 # --------------------------------------------------------------------------- clocks
 
 class ClockSampler:
@@ -513,12 +588,14 @@ def main() -> None:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", choices=["hadros", "reference"], default="hadros")
+    ap.add_argument("--impl", choices=["hadros", "reference", "reference-cuda"], default="hadros",
+                    help="reference: the reference CPU code (the contract's reference arm); reference-cuda: "
+                         "the reference's own GPU executable beside this library on one image")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["image", "surrogate"], default="image",
                     help="image: the trace kernel on mixed_512 (default); surrogate: the "
                          "surrogate inference kernel")
-    ap.add_argument("--side", type=int, default=None, help="surrogate workload: image side")
+    ap.add_argument("--side", type=int, default=None, help="surrogate workload / reference-cuda: image side")
     ap.add_argument("--bins", type=int, default=None, help="surrogate workload: bins")
     ap.add_argument("--mev", action="store_true",
                     help="image workload: also run the MeV thermal channel (the reference arm's CPU "
@@ -526,6 +603,8 @@ def main() -> None:
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.impl == "reference-cuda":
+        reference_cuda_arm(args)
     elif args.workload == "surrogate":
         surrogate_arm(args)
     else:

@@ -1,6 +1,6 @@
 #!/usr/bin/env bash
 # Builds oracle/_ref/libhadros_ref.so (and the reference's two cache
-# executables): the reference's own hot-path sources,
+# executables and its GPU executable): the reference's own hot-path sources,
 # compiled where they lie (read-only, unmodified) with the reference Makefile's
 # flags (-O3 -std=c++17 -fopenmp, no -march), plus oracle/ref_driver.cpp.
 # Test infrastructure only; outputs go to oracle/_ref/ (git-ignored).
@@ -26,4 +26,11 @@ g++ -O3 -std=c++17 -fopenmp -fPIC -shared -I"$ref/include" \
 for app in compute_kerr_geodesics compute_kerr_image_from_cache; do
     g++ -O3 -std=c++17 -fopenmp -I"$ref/include" -o "$out/$app" $srcs "$ref/apps/$app.cpp"
 done
+# the reference's own GPU executable (a single .cu, reference flags plus the
+# B200 target), for the reference-CUDA leg of bench.py
+if command -v nvcc >/dev/null 2>&1 || [ -x /usr/local/cuda/bin/nvcc ]; then
+    NVCC="$(command -v nvcc || echo /usr/local/cuda/bin/nvcc)"
+    "$NVCC" -O3 -std=c++17 -gencode arch=compute_100a,code=sm_100a \
+        -o "$out/compute_kerr_image_cuda" "$ref/apps/compute_kerr_image_cuda.cu"
+fi
 echo "built $out/libhadros_ref.so and reference cache executables"
