@@ -64,14 +64,21 @@ def env_int(name: str, default: int) -> int:
 
 # --------------------------------------------------------------------------- CPU baseline
 
-def cpu_sample(params_kw: dict, stride: int, threads: int) -> dict:
+def cpu_sample(params_kw: dict, stride: int, threads: int, mev_off: bool = False) -> dict:
     """Time the reference CPU implementation (oracle/_ref, or the oracle port)
-    on every `stride`-th pixel in i and j of the image."""
+    on every `stride`-th pixel in i and j of the image.  The reference always
+    runs its MeV block; mev_off=True gives it the cheapest setting the CPU app
+    accepts (MEV_MODEL toy with URCA, pair, bremsstrahlung, absorption and
+    scattering off: apps/compute_kerr_image_from_cache.cpp argv 45-51)."""
     import hadros_b200 as hb
     from hadros_b200 import workloads as W
     from oracle import pyoracle as O
     E, g2, s = W.synthetic_sigma_arrays()
-    p = hb.params(**params_kw)
+    kw = dict(params_kw)
+    if mev_off:
+        kw.update(mev_channel=1, mev_model="toy", mev_urca=False, mev_pair=False, mev_brems=False,
+                  mev_absorption=False, mev_scattering=False)
+    p = hb.params(**kw)
     ids = W.strided_pixels(p.nx, p.ny, stride)
     B = 1 if p.spectral_kind == 0 else p.n_bins
     kind = "reference" if O.ref_available() else "port"
@@ -82,7 +89,7 @@ def cpu_sample(params_kw: dict, stride: int, threads: int) -> dict:
         O.oracle_image(p, E, s, pixel_ids=ids, threads=threads)
     dt = time.perf_counter() - t0
     return {"value": ids.size * B / dt, "seconds": dt, "rays": int(ids.size), "kind": kind,
-            "cores": threads, "stride": stride}
+            "cores": threads, "stride": stride, "mev_off": mev_off}
 
 
 def describe_cpu(c: dict, nx: int, ny: int) -> str:
@@ -117,6 +124,7 @@ def reference_arm(args) -> None:
         times.append(last["seconds"])
     per_step = sum(times) / len(times)
     value = last["rays"] * kw["n_bins"] / per_step
+    off = cpu_sample(kw, stride, threads, mev_off=True)
     line = {
         "impl": "reference", "metric": "pixel-bins/sec", "value": value, "unit": "pixel-bins/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -125,7 +133,10 @@ def reference_arm(args) -> None:
         "config": {"workload": "mixed_512: " + WORKLOAD_DESC,
                    "sample": f"every {stride}th pixel in i and j ({last['rays']} rays) per step"},
         "cpu_baseline": {"value": value, "unit": "pixel-bins/s", "cores": threads,
-                         "kind": last["kind"], "sample": describe_cpu(last, 512, 512)},
+                         "kind": last["kind"], "sample": describe_cpu(last, 512, 512),
+                         "value_mev_off": off["value"],
+                         "mev_off": "the same sample with the MeV block at its cheapest setting "
+                                    "(toy model, five terms off)"},
         "e2e": {"value": value, "unit": "pixel-bins/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -419,6 +430,10 @@ def gpu_arm(args) -> None:
         c = cpu_sample(kw, 24, host_threads())
         cpu = {"value": c["value"], "unit": "pixel-bins/s", "cores": c["cores"], "kind": c["kind"],
                "sample": describe_cpu(c, p.nx, p.ny)}
+        if not args.mev and c["kind"] == "reference":   # the like-for-like figure for a UHE-only GPU line
+            cpu["value_mev_off"] = cpu_sample(kw, 24, host_threads(), mev_off=True)["value"]
+            cpu["mev_off"] = ("the same sample with the reference's MeV block at its cheapest setting "
+                              "(toy model, five terms off)")
     total_steps = sum_over_ranks(steps_sum)
     if rank == 0:
         line = {
