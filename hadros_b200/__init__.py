@@ -218,16 +218,17 @@ def pack_paths(points: np.ndarray, npoints: np.ndarray) -> np.ndarray:
                           [np.zeros((0, 7))])
 
 
-def write_kgeo(path, p: HadrosParams, npoints, points, pixel_ids=None, fate=None) -> None:
-    """KGEO geodesic cache file (the reference's compute_kerr_geodesics format)."""
+def write_kgeo(path, p: HadrosParams, npoints, points, pixel_ids=None, fate=None, append: bool = False) -> None:
+    """KGEO geodesic cache file (the reference's compute_kerr_geodesics format);
+    append=True adds the rays to an existing file (batched writing)."""
     n = np.ascontiguousarray(npoints, dtype=np.int32)
     pts = np.ascontiguousarray(points, dtype=np.float64)
     ids = None if pixel_ids is None else np.ascontiguousarray(pixel_ids, dtype=np.int32)
     fa = None if fate is None else np.ascontiguousarray(fate, dtype=np.int8)
-    _check(lib().hadros_write_kgeo(str(path).encode(), C.byref(p), int(n.size),
-                                   None if ids is None else ids.ctypes.data,
-                                   None if fa is None else fa.ctypes.data, n.ctypes.data,
-                                   pts.ctypes.data if pts.size else None))
+    _check(lib().hadros_write_kgeo_rays(str(path).encode(), C.byref(p), int(n.size),
+                                        None if ids is None else ids.ctypes.data,
+                                        None if fa is None else fa.ctypes.data, n.ctypes.data,
+                                        pts.ctypes.data if pts.size else None, 1 if append else 0))
 
 
 def read_kgeo(path) -> dict:

@@ -239,6 +239,8 @@ SIGNATURES = {
                                           C.c_void_p, C.c_void_p, C.c_void_p, P(HadrosImageOut)]),
     "hadros_write_kgeo": (C.c_int32, [C.c_char_p, P(HadrosParams), C.c_int32, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p]),
+    "hadros_write_kgeo_rays": (C.c_int32, [C.c_char_p, P(HadrosParams), C.c_int32, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_int32]),
     "hadros_kgeo_info": (C.c_int32, [C.c_char_p, P(C.c_int32), P(C.c_int32), P(C.c_double),
                                      P(C.c_int32), P(C.c_int64)]),
     "hadros_read_kgeo": (C.c_int32, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -33,6 +33,22 @@
 // Writes DIR/<name>.bin (KIMG) and DIR/<name>.dat with the reference's file
 // name (apps/compute_kerr_image_cuda.cu:2108-2128) and prints the reference's
 // "Saved:" and "CUDA timing:" lines.  Errors go to stderr with exit code 1.
+//
+// The reference executable's two cache modes (:1624-2200) are here too:
+//   --geodesic-cache ASPIN CAM_R_OBS CAM_THETA_DEG CAM_FOV_DEG CAM_NX CAM_NY
+//       CAM_R_MAX CAM_STEP GPU_CACHE_RAYS GPU_CACHE_MAX_POINTS GPU_TOL
+//     traces every pixel, keeps at most GPU_CACHE_MAX_POINTS points per ray (a
+//     ray that reaches the limit stops there, uncaptured), and writes the KGEO
+//     cache output/rays/kerr_geodesics_cuda.bin; exit code 2 when a ray was
+//     cut, as the reference does;
+//   --image-from-cache ENU ASPIN MBH_MSUN TORUS_RHO0 TORUS_R0 TORUS_SIGMA
+//       TORUS_H_OVER_R SOURCE_R SOURCE_SIGMA SOURCE_THETA_DEG SOURCE_POWERLAW
+//       SOURCE_EMAX SOURCE_NORM MEV_ENU MEV_NORM CAM_THETA_DEG GPU_CACHE_RAYS
+//       [PROFILE ... SOURCE_CUTOFF_MAX, the in-line mode's arguments 27-44]
+//     transfers over that cache (FP64) and writes
+//     kerr_image_cuda_cache_rho0_torus_....{bin,dat}.
+// GPU_CACHE_RAYS only sizes the reference's batches; here batches are sized by
+// memory.  GPU_TOL defaults to 1e-6 as in the in-line mode.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -122,6 +138,217 @@ bool mev_option(hadros_params& p, const std::string& key, const std::string& val
 
 }  // namespace
 
+double num(const std::vector<std::string>& pos, size_t k, double def)
+{
+    return pos.size() > k ? std::atof(pos[k].c_str()) : def;
+}
+
+// --geodesic-cache (apps/compute_kerr_image_cuda.cu:1624-1824)
+int geodesic_cache(const std::vector<std::string>& pos, int device)
+{
+    hadros_params p;
+    hadros_params_default(&p);
+    p.a_spin = num(pos, 0, 0.9);
+    p.r_obs_rg = num(pos, 1, 60.0);
+    p.theta_obs_rad = num(pos, 2, 80.0) * PI / 180.0;
+    p.fov_deg = num(pos, 3, 25.0);
+    p.nx = pos.size() > 4 ? std::atoi(pos[4].c_str()) : 100;
+    p.ny = pos.size() > 5 ? std::atoi(pos[5].c_str()) : 100;
+    p.r_max_rg = num(pos, 6, 120.0);
+    p.h = num(pos, 7, 0.001);
+    const int cache_rays = pos.size() > 8 ? std::atoi(pos[8].c_str()) : 32;
+    const int max_points = pos.size() > 9 ? std::atoi(pos[9].c_str()) : 50000;
+    p.tolerance = num(pos, 10, 1.0e-6);
+    if (p.nx <= 0 || p.ny <= 0 || cache_rays <= 0 || max_points <= 0) {
+        std::fprintf(stderr, "Usage: compute_kerr_image --geodesic-cache ASPIN CAM_R_OBS CAM_THETA_DEG "
+                             "CAM_FOV_DEG CAM_NX CAM_NY CAM_R_MAX CAM_STEP GPU_CACHE_RAYS "
+                             "GPU_CACHE_MAX_POINTS GPU_TOL\n");
+        return 1;
+    }
+    // a ray stops at its max_points-th point (trace_cache_kernel, :1478-1535)
+    if (max_points < p.max_steps) p.max_steps = max_points;
+    if (hadros_params_validate(&p)) return die("parameters");
+    hadros_ctx* ctx = nullptr;
+    if (hadros_ctx_create(device, &ctx)) return die("CUDA");
+    const int64_t total = static_cast<int64_t>(p.nx) * p.ny;
+    // batches of whole rays within ~512 MiB of path buffer
+    int64_t batch = (512ll << 20) / (static_cast<int64_t>(max_points) * 56);
+    if (batch < cache_rays) batch = cache_rays;
+    if (batch > total) batch = total;
+    if (batch < 1) batch = 1;
+    std::printf("Geodesic cache grid: %d x %d\nBatch rays: %lld, max points/ray: %d, RKF45 tol: %g\n", p.nx,
+                p.ny, static_cast<long long>(batch), max_points, p.tolerance);
+    const std::string path = "output/rays/kerr_geodesics_cuda.bin";
+    std::vector<double> buf(static_cast<size_t>(batch) * max_points * 7), packed;
+    std::vector<int32_t> ids(static_cast<size_t>(batch)), npts(static_cast<size_t>(batch));
+    std::vector<int8_t> fate(static_cast<size_t>(batch));
+    int64_t total_points = 0, truncated = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int64_t start = 0; start < total; start += batch) {
+        const int32_t n = static_cast<int32_t>(std::min<int64_t>(batch, total - start));
+        for (int32_t k = 0; k < n; ++k) {   // ray id = i * ny + j (init_linear_rays_kernel, :1412-1430)
+            const int64_t id = start + k;
+            const int32_t i = static_cast<int32_t>(id / p.ny), j = static_cast<int32_t>(id % p.ny);
+            ids[k] = j * p.nx + i;
+        }
+        if (hadros_trace_paths(ctx, &p, ids.data(), n, max_points, buf.data(), npts.data(), fate.data()))
+            return die("trace");
+        packed.clear();
+        for (int32_t k = 0; k < n; ++k) {
+            const double* q = buf.data() + static_cast<size_t>(k) * max_points * 7;
+            packed.insert(packed.end(), q, q + static_cast<size_t>(npts[k]) * 7);
+            total_points += npts[k];
+            if (npts[k] >= max_points && fate[k] != HADROS_FATE_CAPTURED) ++truncated;
+        }
+        if (hadros_write_kgeo_rays(path.c_str(), &p, n, ids.data(), fate.data(), npts.data(),
+                                   packed.empty() ? nullptr : packed.data(), start > 0 ? 1 : 0))
+            return die("write");
+    }
+    const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::printf("Saved: %s\nCached points: %lld\nGeodesic GPU timing: %g s, %g rays/s\n", path.c_str(),
+                static_cast<long long>(total_points), elapsed,
+                static_cast<double>(total) / std::max(elapsed, 1.0e-300));
+    hadros_ctx_destroy(ctx);
+    if (truncated > 0) {   // :1811-1820
+        std::fprintf(stderr, "ERROR: %lld rays reached GPU_CACHE_MAX_POINTS. Do not use this cache for science. "
+                             "Increase GPU_CACHE_MAX_POINTS or CAM_STEP, then regenerate %s.\n",
+                     static_cast<long long>(truncated), path.c_str());
+        return 2;
+    }
+    return 0;
+}
+
+// --image-from-cache (apps/compute_kerr_image_cuda.cu:1826-2200): the
+// in-line mode's physics over the cached paths, FP64, with the MeV channel.
+int image_from_cache(const std::vector<std::string>& pos, int device, const std::string& sigma_path,
+                     const std::string& outdir, hadros_params p)
+{
+    // defaults of run_image_from_cache_gpu (:1830-1868)
+    p.Enu_obs_GeV = num(pos, 0, 1.0e9);
+    p.a_spin = num(pos, 1, 0.9);
+    p.M_bh_msun = num(pos, 2, 3.0);
+    p.rho0_gcm3 = num(pos, 3, 1.0e-2);
+    p.r0_rg = num(pos, 4, 10.0);
+    p.sigma_r_rg = num(pos, 5, 5.0);
+    p.H_over_R = num(pos, 6, 0.25);
+    p.src_r_center_rg = num(pos, 7, 3.5);
+    p.src_sigma_r_rg = num(pos, 8, 1.0);
+    p.src_theta_width_rad = num(pos, 9, 15.0) * PI / 180.0;
+    p.src_powerlaw = num(pos, 10, 2.0);
+    p.src_emax_GeV = num(pos, 11, 1.0e12);
+    p.src_norm = num(pos, 12, 1.0);
+    p.mev_Enu_obs_MeV = num(pos, 13, 10.0);
+    p.mev_norm = num(pos, 14, 1.0);
+    p.theta_obs_rad = num(pos, 15, 80.0) * PI / 180.0;
+    const int chunk = pos.size() > 16 ? std::atoi(pos[16].c_str()) : 256;
+    if (pos.size() > 17 && hadros_parse_profile(pos[17].c_str(), &p.profile_kind)) return die("profile");
+    p.radial_power = num(pos, 18, 2.0);
+    p.funnel_depletion = num(pos, 19, 0.0);
+    p.funnel_theta_rad = num(pos, 20, 15.0) * PI / 180.0;
+    p.envelope_rho0_gcm3 = num(pos, 21, 0.0);
+    p.envelope_alpha = num(pos, 22, 2.5);
+    p.torus_r_min_rg = num(pos, 23, 4.0);
+    p.torus_r_max_rg = num(pos, 24, 60.0);
+    p.rho_floor_gcm3 = num(pos, 25, 1.0e-99);
+    if (pos.size() > 26 && hadros_parse_source(pos[26].c_str(), &p.source_kind)) return die("source model");
+    p.src_funnel_theta_rad = num(pos, 27, 20.0) * PI / 180.0;
+    p.src_density_power_q = num(pos, 28, 1.0);
+    p.src_radial_power_s = num(pos, 29, 2.0);
+    p.src_gradient_dr_rg = num(pos, 30, 0.1);
+    p.src_gradient_dtheta_rad = num(pos, 31, 1.0) * PI / 180.0;
+    p.src_rho_ref_gcm3 = num(pos, 32, -1.0);
+    p.src_cutoff_min = num(pos, 33, 0.0);
+    p.src_cutoff_max = num(pos, 34, 1.0e2);
+    if (chunk <= 0) {
+        std::fprintf(stderr, "Usage: compute_kerr_image --image-from-cache ENU ASPIN MBH_MSUN TORUS_RHO0 TORUS_R0 "
+                             "TORUS_SIGMA TORUS_H_OVER_R SOURCE_R SOURCE_SIGMA SOURCE_THETA_DEG SOURCE_POWERLAW "
+                             "SOURCE_EMAX SOURCE_NORM MEV_ENU MEV_NORM CAM_THETA_DEG GPU_CACHE_RAYS [PROFILE "
+                             "RADIAL_POWER FUNNEL_DEPLETION FUNNEL_THETA_DEG ENVELOPE_RHO0 ENVELOPE_ALPHA R_MIN "
+                             "R_MAX RHO_FLOOR SOURCE_MODEL SOURCE_FUNNEL_THETA_DEG SOURCE_DENSITY_Q "
+                             "SOURCE_RADIAL_S SOURCE_GRADIENT_DR SOURCE_GRADIENT_DTHETA_DEG]\n");
+        return 1;
+    }
+    p.spectral_kind = HADROS_SPECTRAL_MONOCHROMATIC;
+    p.precision = HADROS_PRECISION_FP64;
+    const std::string path = "output/rays/kerr_geodesics_cuda.bin";
+    int32_t nx = 0, ny = 0, n_rays = 0;
+    double cache_a = 0.0;
+    int64_t n_points = 0;
+    if (hadros_kgeo_info(path.c_str(), &nx, &ny, &cache_a, &n_rays, &n_points)) return die("cache");
+    p.nx = nx;
+    p.ny = ny;
+    if (std::fabs(cache_a - p.a_spin) > 1.0e-12)   // :1970-1975
+        std::fprintf(stderr, "Warning: cache spin a=%g differs from requested ASPIN=%g\n", cache_a, p.a_spin);
+    if (hadros_params_validate(&p)) return die("parameters");
+    std::vector<int32_t> pid(static_cast<size_t>(n_rays)), npts(static_cast<size_t>(n_rays));
+    std::vector<int8_t> captured(static_cast<size_t>(n_rays)), fate(static_cast<size_t>(n_rays));
+    std::vector<double> alpha(static_cast<size_t>(n_rays)), beta(static_cast<size_t>(n_rays));
+    std::vector<double> pts(static_cast<size_t>(n_points) * 7 + 1);
+    if (hadros_read_kgeo(path.c_str(), pid.data(), captured.data(), npts.data(), alpha.data(), beta.data(),
+                         pts.data()))
+        return die("cache");
+    for (int32_t k = 0; k < n_rays; ++k) fate[k] = captured[k] ? HADROS_FATE_CAPTURED : HADROS_FATE_ESCAPED;
+    hadros_sigma* sig = nullptr;
+    if (hadros_sigma_load(sigma_path.c_str(), &sig)) return die("sigma table");
+    hadros_ctx* ctx = nullptr;
+    if (hadros_ctx_create(device, &ctx)) return die("CUDA");
+    std::vector<double> r_tau(static_cast<size_t>(n_rays)), r_P(static_cast<size_t>(n_rays)),
+        r_I(static_cast<size_t>(n_rays)), r_mev[5];
+    for (auto& v : r_mev) v.resize(static_cast<size_t>(n_rays));
+    hadros_image_out ro{};
+    ro.tau = r_tau.data();
+    ro.P_surv = r_P.data();
+    ro.I_obs = r_I.data();
+    ro.tau_mev = r_mev[0].data();
+    ro.P_surv_mev = r_mev[1].data();
+    ro.I_obs_mev = r_mev[2].data();
+    ro.r_nu = r_mev[3].data();
+    ro.leakage = r_mev[4].data();
+    const auto t0 = std::chrono::steady_clock::now();
+    if (hadros_transfer_paths(ctx, &p, sig, n_rays, npts.data(), fate.data(), pts.data(), &ro))
+        return die("transfer");
+    const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    // rays in cache order -> pixel rows j*nx+i (a pixel missing from the cache keeps the defaults)
+    const size_t P = static_cast<size_t>(nx) * ny;
+    std::vector<double> tau(P, 0.0), Ps(P, 1.0), I(P, 0.0), mev[5];
+    const double mev_def[5] = {0.0, 1.0, 0.0, -1.0, 1.0};
+    for (int c = 0; c < 5; ++c) mev[c].assign(P, mev_def[c]);
+    std::vector<int8_t> pfate(P, HADROS_FATE_ESCAPED);
+    for (int32_t k = 0; k < n_rays; ++k) {
+        const size_t q = static_cast<size_t>(pid[k]);
+        if (q >= P) continue;
+        tau[q] = r_tau[k];
+        Ps[q] = r_P[k];
+        I[q] = r_I[k];
+        pfate[q] = fate[k];
+        for (int c = 0; c < 5; ++c) mev[c][q] = r_mev[c][k];
+    }
+    hadros_image_out out{};
+    out.tau = tau.data();
+    out.P_surv = Ps.data();
+    out.I_obs = I.data();
+    out.fate = pfate.data();
+    out.tau_mev = mev[0].data();
+    out.P_surv_mev = mev[1].data();
+    out.I_obs_mev = mev[2].data();
+    out.r_nu = mev[3].data();
+    out.leakage = mev[4].data();
+    char name[512];   // the in-line name with "cache_" after "kerr_image_cuda_" (:2110-2126)
+    if (hadros_image_filename(&p, 0, nullptr, p.mev_Enu_obs_MeV, p.mev_norm, "", name, sizeof(name)))
+        return die("file name");
+    const std::string stem = std::string("kerr_image_cuda_cache_") + (name + std::strlen("kerr_image_cuda_"));
+    const std::string bin_path = outdir + "/" + stem + ".bin", dat_path = outdir + "/" + stem + ".dat";
+    if (hadros_write_kimg_mev(bin_path.c_str(), &p, &out)) return die("write");
+    if (hadros_write_dat_mev(dat_path.c_str(), &p, "GBW", &out)) return die("write");
+    std::printf("Cache grid: %d x %d\nLoaded rays: %d\nSaved: %s\nSaved: %s\n", nx, ny, n_rays, bin_path.c_str(),
+                dat_path.c_str());
+    std::printf("CUDA cache image timing: %g s, %g rays/s\n", elapsed,
+                static_cast<double>(n_rays) / std::max(elapsed, 1.0e-300));
+    hadros_ctx_destroy(ctx);
+    hadros_sigma_destroy(sig);
+    return 0;
+}
+
 int main(int argc, char** argv)
 {
     std::vector<std::string> pos;
@@ -129,7 +356,7 @@ int main(int argc, char** argv)
     std::string sigma_path = "data/sigma/sigma_nuN_CC_GBW.dat", outdir = "output/images";
     std::string spectral, precision;
     double gamma = NAN, ecut = NAN, emin = NAN, emax = NAN;
-    int nbins = -1, device = 0;
+    int nbins = -1, device = 0, mode = 0;
     for (int k = 1; k < argc; ++k) {
         std::string a(argv[k]);
         if (a.rfind("--", 0) == 0) {
@@ -147,12 +374,15 @@ int main(int argc, char** argv)
             else if (key == "nbins") nbins = std::atoi(val.c_str());
             else if (key == "device") device = std::atoi(val.c_str());
             else if (key == "help") { usage(argv[0]); return 0; }
+            else if (key == "geodesic-cache") mode = 1;
+            else if (key == "image-from-cache") mode = 2;
             else if (key.rfind("mev", 0) == 0) mev_opts.emplace_back(key, val);
             else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); usage(argv[0]); return 1; }
         } else {
             pos.push_back(a);
         }
     }
+    if (mode == 1) return geodesic_cache(pos, device);
     auto has = [&](size_t i) { return pos.size() >= i; };
     auto f = [&](size_t i) { return std::atof(pos[i - 1].c_str()); };
     auto n = [&](size_t i) { return std::atoi(pos[i - 1].c_str()); };
@@ -178,6 +408,17 @@ int main(int argc, char** argv)
     p.max_steps = 200000;
     int tile = 32, steps_per_launch = 128;
 
+    if (mode == 2) {   // the cached-image mode: its own positional order, the named MeV options
+        for (const auto& kv : mev_opts) {
+            bool bad = false;
+            if (!mev_option(p, kv.first, kv.second, &bad)) {
+                std::fprintf(stderr, "unknown option --%s\n", kv.first.c_str());
+                return 1;
+            }
+            if (bad) return die("MeV channel");
+        }
+        return image_from_cache(pos, device, sigma_path, outdir, p);
+    }
     if (has(1)) p.Enu_obs_GeV = f(1);
     if (has(2)) p.a_spin = f(2);
     if (has(3)) p.M_bh_msun = f(3);

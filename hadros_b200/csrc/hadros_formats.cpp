@@ -305,13 +305,21 @@ int32_t hadros_write_kimg_mev(const char* path, const hadros_params* p, const ha
 int32_t hadros_write_kgeo(const char* path, const hadros_params* p, int32_t n_rays, const int32_t* pixel_ids,
                           const int8_t* fate, const int32_t* npoints, const double* points)
 {
+    return hadros_write_kgeo_rays(path, p, n_rays, pixel_ids, fate, npoints, points, 0);
+}
+
+int32_t hadros_write_kgeo_rays(const char* path, const hadros_params* p, int32_t n_rays, const int32_t* pixel_ids,
+                               const int8_t* fate, const int32_t* npoints, const double* points, int32_t append)
+{
     if (!path || !kinds_ok(p) || n_rays < 0 || (n_rays > 0 && (!npoints || !points)))
         return ferr(HADROS_E_ARG, "bad argument");
-    FILE* f = std::fopen(path, "wb");
+    FILE* f = std::fopen(path, append ? "ab" : "wb");
     if (!f) return ferr(HADROS_E_IO, std::string("Could not open ") + path);
-    const int32_t hdr[4] = {0x4B47454F, 1, p->nx, p->ny};
-    std::fwrite(hdr, sizeof(hdr), 1, f);
-    std::fwrite(&p->a_spin, sizeof(double), 1, f);
+    if (!append) {
+        const int32_t hdr[4] = {0x4B47454F, 1, p->nx, p->ny};
+        std::fwrite(hdr, sizeof(hdr), 1, f);
+        std::fwrite(&p->a_spin, sizeof(double), 1, f);
+    }
     int64_t off = 0;
     for (int32_t k = 0; k < n_rays; ++k) {
         const int32_t pid = pixel_ids ? pixel_ids[k] : k;

@@ -529,6 +529,12 @@ int32_t hadros_write_kimg_mev(const char* path, const hadros_params* p, const ha
 int32_t hadros_write_kgeo(const char* path, const hadros_params* p, int32_t n_rays,
                           const int32_t* pixel_ids, const int8_t* fate,
                           const int32_t* npoints, const double* points);
+/* The same rays written in batches, as the reference's cache writers stream
+ * them (apps/compute_kerr_image_cuda.cu:1718-1780): append = 0 creates the
+ * file with its header, append = 1 adds rays to it. */
+int32_t hadros_write_kgeo_rays(const char* path, const hadros_params* p, int32_t n_rays,
+                               const int32_t* pixel_ids, const int8_t* fate,
+                               const int32_t* npoints, const double* points, int32_t append);
 /* First pass: sizes of a KGEO file (reference read loop,
  * apps/compute_kerr_image_from_cache.cpp:374-406, :655-707). */
 int32_t hadros_kgeo_info(const char* path, int32_t* nx, int32_t* ny, double* a_spin,

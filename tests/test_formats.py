@@ -193,3 +193,23 @@ def test_cli_usage_and_errors():
                         "1e12", "1", "10", "1", "80", "60", "25", "4", "4", "120", "0.01", "32", "128",
                         "200000", "1e-6", "no_such_profile"], capture_output=True, text=True)
     assert r.returncode == 1 and "Unknown density profile 'no_such_profile'" in r.stderr
+
+
+def test_cli_cache_modes_usage_and_errors(tmp_path):
+    """--geodesic-cache and --image-from-cache (the reference executable's
+    cache modes) reject what the reference rejects, before any GPU work."""
+    cli = ROOT / "hadros_b200" / "bin" / "compute_kerr_image"
+    if not cli.exists():
+        pytest.skip("CLI not built")
+    r = subprocess.run([str(cli), "--geodesic-cache", "0.9", "60", "80", "25", "0", "4"], capture_output=True,
+                       text=True, cwd=tmp_path)
+    assert r.returncode == 1 and "--geodesic-cache ASPIN CAM_R_OBS" in r.stderr
+    r = subprocess.run([str(cli), "--image-from-cache", "1e9", "0.9", "3", "1e-2", "10", "5", "0.25", "3.5", "1",
+                        "15", "2", "1e12", "1", "10", "1", "80", "0"], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 1 and "--image-from-cache ENU ASPIN" in r.stderr
+    r = subprocess.run([str(cli), "--image-from-cache", "1e9"], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 1 and "output/rays/kerr_geodesics_cuda.bin" in r.stderr
+    r = subprocess.run([str(cli), "--image-from-cache", "1e9", "--mev=bogus"], capture_output=True, text=True,
+                       cwd=tmp_path)
+    assert r.returncode == 1 and "Unknown MEV_MODEL 'bogus'" in r.stderr
+

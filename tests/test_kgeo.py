@@ -61,6 +61,22 @@ def test_kgeo_roundtrip(hb, tmp_path):
     assert d["alpha"][4] == (2.0 * (1 + 0.5) / 3 - 1.0) * t
 
 
+def test_kgeo_written_in_batches_equals_one_write(hb, tmp_path):
+    """hadros_write_kgeo_rays: a file written in three batches (header with
+    the first) has the bytes of the single write."""
+    p = hb.params(nx=3, ny=2, a_spin=0.7)
+    n = np.array([2, 0, 3, 1, 0, 4], np.int32)
+    pts = np.random.default_rng(2).normal(size=(int(n.sum()), 7))
+    fate = np.array([1, 0, 0, 2, 1, 0], np.int8)
+    one, parts = tmp_path / "one.bin", tmp_path / "parts.bin"
+    hb.write_kgeo(one, p, n, pts, fate=fate)
+    off = np.concatenate([[0], np.cumsum(n)])
+    for b, (lo, hi) in enumerate(((0, 2), (2, 3), (3, 6))):
+        hb.write_kgeo(parts, p, n[lo:hi], pts[off[lo]:off[hi]], pixel_ids=np.arange(lo, hi, dtype=np.int32),
+                      fate=fate[lo:hi], append=b > 0)
+    assert parts.read_bytes() == one.read_bytes()
+
+
 def test_kgeo_errors(hb, tmp_path):
     p = hb.params(nx=2, ny=1)
     f = tmp_path / "c.bin"
