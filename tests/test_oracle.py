@@ -127,3 +127,39 @@ def test_oracle_vs_reference_live_random(hb, sigma_arrays):
         b = O.ref_image(p, E, g2, s)
         for f in FIELDS:
             np.testing.assert_array_equal(a[f], b[f], err_msg=f"case {k}: {f}")
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference not built here (oracle/build_ref.sh)")
+def test_oracle_mev_channel_vs_reference_live_random(hb, sigma_arrays):
+    """Seeded random MeV settings (model, flavor, profiles, band, switches,
+    temperatures and Ye bounds) on random small cameras: the oracle's MeV
+    channel == the reference's, bit for bit."""
+    from hadros_b200 import workloads as W
+    E, g2, s = sigma_arrays
+    rng = np.random.default_rng(23)
+    names = dict(mev_thermal=["constant", "inner_hot_torus", "radial_powerlaw", "torus_plus_cool_envelope",
+                              "collapsar_inner_hot"],
+                 mev_ye=["constant", "neutron_rich_torus", "funnel_proton_rich", "torus_envelope_contrast",
+                         "collapsar_neutron_rich"],
+                 mev_flavor=["nu_e", "anti_nu_e", "nu_x"], mev_model=["toy", "physical"],
+                 mev_spectral=["monochromatic", "fermi_dirac_band"])
+    switches = ["urca", "pair", "brems", "absorption", "scattering", "degeneracy_correction", "abs_n", "abs_p",
+                "scat_n", "scat_p", "scat_e"]
+    for k in range(8):
+        kw = W.mixed_512(nx=3, ny=2, precision="fp64", h=float(rng.uniform(0.03, 0.08)),
+                         a_spin=float(rng.uniform(0.0, 0.998)), theta_obs_deg=float(rng.uniform(5.0, 85.0)),
+                         profile=int(rng.integers(0, 8)), source=int(rng.integers(0, 5)),
+                         spectral=int(rng.integers(0, 3)), n_bins=int(rng.integers(1, 6)),
+                         rho0_gcm3=float(10.0 ** rng.uniform(8, 12)), mev_channel=1,
+                         mev_n_bins=int(rng.integers(1, 7)), mev_T0_MeV=float(rng.uniform(1.0, 15.0)),
+                         mev_T_floor_MeV=float(rng.uniform(0.01, 0.5)), mev_T_power=float(rng.uniform(0.0, 1.0)),
+                         mev_Ye_floor=float(rng.uniform(0.0, 0.2)), mev_Ye_ceil=float(rng.uniform(0.4, 1.0)),
+                         mev_Enu_obs_MeV=float(rng.uniform(3.0, 40.0)),
+                         mev_E_min_MeV=float(rng.uniform(1.0, 5.0)), mev_E_max_MeV=float(rng.uniform(20.0, 80.0)),
+                         **{key: str(rng.choice(v)) for key, v in names.items()},
+                         **{f"mev_{sw}": bool(rng.integers(0, 2)) for sw in switches})
+        p = hb.params(**kw)
+        a = O.oracle_image(p, E, s, mev=True)
+        b = O.ref_image(p, E, g2, s, mev=True)
+        for f in O.MEV_KEYS:
+            np.testing.assert_array_equal(a[f], b[f], err_msg=f"case {k}: {f}")
