@@ -25,7 +25,6 @@ import argparse
 import csv
 import io
 import json
-import math
 import os
 import statistics
 import subprocess

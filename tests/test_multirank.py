@@ -11,7 +11,6 @@ import sys
 from pathlib import Path
 
 import numpy as np
-import pytest
 import torch.multiprocessing as mp
 
 ROOT = Path(__file__).resolve().parent.parent
