@@ -184,3 +184,39 @@ def test_context_without_gpu_reports_cuda_error(hb):
     with pytest.raises(hb.HadrosError) as e:
         hb.Context(0)
     assert e.value.status == 3
+
+
+def test_ctypes_layouts_match_the_c_header(hb, tmp_path):
+    """Every field of every struct in include/hadros_b200.h sits at the same
+    offset (and every struct has the same size) in hadros_b200/abi.py: a C
+    program compiled against the header prints them."""
+    import shutil
+    import subprocess
+    from conftest import ROOT
+    from hadros_b200 import abi
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = {"hadros_params": abi.HadrosParams, "hadros_image_out": abi.HadrosImageOut,
+               "hadros_stats": abi.HadrosStats, "hadros_schedule": abi.HadrosSchedule,
+               "hadros_mlp_norm": abi.HadrosMlpNorm, "hadros_adam": abi.HadrosAdam,
+               "hadros_surrogate_out": abi.HadrosSurrogateOut}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "hadros_b200.h"', "int main(void) {"]
+    for name, cls in structs.items():
+        lines.append(f'  printf("{name} sizeof %zu\\n", sizeof({name}));')
+        for field, _ in cls._fields_:
+            lines.append(f'  printf("{name} {field} %zu\\n", offsetof({name}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(ROOT / "include"), "-o", str(exe), str(src)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        name, field, value = line.split()
+        got[(name, field)] = int(value)
+    for name, cls in structs.items():
+        assert got[(name, "sizeof")] == C.sizeof(cls), name
+        for field, _ in cls._fields_:
+            assert got[(name, field)] == getattr(cls, field).offset, (name, field)
+
