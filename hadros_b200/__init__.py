@@ -296,7 +296,9 @@ class Context:
 
     def image(self, p: HadrosParams, sigma: SigmaTable, pixel_ids=None,
               outputs=OUTPUTS) -> dict:
-        """Trace an image (or a pixel list) into host numpy arrays."""
+        """Trace an image (or a pixel list) into host numpy arrays; the default
+        outputs gain tau_mev, P_surv_mev, I_obs_mev, r_nu and leakage when
+        p.mev_channel is set."""
         outputs = _with_mev(outputs, [p])
         B = n_bins_of(p)
         P = int(p.nx) * int(p.ny) if pixel_ids is None else len(pixel_ids)
