@@ -313,6 +313,11 @@ int32_t hadros_write_kgeo_rays(const char* path, const hadros_params* p, int32_t
 {
     if (!path || !kinds_ok(p) || n_rays < 0 || (n_rays > 0 && (!npoints || !points)))
         return ferr(HADROS_E_ARG, "bad argument");
+    if (append) {   // rays only go after a header: the file must exist
+        FILE* g = std::fopen(path, "rb");
+        if (!g) return ferr(HADROS_E_IO, std::string("No KGEO file to append to: ") + path);
+        std::fclose(g);
+    }
     FILE* f = std::fopen(path, append ? "ab" : "wb");
     if (!f) return ferr(HADROS_E_IO, std::string("Could not open ") + path);
     if (!append) {

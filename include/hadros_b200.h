@@ -531,7 +531,8 @@ int32_t hadros_write_kgeo(const char* path, const hadros_params* p, int32_t n_ra
                           const int32_t* npoints, const double* points);
 /* The same rays written in batches, as the reference's cache writers stream
  * them (apps/compute_kerr_image_cuda.cu:1718-1780): append = 0 creates the
- * file with its header, append = 1 adds rays to it. */
+ * file with its header, append = 1 adds rays to it (HADROS_E_IO if the file
+ * does not exist). */
 int32_t hadros_write_kgeo_rays(const char* path, const hadros_params* p, int32_t n_rays,
                                const int32_t* pixel_ids, const int8_t* fate,
                                const int32_t* npoints, const double* points, int32_t append);

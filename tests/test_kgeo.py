@@ -75,6 +75,8 @@ def test_kgeo_written_in_batches_equals_one_write(hb, tmp_path):
         hb.write_kgeo(parts, p, n[lo:hi], pts[off[lo]:off[hi]], pixel_ids=np.arange(lo, hi, dtype=np.int32),
                       fate=fate[lo:hi], append=b > 0)
     assert parts.read_bytes() == one.read_bytes()
+    with pytest.raises(hb.HadrosError, match="No KGEO file to append to"):
+        hb.write_kgeo(tmp_path / "missing.bin", p, n[:1], pts[:2], append=True)
 
 
 def test_kgeo_errors(hb, tmp_path):
