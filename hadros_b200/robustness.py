@@ -26,6 +26,15 @@ spectral_validation.md are the script's.
 
     python -m hadros_b200.robustness spectral [--outdir output/spectra] ...
 
+mev-bands: scripts/make_mev_multiband_image.py (:19-23 bands, :56-141
+parameters, :144-201 outputs) runs the CPU app once per Fermi-Dirac MeV band
+(3-8, 8-20, 20-50 MeV) on the small cache and turns the three I_obs_mev images
+into mev_multiband_flux.csv and a false-colour image.  Here the three bands
+are one batch launch; the CSV is the script's and the image is written as a
+binary PPM (mev_multiband_false_color_image.ppm) instead of a matplotlib PNG.
+
+    python -m hadros_b200.robustness mev-bands [--outdir output/mev_neutrinosphere] ...
+
 Argument mapping (compute_kerr_image_from_cache argv, apps/
 compute_kerr_image_from_cache.cpp:57-201): the "h" of the parameter table is
 the torus H/R, angles are degrees, and the camera is the cache's
@@ -344,10 +353,92 @@ def write_spectral(rows: list[dict], outdir: Path) -> tuple[Path, Path]:
     return csv_path, md_path
 
 
+# scripts/make_mev_multiband_image.py:19-23
+MEV_BANDS = [("low-energy MeV band", "blue", 3.0, 8.0),
+             ("intermediate-energy MeV band", "green", 8.0, 20.0),
+             ("high-energy MeV band", "red", 20.0, 50.0)]
+
+
+def mev_band_params(e_min: float, e_max: float, pixels: int = 32, precision: str = "fp64", **over):
+    """compute_band() of the script (:56-141) with its environment defaults:
+    the small cache, gaussian torus rho0 1e10, floor 1e-20, inner_ring source
+    with rho_ref = rho0, monochromatic 1e11 GeV, the physical anti_nu_e MeV
+    model with the Fermi-Dirac band [e_min, e_max] in 8 bins."""
+    rho0 = 1.0e10
+    kw = dict(
+        a_spin=SMALL_CACHE["a"], r_obs_rg=SMALL_CACHE["r_obs"], theta_obs_deg=SMALL_CACHE["theta"],
+        fov_deg=SMALL_CACHE["fov_deg"], nx=pixels, ny=pixels, r_max_rg=SMALL_CACHE["r_max"],
+        h=SMALL_CACHE["step"],
+        Enu_obs_GeV=1.0e11, M_bh_msun=3.0, rho0_gcm3=rho0, r0_rg=10.0, sigma_r_rg=5.0, H_over_R=0.25,
+        src_r_center_rg=3.5, src_sigma_r_rg=1.0, src_theta_width_deg=15.0, src_powerlaw=2.0, src_emax_GeV=1.0e12,
+        src_norm=1.0, profile="gaussian", radial_power=2.0, funnel_depletion=0.0, funnel_theta_deg=15.0,
+        envelope_rho0_gcm3=0.0, envelope_alpha=2.5, torus_r_min_rg=4.0, torus_r_max_rg=60.0,
+        rho_floor_gcm3=1.0e-20, source="inner_ring", src_funnel_theta_deg=20.0, src_density_power_q=1.0,
+        src_radial_power_s=2.0, src_gradient_dr_rg=0.1, src_gradient_dtheta_deg=1.0, src_rho_ref_gcm3=rho0,
+        src_cutoff_min=0.0, src_cutoff_max=1.0e2, spectral="monochromatic", spec_gamma=2.0,
+        spec_ecut_GeV=1.0e12, spec_e_min_GeV=1.0e5, spec_e_max_GeV=1.0e12, n_bins=8,
+        mev_channel=1, mev_model="physical", mev_flavor="anti_nu_e", mev_thermal="inner_hot_torus",
+        mev_ye="neutron_rich_torus", mev_T0_MeV=6.0, mev_T_floor_MeV=0.1, mev_T_power=0.2, mev_Ye_torus=0.25,
+        mev_Ye_funnel=0.55, mev_Ye_envelope=0.45, mev_Ye_floor=0.01, mev_Ye_ceil=0.60,
+        mev_spectral="fermi_dirac_band", mev_E_min_MeV=e_min, mev_E_max_MeV=e_max, mev_n_bins=8,
+        mev_Enu_obs_MeV=10.0, mev_norm=1.0, mev_degeneracy_correction=False, precision=precision)
+    kw.update(over)
+    return params(**kw)
+
+
+def band_grid(I_mev, nx: int, ny: int) -> np.ndarray:
+    """load_grid() of the script (:144-156): grid[ny - 1 - j, i] = I_obs_mev."""
+    v = dat_round(I_mev).reshape(ny, nx)   # rows j*nx + i
+    return v[::-1, :].copy()
+
+
+def run_mev_bands(ctx: Context, sigma: SigmaTable, pixels: int = 32, precision: str = "fp64"):
+    """The three bands in one hadros_batch launch; returns (rows, grids, stats)."""
+    cams = [mev_band_params(lo, hi, pixels, precision) for _, _, lo, hi in MEV_BANDS]
+    outs = ctx.batch(cams, sigma, outputs=("tau", "P_surv", "I_obs", "fate", "steps", "tau_mev", "P_surv_mev",
+                                            "I_obs_mev", "r_nu", "leakage"))
+    grids, rows = [], []
+    for (label, color, lo, hi), out in zip(MEV_BANDS, outs):
+        grids.append(band_grid(out["I_obs_mev"], pixels, pixels))
+        rows.append({"band": label, "false_color": color, "E_min_MeV": lo, "E_max_MeV": hi,
+                     "integrated_I_mev": float(np.sum(dat_round(out["I_obs_mev"]))), "data_path": ""})
+    return rows, grids, ctx.stats()
+
+
+def write_mev_bands(rows: list[dict], grids: list[np.ndarray], outdir: Path) -> tuple[Path, Path]:
+    """mev_multiband_flux.csv (:162-191) and the false-colour image: channel =
+    sqrt(I / max I) clipped at 0, red = 20-50 MeV, green = 8-20, blue = 3-8
+    (:159-170), as an 8-bit binary PPM shown the way the script's
+    imshow(origin="lower") shows it."""
+    outdir.mkdir(parents=True, exist_ok=True)
+    lines = ["# product false-color MeV energy-band diagnostic image", "# blue low-energy MeV band 3-8 MeV",
+             "# green intermediate-energy MeV band 8-20 MeV", "# red high-energy MeV band 20-50 MeV",
+             "# note colors encode MeV neutrino energy intervals, not photon colors",
+             "band,false_color,E_min_MeV,E_max_MeV,integrated_I_mev,data_path"]
+    for r in rows:
+        lines.append(f"{r['band']},{r['false_color']},{r['E_min_MeV']:g},{r['E_max_MeV']:g},"
+                     f"{r['integrated_I_mev']:.8e},{r['data_path']}")
+    csv_path = outdir / "mev_multiband_flux.csv"
+    csv_path.write_text("\n".join(lines) + "\n")
+
+    def norm(g):
+        g = np.clip(g, 0.0, None)
+        m = float(np.nanmax(g)) if g.size else 0.0
+        return np.zeros_like(g) if m <= 0.0 else np.sqrt(g / m)
+    blue, green, red = (norm(g) for g in grids)
+    rgb = np.dstack([red, green, blue])[::-1]   # origin="lower": the grid's last row on top
+    img = np.clip(np.rint(rgb * 255.0), 0, 255).astype(np.uint8)
+    ppm = outdir / "mev_multiband_false_color_image.ppm"
+    with ppm.open("wb") as f:
+        f.write(f"P6\n{img.shape[1]} {img.shape[0]}\n255\n".encode())
+        f.write(img.tobytes())
+    return csv_path, ppm
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(prog="python -m hadros_b200.robustness", description=__doc__,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("scan", nargs="?", choices=("robustness", "spectral"), default="robustness")
+    ap.add_argument("scan", nargs="?", choices=("robustness", "spectral", "mev-bands"), default="robustness")
     ap.add_argument("--outdir", default=None, help="default output/scans (robustness), output/spectra (spectral)")
     ap.add_argument("--sigma", default=None, help="sigma table (reference format); default: the synthetic table")
     ap.add_argument("--pixels", type=int, default=None, help="image side (default 16 robustness, 32 spectral)")
@@ -360,6 +451,13 @@ def main(argv=None) -> int:
     else:
         E, g2, s = W.synthetic_sigma_arrays()
         sig = SigmaTable.from_arrays(E, s, g2)
+    if a.scan == "mev-bands":
+        with Context(a.device) as ctx:
+            rows, grids, st = run_mev_bands(ctx, sig, a.pixels or SMALL_CACHE["pixels"], a.precision)
+        csv_path, ppm = write_mev_bands(rows, grids, Path(a.outdir or "output/mev_neutrinosphere"))
+        print(json.dumps({"bands_per_launch": len(rows), "launches": st["launches"], "rays": st["rays"],
+                          "kernel_ms": st["kernel_ms"], "csv": str(csv_path), "image": str(ppm)}))
+        return 0
     if a.scan == "spectral":
         with Context(a.device) as ctx:
             rows, st = run_spectral(ctx, sig, a.pixels or SMALL_CACHE["pixels"], a.precision)

@@ -47,3 +47,17 @@ def test_spectral_validation_in_one_launch_matches_oracle(hb, gpu_ctx, sigma_tab
                                                     "integrated_intensity,valid_pixels,finite_outputs,"
                                                     "positive_weights")
     assert "powerlaw_cutoff convergence" in md_path.read_text()
+
+
+def test_mev_bands_in_one_launch_match_oracle(hb, gpu_ctx, sigma_table, sigma_arrays, tmp_path):
+    from hadros_b200 import robustness as R
+    from test_robustness import _OracleContext
+    E, _, s = sigma_arrays
+    rows, grids, stats = R.run_mev_bands(gpu_ctx, sigma_table, pixels=8)
+    assert len(rows) == 3 and stats["launches"] == 1
+    ref_rows, ref_grids, _ = R.run_mev_bands(_OracleContext(E, s), None, pixels=8)
+    for got, ref, g, rg in zip(rows, ref_rows, grids, ref_grids):
+        assert got["integrated_I_mev"] == pytest.approx(ref["integrated_I_mev"], rel=1e-6), got["band"]
+        np.testing.assert_allclose(g, rg, rtol=1e-6, atol=0.0)
+    csv_path, ppm = R.write_mev_bands(rows, grids, tmp_path)
+    assert ppm.read_bytes().startswith(b"P6\n8 8\n255\n")

@@ -158,3 +158,61 @@ def test_spectral_rows_equal_the_reference_executables(hb, tmp_path, sigma_array
     assert ours["mean_Psurv"] == pytest.approx(np.mean(psurv), rel=1e-12)
     assert ours["integrated_intensity"] == pytest.approx(np.sum(inten), rel=1e-12, abs=0.0)
     assert ours["valid_pixels"] == 16 and ours["finite_outputs"]
+
+
+class _OracleContext:
+    """Context.batch / Context.stats answered by the CPU oracle, so the scan
+    modules' host logic runs without a GPU."""
+
+    def __init__(self, E, s):
+        self.E, self.s, self.rays = E, s, 0
+
+    def batch(self, cams, sigma, outputs):
+        from oracle import pyoracle as O
+        self.rays = sum(int(c.nx) * int(c.ny) for c in cams)
+        return [O.oracle_image(c, self.E, self.s, mev=True) for c in cams]
+
+    def stats(self):
+        return {"launches": 1, "rays": self.rays, "kernel_ms": 0.0}
+
+
+@pytest.mark.skipif(not (REF_GEO.exists() and REF_IMG.exists()), reason="reference executables not built here")
+def test_mev_bands_equal_the_reference_executables(hb, tmp_path, sigma_arrays):
+    """make_mev_multiband_image.py's compute_band() for the 8-20 MeV band on a
+    4x4 small cache, run as the script runs it (71 arguments), against the
+    module's row; the CSV and the PPM image it writes."""
+    from hadros_b200 import robustness as R
+    from hadros_b200 import workloads as W
+    E, g2, s = sigma_arrays
+    sig = tmp_path / "sigma.dat"
+    W.write_sigma_file(sig, E, g2, s)
+    (tmp_path / "output" / "images").mkdir(parents=True)
+    cache = tmp_path / "small.bin"
+    r = subprocess.run([str(REF_GEO), "0.0001", "60.0", "80.0", "25.0", "4", "4", "40.0", "0.01", str(cache)],
+                       capture_output=True, text=True, timeout=600, env={"OMP_NUM_THREADS": "4"})
+    assert r.returncode == 0, r.stderr
+    argv = [str(REF_IMG), "100000000000.0", "0.0001", "3.0", "10000000000.0", "10.0", "5.0", "0.25", "3.5", "1.0",
+            "15.0", "2.0", "1.0e12", "1.0", "10.0", "1.0", "80.0", str(sig), "gaussian", "2.0", "0.0", "15.0",
+            "0.0", "2.5", "4.0", "60.0", "1.0e-20", "60.0", "1", str(cache), "inner_ring", "20.0", "1.0", "2.0",
+            "0.1", "1.0", "10000000000.0", "0.0", "1.0e2", "monochromatic", "2.0", "1.0e12", "1.0e5", "1.0e12",
+            "8", "physical", "anti_nu_e", "1", "1", "1", "1", "1", "inner_hot_torus", "neutron_rich_torus", "6.0",
+            "0.1", "0.2", "0.25", "0.55", "0.45", "0.01", "0.60", "fermi_dirac_band", "8.0", "20.0", "8", "0", "1",
+            "1", "1", "1", "1"]
+    r = subprocess.run(argv, cwd=tmp_path, capture_output=True, text=True, timeout=600,
+                       env={"OMP_NUM_THREADS": "4"})
+    assert r.returncode == 0, r.stderr
+    saved = [ln.split("Saved: ", 1)[1] for ln in r.stdout.splitlines() if ln.startswith("Saved: ")]
+    assert "_MeVSpectrum_fermi_dirac_band_E8e_00_2e_01_" in saved[0]
+    data = np.loadtxt(tmp_path / saved[0], comments="#")
+    rows, grids, st = R.run_mev_bands(_OracleContext(E, s), None, pixels=4)
+    assert [r["E_min_MeV"] for r in rows] == [3.0, 8.0, 20.0] and st["rays"] == 48
+    assert rows[1]["integrated_I_mev"] == pytest.approx(float(np.sum(data[:, 10])), rel=1e-12, abs=0.0)
+    assert rows[1]["integrated_I_mev"] > 0.0
+    for line in data:   # load_grid: grid[ny - 1 - j, i] = I_obs_mev
+        assert grids[1][3 - int(line[1]), int(line[0])] == pytest.approx(line[10], rel=1e-8, abs=1e-300)
+    csv_path, ppm = R.write_mev_bands(rows, grids, tmp_path / "bands")
+    text = csv_path.read_text().splitlines()
+    assert text[5] == "band,false_color,E_min_MeV,E_max_MeV,integrated_I_mev,data_path"
+    assert text[7].startswith("intermediate-energy MeV band,green,8,20,")
+    raw = ppm.read_bytes()
+    assert raw.startswith(b"P6\n4 4\n255\n") and len(raw) == len(b"P6\n4 4\n255\n") + 4 * 4 * 3
