@@ -165,7 +165,12 @@ inline void fill_mixed_constants(DevCam& cam, double sigma_scale)
     cam.k_nb = sigma_scale / kMuG;
 }
 
-// Camera plan building (host, hadros_trace.cu).
+// Camera plan building (host, hadros_trace.cu).  build_cam_into writes the
+// camera's bins into caller storage of `cap` rows with no heap use (n_bins_out
+// rows; bin_offset 0) and fails with HADROS_E_ARG beyond cap; build_cam appends
+// them to `bins` and sets bin_offset.
+int build_cam_into(const hadros_params& p, const SigmaHost& sig, DevCam& cam, DevBin* bins, int cap,
+                   int* n_bins_out, const char** err);
 int build_cam(const hadros_params& p, const SigmaHost& sig, DevCam& cam,
               std::vector<DevBin>& bins, std::string& err);
 void prepare_sigma(SigmaHost& s);

@@ -112,8 +112,8 @@ void prepare_sigma(SigmaHost& s)
     }
 }
 
-int build_cam(const hadros_params& p, const SigmaHost& sig, DevCam& cam,
-              std::vector<DevBin>& bins, std::string& err)
+int build_cam_into(const hadros_params& p, const SigmaHost& sig, DevCam& cam, DevBin* bins, int cap,
+                   int* n_bins_out, const char** err)
 {
     std::memset(&cam, 0, sizeof(cam));
     const double a = p.a_spin;
@@ -193,7 +193,7 @@ int build_cam(const hadros_params& p, const SigmaHost& sig, DevCam& cam,
 
     // spectral bins, radiative_transfer.cpp:711-737
     const double sEmin = sig.E.front(), sEmax = sig.E.back();
-    std::vector<DevBin> bb;
+    int nb = 0;
     auto ratio_consts = [&](DevBin& b) {
         if (cam.mono) {
             b.gamma = static_cast<float>(p.src_powerlaw);
@@ -215,13 +215,18 @@ int build_cam(const hadros_params& p, const SigmaHost& sig, DevCam& cam,
         b.w = 1.0;
         b.valid = 1;
         if (!(b.E_mid > 0.0) || !std::isfinite(b.E_mid)) {
-            err = "Enu_obs_GeV must be positive and finite";
+            *err = "Enu_obs_GeV must be positive and finite";
             return HADROS_E_ARG;
         }
         ratio_consts(b);
-        bb.push_back(b);
+        if (nb < cap) bins[nb] = b;
+        ++nb;
     } else {
         const int n_bins = std::max(p.n_bins, 1);
+        if (n_bins > cap) {
+            *err = "n_bins exceeds the bin capacity of this entry point";
+            return HADROS_E_ARG;
+        }
         const double e_min = smax(p.spec_e_min_GeV, sEmin);
         const double e_max = smin(p.spec_e_max_GeV, sEmax);
         const bool ok = !(e_min <= 0.0 || e_max <= e_min);
@@ -246,21 +251,37 @@ int build_cam(const hadros_params& p, const SigmaHost& sig, DevCam& cam,
                 b.gg_lo = std::numeric_limits<double>::infinity();
                 b.gg_hi = -std::numeric_limits<double>::infinity();
             }
-            bb.push_back(b);
+            bins[nb++] = b;
         }
     }
-    cam.n_bins = static_cast<int32_t>(bb.size());
-    if (cam.n_bins > kMaxBins) {
-        err = "n_bins exceeds 256";
+    if (nb > cap) {
+        *err = "n_bins exceeds the bin capacity of this entry point";
         return HADROS_E_ARG;
     }
+    cam.n_bins = nb;
     // MeV channel: the spectral aggregate keeps the first valid bin's MeV
     // result (radiative_transfer.cpp:741-774), none without a valid bin
     bool have_ref = false;
-    for (const DevBin& b : bb) have_ref = have_ref || b.valid != 0;
+    for (int k = 0; k < nb; ++k) have_ref = have_ref || bins[k].valid != 0;
     cam.mev = make_mev(p, cam.torus, have_ref);
+    cam.bin_offset = 0;
+    *n_bins_out = nb;
+    return HADROS_OK;
+}
+
+int build_cam(const hadros_params& p, const SigmaHost& sig, DevCam& cam,
+              std::vector<DevBin>& bins, std::string& err)
+{
+    DevBin bb[kMaxBins];
+    int nb = 0;
+    const char* e = "";
+    const int rc = build_cam_into(p, sig, cam, bb, kMaxBins, &nb, &e);
+    if (rc) {
+        err = (nb > kMaxBins || p.n_bins > kMaxBins) ? "n_bins exceeds 256" : e;
+        return rc;
+    }
     cam.bin_offset = static_cast<int32_t>(bins.size());
-    bins.insert(bins.end(), bb.begin(), bb.end());
+    bins.insert(bins.end(), bb, bb + nb);
     return HADROS_OK;
 }
 

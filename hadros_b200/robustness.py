@@ -427,6 +427,8 @@ def write_mev_bands(rows: list[dict], grids: list[np.ndarray], outdir: Path) -> 
         return np.zeros_like(g) if m <= 0.0 else np.sqrt(g / m)
     blue, green, red = (norm(g) for g in grids)
     rgb = np.dstack([red, green, blue])[::-1]   # origin="lower": the grid's last row on top
+    # a NaN cell is blank, as imshow leaves it, not an undefined byte
+    rgb = np.nan_to_num(rgb, nan=0.0, posinf=1.0, neginf=0.0)
     img = np.clip(np.rint(rgb * 255.0), 0, 255).astype(np.uint8)
     ppm = outdir / "mev_multiband_false_color_image.ppm"
     with ppm.open("wb") as f:

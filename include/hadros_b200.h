@@ -481,9 +481,14 @@ int32_t hadros_ctx_synchronize(hadros_ctx* ctx);
  * (a cudaStream_t; NULL = the legacy default stream), with the
  * reference-arithmetic kernel, and returns when the image is done.  Limits:
  * at most 1024 sigma rows and 64 spectral bins (else HADROS_E_ARG);
- * fast_geodesic must be 0.  The first call on a device looks up the array's
- * address (make it outside stream capture).  All calls share the array:
- * calls that overlap on the GPU race; serialize them. */
+ * fast_geodesic must be 0.  Every call looks up the array's address in the
+ * current context (a device reset or another current context cannot leave
+ * it stale); the first call on a device loads the library's kernels there,
+ * so make that first call outside stream capture.  All calls share the
+ * array, which keeps the last call's contents (the work counters are cleared
+ * at the start of each call): calls that overlap on the GPU race; serialize
+ * them.  With 64 bins in mixed precision the kernel keeps the bins in shared
+ * memory (up to ~213 KB per block with a 1024-row table): one block per SM. */
 int32_t hadros_image_device_noalloc(const hadros_params* p, const hadros_sigma* s,
                                     const hadros_image_out* dev_out, void* stream);
 

@@ -4,16 +4,19 @@
 # compiled where they lie (read-only, unmodified) with the reference Makefile's
 # flags (-O3 -std=c++17 -fopenmp, no -march), plus oracle/ref_driver.cpp.
 # Test infrastructure only; outputs go to oracle/_ref/ (git-ignored).
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]
+# REFERENCE_ROOT defaults to $HADROS_REFERENCE_ROOT, else /root/reference.
 set -euo pipefail
 here="$(cd "$(dirname "$0")" && pwd)"
-ref="${1:-/root/reference}"
+ref="${1:-${HADROS_REFERENCE_ROOT:-/root/reference}}"
 out="$here/_ref"
 if [ ! -d "$ref/src" ]; then
     echo "build_ref: no reference sources at $ref; skipping" >&2
     exit 0
 fi
 mkdir -p "$out"
+# where the sources were found, for tests that run the reference's own scripts
+printf '%s\n' "$ref" > "$out/REFERENCE_ROOT"
 srcs=""
 for f in kerr_metric kerr_geodesic kerr_camera sigma_table torus_profile \
          radiative_transfer mev_neutrino_physics; do

@@ -63,6 +63,15 @@ def ref_available() -> bool:
     return REF_SO.exists()
 
 
+def reference_root() -> Path | None:
+    """The reference source tree: $HADROS_REFERENCE_ROOT, else the tree
+    oracle/build_ref.sh built oracle/_ref from; None where neither exists."""
+    cand = os.environ.get("HADROS_REFERENCE_ROOT")
+    if not cand and (HERE / "_ref" / "REFERENCE_ROOT").exists():
+        cand = (HERE / "_ref" / "REFERENCE_ROOT").read_text().strip()
+    return Path(cand) if cand and Path(cand).is_dir() else None
+
+
 def ref_lib() -> C.CDLL:
     global _REF
     if _REF is None:

@@ -154,7 +154,9 @@ def test_alpha_beta_are_reference_camera_coordinates(hb, tmp_path):
 
 def test_compare_module_matches_reference_script(hb, tmp_path):
     """hadros_b200.compare's aggregates equal the reference comparer's."""
-    script = Path("/root/reference/scripts/compare_cuda_cpu_metrics.py")
+    from oracle import pyoracle as O
+    root = O.reference_root()
+    script = (root / "scripts" / "compare_cuda_cpu_metrics.py") if root else Path("/nonexistent")
     kw, ref = load_golden("edge_ragged_3x5")
     _, dat_a, _ = _write(hb, tmp_path, kw, ref)
     ref2 = dict(ref)
