@@ -1,23 +1,30 @@
 #!/usr/bin/env python
 """bench.py — pixel-bins/s of the HADROS per-pixel image pipeline on B200.
 
-A step traces one image of the workload (default: the 512x512 mixed-precision
-image with 8 powerlaw_cutoff bins, hadros_b200.workloads.mixed_512) through
-the trace kernel.  One process per GPU; each GPU traces its own image per step
-(pixels are independent, no data-path collective: weak scaling).
+Default workload (the production scan, 4096 x 4096 pixels x 64 bins): a step
+is one parameter point of the scan evaluated by the learned surrogate with
+its exact-tracer fallback and a seeded random 1% of the pixels judged by the
+exact tracer (hadros_b200.scan.PointRunner).  The ensemble is trained before
+the timed region on rays the tracer traces at other points of the same
+parameter box; the plain tracer (every pixel exact) is timed once on one
+point beside it.  One process per GPU; each GPU evaluates its own scan
+points (no data-path collective: weak scaling).
 
-  value       device-timed throughput, outputs resident in HBM (CUDA events
-              around K steps, L2 flushed between steps, max over ranks)
-  e2e         the same metric through the C-ABI call a user makes
-              (hadros_image: parameters host->device, image device->host)
-  roofline    the trace kernel's FP64 arithmetic rate against the measured
-              FP64 peak (cuBLAS DGEMM on this GPU, measured in the same run)
-  cpu_baseline the reference CPU code (or the oracle port) on the host cores
-              over a strided pixel subset of the same image
+  value        device-timed throughput of the steps (CUDA events, max over
+               ranks), outputs resident in HBM
+  e2e          the same steps from host memory to host memory
+               (PointRunner.run_host: judge ids in, the image out)
+  roofline     the trace kernel's FP64 rate on the plain-tracer point against
+               the measured FP64 peak (cuBLAS DGEMM in the same run);
+               roofline_inference: the surrogate kernel against BF16 peak
+  cpu_baseline the reference CPU code on the host cores over a strided pixel
+               sample of a scan point (every pixel traced exactly, as the
+               reference does)
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-    python bench.py --workload surrogate     # the surrogate's tcgen05 inference kernel
-    python bench.py --mev                    # image workload with the MeV thermal channel
+    python bench.py --workload image       # the 512x512x8 mixed image, trace kernel only
+    python bench.py --workload surrogate   # the surrogate's tcgen05 inference kernel
+    python bench.py --mev                  # image workload with the MeV thermal channel
 """
 from __future__ import annotations
 
@@ -214,6 +221,105 @@ def reference_cuda_arm(args) -> None:
                                    "powerlaw_funnel_envelope, funnel_wall, RKF45 tol 1e-6"},
             "reference_cuda": runs, "hadros_b200": ours,
             "gpu": torch.cuda.get_device_name(0)}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- production scan
+
+SCAN_DESC = ("production scan, one parameter point per step: 4096x4096 px x 64 powerlaw_cutoff bins "
+             "(1e5-1e12 GeV, gamma 2, Ecut 1e12), collapsar_ndaf_like (r0 12, sigma_r 8, H 0.45, r 3-80), "
+             "density_weighted source, a=0.95, rho0 log-uniform 1e9-1e12, inclination U[10,80] deg, "
+             "r_obs 60 M, fov 25 deg, h0 0.01; surrogate (4-network BF16 ensemble) + exact fallback + "
+             "exact judge of a seeded random 1% of pixels per point; exact tracer FP64 RKF45 geodesics + "
+             "FP32 Kahan transfer")
+SCAN_SIDE, SCAN_BINS, SCAN_POINTS = 4096, 64, 256
+REF_GRID = 15          # reference sample per step: a 15 x 15 strided grid of pixels
+
+
+def scan_config(world: int) -> dict:
+    return {"workload": SCAN_DESC, "side": SCAN_SIDE, "bins": SCAN_BINS,
+            "l2": "image outputs (403 MB) larger than L2, and a 256 MiB write between steps",
+            "parallelism": f"scan points split over {world} GPU(s), no collective on the data path"}
+
+
+def scan_point_kw(k: int) -> dict:
+    """Camera keywords of scan point k (of SCAN_POINTS, seeded)."""
+    from hadros_b200 import workloads as W
+    rho0, theta = W.scan_points(SCAN_POINTS)[k % SCAN_POINTS]
+    return W.production_point(nx=SCAN_SIDE, ny=SCAN_SIDE, n_bins=SCAN_BINS, rho0_gcm3=rho0,
+                              theta_obs_deg=theta)
+
+
+def ref_sample_ids(k: int, grid: int = REF_GRID, side: int = SCAN_SIDE) -> np.ndarray:
+    """Step k's reference sample: a grid x grid strided pixel set whose offset
+    moves with k, so the steps' samples are disjoint."""
+    stride = side // grid
+    oi, oj = (k * 37) % stride, (k * 101) % stride
+    ii = oi + stride * np.arange(grid)
+    jj = oj + stride * np.arange(grid)
+    return (jj[:, None] * side + ii[None, :]).ravel().astype(np.int32)
+
+
+def cpu_scan_sample(k: int, threads: int, grid: int = REF_GRID, mev_off: bool = False) -> dict:
+    """The reference CPU code (oracle/_ref, else the oracle port) on step k's
+    sample of scan point k: every pixel exact, all bins, MeV block as shipped
+    (or at its cheapest setting with mev_off)."""
+    import hadros_b200 as hb
+    from hadros_b200 import workloads as W
+    from oracle import pyoracle as O
+    E, g2, s = W.synthetic_sigma_arrays()
+    kw = scan_point_kw(k)
+    if mev_off:
+        kw.update(mev_channel=1, mev_model="toy", mev_urca=False, mev_pair=False, mev_brems=False,
+                  mev_absorption=False, mev_scattering=False)
+    p = hb.params(**kw)
+    ids = ref_sample_ids(k, grid)
+    kind = "reference" if O.ref_available() else "port"
+    t0 = time.perf_counter()
+    if kind == "reference":
+        r = O.ref_image(p, E, g2, s, pixel_ids=ids, threads=threads, per_bin=False)
+    else:
+        r = O.oracle_image(p, E, s, pixel_ids=ids, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": ids.size * SCAN_BINS / dt, "seconds": dt, "rays": int(ids.size), "kind": kind,
+            "cores": threads, "steps_per_ray": float(np.mean(r["steps"])), "point": k % SCAN_POINTS}
+
+
+def reference_scan_arm(args) -> None:
+    """--impl reference on the scan workload: the reference computes every
+    pixel of a scan point exactly (it has no surrogate); each step times its
+    CPU code on a different strided sample of a different point (ref_grid^2
+    rays, disjoint across steps), with all host threads."""
+    if env_int("RANK", 0) != 0:
+        return
+    threads = host_threads()
+    for w in range(args.warmup):        # untimed: small samples of the warm-up points
+        cpu_scan_sample(w, threads, grid=2)
+    g = args.ref_grid
+    rows = [cpu_scan_sample(args.warmup + k, threads, grid=g) for k in range(args.steps)]
+    per_step = sum(r["seconds"] for r in rows) / len(rows)
+    value = g * g * SCAN_BINS / per_step
+    off = cpu_scan_sample(args.warmup, threads, grid=g, mev_off=True)
+    kind = rows[0]["kind"]
+    sample = (f"{len(rows)} steps x {g}x{g} strided pixels (stride {SCAN_SIDE // g}, "
+              f"offset moving per step: {len(rows) * g * g} distinct rays) of scan points "
+              f"{args.warmup}..{args.warmup + len(rows) - 1}, all {SCAN_BINS} bins, "
+              + ("reference CPU code built from its sources (KerrCamera::trace_pixel + "
+                 "integrate_kerr_ray_spectral, MeV block as shipped)" if kind == "reference"
+                 else "CPU oracle port (oracle/hadros_oracle.c)") + f", OpenMP {threads} threads")
+    line = {
+        "impl": "reference", "metric": "pixel-bins/sec", "value": value, "unit": "pixel-bins/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": scan_config(args.gpus),
+        "cpu_baseline": {"value": value, "unit": "pixel-bins/s", "cores": threads, "kind": kind,
+                         "sample": sample, "rays": len(rows) * g * g,
+                         "steps_per_ray": float(np.mean([r["steps_per_ray"] for r in rows])),
+                         "value_mev_off": off["value"],
+                         "mev_off": "step 0's sample with the MeV block at its cheapest setting "
+                                    "(toy model, five terms off)"},
+        "e2e": {"value": value, "unit": "pixel-bins/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
     print(json.dumps(line), flush=True)
 
 
@@ -469,6 +575,203 @@ def gpu_arm(args) -> None:
         dist.destroy_process_group()
 
 
+def _dist_setup(torch, device, world: int, timeout_s: int):
+    """NCCL process group (world > 1) and the barrier / max / sum helpers."""
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=timeout_s), device_id=device)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def reduce(x: float, op: str) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+        return float(t.item())
+    return dist, barrier, reduce
+
+
+def gpu_index_of(local: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        try:
+            return int(vis.split(",")[local])
+        except (ValueError, IndexError):
+            return local
+    return local
+
+
+def scan_arm(args) -> None:
+    """The production scan: one surrogate-evaluated scan point per step."""
+    import torch
+
+    import hadros_b200 as hb
+    from hadros_b200 import scan as SC
+    from hadros_b200 import workloads as W
+
+    rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    # every rank trains its own copy of the ensemble (same seeds) before the
+    # first collective, so no rank waits on another through the setup
+    dist, barrier, reduce = _dist_setup(torch, device, world, 1800)
+    E, g2, s = W.synthetic_sigma_arrays()
+    sig = hb.SigmaTable.from_arrays(E, s, g2)
+    ctx = hb.Context(local)
+    P, B = SCAN_SIDE * SCAN_SIDE, SCAN_BINS
+
+    # ---- setup (untimed): training rays, ensemble, fallback threshold ----------
+    t_setup = time.perf_counter()
+    tpts = W.scan_points(args.train_points, seed=W.SEED + 17)
+    cams = [SC.production_cam(r, t, SCAN_SIDE, SCAN_BINS) for r, t in tpts]
+    sur, info = SC.train(ctx, sig, cams, args.pixels_per_cam, 4, args.epochs, W.SEED, args.batch, args.lr,
+                         device=local)
+    vcams, vraw, vy = SC.held_out_samples(ctx, sig, cams, args.pixels_per_cam, W.SEED, info["i_floor"], local)
+    calib = SC.calibrate(sur, sig, vcams, vraw, vy, info["i_floor"], args.bound)
+    del vraw, vy
+    thr = calib["threshold"]
+    setup_s = time.perf_counter() - t_setup
+
+    stream = torch.cuda.Stream(device=device)
+    torch.cuda.set_stream(stream)
+    runner = SC.PointRunner(ctx, sig, sur, SCAN_SIDE, SCAN_BINS, args.judge, stream=stream)
+    # this rank's scan points (every world-th), their judge subsets drawn ahead
+    ks = [rank + world * k for k in range(args.warmup + args.steps)]
+    pars = [hb.params(**scan_point_kw(k)) for k in ks]
+    jrng = np.random.default_rng(W.SEED + 5 + rank)
+    jids = [torch.from_numpy(SC.judge_ids(P, args.judge, jrng)).to(device) for _ in ks]
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)   # > 126 MB L2
+    for w in range(args.warmup):
+        runner.run(pars[w], thr, jids[w])
+        flush.zero_()
+    barrier()
+
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    rows = []
+    with ClockSampler(gpu_index_of(local)) as clocks:
+        t_start.record(stream)
+        for k in range(args.steps):
+            rows.append(runner.run(pars[args.warmup + k], thr, jids[args.warmup + k]))
+            flush.zero_()
+        t_end.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    clk = clocks.summary()
+    elapsed = t_start.elapsed_time(t_end) / 1e3
+    per_step = reduce(elapsed, "max") / args.steps
+    value = world * P * B / per_step
+    worst = reduce(max(r["error"]["worst"] for r in rows), "max")
+    p99 = reduce(max(r["error"]["p99"] for r in rows), "max")
+    fb_max = reduce(max(r["fallback_frac"] for r in rows), "max")
+    inf_ms = statistics.mean(r["inference_ms"] for r in rows)
+    ex_ms = statistics.mean(r["exact_ms"] for r in rows)
+
+    # ---- the plain tracer on the last timed point: every pixel exact ----------
+    k_plain = ks[args.warmup + args.steps - 1]
+    pp = pars[args.warmup + args.steps - 1]
+    plain = {"tau": torch.empty(P, dtype=torch.float64, device=device),
+             "P_surv": torch.empty(P, dtype=torch.float64, device=device),
+             "I_obs": torch.empty(P, dtype=torch.float64, device=device),
+             "fate": torch.empty(P, dtype=torch.int8, device=device),
+             "steps": torch.empty(P, dtype=torch.int32, device=device),
+             "attempts": torch.empty(P, dtype=torch.int32, device=device)}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.image_device(pp, sig, plain, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_s = e0.elapsed_time(e1) / 1e3
+    attempts = float(plain["attempts"].to(torch.int64).sum().item())
+    steps_sum = float(plain["steps"].to(torch.int64).sum().item())
+    flop64 = attempts * F_ATT + steps_sum * F_GEO
+    peak64 = fp64_peak_tflops(torch, device)
+    achieved = flop64 / plain_s / 1e12
+    # the last step's finished image against the exact image, every pixel
+    full = SC._device_errors(plain["I_obs"], runner.out["I_obs"])
+    full_check = {"point": k_plain, "pixels": int(full[0].item()), "worst": float(full[1].item()),
+                  "p99": float(full[2].item()), "median": float(full[3].item())}
+    del plain
+    traffic, traffic_src = read_traffic()
+
+    # ---- e2e: the same steps from host memory to host memory --------------------
+    host = runner.alloc_host()
+    barrier()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for k in range(args.steps):
+        host["judge_ids"].copy_(jids[args.warmup + k].cpu())
+        r = runner.run_host(pars[args.warmup + k], thr, host)
+        h2d, d2h = r["h2d_bytes"], r["d2h_bytes"]
+    e2e_s = reduce(time.perf_counter() - t0, "max") / args.steps
+    del host
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        c = cpu_scan_sample(k_plain, host_threads(), grid=args.cpu_grid)
+        cpu = {"value": c["value"], "unit": "pixel-bins/s", "cores": c["cores"], "kind": c["kind"],
+               "sample": (f"{c['rays']} pixels ({args.cpu_grid}x{args.cpu_grid} strided grid) of scan point "
+                          f"{k_plain}, all {B} bins, every pixel exact, "
+                          + ("reference CPU code built from its sources, MeV block as shipped"
+                             if c["kind"] == "reference" else "CPU oracle port")
+                          + f", OpenMP {c['cores']} threads, {c['seconds']:.1f} s"),
+               "steps_per_ray_sample": c["steps_per_ray"],
+               "steps_per_ray_gpu_image": steps_sum / P}
+    peak16, peak16_src = measured_bf16_peak()
+    inf_flop = P * B * len(sur.nets) * F_MLP
+    if rank == 0:
+        line = {
+            "metric": "pixel-bins/sec", "value": value, "unit": "pixel-bins/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16+f64+f32",
+            "data": "synthetic: seeded scan points; the ensemble is trained in this run (before the timed "
+                    f"region) on rays the tracer traced at {args.train_points} other points of the box",
+            "config": scan_config(world),
+            "surrogate": {"worst_judged_error": worst, "p99_judged_error_max": p99,
+                          "median_judged_error_mean": statistics.mean(r["error"]["median"] for r in rows),
+                          "judged_pixels_per_point": rows[0]["judged"],
+                          "fallback_frac_mean": statistics.mean(r["fallback_frac"] for r in rows),
+                          "fallback_frac_max": fb_max, "threshold": thr, "bound": args.bound,
+                          "calibration": calib, "members": len(sur.nets),
+                          "train": {k: info[k] for k in ("samples", "trace_s", "fit_s", "val_rms_ln_tau",
+                                                         "val_rms_ln_I") if k in info},
+                          "epochs": args.epochs, "setup_s": setup_s},
+            "plain_tracer": {"seconds_per_point": plain_s, "pixel_bins_per_s": P * B / plain_s,
+                             "point": k_plain, "speedup_of_surrogate_step": plain_s / per_step,
+                             "accepted_steps_per_ray": steps_sum / P, "full_image_check": full_check},
+            "step_ms": {"inference": inf_ms, "exact_judge_and_fallback": ex_ms,
+                        "rest": per_step * 1e3 - inf_ms - ex_ms},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                         "frac": achieved / peak64, "kernel": "trace kernel on the plain-tracer point",
+                         "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 "
+                                        f"(datasheet {FP64_PEAK_DATASHEET_TFLOPS} TFLOP/s)",
+                         "flop64_per_launch": flop64, "kernel_ms": plain_s * 1e3,
+                         "traffic": traffic, "traffic_source": traffic_src},
+            "roofline_inference": {"bound": "tensor", "achieved": inf_flop / (inf_ms / 1e3) / 1e12,
+                                   "peak": peak16, "unit": "TFLOP/s",
+                                   "frac": inf_flop / (inf_ms / 1e3) / 1e12 / peak16,
+                                   "peak_source": peak16_src, "flop_per_launch": inf_flop,
+                                   "kernel_ms": inf_ms, "kernel": "surrogate inference (tcgen05), per step"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * P * B / e2e_s, "unit": "pixel-bins/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 # Algorithmic BF16 work of one surrogate network on one (pixel, bin) sample:
 # 64 -> 256, 3 x (256 -> 256), 256 -> 2 (multiply-add = 2 flop).
 F_MLP = 2 * (64 * 256 + 3 * 256 * 256 + 256 * 2)
@@ -606,9 +909,20 @@ def main() -> None:
                     help="reference: the reference CPU code (the contract's reference arm); reference-cuda: "
                          "the reference's own GPU executable beside this library on one image")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["image", "surrogate"], default="image",
-                    help="image: the trace kernel on mixed_512 (default); surrogate: the "
-                         "surrogate inference kernel")
+    ap.add_argument("--workload", choices=["scan", "image", "surrogate"], default="scan",
+                    help="scan: one production-scan point per step, surrogate + fallback + 1%% exact "
+                         "judge (default); image: the trace kernel on mixed_512; surrogate: the "
+                         "surrogate inference kernel alone")
+    ap.add_argument("--epochs", type=int, default=40, help="scan: training epochs of the ensemble")
+    ap.add_argument("--train-points", type=int, default=128, help="scan: training cameras (incl. held out)")
+    ap.add_argument("--pixels-per-cam", type=int, default=4096, help="scan: training pixels per camera")
+    ap.add_argument("--batch", type=int, default=8192, help="scan: training batch")
+    ap.add_argument("--lr", type=float, default=2e-3, help="scan: peak learning rate")
+    ap.add_argument("--bound", type=float, default=0.01, help="scan: intensity error bound (fallback)")
+    ap.add_argument("--judge", type=float, default=0.01, help="scan: judged fraction of pixels")
+    ap.add_argument("--cpu-grid", type=int, default=12, help="scan: CPU-baseline sample grid per side")
+    ap.add_argument("--ref-grid", type=int, default=REF_GRID,
+                    help="scan, --impl reference: sample grid per side per step")
     ap.add_argument("--side", type=int, default=None, help="surrogate workload / reference-cuda: image side")
     ap.add_argument("--bins", type=int, default=None, help="surrogate workload: bins")
     ap.add_argument("--mev", action="store_true",
@@ -616,11 +930,16 @@ def main() -> None:
                          "code always runs it)")
     args = ap.parse_args()
     if args.impl == "reference":
-        reference_arm(args)
+        if args.workload == "scan":
+            reference_scan_arm(args)
+        else:
+            reference_arm(args)
     elif args.impl == "reference-cuda":
         reference_cuda_arm(args)
     elif args.workload == "surrogate":
         surrogate_arm(args)
+    elif args.workload == "scan":
+        scan_arm(args)
     else:
         gpu_arm(args)
 

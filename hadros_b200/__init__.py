@@ -436,6 +436,18 @@ class Context:
                                                     else stream.cuda_stream)
         _check(lib().hadros_image_device(self.handle, C.byref(p), sigma.handle, C.byref(o), st))
 
+    def pixels_device(self, p: HadrosParams, sigma: SigmaTable, ids, out: dict, n: int | None = None,
+                      stream=None) -> None:
+        """Enqueue the exact trace of a DEVICE pixel-id list (int32 tensor or
+        pointer; first n ids, default all) into device buffers in list order."""
+        o = HadrosImageOut()
+        for k, v in out.items():
+            setattr(o, k, v if isinstance(v, int) else v.data_ptr())
+        count = int(ids.numel()) if n is None else int(n)
+        ptr = ids if isinstance(ids, int) else ids.data_ptr()
+        _check(lib().hadros_image_pixels_device(self.handle, C.byref(p), sigma.handle, C.c_void_p(ptr), count,
+                                                C.byref(o), _ptr_stream(stream)))
+
     def synchronize(self) -> None:
         _check(lib().hadros_ctx_synchronize(self.handle))
 

@@ -216,6 +216,8 @@ SIGNATURES = {
                                         C.c_int32, P(HadrosImageOut)]),
     "hadros_image_device": (C.c_int32, [C.c_void_p, P(HadrosParams), C.c_void_p,
                                         P(HadrosImageOut), C.c_void_p]),
+    "hadros_image_pixels_device": (C.c_int32, [C.c_void_p, P(HadrosParams), C.c_void_p, C.c_void_p,
+                                               C.c_int32, P(HadrosImageOut), C.c_void_p]),
     "hadros_ctx_synchronize": (C.c_int32, [C.c_void_p]),
     "hadros_batch": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, P(HadrosImageOut)]),
     "hadros_batch_device": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,

@@ -766,9 +766,12 @@ struct PathRec {
 thread_local PathRec g_path_rec{nullptr, 0};
 
 // Shared body of the image calls.  dev_out holds DEVICE pointers.
+// With pixel_ids_dev (a DEVICE list of n_pixels ids), the list is traced
+// as it is, without the host range check: an id only sets the ray's screen
+// position, and outputs go to list rows.
 int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s,
                   const int32_t* pixel_ids_host, int32_t n_pixels, const hadros_image_out& dev_out,
-                  cudaStream_t st, bool time_kernel)
+                  cudaStream_t st, bool time_kernel, const int32_t* pixel_ids_dev = nullptr)
 {
     if (!ctx) return fail(HADROS_E_STATE, "context is NULL");
     if (ctx->failed) return fail(HADROS_E_STATE, "context is in a failed state: " + ctx->err);
@@ -783,7 +786,8 @@ int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s
     std::string err;
     rc = build_cam(*p, s->h, cam, bins, err);
     if (rc) return fail(rc, err);
-    const int64_t P = pixel_ids_host ? n_pixels : static_cast<int64_t>(p->nx) * p->ny;
+    const bool listed = pixel_ids_host || pixel_ids_dev;
+    const int64_t P = listed ? n_pixels : static_cast<int64_t>(p->nx) * p->ny;
     if (pixel_ids_host) {
         const int64_t total = static_cast<int64_t>(p->nx) * p->ny;
         for (int32_t k = 0; k < n_pixels; ++k)
@@ -806,7 +810,7 @@ int32_t run_image(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s
         return cuda_fail(ctx, e, "bin upload");
     int64_t h2d = static_cast<int64_t>(sizeof(DevCam) + sizeof(DevBin) * bins.size());
     if (sigma_new) h2d += static_cast<int64_t>(ctx->sig_cap);
-    const int32_t* d_pix = nullptr;
+    const int32_t* d_pix = pixel_ids_dev;
     if (pixel_ids_host && n_pixels > 0) {
         h2d += static_cast<int64_t>(sizeof(int32_t)) * n_pixels;
         if ((rc = grow(ctx, &ctx->d_pix, &ctx->pix_cap, sizeof(int32_t) * n_pixels, "pixel list"))) return rc;
@@ -1037,6 +1041,23 @@ int32_t hadros_image_device(hadros_ctx* ctx, const hadros_params* p, const hadro
     try {
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : (ctx ? ctx->stream : nullptr);
         const int32_t rc = run_image(ctx, p, s, nullptr, 0, *dev_out, st, false);
+        return rc ? rc : ok();
+    } catch (const std::exception& ex) {
+        return fail(HADROS_E_NOMEM, ex.what());
+    }
+}
+
+int32_t hadros_image_pixels_device(hadros_ctx* ctx, const hadros_params* p, const hadros_sigma* s,
+                                   const int32_t* dev_pixel_ids, int32_t n_pixels,
+                                   const hadros_image_out* dev_out, void* stream)
+{
+    if (!dev_out) return fail(HADROS_E_ARG, "output struct is NULL");
+    if (n_pixels < 0 || (n_pixels > 0 && !dev_pixel_ids))
+        return fail(HADROS_E_ARG, "pixel list is NULL or negative length");
+    try {
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : (ctx ? ctx->stream : nullptr);
+        const int32_t rc = run_image(ctx, p, s, nullptr, n_pixels, *dev_out, st, false,
+                                     n_pixels > 0 ? dev_pixel_ids : nullptr);
         return rc ? rc : ok();
     } catch (const std::exception& ex) {
         return fail(HADROS_E_NOMEM, ex.what());

@@ -45,10 +45,11 @@ def _torch():
 
 
 def plain_image(ctx, p, sigma) -> tuple[dict, float]:
-    """The exact tracer's per-pixel outputs in device memory, and its time (s)."""
+    """The exact tracer's per-pixel outputs in device memory (the current
+    device), and its time (s)."""
     torch = _torch()
     P = int(p.nx) * int(p.ny)
-    dev = torch.device("cuda", 0)
+    dev = torch.device("cuda", torch.cuda.current_device())
     out = {"tau": torch.empty(P, dtype=torch.float64, device=dev),
            "P_surv": torch.empty(P, dtype=torch.float64, device=dev),
            "I_obs": torch.empty(P, dtype=torch.float64, device=dev),
@@ -78,58 +79,178 @@ def errors(I_ex: np.ndarray, I_sur: np.ndarray, floor_rel: float = 1e-6) -> dict
 CANDIDATE_THRESHOLDS = (0.002, 0.0025, 0.0033, 0.004, 0.005, 0.0067, 0.01)
 
 
+def judge_ids(P: int, frac: float, rng) -> np.ndarray:
+    """A seeded random judge subset: round(frac P) distinct pixel ids (int32)."""
+    n = max(1, int(round(frac * P)))
+    return rng.choice(P, size=n, replace=False).astype(np.int32)
+
+
+class PointRunner:
+    """Scan points evaluated on one device with buffers allocated once.
+
+    run() enqueues, on `stream`: the ensemble's image of the camera (the
+    inference kernel, which lists the pixels whose spread exceeds the
+    threshold), then ONE exact trace of the judge pixels followed by the
+    fallback pixels (the fallback ids land right after the judge ids in one
+    device list), then the fallback pixels' exact values into the image.  It
+    waits on the stream for the fallback count and for the judged errors it
+    returns."""
+
+    KEYS = ("tau", "P_surv", "I_obs")
+
+    def __init__(self, ctx, sigma, sur, side: int, n_bins: int, judge_frac: float = 0.01, stream=None):
+        torch = _torch()
+        self.ctx, self.sigma, self.sur = ctx, sigma, sur
+        self.P = side * side
+        self.n_judge = max(1, int(round(judge_frac * self.P)))
+        dev = sur.device
+        self.stream = stream
+        # judge ids, then room for every pixel as a fallback
+        self.ids = torch.empty(self.n_judge + self.P, dtype=torch.int32, device=dev)
+        self.out = S.alloc_image(self.P, n_bins, dev, per_bin=False)
+        del self.out["fallback_ids"]
+        self.out["fallback_ids"] = self.ids[self.n_judge:]
+        self.exact = {k: torch.empty(self.n_judge + self.P, dtype=torch.float64, device=dev) for k in self.KEYS}
+
+    def run(self, p, threshold: float, jids, spread_of: int = 0, detail: bool = False) -> dict:
+        """One scan point.  jids: the judge pixel ids (device int32 tensor of
+        n_judge, or host array).  Returns host values: fallback count, judged
+        errors, device times of the parts (ms)."""
+        torch = _torch()
+        st = self.stream if self.stream is not None else torch.cuda.current_stream()
+        nj = self.n_judge
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        with torch.cuda.stream(st):
+            if isinstance(jids, np.ndarray):
+                jids = torch.from_numpy(np.ascontiguousarray(jids, dtype=np.int32)).to(self.ids.device)
+            if jids.data_ptr() != self.ids.data_ptr():
+                self.ids[:nj].copy_(jids, non_blocking=True)
+            ev[0].record(st)
+            self.sur.image(p, self.sigma, threshold=threshold, per_bin=False, out=self.out, stream=st,
+                           spread_of=spread_of)
+            ev[1].record(st)
+            cnt = self.out["counters"].cpu()        # waits for the inference kernel
+            if int(cnt[1]):
+                raise RuntimeError("surrogate inference kernel timed out")
+            nf = int(cnt[0])
+            jt = self.ids[:nj].long()
+            raw = {k: self.out[k][jt] for k in self.KEYS}   # surrogate values before the fallback
+            spread_j = self.out["spread"][jt]
+            self.ctx.pixels_device(p, self.sigma, self.ids, self.exact, n=nj + nf, stream=st)
+            ev[2].record(st)
+            if nf:
+                fb = self.ids[nj:nj + nf].long()
+                for k in self.KEYS:
+                    self.out[k].index_copy_(0, fb, self.exact[k][nj:nj + nf])
+            key = "I_obs" if spread_of == 0 else "tau"
+            ex = self.exact[key][:nj]
+            e_all = _device_errors(ex, self.out[key][jt])
+            fbmask = torch.zeros(nj, dtype=torch.bool, device=ex.device)
+            if nf:
+                # judged pixels that fell back hold exact values; the surrogate's own errors exclude them
+                fbmask = torch.isin(self.ids[:nj], self.ids[nj:nj + nf])
+            e_sur = _device_errors(ex[~fbmask], raw[key][~fbmask])
+            pmax = (self.exact["P_surv"][:nj] - self.out["P_surv"][jt]).abs().max()
+            ev[3].record(st)
+            vals = torch.stack([*e_all, *e_sur, pmax.double()]).cpu()      # waits for the step
+        v = vals.numpy()
+        res = {"fallback_pixels": nf, "fallback_frac": nf / self.P, "judged": nj, "judged_quantity": key,
+               "error": {"n": int(v[0]), "worst": float(v[1]), "p99": float(v[2]), "median": float(v[3])},
+               "error_surrogate_pixels": {"n": int(v[4]), "worst": float(v[5]), "p99": float(v[6]),
+                                          "median": float(v[7])},
+               "P_surv_max_abs_error": float(v[8]),
+               "inference_ms": ev[0].elapsed_time(ev[1]), "exact_ms": ev[1].elapsed_time(ev[2]),
+               "device_ms": ev[0].elapsed_time(ev[3])}
+        if detail:
+            res["judge"] = {"ids": self.ids[:nj].cpu().numpy(), "spread": spread_j.cpu().numpy(),
+                            "exact": {k: self.exact[k][:nj].cpu().numpy() for k in self.KEYS},
+                            "raw": {k: t.cpu().numpy() for k, t in raw.items()}}
+        return res
+
+    def alloc_host(self) -> dict:
+        """Pinned host buffers for run_host: the judge ids and the image."""
+        torch = _torch()
+        h = {k: torch.empty(self.P, dtype=torch.float64, pin_memory=True) for k in self.KEYS}
+        h["judge_ids"] = torch.empty(self.n_judge, dtype=torch.int32, pin_memory=True)
+        return h
+
+    def run_host(self, p, threshold: float, host: dict, spread_of: int = 0) -> dict:
+        """run() from host memory to host memory: the judge ids in
+        host["judge_ids"] go to the device, the finished image (tau, P_surv,
+        I_obs) comes back into host[...]; returns run()'s dict plus the bytes
+        copied each way."""
+        torch = _torch()
+        st = self.stream if self.stream is not None else torch.cuda.current_stream()
+        with torch.cuda.stream(st):
+            self.ids[:self.n_judge].copy_(host["judge_ids"], non_blocking=True)
+            res = self.run(p, threshold, self.ids[:self.n_judge], spread_of=spread_of)
+            for k in self.KEYS:
+                host[k].copy_(self.out[k], non_blocking=True)
+            st.synchronize()
+        # judge ids and the exact trace's camera tables in; the image, the
+        # fallback count and the judged errors out
+        res["h2d_bytes"] = self.n_judge * 4 + int(self.ctx.stats()["h2d_bytes"])
+        res["d2h_bytes"] = 8 * self.P * len(self.KEYS) + 8 + 9 * 8
+        return res
+
+
+def _device_errors(ex, got, floor_rel: float = 1e-6):
+    """(n, worst, p99, median) of |got - ex| / ex over the pixels with ex at
+    least floor_rel of the largest ex, as 0-d device tensors (zeros if none)."""
+    torch = _torch()
+    z = torch.zeros((), dtype=torch.float64, device=ex.device)
+    if ex.numel() == 0:
+        return z, z, z, z
+    top = ex.max()
+    m = (ex >= floor_rel * top) & (top > 0)
+    rel = torch.where(m, (got - ex).abs() / torch.where(m, ex, torch.ones_like(ex)), torch.zeros_like(ex))
+    n = m.sum().double()
+    worst = rel.max().double()
+    # quantiles over the kept pixels: the others sort below every kept one
+    srt = torch.sort(torch.where(m, rel, torch.full_like(rel, -1.0))).values
+    k0 = rel.numel() - m.sum()
+
+    def q(f):
+        idx = (k0 + (f * (n - 1)).floor().long()).clamp(0, rel.numel() - 1)
+        return torch.where(n > 0, srt[idx].double(), z)
+    return n, worst, q(0.99), q(0.5)
+
+
 def surrogate_point(ctx, sigma, sur, p, threshold: float, judge_frac: float, rng, buf=None,
                     spread_of: int = 0) -> dict:
-    """One scan point: surrogate image, exact fallback, exact judge subset.
+    """One scan point: surrogate image, exact fallback, exact judge subset
+    (PointRunner), with its wall-clock time.
 
     Besides the errors of the result, reports for other spread thresholds what
     they would have given: the fraction of pixels above them and the worst
-    judged error among the pixels below them (the surrogate's values there)."""
+    judged error among the pixels below them (the surrogate's values there).
+    `buf`: a PointRunner to reuse (else one is made for this camera)."""
     torch = _torch()
+    if int(p.nx) != int(p.ny):
+        raise ValueError("scan points are square images")
     P = int(p.nx) * int(p.ny)
+    runner = buf if isinstance(buf, PointRunner) else PointRunner(ctx, sigma, sur, int(p.nx), n_bins_of(p),
+                                                                  judge_frac)
+    jids = judge_ids(P, judge_frac, rng)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    res = sur.image(p, sigma, threshold=threshold, per_bin=False, out=buf, spread_of=spread_of)
-    cnt = res["counters"].cpu().numpy()
-    if cnt[1]:
-        raise RuntimeError("surrogate inference kernel timed out")
-    t_inf = time.perf_counter() - t0
-    ids = np.sort(res["fallback_ids"][:int(cnt[0])].cpu().numpy()).astype(np.int32)
-    # the fallback pixels and the judged pixels are traced exactly in one launch
-    jn = max(1, int(round(judge_frac * P)))
-    jids = np.sort(rng.choice(P, size=jn, replace=False)).astype(np.int32)
-    jt = torch.from_numpy(jids.astype(np.int64)).cuda()
-    keys = ("I_obs", "tau", "P_surv")
-    raw_j = {k: res[k][jt] for k in keys}                 # surrogate values before the fallback
-    spread_j = res["spread"][jt]
-    fb, jex = ctx.batch_pixels([p, p], sigma, [ids, jids], outputs=("tau", "P_surv", "I_obs"))
-    if ids.size:
-        idx = torch.from_numpy(ids.astype(np.int64)).cuda()
-        for k in keys:
-            res[k].index_copy_(0, idx, torch.from_numpy(fb[k]).cuda())
-    torch.cuda.synchronize()
+    res = runner.run(p, threshold, jids, spread_of=spread_of, detail=True)
     t_total = time.perf_counter() - t0
-    t_fb = t_total - t_inf
-    sur_v = {k: res[k][jt].cpu().numpy() for k in keys}
-    raw_v = {k: v.cpu().numpy() for k, v in raw_j.items()}
-    sj = spread_j.cpu().numpy()
-    fb_mask = np.isin(jids, ids)
-    key = "I_obs" if spread_of == 0 else "tau"
+    jd = res.pop("judge")
+    key = res["judged_quantity"]
+    sj = jd["spread"]
+    sp = runner.out["spread"]
     what_if = []
-    sp = res["spread"]
     for thr in CANDIDATE_THRESHOLDS:
         keep = sj <= thr
-        e = errors(jex[key][keep], raw_v[key][keep]) if keep.any() else {"worst": 0.0, "n": 0}
+        e = errors(jd["exact"][key][keep], jd["raw"][key][keep]) if keep.any() else {"worst": 0.0, "n": 0}
         what_if.append({"threshold": thr, "fallback_frac": float((sp > thr).float().mean().item()),
                         "worst": e["worst"], "n": e["n"]})
-    return {"seconds": t_total, "inference_s": t_inf, "exact_s": t_fb,
-            "fallback_pixels": int(ids.size), "fallback_frac": ids.size / P, "judged": int(jn),
-            "judged_quantity": key,
-            "error": errors(jex[key], sur_v[key]),
-            "error_surrogate_pixels": errors(jex[key][~fb_mask], sur_v[key][~fb_mask]),
-            "P_surv_max_abs_error": float(np.abs(jex["P_surv"] - sur_v["P_surv"]).max()),
-            "spread_quantiles": [float(q) for q in np.quantile(sj, [0.5, 0.9, 0.99, 0.999])],
-            "what_if": what_if}
+    res.update({"seconds": t_total, "inference_s": res["inference_ms"] / 1e3,
+                "exact_s": t_total - res["inference_ms"] / 1e3,
+                "spread_quantiles": [float(q) for q in np.quantile(sj, [0.5, 0.9, 0.99, 0.999])],
+                "what_if": what_if})
+    return res
 
 
 def production_cam(rho0: float, theta_deg: float, side: int, n_bins: int):
@@ -141,10 +262,11 @@ def n_held_out(n_cams: int, val_frac: float = 0.1) -> int:
     return max(1, int(round(val_frac * n_cams)))
 
 
-def held_out_samples(ctx, sigma, cams, pixels_per_cam: int, seed: int, i_floor: float):
+def held_out_samples(ctx, sigma, cams, pixels_per_cam: int, seed: int, i_floor: float, device=0):
     """The held-out cameras' samples (the last n_held_out cameras), as train() traces them."""
     n_val = n_held_out(len(cams))
-    vraw, vy, _ = S.trace_samples(ctx, sigma, cams[-n_val:], pixels_per_cam, seed=seed + 1, i_floor=i_floor)
+    vraw, vy, _ = S.trace_samples(ctx, sigma, cams[-n_val:], pixels_per_cam, seed=seed + 1, i_floor=i_floor,
+                                  device=device)
     return cams[-n_val:], vraw, vy
 
 
@@ -191,14 +313,14 @@ def calibrate(sur, sigma, cams, raw, y, i_floor: float, bound: float, q: float =
 
 
 def train(ctx, sigma, cams, pixels_per_cam: int, members: int, epochs: int, seed: int, batch: int,
-          lr: float) -> tuple[object, dict]:
+          lr: float, device=0) -> tuple[object, dict]:
     """Trace training samples on `cams`, hold out the last cameras
     (n_held_out), train the ensemble; returns it with timing and validation RMS."""
     torch = _torch()
     n_val = n_held_out(len(cams))
-    raw, y, info = S.trace_samples(ctx, sigma, cams[:-n_val], pixels_per_cam, seed=seed)
-    _, vraw, vy = held_out_samples(ctx, sigma, cams, pixels_per_cam, seed, info["i_floor"])
-    sur = S.Surrogate(members=members, seed=seed)
+    raw, y, info = S.trace_samples(ctx, sigma, cams[:-n_val], pixels_per_cam, seed=seed, device=device)
+    _, vraw, vy = held_out_samples(ctx, sigma, cams, pixels_per_cam, seed, info["i_floor"], device)
+    sur = S.Surrogate(members=members, device=device, seed=seed)
     t0 = time.perf_counter()
     sur.fit(raw, y, epochs=epochs, batch=batch, lr=lr, floors=(S.TAU_FLOOR, info["i_floor"]))
     torch.cuda.synchronize()
@@ -248,7 +370,7 @@ def run_production(a) -> dict:
             print(json.dumps({"calibration": calib}), file=sys.stderr, flush=True)
         pts = W.scan_points(a.points, seed=W.SEED)
         rng = np.random.default_rng(W.SEED + 5)
-        buf = S.alloc_image(a.side * a.side, a.bins, sur.device, per_bin=False)
+        buf = PointRunner(ctx, sigma, sur, a.side, a.bins, a.judge)
         rows = []
         for r, t in pts:
             rows.append(surrogate_point(ctx, sigma, sur, production_cam(r, t, a.side, a.bins), a.threshold,

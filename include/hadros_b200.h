@@ -388,6 +388,17 @@ int32_t hadros_image_pixels(hadros_ctx* ctx, const hadros_params* p,
 int32_t hadros_image_device(hadros_ctx* ctx, const hadros_params* p,
                             const hadros_sigma* s,
                             const hadros_image_out* dev_out, void* stream);
+/* Pixel subset whose ids (j*nx+i) are already in DEVICE memory (the
+ * surrogate's fallback list, a judge subset drawn on the device), outputs
+ * into DEVICE buffers in list order, on `stream`; asynchronous.  Ids are not
+ * range-checked (they are device data): an id outside the image only moves
+ * the ray off the screen.  Replaces, for device-resident scans, the judge
+ * and fallback traces the reference would run as separate executables per
+ * parameter point (scripts/run_robustness_scans.py:81-145). */
+int32_t hadros_image_pixels_device(hadros_ctx* ctx, const hadros_params* p,
+                                   const hadros_sigma* s, const int32_t* dev_pixel_ids,
+                                   int32_t n_pixels, const hadros_image_out* dev_out,
+                                   void* stream);
 /* Many cameras in one persistent launch (parameter scans: cameras of
  * different size, spin, inclination, profile, rho0 and bins).  Outputs are
  * concatenated in camera order: per-pixel arrays hold sum(nx*ny) entries,

@@ -9,7 +9,8 @@ reference sources are available:
     oracle/build_ref.sh && python tests/golden/make_golden.py [name-prefix]
 
 The fixtures pin the CPU oracle (tests/test_oracle.py) and are what the GPU
-parity tests compare against on machines without the reference.
+parity tests compare against on machines without the reference.  A fixture
+of a pixel subset stores the ids as `pixel_ids` (outputs in list order).
 """
 from __future__ import annotations
 
@@ -84,6 +85,15 @@ def cases() -> dict[str, dict]:
                                  mev_neutrinosphere_tau=5.0)
     c["mev_gaussian_thin"] = W.mixed_512(nx=4, ny=4, precision="fp64", h=0.05, mev_channel=1,
                                          rho0_gcm3=1.0e8, mev_thermal="radial_powerlaw")
+    # The production-scan camera at its own settings (4096x4096, h0 0.01, 64
+    # bins): an 8x8 strided pixel sample (every 512th pixel in i and j, from
+    # 256), at a mid-box point and at a dense, nearly face-on one.
+    side = 4096
+    ii = 256 + 512 * np.arange(8)
+    ids = (ii[:, None] * side + ii[None, :]).ravel().astype(np.int32)
+    c["production_c5_mid_8x8"] = dict(W.production_point(precision="fp64"), _pixel_ids=ids)
+    c["production_c5_dense_8x8"] = dict(W.production_point(precision="fp64", rho0_gcm3=1.0e12,
+                                                           theta_obs_deg=15.0), _pixel_ids=ids)
     return c
 
 
@@ -96,8 +106,12 @@ def main() -> None:
     for name, kw in cases().items():
         if not name.startswith(only):
             continue
+        kw = dict(kw)
+        ids = kw.pop("_pixel_ids", None)   # a pixel subset, stored as pixel_ids
         p = hb.params(**kw)
-        out = O.ref_image(p, E, g2, s, mev=name.startswith("mev_"))
+        out = O.ref_image(p, E, g2, s, pixel_ids=ids, mev=name.startswith("mev_"))
+        if ids is not None:
+            out["pixel_ids"] = ids
         meta = {k: (v if not isinstance(v, (np.floating, np.integer)) else v.item())
                 for k, v in kw.items()}
         np.savez_compressed(HERE / f"{name}.npz", params=json.dumps(meta), **out)

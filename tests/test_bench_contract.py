@@ -18,7 +18,7 @@ def _bench(*args, env=None):
 
 
 def test_reference_arm_prints_one_contract_line():
-    r = _bench("--impl", "reference", "--steps", "1", "--warmup", "0")
+    r = _bench("--impl", "reference", "--steps", "2", "--warmup", "1", "--ref-grid", "2")
     assert r.returncode == 0, r.stderr
     lines = [ln for ln in r.stdout.splitlines() if ln.strip()]
     assert len(lines) == 1
@@ -31,6 +31,19 @@ def test_reference_arm_prints_one_contract_line():
     c = d["cpu_baseline"]
     assert c["kind"] in ("reference", "port") and c["cores"] >= 1 and c["value"] == d["value"]
     assert c["value_mev_off"] > 0 and "workload" in d["config"]
+    assert c["rays"] == 2 * 2 * 2 and c["steps_per_ray"] > 0
+
+
+def test_reference_samples_are_disjoint_across_steps():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    seen = set()
+    for k in range(20):
+        ids = bench.ref_sample_ids(k)
+        assert ids.size == bench.REF_GRID ** 2 and ids.min() >= 0 and ids.max() < bench.SCAN_SIDE ** 2
+        assert seen.isdisjoint(ids.tolist())
+        seen.update(ids.tolist())
+    assert len(seen) >= 4096
 
 
 def test_reference_arm_other_ranks_are_silent():

@@ -14,14 +14,16 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("name", golden_names())
 def test_fp64_matches_reference(hb, gpu_ctx, sigma_table, name):
     kw, ref = load_golden(name)
-    got = gpu_ctx.image(hb.params(**dict(kw, precision="fp64", fast=False)), sigma_table)
+    got = gpu_ctx.image(hb.params(**dict(kw, precision="fp64", fast=False)), sigma_table,
+                        pixel_ids=ref.get("pixel_ids"))
     assert_parity(got, ref, RTOL_FP64, f"{name}/fp64")
 
 
 @pytest.mark.parametrize("name", golden_names())
 def test_mixed_matches_reference(hb, gpu_ctx, sigma_table, name):
     kw, ref = load_golden(name)
-    got = gpu_ctx.image(hb.params(**dict(kw, precision="mixed", fast=False)), sigma_table)
+    got = gpu_ctx.image(hb.params(**dict(kw, precision="mixed", fast=False)), sigma_table,
+                        pixel_ids=ref.get("pixel_ids"))
     assert got["tau_E"].dtype == np.float32
     assert_parity(got, ref, RTOL_MIXED, f"{name}/mixed", p_absolute=True)
 
@@ -89,9 +91,10 @@ def test_fast_geodesic_matches_reference(hb, gpu_ctx, sigma_table, name):
     """fast_geodesic=1: same RKF45 and centred differences with fewer
     divisions/transcendentals and FMA; fate and steps still exact."""
     kw, ref = load_golden(name)
-    got = gpu_ctx.image(hb.params(**dict(kw, precision="fp64", fast=True)), sigma_table)
+    ids = ref.get("pixel_ids")
+    got = gpu_ctx.image(hb.params(**dict(kw, precision="fp64", fast=True)), sigma_table, pixel_ids=ids)
     assert_parity(got, ref, RTOL_FP64, f"{name}/fast-fp64")
-    got = gpu_ctx.image(hb.params(**dict(kw, precision="mixed", fast=True)), sigma_table)
+    got = gpu_ctx.image(hb.params(**dict(kw, precision="mixed", fast=True)), sigma_table, pixel_ids=ids)
     assert_parity(got, ref, RTOL_MIXED, f"{name}/fast-mixed", p_absolute=True)
 
 
