@@ -40,6 +40,8 @@ struct DevCam {
     Mev mev;                          // MeV thermal channel (radiative_transfer.cpp:522-638)
     int32_t nx, ny, max_steps, n_bins;
     int32_t mono;
+    int32_t sp_emit;                  // some bin has E_mid > 0 (an empty band emits nothing)
+    float sp_gamma;                   // spectral index shared by the bins' w(E)/w(E_mid)
     int32_t bin_offset;               // first row in the bin tables
     int64_t item_begin;               // first work item of this camera
     int64_t item_end;
@@ -58,6 +60,8 @@ struct DevBin {
     float kcut;         // E_mid / E_cut (or / E_max for monochromatic), 0 if none
     float gamma;        // spectral index of the ratio w(E)/w(E_mid)
     int32_t valid;      // counted in the spectral aggregates
+    float kcut2;        // kcut * log2(e): the cutoff term in base-2 exponents
+    float qbase;        // (log(E_mid) - log(E_0)) / (sigma table step): segment coordinate at g = 1
 };
 
 // Sigma table staged in shared memory.  FP64 arrays follow SigmaTable::
@@ -73,17 +77,17 @@ struct SigmaDev {
     const double* lnE;   // [n]  log(E_k)
     const double* lnS;   // [n]  log(sigma_k)
     const float* lx;     // [n]  (float)log(E_k)
-    const float* seg;    // [4n] per segment k>=1: lx1, 1/(lx2-lx1), s1, dly
+    const float* seg;    // [4n] per segment k>=1: lx1, 1/(lx2-lx1), s1, dly*log2(e)
 };
 
-// Deferred transfer (mixed precision): one path point's bin-independent
-// transfer terms, as the trace kernel buffers them (24 bytes).
+// One path point's bin-independent transfer terms in mixed precision (24
+// bytes; the deferred transfer buffers them).  Exponents are base 2.
 struct PointRec {
-    double gg;     // max(1/z, 1e-300): the exact E_local range test per bin
-    float lnzp;    // ln(E_local / E_mid) = ln(1/gg)
+    float lnzp;    // ln(E_local / E_mid) = ln(1/g)
     float zm1;     // E_local / E_mid - 1
-    float lnK;     // ln(g^3 C dl_cm); -inf: no emission at this point
-    float nbdl;    // n_b dl_cm; negative: no density
+    float u2;      // log2(g^3 C dl_cm) - gamma log2(1/g); -inf: no emission at this point
+    float nbdl2;   // n_b dl_cm log2(e); negative: no density
+    int32_t b0, b1;// bins whose E_local lies in the sigma table's range: b0..b1 (decided in FP64)
 };
 constexpr int kRecDepth = 64;       // points a thread buffers between deferred transfers
 constexpr int kDeferMinBins = 24;   // bins from which the host picks deferred transfer
@@ -154,6 +158,7 @@ struct SigmaHost {
     double sigma_scale = 1.0;
     int32_t uniform = 0;
     float lx0 = 0.0f, inv_dlx = 0.0f;
+    double inv_step = 0.0;   // 1 / (ln E step) of an evenly spaced table
 };
 
 // FP32 constants of the mixed transfer (torus_f, src_f, k_nb) from a camera's

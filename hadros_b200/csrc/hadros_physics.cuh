@@ -20,6 +20,8 @@
 namespace hadros {
 
 constexpr double kPi = 3.141592653589793238462643383279502884;
+constexpr double kLog2E = 1.442695040888963407359924681001892137;   // log2(e)
+constexpr double kLn2 = 0.693147180559945309417232121458176568;     // ln(2)
 // include/constants.hpp:9-13
 constexpr double kCcgs = 2.99792458e10;
 constexpr double kGcgs = 6.67430e-8;

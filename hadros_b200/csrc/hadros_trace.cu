@@ -93,22 +93,25 @@ void prepare_sigma(SigmaHost& s)
         smax_v = std::max(smax_v, s.s_cm2[k]);
     }
     s.sigma_scale = smax_v > 0.0 ? smax_v : 1.0;
-    // nearly even spacing in ln E (within 1e-3 of a step): the kernel indexes
-    // the segment directly and corrects it by at most one knot
+    // even spacing in ln E (within 1e-5 of a step): the kernel indexes the
+    // segment directly from the coordinate (ln E - ln E_0) / step; a point
+    // within rounding of a knot may take the neighbouring segment, whose
+    // log-log line meets this one at the knot
     if (n >= 2) {
         const double step = (s.lnE[n - 1] - s.lnE[0]) / static_cast<double>(n - 1);
         bool even = step > 0.0;
         for (size_t k = 1; k < n && even; ++k)
-            even = std::fabs((s.lnE[k] - s.lnE[k - 1]) - step) <= 1.0e-3 * step;
+            even = std::fabs((s.lnE[k] - s.lnE[k - 1]) - step) <= 1.0e-5 * step;
         s.uniform = even ? 1 : 0;
         s.lx0 = static_cast<float>(s.lnE[0]);
         s.inv_dlx = static_cast<float>(1.0 / step);
+        s.inv_step = 1.0 / step;
     }
     for (size_t k = 1; k < n; ++k) {
         s.seg[4 * k + 0] = static_cast<float>(s.lnE[k - 1]);
         s.seg[4 * k + 1] = static_cast<float>(1.0 / (s.lnE[k] - s.lnE[k - 1]));
         s.seg[4 * k + 2] = static_cast<float>(s.s_cm2[k - 1] / s.sigma_scale);
-        s.seg[4 * k + 3] = static_cast<float>(s.lnS[k] - s.lnS[k - 1]);
+        s.seg[4 * k + 3] = static_cast<float>((s.lnS[k] - s.lnS[k - 1]) * kLog2E);   // base-2 slope
     }
 }
 
@@ -207,6 +210,8 @@ int build_cam_into(const hadros_params& p, const SigmaHost& sig, DevCam& cam, De
         b.lnE = static_cast<float>(std::log(b.E_mid));
         b.gg_lo = gg_lower(b.E_mid, sEmax);
         b.gg_hi = gg_upper(b.E_mid, sEmin);
+        b.kcut2 = static_cast<float>(static_cast<double>(b.kcut) * kLog2E);
+        b.qbase = sig.uniform ? static_cast<float>((std::log(b.E_mid) - sig.lnE.front()) * sig.inv_step) : 0.0f;
     };
     if (cam.mono) {
         DevBin b{};
@@ -259,6 +264,9 @@ int build_cam_into(const hadros_params& p, const SigmaHost& sig, DevCam& cam, De
         return HADROS_E_ARG;
     }
     cam.n_bins = nb;
+    cam.sp_gamma = cam.mono ? static_cast<float>(p.src_powerlaw) : static_cast<float>(p.spec_gamma);
+    cam.sp_emit = 0;
+    for (int k = 0; k < nb; ++k) cam.sp_emit |= bins[k].E_mid > 0.0 ? 1 : 0;
     // MeV channel: the spectral aggregate keeps the first valid bin's MeV
     // result (radiative_transfer.cpp:741-774), none without a valid bin
     bool have_ref = false;

@@ -275,12 +275,15 @@ struct SmemTables {
     float lx0, inv_dlx;
 };
 
-// This thread's column of per-bin accumulators (stride kTPB).
+// This thread's column of per-bin accumulators (stride kTPB).  FP64 mode:
+// tau and I.  Mixed mode, exponents in base 2: V - Vc is the Kahan pair of
+// S - tau log2(e), I - Ic the Kahan pair of the intensity scaled by 2^S, and
+// S an integer-valued anchor.
 struct BinAcc {
     double* T64;
     double* I64;
-    float* T;
-    float* Tc;
+    float* V;
+    float* Vc;
     float* I;
     float* Ic;
     float* S;
@@ -288,78 +291,123 @@ struct BinAcc {
 };
 
 // The mixed-precision transfer of one path point, in two parts: the
-// bin-independent terms (point_terms_body) and the update of one bin's FP32
-// accumulators (bin_point).  Density and ln(emissivity) are FP32
-// (hadros_physics_f32.cuh).  Each bin's intensity is kept as a Kahan sum I
-// scaled by exp(S): every contribution K w(E_loc)/w(E_mid) exp(-tau) enters
-// as exp(e) with e = ln(...) - tau + S, and S is re-anchored when the sum is
-// empty or a term would exceed e^40, so intensities behind optically thick gas
-// (exp(-tau) far below FP32's range) keep their relative precision.
-__device__ __forceinline__ void point_terms_body(const DevCam* cam, double r, double th, double gg,
-                                                 double dl_cm, PointRec& p)
+// bin-independent terms (point_terms_body, FP64 where a decision is exact)
+// and the update of one bin's FP32 accumulators (bin_point).  Density and
+// ln(emissivity) are FP32 (hadros_physics_f32.cuh).  Exponents are kept in
+// base 2, so every exponential is one ex2.approx.
+//
+// Intensity: each bin's sum is kept scaled by 2^S with S an integer-valued
+// anchor.  A contribution K w(E_loc)/w(E_mid) exp(-tau) enters as 2^e with
+// e = log2(K w/w0) + (S - tau log2 e).  The second term is carried as one
+// Kahan pair V - Vc, so the large parts cancel inside exact arithmetic and e
+// is accurate to its own rounding even behind optically thick gas.  S moves
+// by whole powers of two when the sum is empty or a term would exceed 2^57.7
+// (e^40); terms below e^-800 are below FP64's range and skipped, as the
+// reference's FP64 sum rounds them away.
+
+// 2^x (PTX ex2.approx.ftz.f32: relative error below 2^-22).
+__device__ __forceinline__ float ex2a(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Exact 2^k for integer k <= 127; 0 below 2^-126.
+__device__ __forceinline__ float pow2i(int k)
+{
+    return k < -126 ? 0.0f : __int_as_float((k + 127) << 23);
+}
+
+constexpr float kAnchorMax2 = 57.70780f;     // 40 / ln 2
+constexpr float kUnderflow2 = -1154.156f;    // -800 / ln 2
+
+__device__ __forceinline__ void point_terms_body(const DevCam* cam, const DevBin* bins, int B, double r,
+                                                 double th, double gg, double dl_cm, PointRec& p)
 {
     const float rho = torus_rho_f(cam->torus, cam->torus_f, r, th);
     const float lnC = ln_emission_f(cam->src, cam->src_f, cam->torus, cam->torus_f, r, th, rho);
     const double zp = 1.0 / gg;   // E_local / E_mid
-    p.gg = gg;
     p.lnzp = static_cast<float>(log(zp));
     p.zm1 = static_cast<float>(zp - 1.0);
-    const bool emit = (lnC > -INFINITY) && dl_cm > 0.0;
-    // ln(g^3 C dl_cm) with g = 1 / zp
-    p.lnK = emit ? __fsub_rn(__fadd_rn(lnC, __logf(static_cast<float>(dl_cm))), __fmul_rn(3.0f, p.lnzp))
-                 : -INFINITY;
-    p.nbdl = rho > 0.0f ? rho * static_cast<float>(dl_cm * cam->k_nb) : -1.0f;
+    const bool emit = cam->sp_emit && (lnC > -INFINITY) && dl_cm > 0.0;
+    // log2(g^3 C dl_cm) - gamma log2(1/g), g = 1 / zp
+    p.u2 = emit ? __fmul_rn(__fsub_rn(__fadd_rn(lnC, __logf(static_cast<float>(dl_cm))),
+                                      __fmul_rn(__fadd_rn(3.0f, cam->sp_gamma), p.lnzp)),
+                            static_cast<float>(kLog2E))
+                : -INFINITY;
+    p.nbdl2 = rho > 0.0f ? rho * static_cast<float>(dl_cm * cam->k_nb * kLog2E) : -1.0f;
+    // The bins whose E_local = E_mid/gg lies in [E_min, E_max] of the sigma
+    // table (radiative_transfer.cpp:661-668), decided in FP64 exactly as the
+    // reference's compares: gg_lo[b] <= gg <= gg_hi[b], both bounds rising
+    // with b, so the bins form one run b0..b1.
+    int lo = 0, cnt = B;   // first b with gg_lo[b] > gg
+    while (cnt > 0) {
+        const int st = cnt >> 1;
+        if (!(gg < bins[lo + st].gg_lo)) { lo += st + 1; cnt -= st + 1; }
+        else cnt = st;
+    }
+    p.b1 = lo - 1;
+    lo = 0;
+    cnt = B;               // first b with gg_hi[b] >= gg
+    while (cnt > 0) {
+        const int st = cnt >> 1;
+        if (bins[lo + st].gg_hi < gg) { lo += st + 1; cnt -= st + 1; }
+        else cnt = st;
+    }
+    p.b0 = lo;
 }
 
 // false for a point the transfer skips (radiative_transfer.cpp:501-505)
-__device__ __forceinline__ bool point_terms(const DevCam* cam, double r, double th, double dl, double z,
-                                            PointRec& p)
+__device__ __forceinline__ bool point_terms(const DevCam* cam, const DevBin* bins, int B, double r, double th,
+                                            double dl, double z, PointRec& p)
 {
     if (r < cam->rt_skip) return false;
     const double g = 1.0 / smax(z, 1.0e-300);
     const double gg = smax(g, 1.0e-300);
-    point_terms_body(cam, r, th, gg, dl * cam->rg_cm, p);
+    point_terms_body(cam, bins, B, r, th, gg, dl * cam->rg_cm, p);
     return true;
 }
 
-// The fields of a DevBin the transfer reads (the deferred replay keeps four
-// of them in registers).
+// The fields of a DevBin the mixed transfer reads (the deferred replay keeps
+// them in registers).
 struct BinK {
-    double E_mid, gg_lo, gg_hi;
-    float lnE, gamma, kcut;
+    float lnE, kcut2, qbase;
 };
 
-template <class Bin>
-__device__ __forceinline__ void bin_point(const PointRec& p, const Bin& bn, const SmemTables& tb, float& T,
-                                          float& Tc, float& I, float& Ic, float& S)
+__device__ __forceinline__ BinK bin_k(const DevBin& d) { return BinK{d.lnE, d.kcut2, d.qbase}; }
+
+// One path point into bin b: emission with the optical depth before the
+// point, then the point's absorption (radiative_transfer.cpp:650-671).
+// Rounding intrinsics throughout: no multiply-add is fused differently in the
+// in-loop and the deferred transfer.
+__device__ __forceinline__ void bin_point(const PointRec& p, const BinK& bn, int b, const SmemTables& tb, float& V,
+                                          float& Vc, float& I, float& Ic, float& S)
 {
-    // Rounding intrinsics throughout: no multiply-add is fused differently in
-    // the in-loop and the deferred transfer.
-    if (p.lnK != -INFINITY && bn.E_mid > 0.0) {
-        const float arg = __fsub_rn(__fsub_rn(p.lnK, __fmul_rn(bn.gamma, p.lnzp)), __fmul_rn(bn.kcut, p.zm1));
-        // ln of this contribution; below -800 it is under FP64's range (the
-        // reference adds an exact or subnormal zero)
-        const double x = __dsub_rn(static_cast<double>(arg), __dsub_rn(static_cast<double>(T), static_cast<double>(Tc)));
-        if (x >= -800.0) {
-            double e = __dadd_rn(x, static_cast<double>(S));
-            if (I == 0.0f || e > 40.0) {
-                const float shrink = (I == 0.0f) ? 0.0f : __expf(static_cast<float>(-e));
-                I = __fmul_rn(I, shrink);
-                Ic = __fmul_rn(Ic, shrink);
-                S = static_cast<float>(-x);   // |S| < ~900: exact to 1e-4
-                e = __dadd_rn(x, static_cast<double>(S));
+    if (p.u2 != -INFINITY) {
+        const float arg = __fmaf_rn(-bn.kcut2, p.zm1, p.u2);
+        float e = __fsub_rn(__fadd_rn(arg, V), Vc);
+        if (__fsub_rn(e, S) >= kUnderflow2) {
+            if (I == 0.0f || e > kAnchorMax2) {
+                const float k = -rintf(e);
+                if (I != 0.0f) {
+                    const float sc = pow2i(static_cast<int>(k));
+                    I = __fmul_rn(I, sc);
+                    Ic = __fmul_rn(Ic, sc);
+                }
+                S = __fadd_rn(S, k);
+                kahan_add(V, Vc, k);
+                e = __fsub_rn(__fadd_rn(arg, V), Vc);
             }
-            kahan_add(I, Ic, __expf(static_cast<float>(e)));
+            kahan_add(I, Ic, ex2a(e));
         }
     }
-    if (!(p.nbdl < 0.0f) && p.gg >= bn.gg_lo && p.gg <= bn.gg_hi) {
+    if (!(p.nbdl2 < 0.0f) && b >= p.b0 && b <= p.b1) {
         const float lnE = __fadd_rn(bn.lnE, p.lnzp);
         int k;
-        if (tb.uniform) {   // evenly spaced ln E: direct index, corrected by one knot
-            k = static_cast<int>(__fmul_rn(__fsub_rn(lnE, tb.lx0), tb.inv_dlx)) + 1;
+        if (tb.uniform) {   // evenly spaced ln E: the segment from the coordinate
+            k = __float2int_rd(__fmaf_rn(p.lnzp, tb.inv_dlx, bn.qbase)) + 1;
             k = k < 1 ? 1 : (k > tb.n - 1 ? tb.n - 1 : k);
-            if (k > 1 && lnE < tb.lx[k - 1]) --k;
-            else if (k < tb.n - 1 && lnE > tb.lx[k]) ++k;
         } else {
             int lo = 0, cnt = tb.n;   // lower_bound over lx
             while (cnt > 0) {
@@ -371,7 +419,7 @@ __device__ __forceinline__ void bin_point(const PointRec& p, const Bin& bn, cons
         }
         const float4 sg = tb.seg[k];
         const float t = __fmul_rn(__fsub_rn(lnE, sg.x), sg.y);
-        kahan_add(T, Tc, __fmul_rn(p.nbdl, __fmul_rn(sg.z, __expf(__fmul_rn(t, sg.w)))));
+        kahan_add(V, Vc, -__fmul_rn(__fmul_rn(p.nbdl2, sg.z), ex2a(__fmul_rn(t, sg.w))));
     }
 }
 
@@ -390,12 +438,12 @@ __device__ __forceinline__ void transfer_point(const DevCam* cam, const DevBin* 
     const double dl_cm = dl * cam->rg_cm;
     if (MIXED) {
         PointRec pr;
-        point_terms_body(cam, r, th, gg, dl_cm, pr);
+        point_terms_body(cam, bins, B, r, th, gg, dl_cm, pr);
         for (int b = 0; b < B; ++b) {
-            float T = acc.T[b * acc.st], Tc = acc.Tc[b * acc.st];
+            float V = acc.V[b * acc.st], Vc = acc.Vc[b * acc.st];
             float I = acc.I[b * acc.st], Ic = acc.Ic[b * acc.st], S = acc.S[b * acc.st];
-            bin_point(pr, bins[b], tb, T, Tc, I, Ic, S);
-            acc.T[b * acc.st] = T; acc.Tc[b * acc.st] = Tc;
+            bin_point(pr, bin_k(bins[b]), b, tb, V, Vc, I, Ic, S);
+            acc.V[b * acc.st] = V; acc.Vc[b * acc.st] = Vc;
             acc.I[b * acc.st] = I; acc.Ic[b * acc.st] = Ic; acc.S[b * acc.st] = S;
         }
     } else {
@@ -447,10 +495,11 @@ __device__ __forceinline__ void finish_pixel(const TraceArgs& A, const DevCam* c
     for (int b = 0; b < B; ++b) {
         double tb, ib;
         if (MIXED) {
-            tb = static_cast<double>(acc.T[b * acc.st]);
-            // I = (I_s - c) * exp(-S) * w(E_mid)
-            ib = (static_cast<double>(acc.I[b * acc.st]) - static_cast<double>(acc.Ic[b * acc.st])) *
-                 exp(-static_cast<double>(acc.S[b * acc.st])) * bins[b].w0;
+            const double S = static_cast<double>(acc.S[b * acc.st]);
+            // tau = (S - (V - Vc)) ln 2;  I = (I_s - c) 2^-S w(E_mid), S integer-valued
+            tb = (S - (static_cast<double>(acc.V[b * acc.st]) - static_cast<double>(acc.Vc[b * acc.st]))) * kLn2;
+            ib = ldexp(static_cast<double>(acc.I[b * acc.st]) - static_cast<double>(acc.Ic[b * acc.st]),
+                       -static_cast<int>(S)) * bins[b].w0;
         } else {
             tb = acc.T64[b * acc.st];
             ib = acc.I64[b * acc.st];
@@ -516,7 +565,7 @@ __device__ __forceinline__ void reset_bins(const BinAcc& acc, int B)
 {
     for (int b = 0; b < B; ++b) {
         if (MIXED) {
-            acc.T[b * acc.st] = 0.0f; acc.Tc[b * acc.st] = 0.0f;
+            acc.V[b * acc.st] = 0.0f; acc.Vc[b * acc.st] = 0.0f;
             acc.I[b * acc.st] = 0.0f; acc.Ic[b * acc.st] = 0.0f;
             acc.S[b * acc.st] = 0.0f;
         } else {
@@ -573,19 +622,18 @@ __device__ __noinline__ void deferred_transfer(PointRec* rec_buf, float* rec_sta
         const long long sl = warp_slot0 + src;
         float* st = rec_state + sl * 5 * bmax;
         const PointRec* rb = rec_buf + sl * kRecDepth;
-        float T[kDeferBins], Tc[kDeferBins], I[kDeferBins], Ic[kDeferBins], S[kDeferBins];
+        float V[kDeferBins], Vc[kDeferBins], I[kDeferBins], Ic[kDeferBins], S[kDeferBins];
         BinK bk[kDeferBins];
         bool on[kDeferBins];
 #pragma unroll
         for (int j = 0; j < kDeferBins; ++j) {
             const int b = b0 + j;
             on[j] = act && b < B_src;
-            T[j] = Tc[j] = I[j] = Ic[j] = S[j] = 0.0f;
-            bk[j] = BinK{0.0, INFINITY, -INFINITY, 0.0f, 0.0f, 0.0f};
+            V[j] = Vc[j] = I[j] = Ic[j] = S[j] = 0.0f;
+            bk[j] = BinK{0.0f, 0.0f, 0.0f};
             if (on[j]) {
-                const DevBin& d = bins[cs->bin_offset + b];
-                bk[j] = BinK{d.E_mid, d.gg_lo, d.gg_hi, d.lnE, d.gamma, d.kcut};
-                T[j] = st[b]; Tc[j] = st[bmax + b]; I[j] = st[2 * bmax + b];
+                bk[j] = bin_k(bins[cs->bin_offset + b]);
+                V[j] = st[b]; Vc[j] = st[bmax + b]; I[j] = st[2 * bmax + b];
                 Ic[j] = st[3 * bmax + b]; S[j] = st[4 * bmax + b];
             }
         }
@@ -596,14 +644,14 @@ __device__ __noinline__ void deferred_transfer(PointRec* rec_buf, float* rec_sta
                 const PointRec pr = rb[q];
 #pragma unroll
                 for (int j = 0; j < kDeferBins; ++j)
-                    if (on[j]) bin_point(pr, bk[j], tb, T[j], Tc[j], I[j], Ic[j], S[j]);
+                    if (on[j]) bin_point(pr, bk[j], b0 + j, tb, V[j], Vc[j], I[j], Ic[j], S[j]);
             }
         }
 #pragma unroll
         for (int j = 0; j < kDeferBins; ++j)
             if (on[j]) {
                 const int b = b0 + j;
-                st[b] = T[j]; st[bmax + b] = Tc[j]; st[2 * bmax + b] = I[j];
+                st[b] = V[j]; st[bmax + b] = Vc[j]; st[2 * bmax + b] = I[j];
                 st[3 * bmax + b] = Ic[j]; st[4 * bmax + b] = S[j];
             }
     }
@@ -643,9 +691,9 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
     // per-bin accumulators of this thread's ray, column tid, stride kTPB
     double* accT64 = reinterpret_cast<double*>(smem + L.off_acc) + tid;
     double* accI64 = accT64 + size_t(kTPB) * A.max_bins;
-    float* accT = reinterpret_cast<float*>(smem + L.off_acc) + tid;
-    float* accTc = accT + size_t(kTPB) * A.max_bins;
-    float* accI = accTc + size_t(kTPB) * A.max_bins;
+    float* accV = reinterpret_cast<float*>(smem + L.off_acc) + tid;
+    float* accVc = accV + size_t(kTPB) * A.max_bins;
+    float* accI = accVc + size_t(kTPB) * A.max_bins;
     float* accIc = accI + size_t(kTPB) * A.max_bins;
     float* accS = accIc + size_t(kTPB) * A.max_bins;
     const SmemTables tb{sE, sS, slnE, slnS, slx, sseg, n_sig, sigEmin, sigEmax, sig_scale, A.sig.uniform, A.sig.lx0, A.sig.inv_dlx};
@@ -653,7 +701,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
     float* dstate = defer ? A.rec_state + slot * 5 * A.rec_bmax : nullptr;
     const BinAcc acc = defer ? BinAcc{nullptr, nullptr, dstate, dstate + A.rec_bmax, dstate + 2 * A.rec_bmax,
                                       dstate + 3 * A.rec_bmax, dstate + 4 * A.rec_bmax, 1}
-                             : BinAcc{accT64, accI64, accT, accTc, accI, accIc, accS, kTPB};
+                             : BinAcc{accT64, accI64, accV, accVc, accI, accIc, accS, kTPB};
     PointRec* my_rec = defer ? A.rec_buf + slot * kRecDepth : nullptr;
     int fill = 0;          // points buffered in my_rec
     unsigned iter = 0;     // loop iterations (warp-uniform)
@@ -822,7 +870,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
             // ---- transfer of this point into every bin ------------------
             if (defer) {
                 PointRec pr;
-                if (point_terms(cam, r, th, dl, z, pr)) my_rec[fill++] = pr;
+                if (point_terms(cam, bins, B, r, th, dl, z, pr)) my_rec[fill++] = pr;
             } else {
                 transfer_point<MIXED>(cam, bins, B, tb, acc, r, th, dl, z);
             }
@@ -995,13 +1043,13 @@ __global__ void __launch_bounds__(kTPB) path_transfer_kernel(const TraceArgs A)
     const int tid = threadIdx.x;
     double* accT64 = reinterpret_cast<double*>(smem + L.off_acc) + tid;
     double* accI64 = accT64 + size_t(kTPB) * A.max_bins;
-    float* accT = reinterpret_cast<float*>(smem + L.off_acc) + tid;
-    float* accTc = accT + size_t(kTPB) * A.max_bins;
-    float* accI = accTc + size_t(kTPB) * A.max_bins;
+    float* accV = reinterpret_cast<float*>(smem + L.off_acc) + tid;
+    float* accVc = accV + size_t(kTPB) * A.max_bins;
+    float* accI = accVc + size_t(kTPB) * A.max_bins;
     float* accIc = accI + size_t(kTPB) * A.max_bins;
     float* accS = accIc + size_t(kTPB) * A.max_bins;
     const SmemTables tb{sE, sS, slnE, slnS, slx, sseg, n_sig, A.sig.E_min, A.sig.E_max, A.sig.sigma_scale, A.sig.uniform, A.sig.lx0, A.sig.inv_dlx};
-    const BinAcc acc{accT64, accI64, accT, accTc, accI, accIc, accS, kTPB};
+    const BinAcc acc{accT64, accI64, accV, accVc, accI, accIc, accS, kTPB};
     const DevCam* cam = A.cams;
     const DevBin* bins = A.bins + cam->bin_offset;
     const int B = cam->n_bins;
