@@ -276,6 +276,11 @@ SIGNATURES = {
                                           C.c_void_p, C.c_void_p, C.c_int64, P(HadrosAdam), C.c_int64,
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p]),
+    "hadros_mlp_members_workspace_bytes": (C.c_int64, [C.c_int32, C.c_int64]),
+    "hadros_mlp_train_members": (C.c_int32, [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, P(HadrosAdam), C.c_int64, C.c_void_p,
+                                             C.c_void_p, C.c_void_p]),
     "hadros_mlp_image_bytes": (C.c_int64, []),
     "hadros_surrogate_schedule": (C.c_int32, [C.c_int32]),
     "hadros_mlp_pack_image": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -1,18 +1,22 @@
 // hadros_mlp.cu — training kernels of the surrogate network and their C-ABI
 // entry points (no counterpart in the reference).
 //
-// Every product of the 256-wide layers runs on the tensor cores through one
-// BF16 GEMM kernel (mma.sync m16n8k16, FP32 accumulation, cp.async double
-// buffering, ldmatrix with or without transposition for the three operand
-// layouts of a forward and backward pass) whose epilogue is fused with the
-// surrounding elementwise work:
+// Every product of the 256-wide layers runs on the 5th-generation tensor
+// cores through one GEMM kernel (tcgen05.mma into tensor memory, BF16
+// operands, FP32 accumulation; operands staged by cp.async in the 128-byte
+// swizzled K-major or MN-major layouts the three products of a forward and
+// backward pass need) whose epilogue is fused with the surrounding
+// elementwise work:
 //   forward      Z_l = H_{l-1} W_l^T + b_l,  H_l = SiLU(Z_l)     (both BF16;
 //                SiLU in packed BF16 from h = Z_l / 2, hadros_mlp.cuh)
 //   data grad    dZ_{l-1} = (dZ_l W_l) * SiLU'(Z_{l-1})          (BF16)
-//   weight grad  G_Wl += dZ_l^T H_{l-1}   (split over the batch, FP32 atomics)
-// The 2-output last layer, the loss, bias gradients and Adam are small
-// CUDA-core kernels.  The FP32 master parameters live in one flat array
-// (layout in hadros_mlp.cuh) so Adam is one elementwise pass.
+//   weight grad  G_Wl += dZ_l^T H_{l-1}   (split over the batch, FP32 vector
+//                reductions)
+// Several networks (the members of an ensemble) train side by side in the
+// same launches (hadros_mlp_train_members).  The 2-output last layer, the
+// loss, bias gradients and Adam are small CUDA-core kernels.  The FP32 master
+// parameters live in one flat array (layout in hadros_mlp.cuh) so Adam is one
+// elementwise pass.
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 
@@ -23,6 +27,7 @@
 #include "hadros_b200.h"
 #include "hadros_internal.h"
 #include "hadros_mlp.cuh"
+#include "hadros_umma.cuh"
 
 namespace hadros {
 namespace mlp {
@@ -30,207 +35,274 @@ namespace {
 
 using bf16 = __nv_bfloat16;
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p)
-{
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
 // 16-byte global->shared copy; zero-fills when !valid (src-size 0).
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid)
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid)
 {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
-                 "r"(valid ? 16 : 0));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-__device__ __forceinline__ void ldsm_x4(uint32_t r[4], const void* p)
-{
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(smem_u32(p)));
-}
-__device__ __forceinline__ void ldsm_x4_t(uint32_t r[4], const void* p)
-{
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(smem_u32(p)));
-}
-__device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const uint32_t b[2])
-{
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-        "{%8,%9}, {%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
+// ---- GEMM on the 5th-generation tensor cores -----------------------------------
+// C[m][n] = sum_k A(m,k) B(k,n) for k in one split [kb, kb + k_split), then
+// epi(member, m, n0, 32 FP32 values of columns n0..n0+31).
+//   A_MN: A(m,k) = A[k*lda + m] (MN-major), else A[m*lda + k] (K-major)
+//   B_MN: B(k,n) = B[k*ldb + n] (MN-major), else B[n*ldb + k] (K-major)
+// One CTA computes a 128 x BN tile (BN = 256 or 64) of one member
+// (grid.z = member * splits + split).  K runs in chunks of 64 through a
+// three-stage shared-memory ring that all four warps fill with cp.async, each
+// 16-byte unit written where the 128-byte swizzle of the UMMA layout puts it:
+// K-major tiles are rows of 64 k (128 B) in 8-row groups 1024 B apart;
+// MN-major tiles are atoms of 64 m or n (one 128-byte row per k) by 8 k,
+// atoms along K 1024 B apart and along MN 8 KB apart.  One thread issues
+// tcgen05.mma (M = 128, N = BN, K = 16, BF16 -> FP32) into a TMEM accumulator
+// and commits each chunk to that stage's mbarrier, which frees the stage for
+// the chunk three ahead.  The epilogue reads each warp's 32 rows with
+// tcgen05.ld.  Rows and k beyond M, K load as zeros and are not stored.
+// Every wait is bounded; a timeout stores NaN in *fail (the step's loss),
+// which the host sees.
+constexpr int UM = 128, UK = 64, kUStages = 3, kUThreads = 128;
+constexpr int kMnLbo = (UK / 8) * 1024;   // MN-major: bytes between 64-wide MN blocks
 
-// ---- GEMM: C[m][n] = sum_k A(m,k) B(k,n), then epi(m, n, c[n], c[n+1]) ------
-//   A_K: A(m,k) = A[m*lda + k]  (else A[k*lda + m])
-//   B_K: B(k,n) = B[n*ldb + k]  (else B[k*ldb + n])
-// M, N, K and the split length are multiples of 8 (16-byte chunks); rows and
-// columns past M, N, K are zero-filled on load and skipped on store.
-constexpr int BM = 128, BN = 128, BK = 32, kGemmThreads = 256;
-constexpr int LDK = BK + 8;    // K-contiguous smem rows (80 B: conflict-free ldmatrix)
-constexpr int LDMN = BM + 8;   // MN-contiguous smem rows (272 B)
-constexpr int kTile = (BM * LDK > BK * LDMN) ? BM * LDK : BK * LDMN;
+template <int BN>
+struct UTile {
+    static constexpr int kA = UM * UK * 2;
+    static constexpr int kB = BN * UK * 2;
+    static constexpr int kStage = kA + kB;
+    static constexpr int kSmem = kUStages * kStage + 1024 + 128;
+};
 
-template <bool A_K, bool B_K, class Epi>
-__global__ void __launch_bounds__(kGemmThreads)
-    gemm_kernel(const bf16* __restrict__ A, long lda, const bf16* __restrict__ B, long ldb, int M,
-                int N, int K, int k_split, Epi epi)
+template <bool A_MN, bool B_MN, int BN, class Epi>
+__global__ void __launch_bounds__(kUThreads, 1)
+    umma_gemm(const bf16* __restrict__ A, long lda, long a_mem, const bf16* __restrict__ B, long ldb, long b_mem,
+              int M, int N, int K, int k_split, int splits, Epi epi, float* fail)
 {
-    __shared__ __align__(16) bf16 sA[2][kTile];
-    __shared__ __align__(16) bf16 sB[2][kTile];
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    const int kb = blockIdx.z * k_split;
-    const int ke = min(K, kb + k_split);
+    using namespace umma;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kUStages * UTile<BN>::kStage);
+    uint64_t* mma_done = bars;                    // [kUStages]
+    uint64_t* acc_ready = bars + kUStages;
+    uint64_t* drain = bars + kUStages + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kUStages + 2);
+    __shared__ int s_abort;
+    volatile int* abort_flag = &s_abort;
+
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int wm = warp >> 2, wn = warp & 3;   // 2 x 4 warps, 64 x 32 each
+    const int mem = blockIdx.z / splits, split = blockIdx.z % splits;
+    A += mem * a_mem;
+    B += mem * b_mem;
+    const int m0 = blockIdx.y * UM, n0 = blockIdx.x * BN;
+    const int kb = split * k_split;
+    const int ke = min(K, kb + k_split);
+    const int nk = ke > kb ? (ke - kb + UK - 1) / UK : 0;
+
+    if (tid == 0) {
+        s_abort = 0;
+        for (int s = 0; s < kUStages; ++s) mbar_init(saddr(&mma_done[s]), 1);
+        mbar_init(saddr(acc_ready), 1);
+        mbar_init(saddr(drain), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(saddr(tmem_slot)),
+                     "r"(BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
 
     auto load = [&](int st, int k0) {
-        for (int c = tid; c < 512; c += kGemmThreads) {
-            if (A_K) {
-                const int row = c >> 2, kc = (c & 3) * 8, gm = m0 + row, gk = k0 + kc;
+        const uint32_t sa = saddr(smem + st * UTile<BN>::kStage);
+        const uint32_t sb = sa + UTile<BN>::kA;
+        if (!A_MN) {
+            for (int c = tid; c < UM * 8; c += kUThreads) {
+                const int row = c >> 3, u = c & 7, gm = m0 + row, gk = k0 + u * 8;
                 const bool v = gm < M && gk < ke;
-                cp_async16(&sA[st][row * LDK + kc], v ? A + long(gm) * lda + gk : A, v);
-            } else {
-                const int row = c >> 4, mc = (c & 15) * 8, gk = k0 + row, gm = m0 + mc;
-                const bool v = gk < ke && gm < M;
-                cp_async16(&sA[st][row * LDMN + mc], v ? A + long(gk) * lda + gm : A, v);
+                cp_async16(sa + row * 128 + ((u ^ (row & 7)) << 4), v ? A + long(gm) * lda + gk : A, v);
             }
-            if (B_K) {
-                const int row = c >> 2, kc = (c & 3) * 8, gn = n0 + row, gk = k0 + kc;
+        } else {
+            for (int c = tid; c < UK * (UM / 8); c += kUThreads) {
+                const int kr = c / (UM / 8), u = c % (UM / 8), gk = k0 + kr, gm = m0 + u * 8;
+                const bool v = gk < ke && gm < M;
+                cp_async16(sa + (u >> 3) * kMnLbo + (kr >> 3) * 1024 + (kr & 7) * 128 + (((u & 7) ^ (kr & 7)) << 4),
+                           v ? A + long(gk) * lda + gm : A, v);
+            }
+        }
+        if (!B_MN) {
+            for (int c = tid; c < BN * 8; c += kUThreads) {
+                const int row = c >> 3, u = c & 7, gn = n0 + row, gk = k0 + u * 8;
                 const bool v = gn < N && gk < ke;
-                cp_async16(&sB[st][row * LDK + kc], v ? B + long(gn) * ldb + gk : B, v);
-            } else {
-                const int row = c >> 4, nc = (c & 15) * 8, gk = k0 + row, gn = n0 + nc;
+                cp_async16(sb + row * 128 + ((u ^ (row & 7)) << 4), v ? B + long(gn) * ldb + gk : B, v);
+            }
+        } else {
+            for (int c = tid; c < UK * (BN / 8); c += kUThreads) {
+                const int kr = c / (BN / 8), u = c % (BN / 8), gk = k0 + kr, gn = n0 + u * 8;
                 const bool v = gk < ke && gn < N;
-                cp_async16(&sB[st][row * LDMN + nc], v ? B + long(gk) * ldb + gn : B, v);
+                cp_async16(sb + (u >> 3) * kMnLbo + (kr >> 3) * 1024 + (kr & 7) * 128 + (((u & 7) ^ (kr & 7)) << 4),
+                           v ? B + long(gk) * ldb + gn : B, v);
             }
         }
     };
 
-    float acc[4][4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0f;
-
-    const int nk = ke > kb ? (ke - kb + BK - 1) / BK : 0;
-    if (nk > 0) load(0, kb);
-    cp_async_commit();
-    for (int t = 0; t < nk; ++t) {
-        if (t + 1 < nk) load((t + 1) & 1, kb + (t + 1) * BK);
+    constexpr uint32_t idesc = idesc_bf16_major(UM, BN, A_MN, B_MN);
+    bool mma_issued = false;
+    for (int t = 0; t < kUStages - 1; ++t) {
+        if (t < nk) load(t, kb + t * UK);
         cp_async_commit();
-        cp_async_wait<1>();
-        __syncthreads();
-        const int s = t & 1;
-#pragma unroll
-        for (int ks = 0; ks < 2; ++ks) {
-            uint32_t af[4][4], bfr[4][2];
-#pragma unroll
-            for (int mt = 0; mt < 4; ++mt) {
-                if (A_K) {
-                    const int row = wm * 64 + mt * 16 + (lane & 15), col = ks * 16 + (lane >> 4) * 8;
-                    ldsm_x4(af[mt], &sA[s][row * LDK + col]);
-                } else {
-                    const int krow = ks * 16 + (lane & 7) + (lane >> 4) * 8;
-                    const int m = wm * 64 + mt * 16 + ((lane >> 3) & 1) * 8;
-                    ldsm_x4_t(af[mt], &sA[s][krow * LDMN + m]);
-                }
-            }
-#pragma unroll
-            for (int np = 0; np < 2; ++np) {
-                uint32_t r[4];
-                if (B_K) {
-                    const int n = wn * 32 + np * 16 + (lane & 7) + (lane >> 4) * 8;
-                    const int k = ks * 16 + ((lane >> 3) & 1) * 8;
-                    ldsm_x4(r, &sB[s][n * LDK + k]);
-                } else {
-                    const int krow = ks * 16 + (lane & 7) + ((lane >> 3) & 1) * 8;
-                    const int n = wn * 32 + np * 16 + (lane >> 4) * 8;
-                    ldsm_x4_t(r, &sB[s][krow * LDMN + n]);
-                }
-                bfr[np * 2][0] = r[0];
-                bfr[np * 2][1] = r[1];
-                bfr[np * 2 + 1][0] = r[2];
-                bfr[np * 2 + 1][1] = r[3];
-            }
-#pragma unroll
-            for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-                for (int nt = 0; nt < 4; ++nt) mma_bf16(acc[mt][nt], af[mt], bfr[nt]);
+    }
+    for (int t = 0; t < nk; ++t) {
+        const int tl = t + kUStages - 1;   // the chunk loaded now, into the stage chunk t-1 used
+        if (tl < nk) {
+            const int st = tl % kUStages;
+            bool ok = true;
+            if (tl >= kUStages) ok = mbar_wait(saddr(&mma_done[st]), uint32_t((tl / kUStages - 1) & 1), abort_flag);
+            if (ok) load(st, kb + tl * UK);
         }
+        cp_async_commit();
+        cp_async_wait<kUStages - 1>();    // this thread's copies of chunk t have landed
+        fence_async_smem();               // and are visible to the tensor cores
         __syncthreads();
+        if (tid == 0 && !*abort_flag) {
+            tc_fence_after();
+            const uint32_t sa = saddr(smem + (t % kUStages) * UTile<BN>::kStage);
+            const uint32_t sb = sa + UTile<BN>::kA;
+            for (int kk = 0; kk < UK / 16; ++kk) {
+                const uint64_t da = A_MN ? sdesc_mn(sa + kk * 2048, kMnLbo, 1024) : sdesc(sa + kk * 32);
+                const uint64_t db = B_MN ? sdesc_mn(sb + kk * 2048, kMnLbo, 1024) : sdesc(sb + kk * 32);
+                tc_mma(tmem, da, db, idesc, (t | kk) != 0);
+            }
+            mma_issued = true;
+            tc_commit(saddr(&mma_done[t % kUStages]));
+        }
     }
     cp_async_wait<0>();
-
-    const int g = lane >> 2, c2 = (lane & 3) * 2;
+    if (tid == 0) {
+        if (mma_issued) tc_commit(saddr(acc_ready));
+        else mbar_arrive(saddr(acc_ready));   // nothing accumulated: the epilogue adds zeros
+    }
+    const bool ok = warp_wait(saddr(acc_ready), 0, abort_flag);
+    tc_fence_after();
+    if (ok && !*abort_flag) {
+        const uint32_t lane_base = tmem + (uint32_t(warp * 32) << 16);
+        const int m = m0 + warp * 32 + lane;
+        uint32_t v[32];
+#pragma unroll 1
+        for (int cb = 0; cb < BN; cb += 32) {
+            tc_ld32(lane_base + uint32_t(cb), v);
+            tc_wait_ld(v);
+            if (nk == 0) {
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-            const int m = m0 + wm * 64 + mt * 16 + g, n = n0 + wn * 32 + nt * 8 + c2;
-            if (n < N) {
-                if (m < M) epi(m, n, acc[mt][nt][0], acc[mt][nt][1]);
-                if (m + 8 < M) epi(m + 8, n, acc[mt][nt][2], acc[mt][nt][3]);
+                for (int q = 0; q < 32; ++q) v[q] = 0u;
             }
+            if (m < M && n0 + cb < N) epi(mem, m, n0 + cb, reinterpret_cast<const float*>(v));
         }
+    }
+    if (*abort_flag && tid == 0) {
+        *fail = __int_as_float(0x7fc00000);
+        if (mma_issued) {   // let the MMAs in flight finish before TMEM is released
+            tc_commit(saddr(drain));
+            mbar_wait_plain(saddr(drain), 0);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(BN) : "memory");
 }
 
 struct EpiHidden {   // Z = acc + b (BF16, for the backward pass), H = SiLU(acc + b)
     const float* bias;
+    long bias_mem;    // floats between members' biases
     bf16* Z;
     bf16* H;
-    __device__ void operator()(int m, int n, float v0, float v1) const
+    long act_mem;     // elements between members' activations
+    __device__ void operator()(int mem, int m, int n, const float* v) const
     {
-        const float z0 = v0 + bias[n], z1 = v1 + bias[n + 1];
-        const long o = long(m) * kW + n;
-        if (Z) *reinterpret_cast<uint32_t*>(Z + o) = pack_bf16x2(z0, z1);
-        *reinterpret_cast<uint32_t*>(H + o) = silu_half_bf16x2(0.5f * z0, 0.5f * z1);
+        const float* b = bias + mem * bias_mem + n;
+        const long o = mem * act_mem + long(m) * kW + n;
+        uint32_t z[16], h[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const float z0 = v[2 * q] + b[2 * q], z1 = v[2 * q + 1] + b[2 * q + 1];
+            z[q] = pack_bf16x2(z0, z1);
+            h[q] = silu_half_bf16x2(0.5f * z0, 0.5f * z1);
+        }
+        if (Z)
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                *reinterpret_cast<uint4*>(Z + o + 8 * u) = make_uint4(z[4 * u], z[4 * u + 1], z[4 * u + 2], z[4 * u + 3]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            *reinterpret_cast<uint4*>(H + o + 8 * u) = make_uint4(h[4 * u], h[4 * u + 1], h[4 * u + 2], h[4 * u + 3]);
     }
 };
 
 struct EpiBwdData {   // dZ_prev = acc * SiLU'(Z_prev)
     const bf16* Zp;
     bf16* dZp;
-    __device__ void operator()(int m, int n, float v0, float v1) const
+    long act_mem;
+    __device__ void operator()(int mem, int m, int n, const float* v) const
     {
-        const long o = long(m) * kW + n;
-        const float2 z = unpack_bf16x2(*reinterpret_cast<const uint32_t*>(Zp + o));
-        *reinterpret_cast<uint32_t*>(dZp + o) = pack_bf16x2(v0 * silu_grad_f(z.x), v1 * silu_grad_f(z.y));
+        const long o = mem * act_mem + long(m) * kW + n;
+        uint32_t d[16];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint4 zz = *reinterpret_cast<const uint4*>(Zp + o + 8 * u);
+            const uint32_t zw[4] = {zz.x, zz.y, zz.z, zz.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float2 z = unpack_bf16x2(zw[q]);
+                const int c = 8 * u + 2 * q;
+                d[4 * u + q] = pack_bf16x2(v[c] * silu_grad_f(z.x), v[c + 1] * silu_grad_f(z.y));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            *reinterpret_cast<uint4*>(dZp + o + 8 * u) = make_uint4(d[4 * u], d[4 * u + 1], d[4 * u + 2], d[4 * u + 3]);
     }
 };
 
 struct EpiWgrad {   // G[m][n] += acc (partial sums over a slice of the batch)
     float* G;
     int ldg;
-    __device__ void operator()(int m, int n, float v0, float v1) const
+    long g_mem;       // floats between members' gradients
+    __device__ void operator()(int mem, int m, int n, const float* v) const
     {
-        atomicAdd(G + long(m) * ldg + n, v0);
-        atomicAdd(G + long(m) * ldg + n + 1, v1);
+        float* g = G + mem * g_mem + long(m) * ldg + n;
+#pragma unroll
+        for (int q = 0; q < 32; q += 4)
+            asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"l"(g + q), "f"(v[q]), "f"(v[q + 1]),
+                         "f"(v[q + 2]), "f"(v[q + 3])
+                         : "memory");
     }
 };
 
-template <bool A_K, bool B_K, class Epi>
-void gemm(const bf16* A, long lda, const bf16* B, long ldb, int M, int N, int K, int splits, Epi epi,
-          cudaStream_t st)
+template <bool A_MN, bool B_MN, int BN, class Epi>
+void gemm(const bf16* A, long lda, long a_mem, const bf16* B, long ldb, long b_mem, int M, int N, int K, int splits,
+          int members, Epi epi, float* fail, cudaStream_t st)
 {
     int k_split = (K + splits - 1) / splits;
-    k_split = (k_split + BK - 1) / BK * BK;
-    splits = (K + k_split - 1) / k_split;
-    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, std::max(splits, 1));
-    gemm_kernel<A_K, B_K, Epi><<<grid, kGemmThreads, 0, st>>>(A, lda, B, ldb, M, N, K, k_split, epi);
+    k_split = (k_split + UK - 1) / UK * UK;
+    splits = std::max((K + k_split - 1) / k_split, 1);
+    auto kern = umma_gemm<A_MN, B_MN, BN, Epi>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, UTile<BN>::kSmem);
+    dim3 grid((N + BN - 1) / BN, (M + UM - 1) / UM, members * splits);
+    kern<<<grid, kUThreads, UTile<BN>::kSmem, st>>>(A, lda, a_mem, B, ldb, b_mem, M, N, K, k_split, splits, epi,
+                                                   fail);
 }
 
 // ---- small kernels ----------------------------------------------------------
 
 __global__ void k_pack(const float* __restrict__ master, bf16* __restrict__ packed)
 {
+    master += long(blockIdx.y) * kParams;
+    packed += long(blockIdx.y) * kPacked;
     const long idx = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= kPacked) return;
     float v;
@@ -263,11 +335,28 @@ __global__ void k_featurize(const float* __restrict__ raw, long n, Norm nm, bf16
         reinterpret_cast<uint4*>(X + s * kIn)[q] = reinterpret_cast<const uint4*>(row)[q];
 }
 
+// Strides between the arrays of networks trained side by side; the small
+// kernels take their member from blockIdx.y.
+struct Mem {
+    long x;     // input rows X (elements)
+    long p;     // packed weights (elements)
+    long m;     // master parameters and gradients (floats)
+    long act;   // workspace activations (elements)
+    long n;     // samples per member
+};
+
 // out[s][o] = W5[o] . H4[s] + b5[o] + Ws[o] . x[s]   (one warp per sample)
 __global__ void k_top_forward(const bf16* __restrict__ H4, const bf16* __restrict__ X,
-                              const bf16* __restrict__ W5b, const float* __restrict__ master, long n,
+                              const bf16* __restrict__ W5b, const float* __restrict__ master, Mem mm,
                               float* __restrict__ out)
 {
+    const int k = blockIdx.y;
+    H4 += k * mm.act;
+    X += k * mm.x;
+    W5b += k * mm.p;
+    master += k * mm.m;
+    out += k * mm.n * kOut;
+    const long n = mm.n;
     const long s = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (s >= n) return;
@@ -299,12 +388,17 @@ __global__ void k_top_forward(const bf16* __restrict__ H4, const bf16* __restric
     }
 }
 
-// Weighted squared error: loss += scale * w * (out - t)^2, dout = 2 scale w (out - t).
+// Weighted squared error: loss[k] += scale * w * (out - t)^2, dout = 2 scale w (out - t).
 __global__ void k_loss(const float* __restrict__ out, const float* __restrict__ t,
                        const float* __restrict__ w, long n, float scale, float* __restrict__ dout,
                        float* __restrict__ loss)
 {
     __shared__ float red[32];
+    const int k = blockIdx.y;
+    out += k * n * kOut;
+    t += k * n * kOut;
+    dout += k * n * kOut;
+    if (w) w += k * n;
     float l = 0.0f;
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n * kOut; i += long(gridDim.x) * blockDim.x) {
         const float ws = w ? w[i / kOut] : 1.0f;
@@ -318,7 +412,7 @@ __global__ void k_loss(const float* __restrict__ out, const float* __restrict__ 
     if (threadIdx.x < 32) {
         l = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0f;
         for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
-        if (threadIdx.x == 0 && loss) atomicAdd(loss, l);
+        if (threadIdx.x == 0 && loss) atomicAdd(loss + k, l);
     }
 }
 
@@ -327,9 +421,18 @@ __global__ void k_loss(const float* __restrict__ out, const float* __restrict__ 
 //   G_Ws += dout^T x.
 __global__ void __launch_bounds__(kW) k_top_backward(const float* __restrict__ dout, const bf16* __restrict__ W5b,
                                                       const bf16* __restrict__ Z4, const bf16* __restrict__ H4,
-                                                      const bf16* __restrict__ X, long n, int chunk,
+                                                      const bf16* __restrict__ X, Mem mm, int chunk,
                                                       bf16* __restrict__ dZ4, float* __restrict__ G)
 {
+    const int k = blockIdx.y;
+    const long n = mm.n;
+    dout += k * n * kOut;
+    W5b += k * mm.p;
+    Z4 += k * mm.act;
+    H4 += k * mm.act;
+    X += k * mm.x;
+    dZ4 += k * mm.act;
+    G += k * mm.m;
     const int i = threadIdx.x;
     const long s0 = long(blockIdx.x) * chunk, s1 = min(n, s0 + chunk);
     const float w0 = __bfloat162float(W5b[i]), w1 = __bfloat162float(W5b[kW + i]);
@@ -354,11 +457,14 @@ __global__ void __launch_bounds__(kW) k_top_backward(const float* __restrict__ d
     else if (i < 2 * kF + kOut) atomicAdd(G + kOffB5 + (i - 2 * kF), gx);
 }
 
-__global__ void __launch_bounds__(kW) k_bias_grad(const bf16* __restrict__ dZ, long n, int chunk,
-                                                   float* __restrict__ Gb)
+__global__ void __launch_bounds__(kW) k_bias_grad(const bf16* __restrict__ dZ, Mem mm, int chunk, long g_off,
+                                                   float* __restrict__ G)
 {
+    const int k = blockIdx.y;
+    dZ += k * mm.act;
+    float* Gb = G + k * mm.m + g_off;
     const int i = threadIdx.x;
-    const long s0 = long(blockIdx.x) * chunk, s1 = min(n, s0 + chunk);
+    const long s0 = long(blockIdx.x) * chunk, s1 = min(mm.n, s0 + chunk);
     float g = 0.0f;
     for (long s = s0; s < s1; ++s) g += __bfloat162float(dZ[s * kW + i]);
     atomicAdd(Gb + i, g);
@@ -366,8 +472,12 @@ __global__ void __launch_bounds__(kW) k_bias_grad(const bf16* __restrict__ dZ, l
 
 // Tied hi/lo first-layer weights: G_W1[o][j] += dW[o][j] + dW[o][j+16] for
 // the features, G_W1[o][16+q] += dW[o][32+q] for the Fourier columns.
-__global__ void k_fold_w1(const float* __restrict__ dW1, float* __restrict__ G)
+// dW1 of member k at dW1 + k * dw_mem floats.
+__global__ void k_fold_w1(const float* __restrict__ dW1, long dw_mem, float* __restrict__ G, long g_mem)
 {
+    const int k = blockIdx.y;
+    dW1 += k * dw_mem;
+    G += k * g_mem;
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= kW * kW1In) return;
     const int o = idx / kW1In, j = idx % kW1In;
@@ -375,17 +485,33 @@ __global__ void k_fold_w1(const float* __restrict__ dW1, float* __restrict__ G)
 }
 
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
-                       const float* __restrict__ g, long count, float lr, float b1, float b2, float eps,
-                       float inv_bc1, float inv_bc2)
+                       const float* __restrict__ g, long count, long stride, float lr, float b1, float b2,
+                       float eps, float inv_bc1, float inv_bc2)
 {
+    const long off = long(blockIdx.y) * stride;
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    const float gi = g[i];
-    const float mi = fmaf(b1, m[i], (1.0f - b1) * gi);
-    const float vi = fmaf(b2, v[i], (1.0f - b2) * gi * gi);
-    m[i] = mi;
-    v[i] = vi;
-    w[i] -= lr * (mi * inv_bc1) / (sqrtf(vi * inv_bc2) + eps);
+    const float gi = g[off + i];
+    const float mi = fmaf(b1, m[off + i], (1.0f - b1) * gi);
+    const float vi = fmaf(b2, v[off + i], (1.0f - b2) * gi * gi);
+    m[off + i] = mi;
+    v[off + i] = vi;
+    w[off + i] -= lr * (mi * inv_bc1) / (sqrtf(vi * inv_bc2) + eps);
+}
+
+// Rows idx[k][s] of the shared inputs and targets -> member k's batch.
+__global__ void k_gather(const bf16* __restrict__ X_all, const float* __restrict__ T_all,
+                         const float* __restrict__ W_all, const int64_t* __restrict__ idx, long idx_mem, long n,
+                         bf16* __restrict__ X, float* __restrict__ T, float* __restrict__ Wt)
+{
+    const int k = blockIdx.y;
+    const long s = long(blockIdx.x) * (blockDim.x / 8) + threadIdx.x / 8;
+    const int u = threadIdx.x & 7;   // 16-byte unit of the 128-byte row
+    if (s >= n) return;
+    const int64_t r = idx[k * idx_mem + s];
+    reinterpret_cast<uint4*>(X + (k * n + s) * kIn)[u] = reinterpret_cast<const uint4*>(X_all + r * kIn)[u];
+    if (u < kOut) T[(k * n + s) * kOut + u] = T_all[r * kOut + u];
+    if (u == kOut && W_all) Wt[k * n + s] = W_all[r];
 }
 
 struct Workspace {
@@ -420,38 +546,62 @@ int32_t cuda_status(const char* what)
 
 int blocks_for(long count, int threads) { return int((count + threads - 1) / threads); }
 
-void forward_impl(const float* master, const bf16* packed, const bf16* X, long n, const Workspace& w,
-                  float* out, cudaStream_t st)
+// One training step's buffers of `members` networks trained side by side
+// (each member's arrays follow one another at the given strides).
+struct Batch {
+    int members;
+    long n;                 // samples per member
+    long x_mem;             // elements between members' input rows X [n][kIn]
+    long p_mem;             // elements between members' packed weights
+    long m_mem;             // floats between members' master parameters / gradients
+    long ws_mem;            // bytes between members' workspaces (a multiple of kWsAlign)
+    Mem mem() const { return Mem{x_mem, p_mem, m_mem, ws_mem / 2, n}; }
+};
+
+void forward_impl(const float* master, const bf16* packed, const bf16* X, const Batch& bt, void* ws, float* out,
+                  float* fail, cudaStream_t st)
 {
-    const int M = int(n);
-    gemm<true, true>(X, kIn, packed + pw(1), kIn, M, kW, kIn, 1,
-                     EpiHidden{master + off_b(1), w.Z[1], w.H[1]}, st);
+    const int M = int(bt.n);
+    const Workspace w = carve(ws, bt.n);
+    const Mem mm = bt.mem();
+    gemm<false, false, 256>(X, kIn, bt.x_mem, packed + pw(1), kIn, bt.p_mem, M, kW, kIn, 1, bt.members,
+                            EpiHidden{master + off_b(1), bt.m_mem, w.Z[1], w.H[1], mm.act}, fail, st);
     for (int l = 2; l <= kDepth; ++l)
-        gemm<true, true>(w.H[l - 1], kW, packed + pw(l), kW, M, kW, kW, 1,
-                         EpiHidden{master + off_b(l), w.Z[l], w.H[l]}, st);
-    k_top_forward<<<blocks_for(n * 32, 256), 256, 0, st>>>(w.H[kDepth], X, packed + pw(5), master, n, out);
+        gemm<false, false, 256>(w.H[l - 1], kW, mm.act, packed + pw(l), kW, bt.p_mem, M, kW, kW, 1, bt.members,
+                                EpiHidden{master + off_b(l), bt.m_mem, w.Z[l], w.H[l], mm.act}, fail, st);
+    k_top_forward<<<dim3(blocks_for(bt.n * 32, 256), bt.members), 256, 0, st>>>(w.H[kDepth], X, packed + pw(5),
+                                                                                master, mm, out);
 }
 
-void backward_impl(const bf16* packed, const bf16* X, long n, const float* dout, const Workspace& w,
-                   float* G, cudaStream_t st)
+void backward_impl(const bf16* packed, const bf16* X, const Batch& bt, const float* dout, void* ws, float* G,
+                   float* fail, cudaStream_t st)
 {
-    const int M = int(n);
+    const int M = int(bt.n);
+    const long n = bt.n;
     const int chunk = 64;
-    const int wsplits = int(std::min<long>(64, std::max<long>(1, n / 512)));
+    const int wsplits = int(std::min<long>(32, std::max<long>(1, n / 256)));
+    const Mem mm = bt.mem();
+    const dim3 gchunk(blocks_for(n, chunk), bt.members);
+    const Workspace w = carve(ws, n);
     bf16* dZ = w.dZa;
     bf16* dZn = w.dZb;
-    k_top_backward<<<blocks_for(n, chunk), kW, 0, st>>>(dout, packed + pw(5), w.Z[kDepth], w.H[kDepth], X, n,
-                                                        chunk, dZ, G);
+    k_top_backward<<<gchunk, kW, 0, st>>>(dout, packed + pw(5), w.Z[kDepth], w.H[kDepth], X, mm, chunk, dZ, G);
     for (int l = kDepth; l >= 2; --l) {
-        gemm<false, false>(dZ, kW, w.H[l - 1], kW, kW, kW, M, wsplits, EpiWgrad{G + off_w(l), kW}, st);
-        k_bias_grad<<<blocks_for(n, chunk), kW, 0, st>>>(dZ, n, chunk, G + off_b(l));
-        gemm<true, false>(dZ, kW, packed + pw(l), kW, M, kW, kW, 1, EpiBwdData{w.Z[l - 1], dZn}, st);
+        // G_l += dZ_l^T H_{l-1}: both operands MN-major (the samples are K)
+        gemm<true, true, 256>(dZ, kW, mm.act, w.H[l - 1], kW, mm.act, kW, kW, M, wsplits, bt.members,
+                              EpiWgrad{G + off_w(l), kW, bt.m_mem}, fail, st);
+        k_bias_grad<<<gchunk, kW, 0, st>>>(dZ, mm, chunk, off_b(l), G);
+        // dZ_{l-1} = (dZ_l W_l) * SiLU'(Z_{l-1}): W_l[out][in] is the MN-major B
+        gemm<false, true, 256>(dZ, kW, mm.act, packed + pw(l), kW, bt.p_mem, M, kW, kW, 1, bt.members,
+                               EpiBwdData{w.Z[l - 1], dZn, mm.act}, fail, st);
         std::swap(dZ, dZn);
     }
-    cudaMemsetAsync(w.dW1, 0, sizeof(float) * kW * kIn, st);
-    gemm<false, false>(dZ, kW, X, kIn, kW, kIn, M, wsplits, EpiWgrad{w.dW1, kIn}, st);
-    k_bias_grad<<<blocks_for(n, chunk), kW, 0, st>>>(dZ, n, chunk, G + off_b(1));
-    k_fold_w1<<<blocks_for(kW * kW1In, 256), 256, 0, st>>>(w.dW1, G);
+    const long dw_mem = bt.ws_mem / 4;   // floats between members' dW1
+    for (int k = 0; k < bt.members; ++k) cudaMemsetAsync(w.dW1 + k * dw_mem, 0, sizeof(float) * kW * kIn, st);
+    gemm<true, true, 64>(dZ, kW, mm.act, X, kIn, bt.x_mem, kW, kIn, M, wsplits, bt.members,
+                         EpiWgrad{w.dW1, kIn, dw_mem}, fail, st);
+    k_bias_grad<<<gchunk, kW, 0, st>>>(dZ, mm, chunk, off_b(1), G);
+    k_fold_w1<<<dim3(blocks_for(kW * kW1In, 256), bt.members), 256, 0, st>>>(w.dW1, dw_mem, G, bt.m_mem);
 }
 
 Norm to_norm(const hadros_mlp_norm& a)
@@ -515,8 +665,9 @@ int32_t hadros_mlp_forward(const float* master, const void* packed, const void* 
 {
     if (!master || !packed || !X || !workspace || !out || n <= 0 || n > (int64_t(1) << 30))
         return set_error(HADROS_E_ARG, "bad argument (n must be in 1..2^30)");
-    const Workspace w = carve(workspace, n);
-    forward_impl(master, static_cast<const bf16*>(packed), static_cast<const bf16*>(X), n, w, out,
+    const Batch bt{1, n, 0, 0, 0, 0};
+    // a timed-out wait in a GEMM stores NaN in out[0]
+    forward_impl(master, static_cast<const bf16*>(packed), static_cast<const bf16*>(X), bt, workspace, out, out,
                  static_cast<cudaStream_t>(stream));
     return cuda_status("hadros_mlp_forward");
 }
@@ -526,8 +677,9 @@ int32_t hadros_mlp_backward(const void* packed, const void* X, int64_t n, const 
 {
     if (!packed || !X || !dout || !workspace || !grad || n <= 0 || n > (int64_t(1) << 30))
         return set_error(HADROS_E_ARG, "bad argument (n must be in 1..2^30)");
-    const Workspace w = carve(workspace, n);
-    backward_impl(static_cast<const bf16*>(packed), static_cast<const bf16*>(X), n, dout, w, grad,
+    const Batch bt{1, n, 0, 0, 0, 0};
+    // a timed-out wait in a GEMM stores NaN in grad[0]
+    backward_impl(static_cast<const bf16*>(packed), static_cast<const bf16*>(X), bt, dout, workspace, grad, grad,
                   static_cast<cudaStream_t>(stream));
     return cuda_status("hadros_mlp_backward");
 }
@@ -549,7 +701,8 @@ int32_t hadros_mlp_adam(float* master, float* m, float* v, const float* grad, co
     const float bc1 = 1.0f - std::pow(opt->beta1, float(step));
     const float bc2 = 1.0f - std::pow(opt->beta2, float(step));
     k_adam<<<blocks_for(kParamsUsed, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        master, m, v, grad, kParamsUsed, opt->lr, opt->beta1, opt->beta2, opt->eps, 1.0f / bc1, 1.0f / bc2);
+        master, m, v, grad, kParamsUsed, kParams, opt->lr, opt->beta1, opt->beta2, opt->eps, 1.0f / bc1,
+        1.0f / bc2);
     return cuda_status("hadros_mlp_adam");
 }
 
@@ -562,16 +715,59 @@ int32_t hadros_mlp_train_step(float* master, void* packed, float* m, float* v, c
         n <= 0 || n > (int64_t(1) << 30) || step < 1)
         return set_error(HADROS_E_ARG, "bad argument");
     auto st = static_cast<cudaStream_t>(stream);
-    const Workspace w = carve(workspace, n);
     auto* pk = static_cast<bf16*>(packed);
     auto* x = static_cast<const bf16*>(X);
-    forward_impl(master, pk, x, n, w, out, st);
+    const Batch bt{1, n, 0, 0, 0, 0};
+    forward_impl(master, pk, x, bt, workspace, out, loss ? loss : out, st);
     if (int32_t rc = hadros_mlp_loss(out, target, weight, n, dout, loss, stream)) return rc;
     cudaMemsetAsync(grad, 0, sizeof(float) * kParams, st);
-    backward_impl(pk, x, n, dout, w, grad, st);
+    backward_impl(pk, x, bt, dout, workspace, grad, loss ? loss : grad, st);
     if (int32_t rc = hadros_mlp_adam(master, m, v, grad, opt, step, stream)) return rc;
     k_pack<<<blocks_for(kPacked, 256), 256, 0, st>>>(master, pk);
     return cuda_status("hadros_mlp_train_step");
+}
+
+int64_t hadros_mlp_members_workspace_bytes(int32_t members, int64_t batch)
+{
+    if (members < 1 || batch < 1) return 0;
+    return int64_t(members) * (ws_bytes(batch) + members_batch_bytes(batch)) + kWsAlign;
+}
+
+int32_t hadros_mlp_train_members(int32_t members, int64_t n, const void* X_all, const float* T_all,
+                                 const float* W_all, const int64_t* idx, int64_t idx_stride, float* masters,
+                                 void* packed, float* m, float* v, float* grad, const hadros_adam* opt,
+                                 int64_t step, void* workspace, float* loss, void* stream)
+{
+    if (members < 1 || members > 64 || n <= 0 || n > (int64_t(1) << 26) || !X_all || !T_all || !idx ||
+        !masters || !packed || !m || !v || !grad || !opt || !workspace || !loss || step < 1 || idx_stride < n)
+        return set_error(HADROS_E_ARG, "bad argument");
+    auto st = static_cast<cudaStream_t>(stream);
+    // workspace: each member's layer workspace, then the members' batch buffers
+    char* base =
+        reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(workspace) + kWsAlign - 1) / kWsAlign * kWsAlign);
+    const long wsb = ws_bytes(n);
+    char* bb = base + long(members) * wsb;
+    auto* X = reinterpret_cast<bf16*>(bb);
+    auto* T = reinterpret_cast<float*>(bb + long(members) * n * kIn * 2);
+    auto* Wt = T + long(members) * n * kOut;
+    auto* out = Wt + long(members) * n;
+    auto* dout = out + long(members) * n * kOut;
+    k_gather<<<dim3(blocks_for(n * 8, 256), members), 256, 0, st>>>(
+        static_cast<const bf16*>(X_all), T_all, W_all, idx, idx_stride, n, X, T, W_all ? Wt : nullptr);
+    auto* pk = static_cast<bf16*>(packed);
+    const Batch bt{members, n, n * kIn, kPacked, kParams, wsb};
+    forward_impl(masters, pk, X, bt, base, out, loss, st);
+    k_loss<<<dim3(std::min(blocks_for(n * kOut, 256), 1024), members), 256, 0, st>>>(
+        out, T, W_all ? Wt : nullptr, n, 1.0f / float(n * kOut), dout, loss);
+    cudaMemsetAsync(grad, 0, sizeof(float) * kParams * members, st);
+    backward_impl(pk, X, bt, dout, base, grad, loss, st);
+    const float bc1 = 1.0f - std::pow(opt->beta1, float(step));
+    const float bc2 = 1.0f - std::pow(opt->beta2, float(step));
+    k_adam<<<dim3(blocks_for(kParamsUsed, 256), members), 256, 0, st>>>(
+        masters, m, v, grad, kParamsUsed, kParams, opt->lr, opt->beta1, opt->beta2, opt->eps, 1.0f / bc1,
+        1.0f / bc2);
+    k_pack<<<dim3(blocks_for(kPacked, 256), members), 256, 0, st>>>(masters, pk);
+    return cuda_status("hadros_mlp_train_members");
 }
 
 }  // extern "C"

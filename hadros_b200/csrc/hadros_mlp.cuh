@@ -1,5 +1,5 @@
 // hadros_mlp.cuh — the surrogate network's fixed shape, parameter layouts and
-// the device helpers its training kernels (mma.sync, hadros_mlp.cu) and its
+// the device helpers its training kernels (tcgen05, hadros_mlp.cu) and its
 // fused inference kernel (tcgen05, hadros_mlp_umma.cu) share.
 //
 // The surrogate has no counterpart in the reference: it predicts
@@ -82,6 +82,12 @@ __host__ __device__ constexpr long pw(int layer)       // layer 1..5
 constexpr long kWsAlign = 256;
 __host__ __device__ constexpr long ws_act_bytes(long n) { return n * kW * 2; }
 __host__ __device__ constexpr long ws_bytes(long n) { return 10 * ws_act_bytes(n) + long(kW) * kIn * 4 + kWsAlign; }
+// Batch buffers of one member in hadros_mlp_train_members: X [n][kIn] BF16,
+// targets, weights, outputs and their gradients (FP32), kWsAlign-rounded.
+__host__ __device__ constexpr long members_batch_bytes(long n)
+{
+    return (n * kIn * 2 + n * (3 * kOut + 1) * 4 + kWsAlign - 1) / kWsAlign * kWsAlign;
+}
 
 // Normalization of one model (FP32): features x = (raw - mu) * inv_sd;
 // targets t = (y - out_mu) / out_sd with y = ln(value + floor).

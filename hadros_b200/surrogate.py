@@ -98,18 +98,27 @@ def make_norm(raw, targets, floors=(TAU_FLOOR, 0.0)) -> HadrosMlpNorm:
 
 
 class Network:
-    """One network's device state: FP32 master, BF16 working copy, Adam moments."""
+    """One network's device state: FP32 master, BF16 working copy, Adam moments
+    and gradient (views into the ensemble's stacked arrays when given)."""
 
-    def __init__(self, device, seed: int):
+    def __init__(self, device, seed: int, views: dict | None = None):
         torch = _torch()
         L = lib()
         self.device = torch.device(device)
         self.n_params = int(L.hadros_mlp_param_count())
-        self.master = torch.from_numpy(init_master(seed)).to(self.device)
-        self.packed = torch.empty(int(L.hadros_mlp_packed_count()), dtype=torch.bfloat16, device=self.device)
-        self.m = torch.zeros_like(self.master)
-        self.v = torch.zeros_like(self.master)
-        self.grad = torch.zeros_like(self.master)
+        if views is None:
+            views = {"master": torch.empty(self.n_params, dtype=torch.float32, device=self.device),
+                     "packed": torch.empty(int(L.hadros_mlp_packed_count()), dtype=torch.bfloat16,
+                                           device=self.device),
+                     "m": torch.empty(self.n_params, dtype=torch.float32, device=self.device),
+                     "v": torch.empty(self.n_params, dtype=torch.float32, device=self.device),
+                     "grad": torch.empty(self.n_params, dtype=torch.float32, device=self.device)}
+        self.master, self.packed = views["master"], views["packed"]
+        self.m, self.v, self.grad = views["m"], views["v"], views["grad"]
+        self.master.copy_(torch.from_numpy(init_master(seed)))
+        self.m.zero_()
+        self.v.zero_()
+        self.grad.zero_()
         self.step = 0
         self.pack()
 
@@ -130,7 +139,15 @@ class Surrogate:
         if not 1 <= members <= 8:
             raise ValueError("members must be in 1..8")
         self.device = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
-        self.nets = [Network(self.device, seed * 1000 + k) for k in range(members)]
+        L = lib()
+        P, Pk = int(L.hadros_mlp_param_count()), int(L.hadros_mlp_packed_count())
+        # the members' arrays stacked, so one call trains them side by side
+        f32 = dict(dtype=torch.float32, device=self.device)
+        self.stack = {"master": torch.empty((members, P), **f32), "m": torch.empty((members, P), **f32),
+                      "v": torch.empty((members, P), **f32), "grad": torch.empty((members, P), **f32),
+                      "packed": torch.empty((members, Pk), dtype=torch.bfloat16, device=self.device)}
+        self.nets = [Network(self.device, seed * 1000 + k, {key: t[k] for key, t in self.stack.items()})
+                     for k in range(members)]
         self.norm: HadrosMlpNorm | None = None
         self.seed = seed
         self._images = None
@@ -155,44 +172,53 @@ class Surrogate:
             lr_min: float = 2e-5, weight=None, floors=(TAU_FLOOR, 0.0),
             log_every: int = 0) -> list[list[float]]:
         """Train every member on (raw features, ln targets) with Adam and a cosine
-        learning rate; members see the data in different orders."""
+        learning rate; the members see the data in different orders and step
+        together (one hadros_mlp_train_members call per batch)."""
         torch = _torch()
+        L = lib()
         if self.norm is None:
             self.norm = make_norm(raw, targets, floors)
         X = self.featurize(raw)
         T = self.standardize(targets)
+        W = None if weight is None else weight.float().contiguous()
         n = int(raw.shape[0])
+        K = len(self.nets)
         batch = min(batch, n)
         steps_per_epoch = max(n // batch, 1)
         total = steps_per_epoch * epochs
-        ws = torch.empty(int(lib().hadros_mlp_workspace_bytes(batch)), dtype=torch.uint8, device=self.device)
-        out = torch.empty((batch, N_OUT), dtype=torch.float32, device=self.device)
-        dout = torch.empty_like(out)
-        loss = torch.zeros(1, dtype=torch.float32, device=self.device)
+        ws = torch.empty(int(L.hadros_mlp_members_workspace_bytes(K, batch)), dtype=torch.uint8, device=self.device)
+        idx = torch.empty((K, n), dtype=torch.int64, device=self.device)
+        loss = torch.zeros(K, dtype=torch.float32, device=self.device)
+        gens = []
+        for k in range(K):
+            g = torch.Generator(device=self.device)
+            g.manual_seed(self.seed * 7919 + k)
+            gens.append(g)
         st = _stream_ptr(None)
-        self.history = []
-        for k, net in enumerate(self.nets):
-            gen = torch.Generator(device=self.device)
-            gen.manual_seed(self.seed * 7919 + k)
-            hist = []
-            for ep in range(epochs):
-                perm = torch.randperm(n, device=self.device, generator=gen)
-                loss.zero_()
-                for b in range(steps_per_epoch):
-                    idx = perm[b * batch:(b + 1) * batch]
-                    xb, tb = X[idx].contiguous(), T[idx].contiguous()
-                    wb = None if weight is None else weight[idx].contiguous()
-                    t = net.step / max(total - 1, 1)
-                    opt = HadrosAdam(lr_min + 0.5 * (lr - lr_min) * (1.0 + math.cos(math.pi * t)), 0.9, 0.999, 1e-8)
-                    net.step += 1
-                    _check(lib().hadros_mlp_train_step(
-                        _vp(net.master), _vp(net.packed), _vp(net.m), _vp(net.v), _vp(xb), _vp(tb),
-                        None if wb is None else _vp(wb), batch, C.byref(opt), net.step, _vp(ws),
-                        _vp(net.grad), _vp(out), _vp(dout), _vp(loss), st))
-                hist.append(float(loss.item()) / steps_per_epoch)
-                if log_every and (ep + 1) % log_every == 0:
-                    print(f"member {k} epoch {ep + 1}: loss {hist[-1]:.3e}", flush=True)
-            self.history.append(hist)
+        M, Pk = self.stack["master"], self.stack["packed"]
+        step = self.nets[0].step
+        self.history = [[] for _ in range(K)]
+        for ep in range(epochs):
+            for k in range(K):
+                idx[k] = torch.randperm(n, device=self.device, generator=gens[k])
+            loss.zero_()
+            for b in range(steps_per_epoch):
+                t = step / max(total - 1, 1)
+                opt = HadrosAdam(lr_min + 0.5 * (lr - lr_min) * (1.0 + math.cos(math.pi * t)), 0.9, 0.999, 1e-8)
+                step += 1
+                _check(L.hadros_mlp_train_members(
+                    K, batch, _vp(X), _vp(T), None if W is None else _vp(W),
+                    C.c_void_p(idx.data_ptr() + 8 * b * batch), n, _vp(M), _vp(Pk), _vp(self.stack["m"]),
+                    _vp(self.stack["v"]), _vp(self.stack["grad"]), C.byref(opt), step, _vp(ws), _vp(loss), st))
+            lv = (loss / steps_per_epoch).tolist()
+            if any(math.isnan(x) for x in lv):
+                raise HadrosError(abi.E_TIMEOUT, "NaN training loss: a tensor-core kernel timed out or training diverged")
+            for k in range(K):
+                self.history[k].append(lv[k])
+            if log_every and (ep + 1) % log_every == 0:
+                print(f"epoch {ep + 1}: loss " + " ".join(f"{x:.3e}" for x in lv), flush=True)
+        for net in self.nets:
+            net.step = step
         self._images = None
         return self.history
 
@@ -225,7 +251,7 @@ class Surrogate:
             L = lib()
             nb = int(L.hadros_mlp_image_bytes())
             K = len(self.nets)
-            self._masters = torch.stack([net.master for net in self.nets]).contiguous()
+            self._masters = self.stack["master"]
             self._images = torch.empty(K * nb, dtype=torch.uint8, device=self.device)
             for k, net in enumerate(self.nets):
                 _check(L.hadros_mlp_pack_image(_vp(net.packed), C.c_void_p(self._images.data_ptr() + k * nb),

@@ -624,6 +624,21 @@ int32_t hadros_mlp_train_step(float* master, void* packed, float* m, float* v, c
                               const hadros_adam* opt, int64_t step, void* workspace, float* grad,
                               float* out, float* dout, float* loss, void* stream);
 
+/* Training workspace bytes of hadros_mlp_train_members. */
+int64_t hadros_mlp_members_workspace_bytes(int32_t members, int64_t batch);
+/* One Adam step of `members` networks (an ensemble) trained side by side in
+ * the same launches, each on its own batch of n rows of the shared training
+ * set: member k's rows are idx[k * idx_stride + s], s < n, of X_all
+ * [rows][64] (featurized), T_all [rows][2] and W_all [rows] (may be NULL).
+ * masters, m, v, grad [members][param_count], packed [members][packed_count];
+ * loss[k] += member k's batch loss (a NaN there reports a timed-out wait in
+ * a tensor-core kernel). */
+int32_t hadros_mlp_train_members(int32_t members, int64_t n, const void* X_all, const float* T_all,
+                                 const float* W_all, const int64_t* idx, int64_t idx_stride,
+                                 float* masters, void* packed, float* m, float* v, float* grad,
+                                 const hadros_adam* opt, int64_t step, void* workspace, float* loss,
+                                 void* stream);
+
 /* Bytes of one network's inference image (weights pre-swizzled for the
  * tensor-core kernel) and its construction from the BF16 working copy. */
 int64_t hadros_mlp_image_bytes(void);
