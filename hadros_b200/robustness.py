@@ -184,14 +184,31 @@ def make_rows(table: list[dict], outputs: list[dict], files: list[str] | None = 
     return rows
 
 
-def run(ctx: Context, sigma: SigmaTable, pixels: int = 16, precision: str = "fp64",
-        write_dat: str | None = None, dis_model: str = "GBW") -> tuple[list[dict], dict]:
-    """Every case in one hadros_batch launch; returns (rows, launch stats)."""
+CASE_OUTPUTS = ("tau", "P_surv", "I_obs", "fate", "steps", "tau_mev", "P_surv_mev", "I_obs_mev", "r_nu",
+                "leakage")
+
+
+def run(ctx: Context | None, sigma: SigmaTable, pixels: int = 16, precision: str = "fp64",
+        write_dat: str | None = None, dis_model: str = "GBW", dist=None, rank: int = 0, world: int = 1,
+        trace=None) -> tuple[list[dict] | None, dict]:
+    """Every case in one hadros_batch launch per rank; returns (rows, launch
+    stats).  Under several ranks (dist, rank, world) the cases are split
+    over them (hadros_b200.shard.run_scan) and rank 0 gets every row, the
+    others None.  `trace(cams) -> outputs` replaces ctx.batch (tests trace
+    with the CPU oracle)."""
     table = cases()
     cams = [case_params(c, pixels, precision)[0] for c in table]
-    outs = ctx.batch(cams, sigma, outputs=("tau", "P_surv", "I_obs", "fate", "steps", "tau_mev",
-                                            "P_surv_mev", "I_obs_mev", "r_nu", "leakage"))
-    stats = ctx.stats()
+    if trace is None:
+        def trace(cs):
+            return ctx.batch(cs, sigma, outputs=CASE_OUTPUTS)
+    if world > 1:
+        from . import shard
+        outs = shard.run_scan(cams, trace, dist, rank, world)
+    else:
+        outs = trace(cams)
+    stats = ctx.stats() if ctx is not None else {}
+    if outs is None:
+        return None, stats
     files = None
     if write_dat:
         files = []
@@ -467,12 +484,21 @@ def main(argv=None) -> int:
         print(json.dumps({"images_per_launch": len(rows), "launches": st["launches"], "rays": st["rays"],
                           "kernel_ms": st["kernel_ms"], "csv": str(csv_path), "md": str(md_path)}))
         return 0
-    with Context(a.device) as ctx:
-        rows, st = run(ctx, sig, a.pixels or 16, a.precision, a.write_dat)
+    from . import shard
+    dist, rank, world, local = shard.init_from_env()   # torchrun: the cases are split over the ranks
+    try:
+        with Context(local if world > 1 else a.device) as ctx:
+            rows, st = run(ctx, sig, a.pixels or 16, a.precision, a.write_dat, dist=dist, rank=rank, world=world)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+    if rows is None:
+        return 0
     out = Path(a.outdir or "output/scans")
     csv_path = write_csv(rows, out)
     md_path = write_markdown(rows, out)
-    print(json.dumps({"cases": len(rows), "cameras_per_launch": len(rows), "launches": st["launches"],
+    print(json.dumps({"cases": len(rows), "ranks": world, "cameras_per_launch": len(rows) // world,
+                      "launches": st["launches"],
                       "rays": st["rays"], "kernel_ms": st["kernel_ms"], "total_ms": st["total_ms"],
                       "csv": str(csv_path), "md": str(md_path)}))
     return 0

@@ -1,6 +1,7 @@
 """Surrogate-accelerated parameter scans, timed against the plain tracer.
 
     python -m hadros_b200.scan production --points 256 --side 4096 --bins 64
+    torchrun --nproc-per-node N -m hadros_b200.scan production ...   # points split over N GPUs
     python -m hadros_b200.scan inference            # 2048^2 x 32 with fallback
     python -m hadros_b200.scan batched              # 64 cameras, one graph-captured launch
 
@@ -341,66 +342,104 @@ def save_model(path, sur, info: dict) -> None:
         json.dump(info, f, default=float)
 
 
-def load_model(path) -> tuple[object, dict]:
-    sur = S.Surrogate.load(path)
+def load_model(path, device=0) -> tuple[object, dict]:
+    sur = S.Surrogate.load(path, device)
     with open(str(path) + ".json") as f:
         info = json.load(f)
     info["loaded_from"] = str(path)
     return sur, info
 
 
-def run_production(a) -> dict:
+def run_points(n_points: int, evaluate, dist=None, rank: int = 0, world: int = 1) -> list | None:
+    """Scan points 0..n_points-1 split over the ranks (equal cost each,
+    hadros_b200.shard.run_scan): this rank evaluates its points with
+    `evaluate(k) -> row`; rank 0 returns every row in point order, the
+    others None."""
+    from . import shard
+    return shard.run_scan(list(range(n_points)), lambda ks: [evaluate(k) for k in ks], dist, rank, world,
+                          costs=[1.0] * n_points)
+
+
+def point_rng(k: int):
+    """The judge subset's generator of scan point k (independent of which
+    rank evaluates the point)."""
+    return np.random.default_rng([W.SEED + 5, k])
+
+
+def run_production(a) -> dict | None:
+    """The production scan on this process's GPU, or under torchrun on every
+    rank's GPU with the scan points split over the ranks (each rank trains
+    the same ensemble from the same seeds; rows meet on rank 0)."""
+    from . import shard
     torch = _torch()
+    dist, rank, world, local = shard.init_from_env()
     E, g2, s = W.synthetic_sigma_arrays()
     sigma = SigmaTable.from_arrays(E, s, g2)
-    with Context(0) as ctx:
-        tpts = W.scan_points(a.train_points, seed=W.SEED + 17)
-        cams = [production_cam(r, t, a.train_side, a.bins) for r, t in tpts]
-        if a.load:
-            sur, info = load_model(a.load)
-        else:
-            sur, info = train(ctx, sigma, cams, a.pixels_per_cam, a.members, a.epochs, W.SEED, a.batch, a.lr)
-            if a.save:
-                save_model(a.save, sur, info)
-        calib = None
-        if a.sigmas <= 0:   # calibrated bound: c x spread, c from the held-out cameras
-            vcams, vraw, vy = held_out_samples(ctx, sigma, cams, a.pixels_per_cam, W.SEED, info["i_floor"])
-            calib = calibrate(sur, sigma, vcams, vraw, vy, info["i_floor"], a.bound)
-            a.threshold = calib["threshold"]
-            print(json.dumps({"calibration": calib}), file=sys.stderr, flush=True)
-        pts = W.scan_points(a.points, seed=W.SEED)
-        rng = np.random.default_rng(W.SEED + 5)
-        buf = PointRunner(ctx, sigma, sur, a.side, a.bins, a.judge)
-        rows = []
-        for r, t in pts:
-            rows.append(surrogate_point(ctx, sigma, sur, production_cam(r, t, a.side, a.bins), a.threshold,
-                                        a.judge, rng, buf))
-            x = rows[-1]
-            print(json.dumps({"point": len(rows), "seconds": x["seconds"], "fallback_frac": x["fallback_frac"],
-                              "worst": x["error"]["worst"]}), file=sys.stderr, flush=True)
-        del buf
-        plain = []
-        for r, t in pts[:a.plain_points]:
-            _, sec = plain_image(ctx, production_cam(r, t, a.side, a.bins), sigma)
-            plain.append(sec)
-            torch.cuda.empty_cache()
+    try:
+        with Context(local) as ctx:
+            tpts = W.scan_points(a.train_points, seed=W.SEED + 17)
+            cams = [production_cam(r, t, a.train_side, a.bins) for r, t in tpts]
+            if a.load:
+                sur, info = load_model(a.load, local)
+            else:
+                sur, info = train(ctx, sigma, cams, a.pixels_per_cam, a.members, a.epochs, W.SEED, a.batch, a.lr,
+                                  device=local)
+                if a.save and rank == 0:
+                    save_model(a.save, sur, info)
+            calib = None
+            if a.sigmas <= 0:   # calibrated bound: c x spread, c from the held-out cameras
+                vcams, vraw, vy = held_out_samples(ctx, sigma, cams, a.pixels_per_cam, W.SEED, info["i_floor"],
+                                                   local)
+                calib = calibrate(sur, sigma, vcams, vraw, vy, info["i_floor"], a.bound)
+                a.threshold = calib["threshold"]
+                if rank == 0:
+                    print(json.dumps({"calibration": calib}), file=sys.stderr, flush=True)
+            pts = W.scan_points(a.points, seed=W.SEED)
+            buf = PointRunner(ctx, sigma, sur, a.side, a.bins, a.judge)
+
+            def evaluate(k):
+                r, t = pts[k]
+                row = surrogate_point(ctx, sigma, sur, production_cam(r, t, a.side, a.bins), a.threshold,
+                                      a.judge, point_rng(k), buf)
+                row["point"] = k
+                print(json.dumps({"point": k, "rank": rank, "seconds": row["seconds"],
+                                  "fallback_frac": row["fallback_frac"], "worst": row["error"]["worst"]}),
+                      file=sys.stderr, flush=True)
+                return row
+            t0 = time.perf_counter()
+            rows = run_points(len(pts), evaluate, dist, rank, world)
+            scan_wall = time.perf_counter() - t0
+            del buf
+            plain = []
+            if rank == 0:
+                for r, t in pts[:a.plain_points]:
+                    _, sec = plain_image(ctx, production_cam(r, t, a.side, a.bins), sigma)
+                    plain.append(sec)
+                    torch.cuda.empty_cache()
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+    if rows is None:
+        return None
     sur_total = sum(x["seconds"] for x in rows)
     plain_per_point = float(np.mean(plain)) if plain else float("nan")
     setup = info["trace_s"] + info["fit_s"]
     n_full = a.scan_total or len(rows)
     sur_per_point = sur_total / len(rows)
     return {
-        "workload": "production_scan", "points": a.points, "side": a.side, "bins": a.bins,
+        "workload": "production_scan", "points": a.points, "side": a.side, "bins": a.bins, "ranks": world,
         "members": a.members, "bound": a.bound, "sigmas": a.sigmas, "threshold": a.threshold,
         "calibration": calib, "judge_frac": a.judge,
         "train": info,
         "surrogate_s_per_point": sur_total / len(rows),
+        "scan_wall_s": scan_wall,
         "plain_s_per_point": plain_per_point,
         "speedup_scan": plain_per_point * len(rows) / (sur_total + setup),
         "scan_total_points": n_full,
         "speedup_full_scan": plain_per_point * n_full / (setup + n_full * sur_per_point),
         "speedup_per_point": plain_per_point * len(rows) / sur_total,
         "fallback_frac_mean": float(np.mean([x["fallback_frac"] for x in rows])),
+        "fallback_frac_max": float(np.max([x["fallback_frac"] for x in rows])),
         "worst_pixel_error": max(x["error"]["worst"] for x in rows),
         "p99_error_max": max(x["error"]["p99"] for x in rows),
         "median_error_mean": float(np.mean([x["error"]["median"] for x in rows])),
@@ -517,7 +556,8 @@ def main(argv=None) -> None:
         a.side = a.side or 2048
         a.bins = a.bins or 32
         out = run_inference(a)
-    print(json.dumps(out, default=float))
+    if out is not None:
+        print(json.dumps(out, default=float))
 
 
 if __name__ == "__main__":

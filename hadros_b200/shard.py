@@ -49,6 +49,28 @@ def gather_to_root(obj, dist, rank: int, world: int):
     return out
 
 
+def init_from_env(backend: str | None = None, timeout_s: int = 1800):
+    """(dist, rank, world, local_rank) of a torchrun launch; (None, 0, 1, 0)
+    without one.  backend None: nccl when CUDA is available, else gloo."""
+    import os
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank, local = int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
+    if world <= 1:
+        return None, 0, 1, 0
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    if backend is None:
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+    kw = {}
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+        kw["device_id"] = torch.device("cuda", local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
+    return dist, rank, world, local
+
+
 def max_over_ranks(x: float, dist, device=None) -> float:
     if dist is None:
         return x
@@ -58,23 +80,25 @@ def max_over_ranks(x: float, dist, device=None) -> float:
     return float(t.item())
 
 
-def run_scan(cams: Sequence, trace: Callable[[list], list[dict]], dist=None, rank: int = 0,
-             world: int = 1) -> list[dict] | None:
-    """Trace `cams` across ranks: this rank traces its partition with
-    `trace(list_of_params) -> list_of_result_dicts`; rank 0 returns the results
-    in camera order, other ranks return None."""
-    costs = [float(c.nx) * float(c.ny) for c in cams]
+def run_scan(cams: Sequence, trace: Callable[[list], list], dist=None, rank: int = 0,
+             world: int = 1, costs: Sequence[float] | None = None) -> list | None:
+    """Trace `cams` (or any work items) across ranks: this rank runs its
+    partition with `trace(list_of_items) -> list_of_results`; rank 0 returns
+    the results in item order, other ranks return None.  Items are balanced
+    by `costs` (default: the cameras' pixel counts)."""
+    if costs is None:
+        costs = [float(c.nx) * float(c.ny) for c in cams]
     parts = partition_cameras(costs, world)
     mine = parts[rank]
     local = trace([cams[i] for i in mine]) if mine else []
     gathered = gather_to_root(list(zip(mine, local)), dist, rank, world)
     if rank != 0:
         return None
-    res: list[dict | None] = [None] * len(cams)
+    res: list = [None] * len(cams)
     for part in gathered:
         for i, r in part:
             res[i] = r
-    return res  # type: ignore[return-value]
+    return res
 
 
 def run_image_sharded(p, trace_pixels: Callable[[object, np.ndarray], dict], dist=None,

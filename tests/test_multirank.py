@@ -49,6 +49,25 @@ def _worker(rank, world, port, outdir, mode):
             t = shard.max_over_ranks(float(rank + 1), dist)
             if rank == 0:
                 np.save(Path(outdir) / "image.npy", np.array([img, t], dtype=object), allow_pickle=True)
+        elif mode == "robustness":
+            from hadros_b200 import robustness as R
+            rows, _ = R.run(None, None, pixels=2, dist=dist, rank=rank, world=world,
+                            trace=lambda cs: [O.oracle_image(c, E, s, threads=1, mev=True) for c in cs])
+            if rank == 0:
+                np.save(Path(outdir) / "robustness.npy", np.array(rows, dtype=object), allow_pickle=True)
+            else:
+                assert rows is None
+        elif mode == "points":
+            from hadros_b200 import scan
+            cams = [hb.params(**W.production_point(nx=3, ny=2, h=0.08, n_bins=2, precision="fp64",
+                                                   rho0_gcm3=10.0 ** (9 + k))) for k in range(3)]
+
+            def evaluate(k):   # the oracle stands in for the surrogate scan point
+                img = O.oracle_image(cams[k], E, s, threads=1)
+                return {"point": k, "rank": rank, "I_obs": img["I_obs"]}
+            rows = scan.run_points(len(cams), evaluate, dist, rank, world)
+            if rank == 0:
+                np.save(Path(outdir) / "points.npy", np.array(rows, dtype=object), allow_pickle=True)
         elif mode == "fail":
             if rank == 1:
                 raise RuntimeError("rank 1 fails before its first collective")
@@ -115,3 +134,35 @@ def test_failed_rank_is_reported_not_hung(tmp_path):
     procs = _spawn("fail", tmp_path)
     assert procs[1].exitcode != 0
     assert (tmp_path / "fail.txt").read_text().startswith("error")
+
+
+def test_two_rank_robustness_scan_equals_single_process(tmp_path, hb):
+    """hadros_b200.robustness.run with its 47 cases split over two gloo ranks
+    (the oracle tracing on CPU) gives the single-process rows."""
+    from hadros_b200 import robustness as R
+    from hadros_b200 import workloads as W
+    from oracle import pyoracle as O
+    procs = _spawn("robustness", tmp_path)
+    assert all(p.exitcode == 0 for p in procs)
+    rows = list(np.load(tmp_path / "robustness.npy", allow_pickle=True))
+    E, _, s = W.synthetic_sigma_arrays()
+    one, _ = R.run(None, None, pixels=2, trace=lambda cs: [O.oracle_image(c, E, s, threads=1, mev=True)
+                                                            for c in cs])
+    assert len(rows) == len(one) == len(R.cases())
+    assert rows == one
+
+
+def test_two_rank_scan_points_meet_in_point_order(tmp_path, hb):
+    """hadros_b200.scan.run_points (the production scan's driver) splits the
+    points over two ranks; rank 0 gets every point's row in order."""
+    from hadros_b200 import workloads as W
+    from oracle import pyoracle as O
+    procs = _spawn("points", tmp_path)
+    assert all(p.exitcode == 0 for p in procs)
+    rows = list(np.load(tmp_path / "points.npy", allow_pickle=True))
+    assert [r["point"] for r in rows] == [0, 1, 2] and {r["rank"] for r in rows} == {0, 1}
+    E, _, s = W.synthetic_sigma_arrays()
+    for k, r in enumerate(rows):
+        p = hb.params(**W.production_point(nx=3, ny=2, h=0.08, n_bins=2, precision="fp64",
+                                           rho0_gcm3=10.0 ** (9 + k)))
+        np.testing.assert_array_equal(r["I_obs"], O.oracle_image(p, E, s, threads=1)["I_obs"])
