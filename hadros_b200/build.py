@@ -36,7 +36,8 @@ CU_SOURCES = [("hadros_trace.cu", ["--fmad=false"]), ("hadros_trace_fast.cu", ["
               ("hadros_noalloc.cu", ["--fmad=false"]), ("hadros_mlp.cu", []), ("hadros_mlp_umma.cu", [])]
 CXX_SOURCES = ["hadros_host.cpp", "hadros_formats.cpp"]
 HEADERS = ["hadros_internal.h", "hadros_physics.cuh", "hadros_physics_f32.cuh", "hadros_mev.cuh",
-           "hadros_trace_kernel.cuh", "hadros_mlp.cuh", "hadros_umma.cuh"]
+           "hadros_trace_kernel.cuh", "hadros_mlp.cuh", "hadros_umma.cuh",
+           "hadros_cr_math.cuh", "hadros_sincos_table.h"]
 
 
 def _nvcc() -> str:

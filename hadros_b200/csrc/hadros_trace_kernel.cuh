@@ -9,6 +9,7 @@
 
 #include <string>
 
+#include "hadros_cr_math.cuh"
 #include "hadros_internal.h"
 
 namespace hadros {
@@ -57,12 +58,30 @@ __device__ __forceinline__ double fd_force(double d00, double d03, double d11, d
     return acc;
 }
 
-// KerrGeodesic::rhs (kerr_geodesic.cpp:83-135) with sin/cos of theta given.
-// The reference evaluates g^{-1}(r +- eps) and g^{-1}(theta +- eps) once per
-// (mu, nu) pair; they are evaluated once here (identical values).
-HADROS_RHS_ATTR void geo_rhs(double a, double r, double th, double s, double c,
-                                        double pr, double pth, double pt, double pph, K5& d)
+// sin/cos of j/128 (double-double) for the rounded-to-nearest sin and cos of
+// the reference-arithmetic kernel (hadros_cr_math.cuh).
+__device__ const double kScTab[4 * HADROS_SC_N] = HADROS_SC_TABLE;
+
+// sin and cos of theta as double-doubles, rounded to nearest in .h.
+__device__ __forceinline__ void sincos_dd(double th, crm::DD* s, crm::DD* c)
 {
+    if (fabs(th) < 1048576.0) {
+        crm::sincos_dd(th, kScTab, s, c);
+    } else {
+        *s = crm::DD{sin(th), 0.0};
+        *c = crm::DD{cos(th), 0.0};
+    }
+}
+
+// KerrGeodesic::rhs (kerr_geodesic.cpp:83-135) with sin/cos of theta given
+// (double-doubles; their .h is the value rounded to nearest, as the host
+// libm gives it for all but rare arguments).  The reference evaluates
+// g^{-1}(r +- eps) and g^{-1}(theta +- eps) once per (mu, nu) pair; they are
+// evaluated once here (identical values).
+HADROS_RHS_ATTR void geo_rhs(double a, double r, double th, const crm::DD& sd, const crm::DD& cd,
+                             double pr, double pth, double pt, double pph, K5& d)
+{
+    const double s = sd.h, c = cd.h;
     M5 gi;
     bl_ginv(a, r, s, c, gi);
     d.r = gi.rr * pr;
@@ -79,9 +98,20 @@ HADROS_RHS_ATTR void geo_rhs(double a, double r, double th, double s, double c,
     }
     {
         const double eps = 1.0e-5;
+        const double thp = th + eps, thm = th - eps;
         double sp, cp, sm, cm;
-        sincos(th + eps, &sp, &cp);
-        sincos(th - eps, &sm, &cm);
+        if (th > 1.0e-3) {   // thp - th and thm - th are exact: angle addition from theta's double-doubles
+            crm::sincos_shift_rn(sd, cd, thp - th, &sp, &cp);
+            crm::sincos_shift_rn(sd, cd, thm - th, &sm, &cm);
+        } else {
+            crm::DD a1, b1;
+            sincos_dd(thp, &a1, &b1);
+            sp = a1.h;
+            cp = b1.h;
+            sincos_dd(thm, &a1, &b1);
+            sm = a1.h;
+            cm = b1.h;
+        }
         M5 gp, gm;
         bl_ginv(a, r, sp, cp, gp);
         bl_ginv(a, r, sm, cm, gm);
@@ -211,8 +241,9 @@ __device__ __forceinline__ void geo_rhs_sel(double a, double r, double th, doubl
         else sincos(th, &s, &c);
         geo_rhs_fast(a, r, th, s, c, pr, pth, pt, pph, d);
     } else {
-        sincos(th, &s, &c);
-        geo_rhs(a, r, th, s, c, pr, pth, pt, pph, d);
+        crm::DD sd, cd;
+        sincos_dd(th, &sd, &cd);
+        geo_rhs(a, r, th, sd, cd, pr, pth, pt, pph, d);
     }
 }
 
@@ -802,7 +833,14 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
             }
 
             double s, c;
-            sincos(th, &s, &c);
+            crm::DD sd{0.0, 0.0}, cd{1.0, 0.0};
+            if (FAST) {
+                sincos(th, &s, &c);
+            } else {
+                sincos_dd(th, &sd, &cd);
+                s = sd.h;
+                c = cd.h;
+            }
             // PathPoint (kerr_camera.cpp:245-273): ZAMO interval and redshift
             double dl = 0.0;
             double z;
@@ -840,8 +878,9 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                 if (step != 0) {
                     const double r_mid = 0.5 * (r + r_prev);
                     const double th_mid = 0.5 * (th + th_prev);
-                    double sm, cm;
-                    sincos(th_mid, &sm, &cm);
+                    crm::DD smd, cmd;
+                    sincos_dd(th_mid, &smd, &cmd);
+                    const double sm = smd.h, cm = cmd.h;
                     M5 gmid;
                     bl_metric(a, r_mid, sm, cm, gmid);
                     const double dr = r - r_prev;
@@ -878,7 +917,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
 
             // ---- k1 of the coming step_adaptive (shares sin/cos) ------------
             if (FAST) geo_rhs_fast(a, r, th, s, c, pr, pth, pt, pph, k1);
-            else geo_rhs(a, r, th, s, c, pr, pth, pt, pph, k1);
+            else geo_rhs(a, r, th, sd, cd, pr, pth, pt, pph, k1);
             r_prev = r;
             th_prev = th;
             ph_prev = ph;
@@ -988,7 +1027,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
             ++step;
             phase = kStepStart;
         } else {
-            const double factor = 0.8 * pow(cam->tol / smax(err, 1.0e-30), 0.25);
+            const double factor = 0.8 * crm::pow025_rn(cam->tol / smax(err, 1.0e-30));
             h *= sclamp(factor, 0.1, 5.0);
             if (h < h_min) h = h_min;
             ++att_in_step;
