@@ -755,7 +755,15 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
     while (true) {
         while (phase == kNeedRay || phase == kStepStart) {
             if (phase == kNeedRay) {
-                item = static_cast<long long>(atomicAdd(&A.counters[0], 1ULL));
+                {   // the lanes that need a ray now take consecutive items, one atomic per warp
+                    const unsigned m = __activemask();
+                    const int lane = threadIdx.x & 31;
+                    const int leader = __ffs(m) - 1;
+                    unsigned long long base = 0;
+                    if (lane == leader) base = atomicAdd(&A.counters[0], static_cast<unsigned long long>(__popc(m)));
+                    base = __shfl_sync(m, base, leader);
+                    item = static_cast<long long>(base) + __popc(m & ((1u << lane) - 1u));
+                }
                 if (item >= A.total_items) {
                     phase = kDone;
                     break;

@@ -244,3 +244,42 @@ def test_umma_inference_matches_training_forward(hb, torch, sigma_table, members
     fb = np.sort(res["fallback_ids"][:int(cnt[0])].cpu().numpy())
     expect = ids[spread > 0.05]       # the kernel's own spread decides
     np.testing.assert_array_equal(fb, expect)
+
+
+@pytest.mark.parametrize("members,n_bins", [(2, 8), (4, 64)])
+def test_umma_inference_matches_oracle(hb, torch, sigma_table, members, n_bins):
+    """The fused tcgen05 inference kernel against the CPU oracle's forward
+    pass (oracle/mlp_oracle.py with the BF16 rounding points of the kernels)
+    on the kernel's own input rows: per sample, the ensemble means of ln tau_E
+    and ln I_E differ by FP32 summation order and the hardware tanh only, and
+    so does the per-pixel spread of ln I_obs."""
+    from hadros_b200 import surrogate as S
+    sur = _random_surrogate(hb, torch, members, seed=20 + members)
+    nx, ny = 20, 16
+    p = hb.params(nx=nx, ny=ny, profile="collapsar_ndaf_like", a_spin=0.95, theta_obs_deg=40.0, rho0_gcm3=1e11,
+                  spectral="powerlaw_cutoff", n_bins=n_bins)
+    res = sur.image(p, sigma_table, threshold=1e30)
+    torch.cuda.synchronize()
+    assert res["counters"].cpu().numpy()[1] == 0, "inference kernel aborted"
+    P, B = nx * ny, n_bins
+    raw = S.raw_features(p, sigma_table, np.arange(P, dtype=np.int32))
+    X = sur.featurize(raw).float().cpu().numpy().astype(np.float64)
+    nm = sur.norm
+    mu = np.array([nm.out_mu[0], nm.out_mu[1]])
+    sd = np.array([nm.out_sd[0], nm.out_sd[1]])
+    ys = np.stack([M.forward(net.master.cpu().numpy(), X)[0] * sd + mu for net in sur.nets])   # [K][n][2]
+    mean = ys.mean(0)
+    got = np.stack([res["ln_tau_E"].cpu().numpy().reshape(-1), res["ln_I_E"].cpu().numpy().reshape(-1)], axis=1)
+    err = np.abs(got - mean) / sd                       # in units of the outputs' spread
+    rms, worst = np.sqrt(np.mean(err ** 2, axis=0)), err.max(axis=0)
+    bins = hb.spectral_bins(p, sigma_table)
+    valid = (bins["valid"] != 0) & (bins["dE"] > 0)
+    lnde = np.where(valid, np.log(np.where(valid, bins["dE"], 1.0)), -np.inf)
+    L_k = np.log(np.sum(np.exp(ys[:, :, 1].reshape(members, P, B) + lnde), axis=2))   # [K][P]
+    spread_ref = L_k.std(0)
+    d_spread = np.abs(res["spread"].cpu().numpy() - spread_ref)
+    stats = (f"rms {rms.tolist()} max {worst.tolist()} (output sd units); spread |diff| max "
+             f"{d_spread.max():.3e} (spread up to {spread_ref.max():.3e})")
+    print(stats)
+    assert rms.max() < 2e-3 and worst.max() < 2e-2, stats
+    assert d_spread.max() < 1e-3 + 1e-3 * spread_ref.max(), stats
