@@ -145,29 +145,49 @@ struct Trig {
     double s2, c2, inv_s2;
 };
 
-__device__ __forceinline__ void ginv_fast(double a, double a2, double r, const Trig& t, M5& g)
+// The radius-only terms of the inverse metric at r (shared by the metrics
+// at theta and theta +- eps).
+struct RTerms {
+    double r2, del, rpa2, tar;
+};
+
+__device__ __forceinline__ RTerms rterms(double a, double a2, double r)
 {
-    const double r2 = r * r;
-    const double sig = r2 + a2 * t.c2;
-    const double del = r2 - 2.0 * r + a2;
-    const double rpa = r2 + a2;
-    const double bigA = rpa * rpa - a2 * del * t.s2;
-    const double inv_sd = rcp_nr(sig * del);
-    g.tt = -bigA * inv_sd;
-    g.tph = -2.0 * a * r * inv_sd;
-    g.thth = del * inv_sd;
-    g.rr = del * g.thth;
-    g.phph = (del - a2 * t.s2) * inv_sd * t.inv_s2;
+    RTerms t;
+    t.r2 = r * r;
+    t.del = t.r2 - 2.0 * r + a2;
+    const double rpa = t.r2 + a2;
+    t.rpa2 = rpa * rpa;
+    t.tar = 2.0 * a * r;
+    return t;
 }
 
-__device__ __forceinline__ double force_fast(const M5& gp, const M5& gm, double inv2e, double p0,
-                                             double p1, double p2, double p3)
+__device__ __forceinline__ void ginv_fast(double a2, const RTerms& R, const Trig& t, M5& g)
 {
-    const double d00 = (gp.tt - gm.tt) * inv2e, d03 = (gp.tph - gm.tph) * inv2e;
-    const double d11 = (gp.rr - gm.rr) * inv2e, d22 = (gp.thth - gm.thth) * inv2e;
-    const double d33 = (gp.phph - gm.phph) * inv2e;
-    const double q = d00 * p0 * p0 + 2.0 * d03 * p0 * p3 + d11 * p1 * p1 + d22 * p2 * p2 + d33 * p3 * p3;
-    return -0.5 * q;
+    const double sig = R.r2 + a2 * t.c2;
+    const double bigA = R.rpa2 - a2 * R.del * t.s2;
+    const double inv_sd = rcp_nr(sig * R.del);
+    g.tt = -bigA * inv_sd;
+    g.tph = -R.tar * inv_sd;
+    g.thth = R.del * inv_sd;
+    g.rr = R.del * g.thth;
+    g.phph = (R.del - a2 * t.s2) * inv_sd * t.inv_s2;
+}
+
+// The momenta's products in -1/2 dg^{mu nu} p_mu p_nu (both forces use them).
+struct PQ {
+    double q00, q03, q11, q22, q33;
+};
+
+// -1/2 sum (gp - gm)^{mu nu} p_mu p_nu / (2 eps), with scale = -1/2 / (2 eps).
+__device__ __forceinline__ double force_fast(const M5& gp, const M5& gm, double scale, const PQ& q)
+{
+    double acc = (gp.tt - gm.tt) * q.q00;
+    acc = fma(gp.tph - gm.tph, q.q03, acc);
+    acc = fma(gp.rr - gm.rr, q.q11, acc);
+    acc = fma(gp.thth - gm.thth, q.q22, acc);
+    acc = fma(gp.phph - gm.phph, q.q33, acc);
+    return scale * acc;
 }
 
 // sin and cos of th + d for |d| ~ 1e-5 (d exact): Taylor terms to d^3.
@@ -186,33 +206,35 @@ __device__ __forceinline__ Trig trig_shift(double s, double c, double d)
 }
 
 HADROS_RHS_ATTR void geo_rhs_fast(double a, double r, double th, double s, double c,
-                                             double pr, double pth, double pt, double pph, K5& d)
+                                  double pr, double pth, double pt, double pph, K5& d)
 {
     const double a2 = a * a;
     Trig t0;
     t0.s2 = s * s;
     t0.c2 = c * c;
     t0.inv_s2 = rcp_nr(t0.s2);
+    const RTerms R0 = rterms(a, a2, r);
     M5 gi;
-    ginv_fast(a, a2, r, t0, gi);
+    ginv_fast(a2, R0, t0, gi);
     d.r = gi.rr * pr;
     d.th = gi.thth * pth;
     d.ph = gi.tph * pt + gi.phph * pph;
+    const PQ q{pt * pt, 2.0 * pt * pph, pr * pr, pth * pth, pph * pph};
     {
         const double eps = 1.0e-5 * smax(1.0, fabs(r));
         M5 gp, gm;
-        ginv_fast(a, a2, r + eps, t0, gp);
-        ginv_fast(a, a2, r - eps, t0, gm);
-        d.pr = force_fast(gp, gm, rcp_nr(2.0 * eps), pt, pr, pth, pph);
+        ginv_fast(a2, rterms(a, a2, r + eps), t0, gp);
+        ginv_fast(a2, rterms(a, a2, r - eps), t0, gm);
+        d.pr = force_fast(gp, gm, -0.25 * rcp_nr(eps), q);
     }
     {
         // the reference differentiates at fl(th +- 1e-5); use those exact offsets
         const double dp = (th + 1.0e-5) - th, dm = (th - 1.0e-5) - th;
         const Trig tp = trig_shift(s, c, dp), tm = trig_shift(s, c, dm);
         M5 gp, gm;
-        ginv_fast(a, a2, r, tp, gp);
-        ginv_fast(a, a2, r, tm, gm);
-        d.pth = force_fast(gp, gm, 1.0 / (2.0 * 1.0e-5), pt, pr, pth, pph);
+        ginv_fast(a2, R0, tp, gp);
+        ginv_fast(a2, R0, tm, gm);
+        d.pth = force_fast(gp, gm, -0.5 * (1.0 / (2.0 * 1.0e-5)), q);
     }
 }
 
