@@ -913,7 +913,7 @@ def main() -> None:
                     help="scan: one production-scan point per step, surrogate + fallback + 1%% exact "
                          "judge (default); image: the trace kernel on mixed_512; surrogate: the "
                          "surrogate inference kernel alone")
-    ap.add_argument("--epochs", type=int, default=40, help="scan: training epochs of the ensemble")
+    ap.add_argument("--epochs", type=int, default=150, help="scan: training epochs of the ensemble")
     ap.add_argument("--train-points", type=int, default=128, help="scan: training cameras (incl. held out)")
     ap.add_argument("--pixels-per-cam", type=int, default=4096, help="scan: training pixels per camera")
     ap.add_argument("--batch", type=int, default=8192, help="scan: training batch")

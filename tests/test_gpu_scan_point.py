@@ -79,9 +79,11 @@ def test_point_runner_with_every_pixel_falling_back_is_the_plain_image(hb, gpu_c
     host = runner.alloc_host()
     host["judge_ids"].copy_(torch.from_numpy(jids))
     r2 = runner.run_host(p, -1.0, host)
+    assert r2["fallback_pixels"] == 256, r2
     assert r2["d2h_bytes"] >= 3 * 8 * 256 and r2["h2d_bytes"] >= 4 * jids.size
     for k in KEYS:
-        np.testing.assert_array_equal(host[k].numpy(), plain[k], err_msg=k)
+        np.testing.assert_array_equal(runner.out[k].cpu().numpy(), plain[k], err_msg=f"device {k}")
+        np.testing.assert_array_equal(host[k].numpy(), plain[k], err_msg=f"host {k}")
 
 
 def test_point_runner_judges_the_surrogate_where_nothing_falls_back(hb, gpu_ctx, sigma_table):
