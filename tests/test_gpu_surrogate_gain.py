@@ -1,13 +1,16 @@
-"""What the trained surrogate gains over the exact tracer alone.
+"""What the trained surrogate gains over the exact tracer alone, at the
+production scan's own bar: worst judged intensity error <= 1%.
 
-A small ensemble (2 networks) is trained on rays that the tracer traces at
-48 points of the production box (collapsar_ndaf_like, density_weighted
-source, a = 0.95, rho0 in [1e9, 1e12], inclination in [10, 80] deg), at
-512 x 512 pixels and 16 bins.  On a held-out point the surrogate image with
-its exact fallback (pixels whose 2-sigma ensemble bound exceeds 2%) is
-compared with the plain tracer's image of the same point: it must be faster,
-and its intensities, judged by the exact tracer on a random pixel subset,
-must be close; pixels sent to the fallback must carry the exact values."""
+An ensemble of 4 networks is trained (tensor-core training kernels) on rays
+the tracer traces at 64 points of the production box (collapsar_ndaf_like,
+density_weighted source, a = 0.95, rho0 in [1e9, 1e12], inclination in
+[10, 80] deg) at 1024 x 1024 pixels and 16 bins; the fallback threshold on
+the ensemble spread is calibrated on the held-out cameras.  On a scan point
+not among them, the surrogate image with its exact fallback and a 1% exact
+judge (hadros_b200.scan.PointRunner) is compared with the plain tracer's
+image of the same point: the judged worst error must be at most 1%, the
+pixels sent to the fallback must carry the exact values, and the point must
+be at least 5x faster than the plain tracer."""
 from __future__ import annotations
 
 import time
@@ -18,41 +21,42 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def test_surrogate_is_faster_than_the_tracer_at_small_error(hb, gpu_ctx, sigma_table):
+def test_surrogate_meets_one_percent_and_beats_the_tracer(hb, gpu_ctx, sigma_table):
     import torch
     from hadros_b200 import scan
-    from hadros_b200 import surrogate as S
     from hadros_b200 import workloads as W
     torch.cuda.set_device(0)
-    side, bins = 512, 16
-    train = [scan.production_cam(r, t, side, bins) for r, t in W.scan_points(48, seed=101)]
-    raw, y, info = S.trace_samples(gpu_ctx, sigma_table, train, 4096, seed=5)
-    sur = S.Surrogate(members=2, seed=3)
-    sur.fit(raw, y, epochs=80, batch=8192, lr=2e-3, floors=(S.TAU_FLOOR, info["i_floor"]))
+    side, bins = 1024, 16
+    cams = [scan.production_cam(r, t, side, bins) for r, t in W.scan_points(64, seed=101)]
+    sur, info = scan.train(gpu_ctx, sigma_table, cams, 2048, 4, 40, 5, 8192, 2e-3)
+    vcams, vraw, vy = scan.held_out_samples(gpu_ctx, sigma_table, cams, 2048, 5, info["i_floor"])
+    calib = scan.calibrate(sur, sigma_table, vcams, vraw, vy, info["i_floor"], 0.01)
     (r0, t0), = W.scan_points(1, seed=202)
     p = scan.production_cam(r0, t0, side, bins)
+    P = side * side
 
     # the method without the network: the exact tracer on every pixel
+    plain, t_plain = scan.plain_image(gpu_ctx, p, sigma_table)
+    # with it: surrogate + fallback + 1% exact judge (warmed once)
+    runner = scan.PointRunner(gpu_ctx, sigma_table, sur, side, bins, 0.01)
+    jids = scan.judge_ids(P, 0.01, np.random.default_rng(7))
+    runner.run(p, calib["threshold"], jids)
     torch.cuda.synchronize()
     a = time.perf_counter()
-    exact = gpu_ctx.image(p, sigma_table, outputs=("tau", "P_surv", "I_obs"))
-    t_plain = time.perf_counter() - a
-
-    # with it: surrogate image + exact fallback (warm the kernel once first)
-    sur.image(p, sigma_table, threshold=0.01, per_bin=False)
-    torch.cuda.synchronize()
-    a = time.perf_counter()
-    img = sur.image_with_fallback(gpu_ctx, p, sigma_table, threshold=0.01)
+    res = runner.run(p, calib["threshold"], jids)
     t_sur = time.perf_counter() - a
 
-    P = side * side
-    fb = img["fallback"]
-    np.testing.assert_array_equal(img["I_obs"][fb], exact["I_obs"][fb])
-    judge = np.random.default_rng(7).choice(P, size=P // 100, replace=False)
-    e = scan.errors(exact["I_obs"][judge], img["I_obs"][judge])
-    print(f"plain {t_plain:.3f} s, surrogate {t_sur:.3f} s ({t_plain / t_sur:.1f}x), "
-          f"fallback {fb.size / P:.4f}, judged error median {e['median']:.4f} worst {e['worst']:.4f}")
-    assert e["n"] > 100
-    assert t_sur < t_plain / 1.5
-    assert fb.size < P // 2
-    assert e["median"] < 0.02 and e["worst"] < 0.15
+    nf = res["fallback_pixels"]
+    fb = runner.ids[runner.n_judge:runner.n_judge + nf].long()
+    for k in ("tau", "P_surv", "I_obs"):
+        assert torch.equal(runner.out[k][fb], plain[k][fb]), k
+    full = scan._device_errors(plain["I_obs"], runner.out["I_obs"])
+    msg = (f"plain {t_plain:.3f} s, surrogate point {t_sur:.3f} s ({t_plain / t_sur:.1f}x), threshold "
+           f"{calib['threshold']:.4f}, fallback {nf / P:.4%}, judged worst {res['error']['worst']:.4%} "
+           f"p99 {res['error']['p99']:.4%}; every pixel: worst {float(full[1]):.4%} p99 {float(full[2]):.4%}; "
+           f"fit {info['fit_s']:.1f} s")
+    print(msg)
+    assert res["error"]["n"] > 1000, msg
+    assert res["error"]["worst"] <= 0.01, msg
+    assert float(full[2]) <= 0.01, msg
+    assert t_sur * 5.0 < t_plain, msg
