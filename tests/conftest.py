@@ -19,8 +19,11 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA B200 and libhadros_b200.so")
 
 
-def golden_names() -> list[str]:
-    return sorted(p.stem for p in GOLDEN.glob("*.npz") if p.stem != "sigma_synthetic")
+def golden_names(near_ties: bool = False) -> list[str]:
+    """Fixture names; the scale_* fixtures (rays with near-tie accept/reject
+    decisions, step counts held to +-1) only with near_ties=True."""
+    names = sorted(p.stem for p in GOLDEN.glob("*.npz") if p.stem != "sigma_synthetic")
+    return names if near_ties else [n for n in names if not n.startswith("scale_")]
 
 
 def load_golden(name: str) -> tuple[dict, dict]:

@@ -94,6 +94,12 @@ def cases() -> dict[str, dict]:
     c["production_c5_mid_8x8"] = dict(W.production_point(precision="fp64"), _pixel_ids=ids)
     c["production_c5_dense_8x8"] = dict(W.production_point(precision="fp64", rho0_gcm3=1.0e12,
                                                            theta_obs_deg=15.0), _pixel_ids=ids)
+    # The pixels of the 512x512 camera traced at 256x256 whose accepted-step
+    # count came out one off the reference in a full-image comparison on the
+    # GPU (65,536 rays): rays with a near-tie accept/reject decision.
+    c["scale_c2_256_near_ties"] = dict(W.mixed_512(nx=256, ny=256, precision="fp64"),
+                                       _pixel_ids=np.array([27795, 31311, 34200, 34658, 38802, 39770, 42099],
+                                                           dtype=np.int32))
     return c
 
 
