@@ -20,6 +20,10 @@ inclination, all eight profiles and rho0, 16 bins, traced in one persistent
 launch from an autotuned plan replayed from a CUDA graph, against the same
 cameras traced one launch each.
 
+learning-curve: the configuration-4 general model's held-out error against
+its training-set size, for one ensemble over all profiles and one per
+profile kind.
+
 inference: the surrogate is trained on cameras with randomized spin,
 inclination, profile, rho0 and two shape parameters, and evaluates the
 mixed_512 camera at 2048 x 2048 x 32 bins with exact fallback.
@@ -463,6 +467,84 @@ def run_inference(a) -> dict:
             "train": info, "surrogate": row, "plain_s": sec, "speedup": sec / row["seconds"]}
 
 
+def _held_out_rms(sur, raw, y) -> list[float]:
+    torch = _torch()
+    d = (sur.forward(raw).mean(0) - y).double()
+    return torch.sqrt((d ** 2).mean(0)).cpu().tolist()
+
+
+def run_learning_curve(a) -> dict:
+    """The general model of the configuration-4 surrogate (spin, inclination,
+    all eight profiles, rho0 and two shape parameters randomized): held-out
+    RMS of ln tau_E and ln I_E against the number of training samples, for
+    one ensemble over all profiles and for one ensemble per profile kind
+    (trained on that kind's cameras only), and the share of the inference
+    image's pixels above the calibrated 1% threshold for each."""
+    torch = _torch()
+    E, g2, s = W.synthetic_sigma_arrays()
+    sigma = SigmaTable.from_arrays(E, s, g2)
+    out = {"workload": "learning_curve", "bins": a.bins, "members": a.members, "epochs": a.epochs,
+           "pixels_per_cam": a.pixels_per_cam, "general": [], "per_profile": {}}
+    with Context(0) as ctx:
+        kws = W.surrogate_training_cams(a.train_points, side=a.train_side, n_bins=a.bins)
+        cams = [params(**c) for c in kws]
+        n_val = n_held_out(len(cams))
+        train_cams, val_cams = cams[:-n_val], cams[-n_val:]
+        raw, y, info = S.trace_samples(ctx, sigma, train_cams, a.pixels_per_cam, seed=W.SEED)
+        vraw, vy, _ = S.trace_samples(ctx, sigma, val_cams, a.pixels_per_cam, seed=W.SEED + 1,
+                                      i_floor=info["i_floor"])
+        per_cam = a.pixels_per_cam * a.bins
+        p_inf = params(**W.surrogate_inference_image(nx=a.side, ny=a.side, n_bins=a.bins))
+        for frac in (0.25, 0.5, 1.0):
+            n = int(len(train_cams) * frac) * per_cam
+            sur = S.Surrogate(members=a.members, seed=W.SEED)
+            t0 = time.perf_counter()
+            sur.fit(raw[:n], y[:n], epochs=a.epochs, batch=a.batch, lr=a.lr, floors=(S.TAU_FLOOR, info["i_floor"]))
+            torch.cuda.synchronize()
+            row = {"samples": n, "fit_s": time.perf_counter() - t0, "val_rms": _held_out_rms(sur, vraw, vy)}
+            if frac == 1.0:
+                res = sur.image(p_inf, sigma, threshold=0.01 / 3.0, per_bin=False, spread_of=1)
+                torch.cuda.synchronize()
+                row["inference_fallback_frac"] = int(res["counters"][0].item()) / (a.side * a.side)
+            out["general"].append(row)
+            print(json.dumps({"general": row}), file=sys.stderr, flush=True)
+        # one ensemble per profile kind
+        kinds = [int(c.profile_kind) for c in cams]
+        se = [0.0, 0.0]
+        nv = 0
+        for kind in range(8):
+            tr = [i for i, c in enumerate(train_cams) if int(c.profile_kind) == kind]
+            va = [i for i, c in enumerate(val_cams) if int(c.profile_kind) == kind]
+            if not tr:
+                continue
+            idx = torch.cat([torch.arange(i * per_cam, (i + 1) * per_cam, device=raw.device) for i in tr])
+            sur = S.Surrogate(members=a.members, seed=W.SEED + kind)
+            sur.fit(raw[idx], y[idx], epochs=a.epochs, batch=a.batch, lr=a.lr, floors=(S.TAU_FLOOR, info["i_floor"]))
+            row = {"train_cams": len(tr), "val_cams": len(va)}
+            if va:
+                vidx = torch.cat([torch.arange(i * per_cam, (i + 1) * per_cam, device=raw.device) for i in va])
+                rms = _held_out_rms(sur, vraw[vidx], vy[vidx])
+                row["val_rms"] = rms
+                for o in range(2):
+                    se[o] += rms[o] ** 2 * vidx.numel()
+                nv += vidx.numel()
+            if kind == int(p_inf.profile_kind):
+                res = sur.image(p_inf, sigma, threshold=0.01 / 3.0, per_bin=False, spread_of=1)
+                torch.cuda.synchronize()
+                row["inference_fallback_frac"] = int(res["counters"][0].item()) / (a.side * a.side)
+            out["per_profile"][hb_profile_name(kind)] = row
+            print(json.dumps({"profile": kind, **row}), file=sys.stderr, flush=True)
+        out["per_profile_val_rms"] = [float(np.sqrt(x / max(nv, 1))) for x in se]
+        del kinds
+    return out
+
+
+def hb_profile_name(kind: int) -> str:
+    from . import lib
+    name = lib().hadros_profile_name(kind)
+    return name.decode() if name else str(kind)
+
+
 def run_batched(a) -> dict:
     """The batched scan: every camera in one persistent launch from a plan
     whose schedule the autotuner picked, captured in a CUDA graph and
@@ -520,7 +602,7 @@ def run_batched(a) -> dict:
 
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("workload", choices=("production", "inference", "batched"))
+    ap.add_argument("workload", choices=("production", "inference", "batched", "learning-curve"))
     ap.add_argument("--points", type=int, default=256)
     ap.add_argument("--scan-total", type=int, default=0,
                     help="points of the whole scan when --points runs its first ones (for the "
@@ -549,6 +631,10 @@ def main(argv=None) -> None:
         a.side = a.side or 4096
         a.bins = a.bins or 64
         out = run_production(a)
+    elif a.workload == "learning-curve":
+        a.side = a.side or 2048
+        a.bins = a.bins or 32
+        out = run_learning_curve(a)
     elif a.workload == "batched":
         a.points = a.points if a.points != 256 else 64
         out = run_batched(a)
