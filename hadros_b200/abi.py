@@ -170,6 +170,11 @@ class HadrosAdam(C.Structure):
     _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float)]
 
 
+class HadrosTrainSched(C.Structure):
+    _fields_ = [("lr_max", C.c_float), ("lr_min", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
+                ("eps", C.c_float), ("total_steps", C.c_int64), ("steps_per_epoch", C.c_int64)]
+
+
 class HadrosSurrogateOut(C.Structure):
     _fields_ = [("ln_tau_E", C.c_void_p), ("ln_I_E", C.c_void_p), ("tau", C.c_void_p),
                 ("P_surv", C.c_void_p), ("I_obs", C.c_void_p), ("spread", C.c_void_p),
@@ -281,6 +286,10 @@ SIGNATURES = {
                                              C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_void_p, P(HadrosAdam), C.c_int64, C.c_void_p,
                                              C.c_void_p, C.c_void_p]),
+    "hadros_mlp_train_members_dev": (C.c_int32, [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, C.c_void_p, P(HadrosTrainSched), C.c_void_p,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p]),
     "hadros_mlp_image_bytes": (C.c_int64, []),
     "hadros_surrogate_schedule": (C.c_int32, [C.c_int32]),
     "hadros_mlp_pack_image": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -291,7 +291,15 @@ void gemm(const bf16* A, long lda, long a_mem, const bf16* B, long ldb, long b_m
     k_split = (k_split + UK - 1) / UK * UK;
     splits = std::max((K + k_split - 1) / k_split, 1);
     auto kern = umma_gemm<A_MN, B_MN, BN, Epi>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, UTile<BN>::kSmem);
+    // set once per process (and device 0's context first): later launches,
+    // such as those captured into a CUDA graph, only enqueue the kernel
+    static thread_local int attr_device = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (attr_device != dev) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, UTile<BN>::kSmem);
+        attr_device = dev;
+    }
     dim3 grid((N + BN - 1) / BN, (M + UM - 1) / UM, members * splits);
     kern<<<grid, kUThreads, UTile<BN>::kSmem, st>>>(A, lda, a_mem, B, ldb, b_mem, M, N, K, k_split, splits, epi,
                                                    fail);
@@ -499,16 +507,53 @@ __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __re
     w[off + i] -= lr * (mi * inv_bc1) / (sqrtf(vi * inv_bc2) + eps);
 }
 
+// Per-step values of a graph-replayed training run, written on the device by
+// k_step_begin (so a captured step reads the values of the step it runs).
+struct StepDev {
+    float lr, inv_bc1, inv_bc2;
+    int64_t idx_off;   // first row of this step's batch in each member's index list
+};
+
+// ++step; the cosine learning rate lr_min + (lr_max - lr_min)(1 + cos(pi t))/2,
+// t = (step - 1) / (total - 1); Adam's bias corrections; the batch offset.
+__global__ void k_step_begin(int64_t* step, hadros_train_sched sc, long n, StepDev* out)
+{
+    const int64_t st = ++*step;
+    const double t = double(st - 1) / double(sc.total_steps > 1 ? sc.total_steps - 1 : 1);
+    out->lr = float(sc.lr_min + 0.5 * (sc.lr_max - sc.lr_min) * (1.0 + cos(3.141592653589793 * (t < 1.0 ? t : 1.0))));
+    out->inv_bc1 = 1.0f / (1.0f - powf(sc.beta1, float(st)));
+    out->inv_bc2 = 1.0f / (1.0f - powf(sc.beta2, float(st)));
+    out->idx_off = ((st - 1) % (sc.steps_per_epoch > 0 ? sc.steps_per_epoch : 1)) * n;
+}
+
+// Adam with the step's values from the device.
+__global__ void k_adam_dev(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                           const float* __restrict__ g, long count, long stride, const StepDev* sd, float b1,
+                           float b2, float eps)
+{
+    const long off = long(blockIdx.y) * stride;
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float lr = sd->lr, inv_bc1 = sd->inv_bc1, inv_bc2 = sd->inv_bc2;
+    const float gi = g[off + i];
+    const float mi = fmaf(b1, m[off + i], (1.0f - b1) * gi);
+    const float vi = fmaf(b2, v[off + i], (1.0f - b2) * gi * gi);
+    m[off + i] = mi;
+    v[off + i] = vi;
+    w[off + i] -= lr * (mi * inv_bc1) / (sqrtf(vi * inv_bc2) + eps);
+}
+
 // Rows idx[k][s] of the shared inputs and targets -> member k's batch.
 __global__ void k_gather(const bf16* __restrict__ X_all, const float* __restrict__ T_all,
                          const float* __restrict__ W_all, const int64_t* __restrict__ idx, long idx_mem, long n,
-                         bf16* __restrict__ X, float* __restrict__ T, float* __restrict__ Wt)
+                         bf16* __restrict__ X, float* __restrict__ T, float* __restrict__ Wt,
+                         const StepDev* sd)
 {
     const int k = blockIdx.y;
     const long s = long(blockIdx.x) * (blockDim.x / 8) + threadIdx.x / 8;
     const int u = threadIdx.x & 7;   // 16-byte unit of the 128-byte row
     if (s >= n) return;
-    const int64_t r = idx[k * idx_mem + s];
+    const int64_t r = idx[k * idx_mem + (sd ? sd->idx_off : 0) + s];
     reinterpret_cast<uint4*>(X + (k * n + s) * kIn)[u] = reinterpret_cast<const uint4*>(X_all + r * kIn)[u];
     if (u < kOut) T[(k * n + s) * kOut + u] = T_all[r * kOut + u];
     if (u == kOut && W_all) Wt[k * n + s] = W_all[r];
@@ -753,7 +798,7 @@ int32_t hadros_mlp_train_members(int32_t members, int64_t n, const void* X_all, 
     auto* out = Wt + long(members) * n;
     auto* dout = out + long(members) * n * kOut;
     k_gather<<<dim3(blocks_for(n * 8, 256), members), 256, 0, st>>>(
-        static_cast<const bf16*>(X_all), T_all, W_all, idx, idx_stride, n, X, T, W_all ? Wt : nullptr);
+        static_cast<const bf16*>(X_all), T_all, W_all, idx, idx_stride, n, X, T, W_all ? Wt : nullptr, nullptr);
     auto* pk = static_cast<bf16*>(packed);
     const Batch bt{members, n, n * kIn, kPacked, kParams, wsb};
     forward_impl(masters, pk, X, bt, base, out, loss, st);
@@ -768,6 +813,44 @@ int32_t hadros_mlp_train_members(int32_t members, int64_t n, const void* X_all, 
         1.0f / bc2);
     k_pack<<<dim3(blocks_for(kPacked, 256), members), 256, 0, st>>>(masters, pk);
     return cuda_status("hadros_mlp_train_members");
+}
+
+int32_t hadros_mlp_train_members_dev(int32_t members, int64_t n, const void* X_all, const float* T_all,
+                                     const float* W_all, const int64_t* idx, int64_t idx_stride, float* masters,
+                                     void* packed, float* m, float* v, float* grad, const hadros_train_sched* sched,
+                                     int64_t* step_dev, void* workspace, float* loss, void* stream)
+{
+    if (members < 1 || members > 64 || n <= 0 || n > (int64_t(1) << 26) || !X_all || !T_all || !idx ||
+        !masters || !packed || !m || !v || !grad || !sched || !step_dev || !workspace || !loss ||
+        sched->steps_per_epoch < 1 || sched->total_steps < 1 || idx_stride < n * sched->steps_per_epoch)
+        return set_error(HADROS_E_ARG, "bad argument");
+    auto st = static_cast<cudaStream_t>(stream);
+    char* base =
+        reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(workspace) + kWsAlign - 1) / kWsAlign * kWsAlign);
+    const long wsb = ws_bytes(n);
+    char* bb = base + long(members) * wsb;
+    auto* X = reinterpret_cast<bf16*>(bb);
+    auto* T = reinterpret_cast<float*>(bb + long(members) * n * kIn * 2);
+    auto* Wt = T + long(members) * n * kOut;
+    auto* out = Wt + long(members) * n;
+    auto* dout = out + long(members) * n * kOut;
+    // the step's values sit past the members' batch buffers (members_batch_bytes rounds up)
+    auto* sd = reinterpret_cast<StepDev*>(
+        (reinterpret_cast<uintptr_t>(dout + long(members) * n * kOut) + 15) / 16 * 16);
+    k_step_begin<<<1, 1, 0, st>>>(step_dev, *sched, n, sd);
+    k_gather<<<dim3(blocks_for(n * 8, 256), members), 256, 0, st>>>(
+        static_cast<const bf16*>(X_all), T_all, W_all, idx, idx_stride, n, X, T, W_all ? Wt : nullptr, sd);
+    auto* pk = static_cast<bf16*>(packed);
+    const Batch bt{members, n, n * kIn, kPacked, kParams, wsb};
+    forward_impl(masters, pk, X, bt, base, out, loss, st);
+    k_loss<<<dim3(std::min(blocks_for(n * kOut, 256), 1024), members), 256, 0, st>>>(
+        out, T, W_all ? Wt : nullptr, n, 1.0f / float(n * kOut), dout, loss);
+    cudaMemsetAsync(grad, 0, sizeof(float) * kParams * members, st);
+    backward_impl(pk, X, bt, dout, base, grad, loss, st);
+    k_adam_dev<<<dim3(blocks_for(kParamsUsed, 256), members), 256, 0, st>>>(
+        masters, m, v, grad, kParamsUsed, kParams, sd, sched->beta1, sched->beta2, sched->eps);
+    k_pack<<<dim3(blocks_for(kPacked, 256), members), 256, 0, st>>>(masters, pk);
+    return cuda_status("hadros_mlp_train_members_dev");
 }
 
 }  // extern "C"

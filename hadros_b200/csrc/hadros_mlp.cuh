@@ -86,7 +86,7 @@ __host__ __device__ constexpr long ws_bytes(long n) { return 10 * ws_act_bytes(n
 // targets, weights, outputs and their gradients (FP32), kWsAlign-rounded.
 __host__ __device__ constexpr long members_batch_bytes(long n)
 {
-    return (n * kIn * 2 + n * (3 * kOut + 1) * 4 + kWsAlign - 1) / kWsAlign * kWsAlign;
+    return (n * kIn * 2 + n * (3 * kOut + 1) * 4 + 64 + kWsAlign - 1) / kWsAlign * kWsAlign;
 }
 
 // Normalization of one model (FP32): features x = (raw - mu) * inv_sd;

@@ -170,10 +170,13 @@ class Surrogate:
     # ---- training -----------------------------------------------------------
     def fit(self, raw, targets, epochs: int = 20, batch: int = 8192, lr: float = 2e-3,
             lr_min: float = 2e-5, weight=None, floors=(TAU_FLOOR, 0.0),
-            log_every: int = 0) -> list[list[float]]:
+            log_every: int = 0, graph: bool = True) -> list[list[float]]:
         """Train every member on (raw features, ln targets) with Adam and a cosine
         learning rate; the members see the data in different orders and step
-        together (one hadros_mlp_train_members call per batch)."""
+        together.  graph=True: the steps run from a CUDA graph that holds a
+        group of training steps (hadros_mlp_train_members_dev, whose step
+        counter and schedule live on the device), replayed through each
+        epoch; graph=False: one hadros_mlp_train_members call per step."""
         torch = _torch()
         L = lib()
         if self.norm is None:
@@ -194,22 +197,50 @@ class Surrogate:
             g = torch.Generator(device=self.device)
             g.manual_seed(self.seed * 7919 + k)
             gens.append(g)
-        st = _stream_ptr(None)
-        M, Pk = self.stack["master"], self.stack["packed"]
+        st = self.stack
         step = self.nets[0].step
+        Wp = None if W is None else _vp(W)
+        graph_obj, group = None, 1
+        if graph:
+            group = max(d for d in range(1, min(64, steps_per_epoch) + 1) if steps_per_epoch % d == 0)
+            sched = abi.HadrosTrainSched(lr, lr_min, 0.9, 0.999, 1e-8, step + total, steps_per_epoch)
+            step_dev = torch.full((1,), step, dtype=torch.int64, device=self.device)
+
+            def call(arrays, counter, stream):
+                _check(L.hadros_mlp_train_members_dev(
+                    K, batch, _vp(X), _vp(T), Wp, _vp(idx), n, _vp(arrays["master"]), _vp(arrays["packed"]),
+                    _vp(arrays["m"]), _vp(arrays["v"]), _vp(arrays["grad"]), C.byref(sched), _vp(counter), _vp(ws),
+                    _vp(loss), C.c_void_p(stream.cuda_stream)))
+            # one call on copies loads the kernels before the capture
+            idx.copy_(torch.arange(n, device=self.device).expand(K, n))
+            call({k: t.clone() for k, t in st.items()}, torch.zeros(1, dtype=torch.int64, device=self.device),
+                 torch.cuda.current_stream(self.device))
+            torch.cuda.synchronize(self.device)
+            cap = torch.cuda.Stream(device=self.device)
+            cap.wait_stream(torch.cuda.current_stream(self.device))
+            graph_obj = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph_obj, stream=cap):
+                for _ in range(group):
+                    call(st, step_dev, cap)
+        sp = _stream_ptr(None)
         self.history = [[] for _ in range(K)]
         for ep in range(epochs):
             for k in range(K):
                 idx[k] = torch.randperm(n, device=self.device, generator=gens[k])
             loss.zero_()
-            for b in range(steps_per_epoch):
-                t = step / max(total - 1, 1)
-                opt = HadrosAdam(lr_min + 0.5 * (lr - lr_min) * (1.0 + math.cos(math.pi * t)), 0.9, 0.999, 1e-8)
-                step += 1
-                _check(L.hadros_mlp_train_members(
-                    K, batch, _vp(X), _vp(T), None if W is None else _vp(W),
-                    C.c_void_p(idx.data_ptr() + 8 * b * batch), n, _vp(M), _vp(Pk), _vp(self.stack["m"]),
-                    _vp(self.stack["v"]), _vp(self.stack["grad"]), C.byref(opt), step, _vp(ws), _vp(loss), st))
+            if graph_obj is not None:
+                for _ in range(steps_per_epoch // group):
+                    graph_obj.replay()
+                step += steps_per_epoch
+            else:
+                for b in range(steps_per_epoch):
+                    t = step / max(total - 1, 1)
+                    opt = HadrosAdam(lr_min + 0.5 * (lr - lr_min) * (1.0 + math.cos(math.pi * t)), 0.9, 0.999, 1e-8)
+                    step += 1
+                    _check(L.hadros_mlp_train_members(
+                        K, batch, _vp(X), _vp(T), Wp, C.c_void_p(idx.data_ptr() + 8 * b * batch), n,
+                        _vp(st["master"]), _vp(st["packed"]), _vp(st["m"]), _vp(st["v"]), _vp(st["grad"]),
+                        C.byref(opt), step, _vp(ws), _vp(loss), sp))
             lv = (loss / steps_per_epoch).tolist()
             if any(math.isnan(x) for x in lv):
                 raise HadrosError(abi.E_TIMEOUT, "NaN training loss: a tensor-core kernel timed out or training diverged")
@@ -217,6 +248,7 @@ class Surrogate:
                 self.history[k].append(lv[k])
             if log_every and (ep + 1) % log_every == 0:
                 print(f"epoch {ep + 1}: loss " + " ".join(f"{x:.3e}" for x in lv), flush=True)
+        del graph_obj
         for net in self.nets:
             net.step = step
         self._images = None

@@ -639,6 +639,24 @@ int32_t hadros_mlp_train_members(int32_t members, int64_t n, const void* X_all, 
                                  const hadros_adam* opt, int64_t step, void* workspace, float* loss,
                                  void* stream);
 
+/* The schedule of a training run whose steps replay from a CUDA graph. */
+typedef struct hadros_train_sched {
+    float lr_max, lr_min;      /* cosine from lr_max (step 1) to lr_min (step total_steps) */
+    float beta1, beta2, eps;   /* Adam */
+    int64_t total_steps;
+    int64_t steps_per_epoch;   /* batches per pass over each member's index list */
+} hadros_train_sched;
+/* hadros_mlp_train_members with the step counter in DEVICE memory: the call
+ * increments *step_dev on the device and takes the step's learning rate,
+ * bias corrections and batch (rows idx[k * idx_stride + ((step - 1) mod
+ * steps_per_epoch) * n + s]) from it, so a sequence of calls captured once in
+ * a CUDA graph replays the following steps.  Launches only (asynchronous). */
+int32_t hadros_mlp_train_members_dev(int32_t members, int64_t n, const void* X_all, const float* T_all,
+                                     const float* W_all, const int64_t* idx, int64_t idx_stride,
+                                     float* masters, void* packed, float* m, float* v, float* grad,
+                                     const hadros_train_sched* sched, int64_t* step_dev,
+                                     void* workspace, float* loss, void* stream);
+
 /* Bytes of one network's inference image (weights pre-swizzled for the
  * tensor-core kernel) and its construction from the BF16 working copy. */
 int64_t hadros_mlp_image_bytes(void);

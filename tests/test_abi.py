@@ -200,7 +200,7 @@ def test_ctypes_layouts_match_the_c_header(hb, tmp_path):
     structs = {"hadros_params": abi.HadrosParams, "hadros_image_out": abi.HadrosImageOut,
                "hadros_stats": abi.HadrosStats, "hadros_schedule": abi.HadrosSchedule,
                "hadros_mlp_norm": abi.HadrosMlpNorm, "hadros_adam": abi.HadrosAdam,
-               "hadros_surrogate_out": abi.HadrosSurrogateOut}
+               "hadros_surrogate_out": abi.HadrosSurrogateOut, "hadros_train_sched": abi.HadrosTrainSched}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "hadros_b200.h"', "int main(void) {"]
     for name, cls in structs.items():
         lines.append(f'  printf("{name} sizeof %zu\\n", sizeof({name}));')
