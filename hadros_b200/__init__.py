@@ -432,9 +432,7 @@ class Context:
         o = HadrosImageOut()
         for k, v in out.items():
             setattr(o, k, v if isinstance(v, int) else v.data_ptr())
-        st = None if stream is None else C.c_void_p(stream if isinstance(stream, int)
-                                                    else stream.cuda_stream)
-        _check(lib().hadros_image_device(self.handle, C.byref(p), sigma.handle, C.byref(o), st))
+        _check(lib().hadros_image_device(self.handle, C.byref(p), sigma.handle, C.byref(o), _ptr_stream(stream)))
 
     def pixels_device(self, p: HadrosParams, sigma: SigmaTable, ids, out: dict, n: int | None = None,
                       stream=None) -> None:
@@ -461,10 +459,20 @@ def schedule(**kw) -> HadrosSchedule:
     return sc
 
 
+# cudaStreamLegacy: the legacy default stream, named explicitly because a
+# NULL stream at the image entry points means the context's own stream.
+_STREAM_LEGACY = 1
+
+
 def _ptr_stream(stream):
+    """The cudaStream_t to pass for `stream` (a torch stream or a raw handle;
+    None = the context's stream).  Torch's default stream has handle 0, which
+    the image entry points would read as the context's own non-blocking
+    stream, unordered with the caller's work; it goes as cudaStreamLegacy."""
     if stream is None:
         return None
-    return C.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+    h = stream if isinstance(stream, int) else stream.cuda_stream
+    return C.c_void_p(h if h else _STREAM_LEGACY)
 
 
 class Plan:

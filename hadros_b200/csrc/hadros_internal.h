@@ -91,6 +91,7 @@ struct PointRec {
 };
 constexpr int kRecDepth = 64;       // points a thread buffers between deferred transfers
 constexpr int kDeferMinBins = 24;   // bins from which the host picks deferred transfer
+constexpr int kAccF = 6;            // FP32 accumulators per bin in mixed precision
 
 struct TraceArgs {
     const DevCam* cams;
@@ -131,8 +132,8 @@ struct TraceArgs {
     const int32_t* order;
     int32_t blocks_per_sm;
     // deferred transfer (mixed only; rec_buf null = per-point transfer in the
-    // loop): per thread slot kRecDepth PointRecs and 5 x rec_bmax FP32
-    // accumulators (T, Tc, I, Ic, S); at most rec_slots threads in the grid
+    // loop): per thread slot kRecDepth PointRecs and 6 x rec_bmax FP32
+    // accumulators (V, Vc, T, Tc, I, Ic); at most rec_slots threads in the grid
     PointRec* rec_buf;
     float* rec_state;
     int32_t rec_bmax;
@@ -141,7 +142,7 @@ struct TraceArgs {
 
 inline size_t rec_bytes(int64_t slots, int bmax)
 {
-    return static_cast<size_t>(slots) * (kRecDepth * sizeof(PointRec) + 5 * sizeof(float) * static_cast<size_t>(bmax));
+    return static_cast<size_t>(slots) * (kRecDepth * sizeof(PointRec) + kAccF * sizeof(float) * static_cast<size_t>(bmax));
 }
 
 struct LaunchCfg {

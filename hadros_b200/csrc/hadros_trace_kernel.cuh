@@ -308,7 +308,7 @@ __host__ __device__ inline SmemLayout smem_layout(int precision, int n, int max_
     L.off_seg = o; o += sizeof(float) * 4 * n;
     o = (o + 15) & ~size_t(15);
     L.off_acc = o;
-    o += (precision == HADROS_PRECISION_MIXED ? 5 * sizeof(float) : 2 * sizeof(double)) *
+    o += (precision == HADROS_PRECISION_MIXED ? kAccF * sizeof(float) : 2 * sizeof(double)) *
          size_t(kTPB) * size_t(max_bins);
     L.total = o;
     return L;
@@ -328,20 +328,41 @@ struct SmemTables {
     float lx0, inv_dlx;
 };
 
-// This thread's column of per-bin accumulators (stride kTPB).  FP64 mode:
-// tau and I.  Mixed mode, exponents in base 2: V - Vc is the Kahan pair of
-// S - tau log2(e), I - Ic the Kahan pair of the intensity scaled by 2^S, and
-// S an integer-valued anchor.
+// This thread's column of per-bin accumulators.  FP64 mode: tau and I
+// (T64, I64, stride kTPB).  Mixed mode, exponents in base 2 (kAccF floats
+// per bin, array j of a column at f + j * fst, bin b at b * st): V - Vc is
+// the Kahan pair of S - tau log2(e) with S the intensity's integer-valued
+// anchor, T - Tc the Kahan pair of tau log2(e) from zero (tau keeps its full
+// relative precision however large S grows), and I - Ic the Kahan pair of the
+// intensity scaled by 2^S.  S itself is rint(V + T).  kAccF = 6 floats.
+
 struct BinAcc {
     double* T64;
     double* I64;
-    float* V;
-    float* Vc;
-    float* I;
-    float* Ic;
-    float* S;
-    int st;   // stride between bins: kTPB in shared memory, 1 in a deferred slot
+    float* f;
+    long fst;   // floats between the arrays V, Vc, T, Tc, I, Ic
+    int st;     // stride between bins: kTPB in shared memory, 1 in a deferred slot
 };
+
+struct Acc6 {
+    float V, Vc, T, Tc, I, Ic;
+};
+
+__device__ __forceinline__ Acc6 acc_load(const BinAcc& a, int b)
+{
+    const float* p = a.f + b * a.st;
+    return Acc6{p[0], p[a.fst], p[2 * a.fst], p[3 * a.fst], p[4 * a.fst], p[5 * a.fst]};
+}
+__device__ __forceinline__ void acc_store(const BinAcc& a, int b, const Acc6& v)
+{
+    float* p = a.f + b * a.st;
+    p[0] = v.V;
+    p[a.fst] = v.Vc;
+    p[2 * a.fst] = v.T;
+    p[3 * a.fst] = v.Tc;
+    p[4 * a.fst] = v.I;
+    p[5 * a.fst] = v.Ic;
+}
 
 // The mixed-precision transfer of one path point, in two parts: the
 // bin-independent terms (point_terms_body, FP64 where a decision is exact)
@@ -356,7 +377,8 @@ struct BinAcc {
 // is accurate to its own rounding even behind optically thick gas.  S moves
 // by whole powers of two when the sum is empty or a term would exceed 2^57.7
 // (e^40); terms below e^-800 are below FP64's range and skipped, as the
-// reference's FP64 sum rounds them away.
+// reference's FP64 sum rounds them away.  tau itself accumulates in its own
+// Kahan pair from zero, so its relative precision does not depend on S.
 
 // 2^x (PTX ex2.approx.ftz.f32: relative error below 2^-22).
 __device__ __forceinline__ float ex2a(float x)
@@ -434,25 +456,24 @@ __device__ __forceinline__ BinK bin_k(const DevBin& d) { return BinK{d.lnE, d.kc
 // point, then the point's absorption (radiative_transfer.cpp:650-671).
 // Rounding intrinsics throughout: no multiply-add is fused differently in the
 // in-loop and the deferred transfer.
-__device__ __forceinline__ void bin_point(const PointRec& p, const BinK& bn, int b, const SmemTables& tb, float& V,
-                                          float& Vc, float& I, float& Ic, float& S)
+__device__ __forceinline__ void bin_point(const PointRec& p, const BinK& bn, int b, const SmemTables& tb, Acc6& a)
 {
     if (p.u2 != -INFINITY) {
         const float arg = __fmaf_rn(-bn.kcut2, p.zm1, p.u2);
-        float e = __fsub_rn(__fadd_rn(arg, V), Vc);
-        if (__fsub_rn(e, S) >= kUnderflow2) {
-            if (I == 0.0f || e > kAnchorMax2) {
+        // log2 of the term itself: below -800 / ln 2 it is under FP64's range
+        if (__fsub_rn(arg, __fsub_rn(a.T, a.Tc)) >= kUnderflow2) {
+            float e = __fsub_rn(__fadd_rn(arg, a.V), a.Vc);
+            if (a.I == 0.0f || e > kAnchorMax2) {
                 const float k = -rintf(e);
-                if (I != 0.0f) {
+                if (a.I != 0.0f) {
                     const float sc = pow2i(static_cast<int>(k));
-                    I = __fmul_rn(I, sc);
-                    Ic = __fmul_rn(Ic, sc);
+                    a.I = __fmul_rn(a.I, sc);
+                    a.Ic = __fmul_rn(a.Ic, sc);
                 }
-                S = __fadd_rn(S, k);
-                kahan_add(V, Vc, k);
-                e = __fsub_rn(__fadd_rn(arg, V), Vc);
+                kahan_add(a.V, a.Vc, k);
+                e = __fsub_rn(__fadd_rn(arg, a.V), a.Vc);
             }
-            kahan_add(I, Ic, ex2a(e));
+            kahan_add(a.I, a.Ic, ex2a(e));
         }
     }
     if (!(p.nbdl2 < 0.0f) && b >= p.b0 && b <= p.b1) {
@@ -472,7 +493,9 @@ __device__ __forceinline__ void bin_point(const PointRec& p, const BinK& bn, int
         }
         const float4 sg = tb.seg[k];
         const float t = __fmul_rn(__fsub_rn(lnE, sg.x), sg.y);
-        kahan_add(V, Vc, -__fmul_rn(__fmul_rn(p.nbdl2, sg.z), ex2a(__fmul_rn(t, sg.w))));
+        const float d = __fmul_rn(__fmul_rn(p.nbdl2, sg.z), ex2a(__fmul_rn(t, sg.w)));
+        kahan_add(a.T, a.Tc, d);
+        kahan_add(a.V, a.Vc, -d);
     }
 }
 
@@ -493,11 +516,9 @@ __device__ __forceinline__ void transfer_point(const DevCam* cam, const DevBin* 
         PointRec pr;
         point_terms_body(cam, bins, B, r, th, gg, dl_cm, pr);
         for (int b = 0; b < B; ++b) {
-            float V = acc.V[b * acc.st], Vc = acc.Vc[b * acc.st];
-            float I = acc.I[b * acc.st], Ic = acc.Ic[b * acc.st], S = acc.S[b * acc.st];
-            bin_point(pr, bin_k(bins[b]), b, tb, V, Vc, I, Ic, S);
-            acc.V[b * acc.st] = V; acc.Vc[b * acc.st] = Vc;
-            acc.I[b * acc.st] = I; acc.Ic[b * acc.st] = Ic; acc.S[b * acc.st] = S;
+            Acc6 a = acc_load(acc, b);
+            bin_point(pr, bin_k(bins[b]), b, tb, a);
+            acc_store(acc, b, a);
         }
     } else {
         const double rho = torus_rho(cam->torus, r, th);
@@ -548,11 +569,12 @@ __device__ __forceinline__ void finish_pixel(const TraceArgs& A, const DevCam* c
     for (int b = 0; b < B; ++b) {
         double tb, ib;
         if (MIXED) {
-            const double S = static_cast<double>(acc.S[b * acc.st]);
-            // tau = (S - (V - Vc)) ln 2;  I = (I_s - c) 2^-S w(E_mid), S integer-valued
-            tb = (S - (static_cast<double>(acc.V[b * acc.st]) - static_cast<double>(acc.Vc[b * acc.st]))) * kLn2;
-            ib = ldexp(static_cast<double>(acc.I[b * acc.st]) - static_cast<double>(acc.Ic[b * acc.st]),
-                       -static_cast<int>(S)) * bins[b].w0;
+            const Acc6 a = acc_load(acc, b);
+            // tau = (T - Tc) ln 2;  S = rint(V + T), integer-valued;  I = (I - Ic) 2^-S w(E_mid)
+            const double t2 = static_cast<double>(a.T) - static_cast<double>(a.Tc);
+            const double S = rint((static_cast<double>(a.V) - static_cast<double>(a.Vc)) + t2);
+            tb = t2 * kLn2;
+            ib = ldexp(static_cast<double>(a.I) - static_cast<double>(a.Ic), -static_cast<int>(S)) * bins[b].w0;
         } else {
             tb = acc.T64[b * acc.st];
             ib = acc.I64[b * acc.st];
@@ -618,9 +640,7 @@ __device__ __forceinline__ void reset_bins(const BinAcc& acc, int B)
 {
     for (int b = 0; b < B; ++b) {
         if (MIXED) {
-            acc.V[b * acc.st] = 0.0f; acc.Vc[b * acc.st] = 0.0f;
-            acc.I[b * acc.st] = 0.0f; acc.Ic[b * acc.st] = 0.0f;
-            acc.S[b * acc.st] = 0.0f;
+            acc_store(acc, b, Acc6{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f});
         } else {
             acc.T64[b * acc.st] = 0.0; acc.I64[b * acc.st] = 0.0;
         }
@@ -673,21 +693,21 @@ __device__ __noinline__ void deferred_transfer(PointRec* rec_buf, float* rec_sta
         const int n = act ? n_src : 0;
         const int b0 = (k - ps) * kDeferBins;
         const long long sl = warp_slot0 + src;
-        float* st = rec_state + sl * 5 * bmax;
+        float* st = rec_state + sl * kAccF * bmax;
+        const BinAcc sacc{nullptr, nullptr, st, bmax, 1};
         const PointRec* rb = rec_buf + sl * kRecDepth;
-        float V[kDeferBins], Vc[kDeferBins], I[kDeferBins], Ic[kDeferBins], S[kDeferBins];
+        Acc6 a[kDeferBins];
         BinK bk[kDeferBins];
         bool on[kDeferBins];
 #pragma unroll
         for (int j = 0; j < kDeferBins; ++j) {
             const int b = b0 + j;
             on[j] = act && b < B_src;
-            V[j] = Vc[j] = I[j] = Ic[j] = S[j] = 0.0f;
+            a[j] = Acc6{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
             bk[j] = BinK{0.0f, 0.0f, 0.0f};
             if (on[j]) {
                 bk[j] = bin_k(bins[cs->bin_offset + b]);
-                V[j] = st[b]; Vc[j] = st[bmax + b]; I[j] = st[2 * bmax + b];
-                Ic[j] = st[3 * bmax + b]; S[j] = st[4 * bmax + b];
+                a[j] = acc_load(sacc, b);
             }
         }
         int nmax = n;
@@ -697,16 +717,12 @@ __device__ __noinline__ void deferred_transfer(PointRec* rec_buf, float* rec_sta
                 const PointRec pr = rb[q];
 #pragma unroll
                 for (int j = 0; j < kDeferBins; ++j)
-                    if (on[j]) bin_point(pr, bk[j], b0 + j, tb, V[j], Vc[j], I[j], Ic[j], S[j]);
+                    if (on[j]) bin_point(pr, bk[j], b0 + j, tb, a[j]);
             }
         }
 #pragma unroll
         for (int j = 0; j < kDeferBins; ++j)
-            if (on[j]) {
-                const int b = b0 + j;
-                st[b] = V[j]; st[bmax + b] = Vc[j]; st[2 * bmax + b] = I[j];
-                st[3 * bmax + b] = Ic[j]; st[4 * bmax + b] = S[j];
-            }
+            if (on[j]) acc_store(sacc, b0 + j, a[j]);
     }
 }
 
@@ -744,17 +760,12 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
     // per-bin accumulators of this thread's ray, column tid, stride kTPB
     double* accT64 = reinterpret_cast<double*>(smem + L.off_acc) + tid;
     double* accI64 = accT64 + size_t(kTPB) * A.max_bins;
-    float* accV = reinterpret_cast<float*>(smem + L.off_acc) + tid;
-    float* accVc = accV + size_t(kTPB) * A.max_bins;
-    float* accI = accVc + size_t(kTPB) * A.max_bins;
-    float* accIc = accI + size_t(kTPB) * A.max_bins;
-    float* accS = accIc + size_t(kTPB) * A.max_bins;
+    float* accF = reinterpret_cast<float*>(smem + L.off_acc) + tid;
     const SmemTables tb{sE, sS, slnE, slnS, slx, sseg, n_sig, sigEmin, sigEmax, sig_scale, A.sig.uniform, A.sig.lx0, A.sig.inv_dlx};
     const long long slot = static_cast<long long>(blockIdx.x) * kTPB + tid;   // deferred-transfer slot
-    float* dstate = defer ? A.rec_state + slot * 5 * A.rec_bmax : nullptr;
-    const BinAcc acc = defer ? BinAcc{nullptr, nullptr, dstate, dstate + A.rec_bmax, dstate + 2 * A.rec_bmax,
-                                      dstate + 3 * A.rec_bmax, dstate + 4 * A.rec_bmax, 1}
-                             : BinAcc{accT64, accI64, accV, accVc, accI, accIc, accS, kTPB};
+    float* dstate = defer ? A.rec_state + slot * kAccF * A.rec_bmax : nullptr;
+    const BinAcc acc = defer ? BinAcc{nullptr, nullptr, dstate, A.rec_bmax, 1}
+                             : BinAcc{accT64, accI64, accF, long(kTPB) * A.max_bins, kTPB};
     PointRec* my_rec = defer ? A.rec_buf + slot * kRecDepth : nullptr;
     int fill = 0;          // points buffered in my_rec
     unsigned iter = 0;     // loop iterations (warp-uniform)
@@ -1112,13 +1123,9 @@ __global__ void __launch_bounds__(kTPB) path_transfer_kernel(const TraceArgs A)
     const int tid = threadIdx.x;
     double* accT64 = reinterpret_cast<double*>(smem + L.off_acc) + tid;
     double* accI64 = accT64 + size_t(kTPB) * A.max_bins;
-    float* accV = reinterpret_cast<float*>(smem + L.off_acc) + tid;
-    float* accVc = accV + size_t(kTPB) * A.max_bins;
-    float* accI = accVc + size_t(kTPB) * A.max_bins;
-    float* accIc = accI + size_t(kTPB) * A.max_bins;
-    float* accS = accIc + size_t(kTPB) * A.max_bins;
+    float* accF = reinterpret_cast<float*>(smem + L.off_acc) + tid;
     const SmemTables tb{sE, sS, slnE, slnS, slx, sseg, n_sig, A.sig.E_min, A.sig.E_max, A.sig.sigma_scale, A.sig.uniform, A.sig.lx0, A.sig.inv_dlx};
-    const BinAcc acc{accT64, accI64, accV, accVc, accI, accIc, accS, kTPB};
+    const BinAcc acc{accT64, accI64, accF, long(kTPB) * A.max_bins, kTPB};
     const DevCam* cam = A.cams;
     const DevBin* bins = A.bins + cam->bin_offset;
     const int B = cam->n_bins;
