@@ -91,7 +91,7 @@ struct PointRec {
 };
 constexpr int kRecDepth = 64;       // points a thread buffers between deferred transfers
 constexpr int kDeferMinBins = 24;   // bins from which the host picks deferred transfer
-constexpr int kAccF = 6;            // FP32 accumulators per bin in mixed precision
+constexpr int kAccF = 5;            // FP32 accumulators per bin in mixed precision
 
 struct TraceArgs {
     const DevCam* cams;

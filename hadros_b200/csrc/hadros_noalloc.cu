@@ -11,14 +11,10 @@
 // (the work cursor and counters, the camera and bin tables, the sigma table).
 // Here that scratch is one file-scope __device__ array instead.
 //
-// The array (kNoAllocScratchBytes, about 32 KB) is part of the library image:
+// The array (kNoAllocScratchBytes, about 60 KB) is part of the library image:
 // every GPU that loads the library holds it until the process exits.  Limits:
-// at most 512 sigma-table rows (the published cross-section tables have 25 to
-// 300) and 64 spectral bins per call; larger requests are rejected with
-// HADROS_E_ARG before anything runs.  The limits are set by the block's shared
-// memory: the sigma table (52 bytes a row) and, in mixed precision, six float
-// accumulators per bin for each of the block's 128 threads (192 KB at 64
-// bins) must fit in 227 KB.  All calls
+// at most 1024 sigma-table rows and 64 spectral bins per call; larger
+// requests are rejected with HADROS_E_ARG before anything runs.  All calls
 // share the one array and each leaves its contents behind; the work counters
 // are cleared at the start of every call.  Two calls whose work overlaps on
 // the GPU (different streams, or different host threads on one device) race
@@ -43,7 +39,7 @@
 namespace hadros {
 namespace {
 
-constexpr int kNoAllocMaxSigma = 512;
+constexpr int kNoAllocMaxSigma = 1024;
 constexpr int kNoAllocMaxBins = 64;
 
 constexpr size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -92,7 +88,7 @@ extern "C" int32_t hadros_image_device_noalloc(const hadros_params* p, const had
                                        "(fast_geodesic must be 0)");
     const int n_sig = static_cast<int>(s->h.E.size());
     if (n_sig > kNoAllocMaxSigma)
-        return set_error(HADROS_E_ARG, "sigma table has more rows than the no-alloc maximum of 512");
+        return set_error(HADROS_E_ARG, "sigma table has more rows than the no-alloc maximum of 1024");
     const int want_bins = p->spectral_kind == HADROS_SPECTRAL_MONOCHROMATIC ? 1 : std::max(p->n_bins, 1);
     if (want_bins > kNoAllocMaxBins)
         return set_error(HADROS_E_ARG, "n_bins exceeds the no-alloc maximum of 64 spectral bins");

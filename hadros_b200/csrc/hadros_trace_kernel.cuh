@@ -329,39 +329,36 @@ struct SmemTables {
 };
 
 // This thread's column of per-bin accumulators.  FP64 mode: tau and I
-// (T64, I64, stride kTPB).  Mixed mode, exponents in base 2 (kAccF floats
-// per bin, array j of a column at f + j * fst, bin b at b * st): V - Vc is
-// the Kahan pair of S - tau log2(e) with S the intensity's integer-valued
-// anchor, T - Tc the Kahan pair of tau log2(e) from zero (tau keeps its full
-// relative precision however large S grows), and I - Ic the Kahan pair of the
-// intensity scaled by 2^S.  S itself is rint(V + T).  kAccF = 6 floats.
+// (T64, I64, stride kTPB).  Mixed mode, exponents in base 2 (kAccF = 5
+// floats per bin, array j of a column at f + j * fst, bin b at b * st): S the
+// intensity's integer-valued anchor (exact), T - Tc the Kahan pair of
+// tau log2(e) from zero, I - Ic the Kahan pair of the intensity scaled by 2^S.
 
 struct BinAcc {
     double* T64;
     double* I64;
     float* f;
-    long fst;   // floats between the arrays V, Vc, T, Tc, I, Ic
+    long fst;   // floats between the arrays S, T, Tc, I, Ic
     int st;     // stride between bins: kTPB in shared memory, 1 in a deferred slot
 };
 
-struct Acc6 {
-    float V, Vc, T, Tc, I, Ic;
+struct BinSums {
+    float S, T, Tc, I, Ic;
 };
 
-__device__ __forceinline__ Acc6 acc_load(const BinAcc& a, int b)
+__device__ __forceinline__ BinSums acc_load(const BinAcc& a, int b)
 {
     const float* p = a.f + b * a.st;
-    return Acc6{p[0], p[a.fst], p[2 * a.fst], p[3 * a.fst], p[4 * a.fst], p[5 * a.fst]};
+    return BinSums{p[0], p[a.fst], p[2 * a.fst], p[3 * a.fst], p[4 * a.fst]};
 }
-__device__ __forceinline__ void acc_store(const BinAcc& a, int b, const Acc6& v)
+__device__ __forceinline__ void acc_store(const BinAcc& a, int b, const BinSums& v)
 {
     float* p = a.f + b * a.st;
-    p[0] = v.V;
-    p[a.fst] = v.Vc;
-    p[2 * a.fst] = v.T;
-    p[3 * a.fst] = v.Tc;
-    p[4 * a.fst] = v.I;
-    p[5 * a.fst] = v.Ic;
+    p[0] = v.S;
+    p[a.fst] = v.T;
+    p[2 * a.fst] = v.Tc;
+    p[3 * a.fst] = v.I;
+    p[4 * a.fst] = v.Ic;
 }
 
 // The mixed-precision transfer of one path point, in two parts: the
@@ -371,14 +368,16 @@ __device__ __forceinline__ void acc_store(const BinAcc& a, int b, const Acc6& v)
 // base 2, so every exponential is one ex2.approx.
 //
 // Intensity: each bin's sum is kept scaled by 2^S with S an integer-valued
-// anchor.  A contribution K w(E_loc)/w(E_mid) exp(-tau) enters as 2^e with
-// e = log2(K w/w0) + (S - tau log2 e).  The second term is carried as one
-// Kahan pair V - Vc, so the large parts cancel inside exact arithmetic and e
-// is accurate to its own rounding even behind optically thick gas.  S moves
-// by whole powers of two when the sum is empty or a term would exceed 2^57.7
-// (e^40); terms below e^-800 are below FP64's range and skipped, as the
-// reference's FP64 sum rounds them away.  tau itself accumulates in its own
-// Kahan pair from zero, so its relative precision does not depend on S.
+// anchor, stored exactly.  A contribution K w(E_loc)/w(E_mid) exp(-tau)
+// enters as 2^e with e = arg + (S - tau log2 e), arg = log2(K w/w0), computed
+// as ((S - T) + arg) + Tc: where the term matters, S - T is within a few
+// hundred of zero (S follows tau minus the emission's own exponent), so its
+// rounding is at most that of arg itself.  S moves by whole powers of two
+// when the sum is empty or a term would exceed 2^57.7 (e^40); terms below
+// e^-800 are below FP64's range and skipped, as the reference's FP64 sum
+// rounds them away.  tau accumulates in its own Kahan pair from zero, so its
+// relative precision does not depend on S, and S stays exact however large
+// tau grows behind optically thick gas.
 
 // 2^x (PTX ex2.approx.ftz.f32: relative error below 2^-22).
 __device__ __forceinline__ float ex2a(float x)
@@ -456,13 +455,13 @@ __device__ __forceinline__ BinK bin_k(const DevBin& d) { return BinK{d.lnE, d.kc
 // point, then the point's absorption (radiative_transfer.cpp:650-671).
 // Rounding intrinsics throughout: no multiply-add is fused differently in the
 // in-loop and the deferred transfer.
-__device__ __forceinline__ void bin_point(const PointRec& p, const BinK& bn, int b, const SmemTables& tb, Acc6& a)
+__device__ __forceinline__ void bin_point(const PointRec& p, const BinK& bn, int b, const SmemTables& tb, BinSums& a)
 {
     if (p.u2 != -INFINITY) {
         const float arg = __fmaf_rn(-bn.kcut2, p.zm1, p.u2);
         // log2 of the term itself: below -800 / ln 2 it is under FP64's range
         if (__fsub_rn(arg, __fsub_rn(a.T, a.Tc)) >= kUnderflow2) {
-            float e = __fsub_rn(__fadd_rn(arg, a.V), a.Vc);
+            float e = __fadd_rn(__fadd_rn(__fsub_rn(a.S, a.T), arg), a.Tc);
             if (a.I == 0.0f || e > kAnchorMax2) {
                 const float k = -rintf(e);
                 if (a.I != 0.0f) {
@@ -470,8 +469,8 @@ __device__ __forceinline__ void bin_point(const PointRec& p, const BinK& bn, int
                     a.I = __fmul_rn(a.I, sc);
                     a.Ic = __fmul_rn(a.Ic, sc);
                 }
-                kahan_add(a.V, a.Vc, k);
-                e = __fsub_rn(__fadd_rn(arg, a.V), a.Vc);
+                a.S = __fadd_rn(a.S, k);
+                e = __fadd_rn(__fadd_rn(__fsub_rn(a.S, a.T), arg), a.Tc);
             }
             kahan_add(a.I, a.Ic, ex2a(e));
         }
@@ -495,7 +494,6 @@ __device__ __forceinline__ void bin_point(const PointRec& p, const BinK& bn, int
         const float t = __fmul_rn(__fsub_rn(lnE, sg.x), sg.y);
         const float d = __fmul_rn(__fmul_rn(p.nbdl2, sg.z), ex2a(__fmul_rn(t, sg.w)));
         kahan_add(a.T, a.Tc, d);
-        kahan_add(a.V, a.Vc, -d);
     }
 }
 
@@ -516,7 +514,7 @@ __device__ __forceinline__ void transfer_point(const DevCam* cam, const DevBin* 
         PointRec pr;
         point_terms_body(cam, bins, B, r, th, gg, dl_cm, pr);
         for (int b = 0; b < B; ++b) {
-            Acc6 a = acc_load(acc, b);
+            BinSums a = acc_load(acc, b);
             bin_point(pr, bin_k(bins[b]), b, tb, a);
             acc_store(acc, b, a);
         }
@@ -569,12 +567,10 @@ __device__ __forceinline__ void finish_pixel(const TraceArgs& A, const DevCam* c
     for (int b = 0; b < B; ++b) {
         double tb, ib;
         if (MIXED) {
-            const Acc6 a = acc_load(acc, b);
-            // tau = (T - Tc) ln 2;  S = rint(V + T), integer-valued;  I = (I - Ic) 2^-S w(E_mid)
-            const double t2 = static_cast<double>(a.T) - static_cast<double>(a.Tc);
-            const double S = rint((static_cast<double>(a.V) - static_cast<double>(a.Vc)) + t2);
-            tb = t2 * kLn2;
-            ib = ldexp(static_cast<double>(a.I) - static_cast<double>(a.Ic), -static_cast<int>(S)) * bins[b].w0;
+            const BinSums a = acc_load(acc, b);
+            // tau = (T - Tc) ln 2;  I = (I - Ic) 2^-S w(E_mid), S integer-valued
+            tb = (static_cast<double>(a.T) - static_cast<double>(a.Tc)) * kLn2;
+            ib = ldexp(static_cast<double>(a.I) - static_cast<double>(a.Ic), -static_cast<int>(a.S)) * bins[b].w0;
         } else {
             tb = acc.T64[b * acc.st];
             ib = acc.I64[b * acc.st];
@@ -640,7 +636,7 @@ __device__ __forceinline__ void reset_bins(const BinAcc& acc, int B)
 {
     for (int b = 0; b < B; ++b) {
         if (MIXED) {
-            acc_store(acc, b, Acc6{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f});
+            acc_store(acc, b, BinSums{0.0f, 0.0f, 0.0f, 0.0f, 0.0f});
         } else {
             acc.T64[b * acc.st] = 0.0; acc.I64[b * acc.st] = 0.0;
         }
@@ -696,14 +692,14 @@ __device__ __noinline__ void deferred_transfer(PointRec* rec_buf, float* rec_sta
         float* st = rec_state + sl * kAccF * bmax;
         const BinAcc sacc{nullptr, nullptr, st, bmax, 1};
         const PointRec* rb = rec_buf + sl * kRecDepth;
-        Acc6 a[kDeferBins];
+        BinSums a[kDeferBins];
         BinK bk[kDeferBins];
         bool on[kDeferBins];
 #pragma unroll
         for (int j = 0; j < kDeferBins; ++j) {
             const int b = b0 + j;
             on[j] = act && b < B_src;
-            a[j] = Acc6{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+            a[j] = BinSums{0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
             bk[j] = BinK{0.0f, 0.0f, 0.0f};
             if (on[j]) {
                 bk[j] = bin_k(bins[cs->bin_offset + b]);

@@ -490,11 +490,11 @@ int32_t hadros_ctx_synchronize(hadros_ctx* ctx);
  * (a framework's caching allocator owns the device memory, or a fixed
  * per-tenant memory budget forbids new allocations): it needs no context,
  * and its scratch (work counters, camera and bin tables, sigma table) is a
- * static ~32 KB device array inside this library, held by every GPU that
+ * static ~60 KB device array inside this library, held by every GPU that
  * loads it until the process exits.  Runs on the current device, on `stream`
  * (a cudaStream_t; NULL = the legacy default stream), with the
  * reference-arithmetic kernel, and returns when the image is done.  Limits:
- * at most 512 sigma rows and 64 spectral bins (else HADROS_E_ARG);
+ * at most 1024 sigma rows and 64 spectral bins (else HADROS_E_ARG);
  * fast_geodesic must be 0.  Every call looks up the array's address in the
  * current context (a device reset or another current context cannot leave
  * it stale); the first call on a device loads the library's kernels there,
@@ -502,7 +502,7 @@ int32_t hadros_ctx_synchronize(hadros_ctx* ctx);
  * array, which keeps the last call's contents (the work counters are cleared
  * at the start of each call): calls that overlap on the GPU race; serialize
  * them.  With 64 bins in mixed precision the kernel keeps the bins in shared
- * memory (up to ~218 KB per block with a 512-row table): one block per SM. */
+ * memory (up to ~213 KB per block with a 1024-row table): one block per SM. */
 int32_t hadros_image_device_noalloc(const hadros_params* p, const hadros_sigma* s,
                                     const hadros_image_out* dev_out, void* stream);
 

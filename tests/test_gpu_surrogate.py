@@ -251,8 +251,12 @@ def test_umma_inference_matches_oracle(hb, torch, sigma_table, members, n_bins):
     """The fused tcgen05 inference kernel against the CPU oracle's forward
     pass (oracle/mlp_oracle.py with the BF16 rounding points of the kernels)
     on the kernel's own input rows: per sample, the ensemble means of ln tau_E
-    and ln I_E differ by FP32 summation order and the hardware tanh only, and
-    so does the per-pixel spread of ln I_obs."""
+    and ln I_E differ by FP32 summation order and the hardware tanh only (an
+    activation that lands near a BF16 rounding boundary can round to the
+    neighbouring BF16 value, a 2^-8 relative step).  The per-pixel spread of
+    ln I_obs is the members' standard deviation of a log-sum-exp over bins;
+    both maps are 1-Lipschitz in the largest per-member difference, so the
+    spread may differ by at most the per-output bound, in ln I units."""
     from hadros_b200 import surrogate as S
     sur = _random_surrogate(hb, torch, members, seed=20 + members)
     nx, ny = 20, 16
@@ -277,11 +281,11 @@ def test_umma_inference_matches_oracle(hb, torch, sigma_table, members, n_bins):
     lnde = np.where(valid, np.log(np.where(valid, bins["dE"], 1.0)), -np.inf)
     L_k = np.log(np.sum(np.exp(ys[:, :, 1].reshape(members, P, B) + lnde), axis=2))   # [K][P]
     spread_ref = L_k.std(0)
-    d_spread = np.abs(res["spread"].cpu().numpy() - spread_ref)
-    excess = (d_spread - 1e-2 * spread_ref).max()
-    stats = (f"rms {rms.tolist()} max {worst.tolist()} (output sd units); spread |diff| max "
-             f"{d_spread.max():.3e} (spread up to {spread_ref.max():.3e}), beyond 1%: {excess:.3e}")
+    d_spread = np.abs(res["spread"].cpu().numpy() - spread_ref) / sd[1]    # in ln I_E sd units
+    stats = (f"rms {rms.tolist()} max {worst.tolist()} (output sd units); spread |diff| rms "
+             f"{np.sqrt(np.mean(d_spread ** 2)):.3e} max {d_spread.max():.3e} (ln I_E sd units; spread up to "
+             f"{spread_ref.max() / sd[1]:.3e})")
     print(stats)
     # a BF16 step is 2^-8 = 0.4% of a unit-scale value: a few steps at worst
     assert rms.max() < 5e-3 and worst.max() < 2e-2, stats
-    assert excess < 1e-3, stats
+    assert np.sqrt(np.mean(d_spread ** 2)) < 5e-3 and d_spread.max() < 2e-2, stats

@@ -85,13 +85,13 @@ def test_noalloc_allocates_nothing_and_runs_the_mev_channel(hb, gpu_ctx, sigma_t
 
 
 def test_noalloc_at_its_limits(hb, gpu_ctx):
-    """64 bins with a 512-row sigma table in mixed precision: the largest
+    """64 bins with a 1024-row sigma table in mixed precision: the largest
     request the entry point accepts (the bins' accumulators then fill most of
     the block's shared memory), twice in a row."""
     import torch
     from hadros_b200 import workloads as W
     torch.cuda.set_device(0)
-    E = np.logspace(4.0, 12.0, 512)
+    E = np.logspace(4.0, 12.0, 1024)
     s = 7.84e-36 * E ** 0.363
     big = hb.SigmaTable.from_arrays(E, s, s / 0.389379e-27)
     p = hb.params(**W.production_point(nx=4, ny=3, h=0.05, n_bins=64, fast=False))
@@ -108,8 +108,8 @@ def test_noalloc_rejects_sizes_beyond_its_limits(hb, sigma_table):
     p = hb.params(spectral="powerlaw_cutoff", n_bins=65, nx=2, ny=2, fast=False)
     rc = hb.lib().hadros_image_device_noalloc(C.byref(p), sigma_table.handle, C.byref(out), None)
     assert rc == 1 and b"64 spectral bins" in hb.lib().hadros_last_error()
-    E = np.logspace(4, 12, 513)
+    E = np.logspace(4, 12, 1025)
     big = hb.SigmaTable.from_arrays(E, 1e-35 * E ** 0.3)
     rc = hb.lib().hadros_image_device_noalloc(C.byref(hb.params(nx=2, ny=2, fast=False)), big.handle,
                                                C.byref(out), None)
-    assert rc == 1 and b"512" in hb.lib().hadros_last_error()
+    assert rc == 1 and b"1024" in hb.lib().hadros_last_error()
