@@ -132,8 +132,8 @@ struct TraceArgs {
     const int32_t* order;
     int32_t blocks_per_sm;
     // deferred transfer (mixed only; rec_buf null = per-point transfer in the
-    // loop): per thread slot kRecDepth PointRecs and 6 x rec_bmax FP32
-    // accumulators (V, Vc, T, Tc, I, Ic); at most rec_slots threads in the grid
+    // loop): per thread slot kRecDepth PointRecs and kAccF x rec_bmax FP32
+    // accumulators (S, T, Tc, I, Ic); at most rec_slots threads in the grid
     PointRec* rec_buf;
     float* rec_state;
     int32_t rec_bmax;
