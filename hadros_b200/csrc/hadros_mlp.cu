@@ -51,18 +51,23 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 //   B_MN: B(k,n) = B[k*ldb + n] (MN-major), else B[n*ldb + k] (K-major)
 // One CTA computes a 128 x BN tile (BN = 256 or 64) of one member
 // (grid.z = member * splits + split).  K runs in chunks of 64 through a
-// three-stage shared-memory ring that all four warps fill with cp.async, each
+// two-stage shared-memory ring that all eight warps fill with cp.async, each
 // 16-byte unit written where the 128-byte swizzle of the UMMA layout puts it:
 // K-major tiles are rows of 64 k (128 B) in 8-row groups 1024 B apart;
 // MN-major tiles are atoms of 64 m or n (one 128-byte row per k) by 8 k,
 // atoms along K 1024 B apart and along MN 8 KB apart.  One thread issues
 // tcgen05.mma (M = 128, N = BN, K = 16, BF16 -> FP32) into a TMEM accumulator
 // and commits each chunk to that stage's mbarrier, which frees the stage for
-// the chunk three ahead.  The epilogue reads each warp's 32 rows with
-// tcgen05.ld.  Rows and k beyond M, K load as zeros and are not stored.
+// the chunk two ahead.  In the epilogue warp w reads, with tcgen05.ld, the 32
+// rows of TMEM lane quarter w % 4 in column half w / 4.  Two stages (98 KB of
+// shared memory) let two CTAs share an SM (2 x BN <= 512 TMEM columns), so one
+// CTA's epilogue overlaps the other's loads and MMAs: the tiles here have
+// only K = 256 (four chunks), and with one CTA per SM the epilogue and the
+// load latency left the tensor pipe idle ~90 % of the time.
+// Rows and k beyond M, K load as zeros and are not stored.
 // Every wait is bounded; a timeout stores NaN in *fail (the step's loss),
 // which the host sees.
-constexpr int UM = 128, UK = 64, kUStages = 3, kUThreads = 128;
+constexpr int UM = 128, UK = 64, kUStages = 2, kUThreads = 256;
 constexpr int kMnLbo = (UK / 8) * 1024;   // MN-major: bytes between 64-wide MN blocks
 
 template <int BN>
@@ -74,7 +79,7 @@ struct UTile {
 };
 
 template <bool A_MN, bool B_MN, int BN, class Epi>
-__global__ void __launch_bounds__(kUThreads, 1)
+__global__ void __launch_bounds__(kUThreads, 2)
     umma_gemm(const bf16* __restrict__ A, long lda, long a_mem, const bf16* __restrict__ B, long ldb, long b_mem,
               int M, int N, int K, int k_split, int splits, Epi epi, float* fail)
 {
@@ -188,11 +193,12 @@ __global__ void __launch_bounds__(kUThreads, 1)
     const bool ok = warp_wait(saddr(acc_ready), 0, abort_flag);
     tc_fence_after();
     if (ok && !*abort_flag) {
-        const uint32_t lane_base = tmem + (uint32_t(warp * 32) << 16);
-        const int m = m0 + warp * 32 + lane;
+        const int quarter = warp & 3, half = warp >> 2;
+        const uint32_t lane_base = tmem + (uint32_t(quarter * 32) << 16);
+        const int m = m0 + quarter * 32 + lane;
         uint32_t v[32];
 #pragma unroll 1
-        for (int cb = 0; cb < BN; cb += 32) {
+        for (int cb = half * (BN / 2); cb < (half + 1) * (BN / 2); cb += 32) {
             tc_ld32(lane_base + uint32_t(cb), v);
             tc_wait_ld(v);
             if (nk == 0) {
@@ -445,6 +451,9 @@ __global__ void __launch_bounds__(kW) k_top_backward(const float* __restrict__ d
     const long s0 = long(blockIdx.x) * chunk, s1 = min(n, s0 + chunk);
     const float w0 = __bfloat162float(W5b[i]), w1 = __bfloat162float(W5b[kW + i]);
     float gw0 = 0.0f, gw1 = 0.0f, gx = 0.0f;
+    // unrolled so that several samples' loads are in flight at once (the
+    // loop is otherwise bound by one load latency per sample)
+#pragma unroll 8
     for (long s = s0; s < s1; ++s) {
         const float d0 = dout[s * kOut], d1 = dout[s * kOut + 1];
         const float z = __bfloat162float(Z4[s * kW + i]), h = __bfloat162float(H4[s * kW + i]);
@@ -473,9 +482,17 @@ __global__ void __launch_bounds__(kW) k_bias_grad(const bf16* __restrict__ dZ, M
     float* Gb = G + k * mm.m + g_off;
     const int i = threadIdx.x;
     const long s0 = long(blockIdx.x) * chunk, s1 = min(mm.n, s0 + chunk);
-    float g = 0.0f;
-    for (long s = s0; s < s1; ++s) g += __bfloat162float(dZ[s * kW + i]);
-    atomicAdd(Gb + i, g);
+    // four partial sums, so that four samples' loads are in flight at once
+    float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f, g3 = 0.0f;
+    long s = s0;
+    for (; s + 4 <= s1; s += 4) {
+        g0 += __bfloat162float(dZ[s * kW + i]);
+        g1 += __bfloat162float(dZ[(s + 1) * kW + i]);
+        g2 += __bfloat162float(dZ[(s + 2) * kW + i]);
+        g3 += __bfloat162float(dZ[(s + 3) * kW + i]);
+    }
+    for (; s < s1; ++s) g0 += __bfloat162float(dZ[s * kW + i]);
+    atomicAdd(Gb + i, (g0 + g1) + (g2 + g3));
 }
 
 // Tied hi/lo first-layer weights: G_W1[o][j] += dW[o][j] + dW[o][j+16] for

@@ -43,16 +43,6 @@ constexpr double B1 = 16.0 / 135.0, B3 = 6656.0 / 12825.0, B4 = 28561.0 / 56430.
 struct K5 {
     double r, th, ph, pr, pth;
 };
-// RKF45 stage coefficients a_ij = num / den (kerr_geodesic.cpp:241-308) in
-// stage order (k2: 1; k3: 2; k4: 3; k5: 4; k6: 5 coefficients); den 0 marks
-// the two integers the reference multiplies by h directly (-8 h, 2 h).
-// Global memory, not __constant__: the lanes of a warp are at different
-// stages and read different entries.
-__device__ const double kStageNum[15] = {1.0,    3.0,   9.0,    1932.0, -7200.0, 7296.0,  439.0, -8.0,
-                                         3680.0, -845.0, -8.0,  2.0,    -3544.0, 1859.0,  -11.0};
-__device__ const double kStageDen[15] = {4.0,    32.0,  32.0,   2197.0, 2197.0,  2197.0,  216.0, 0.0,
-                                         513.0,  4104.0, 27.0,  0.0,    2565.0,  4104.0,  40.0};
-
 
 // -0.5 * sum dg^{mu nu} p_mu p_nu in the reference's (mu, nu) order.
 __device__ __forceinline__ double fd_force(double d00, double d03, double d11, double d22,
@@ -257,6 +247,26 @@ __device__ __forceinline__ void sincos_shift(double s0, double c0, double d, dou
     const double sd = d * (1.0 + d2 * (-1.0 / 6 + d2 * (1.0 / 120 + d2 * (-1.0 / 5040 + d2 * (1.0 / 362880)))));
     *s = s0 * cd + c0 * sd;
     *c = c0 * cd - s0 * sd;
+}
+
+// RHS at a stage point.  The fast variant reuses sin/cos of the step's base
+// angle th0 (s0, c0) through sincos_shift when the stage angle is close.
+template <int FAST>
+__device__ __forceinline__ void geo_rhs_sel(double a, double r, double th, double pr, double pth,
+                                            double pt, double pph, K5& d, double th0, double s0,
+                                            double c0)
+{
+    double s, c;
+    if (FAST) {
+        const double dt = th - th0;
+        if (fabs(dt) < 0.05) sincos_shift(s0, c0, dt, &s, &c);
+        else sincos(th, &s, &c);
+        geo_rhs_fast(a, r, th, s, c, pr, pth, pt, pph, d);
+    } else {
+        crm::DD sd, cd;
+        sincos_dd(th, &sd, &cd);
+        geo_rhs(a, r, th, sd, cd, pr, pth, pt, pph, d);
+    }
 }
 
 // wrapped_delta_phi (kerr_camera.cpp:31-44)
@@ -760,6 +770,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                              : BinAcc{accT64, accI64, accF, long(kTPB) * A.max_bins, kTPB};
     PointRec* my_rec = defer ? A.rec_buf + slot * kRecDepth : nullptr;
     int fill = 0;          // points buffered in my_rec
+    unsigned iter = 0;     // loop iterations (warp-uniform)
 
     int phase = kNeedRay;
     // ray state
@@ -770,27 +781,11 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
     long long att_total = 0;
     double a = 0.0, r = 0.0, th = 0.0, ph = 0.0, pr = 0.0, pth = 0.0, pt = 0.0, pph = 0.0;
     double r_prev = 0.0, th_prev = 0.0, ph_prev = 0.0, E_obs = 1.0, h = 0.0;
+    K5 k1{};
     double s_base = 0.0, c_base = 1.0;   // sin/cos of theta at the step start
     int fate = HADROS_FATE_TRUNCATED;
     MevAcc ma;
     mev_reset(ma);
-    // The stage machine.  `stage` names the RHS evaluation the lane's next
-    // loop iteration makes: 0 = k1 at the step start, 1..5 = k2..k6 of the
-    // RKF45 attempt (kerr_geodesic.cpp:239-308), 6..8 = q2..q4 of the RK4 step
-    // that follows 50 rejected attempts (kerr_geodesic.cpp:137-192, :328).
-    // Every iteration evaluates ONE right-hand side, at one call site, for all
-    // lanes whatever their stage, so the kernel holds a single RHS body.
-    // kst holds k1..k5 (RK4: k1, q2, q3), component order r, theta, phi,
-    // p_r, p_theta; its slot is chosen at run time, so it lives in local
-    // memory (L1) instead of 50 registers.  ysum4 / ysum5 are the weighted sums
-    // of y4 and y5 (RK4: of k1 + 2 q2 + 2 q3 + q4), accumulated in the
-    // reference's operand order as the stages produce their k.
-    int stage = 0;
-    double kst[5][5];
-    double ysum4[5], ysum5[5];
-    // RHS input of the coming evaluation: a stage point, or the step's start
-    double yr = 0.0, yth = 0.0, ypr = 0.0, ypth = 0.0, ys = 0.0, yc = 1.0;
-    crm::DD ysd{0.0, 0.0}, ycd{1.0, 0.0};
 
     while (true) {
         while (phase == kNeedRay || phase == kStepStart) {
@@ -857,7 +852,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                 phase = kStepStart;
             }
 
-            // ---- step start: stop tests, path point, transfer; k1 is next ----
+            // ---- step start: stop tests, path point, transfer, k1 ----------
             bool stop = false;
             if (step >= cam->max_steps) { fate = HADROS_FATE_TRUNCATED; stop = true; }
             else if (r <= cam->r_stop) { fate = HADROS_FATE_CAPTURED; stop = true; }
@@ -872,7 +867,7 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
                 atomicAdd(&A.counters[2], static_cast<unsigned long long>(att_total));
                 if (defer) {   // finished at the warp's next transfer
                     phase = kWaitTransfer;
-                    break;
+                    continue;
                 }
                 finish_pixel<MIXED>(A, cam, bins, B, acc, row, step, fate, att_total);
                 finish_mev(A, cam, ma, row, step);
@@ -956,22 +951,16 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
 
             // ---- transfer of this point into every bin ------------------
             if (defer) {
-                PointRec prec;
-                if (point_terms(cam, bins, B, r, th, dl, z, prec)) my_rec[fill++] = prec;
+                PointRec pr;
+                if (point_terms(cam, bins, B, r, th, dl, z, pr)) my_rec[fill++] = pr;
             } else {
                 transfer_point<MIXED>(cam, bins, B, tb, acc, r, th, dl, z);
             }
             if (MEV) mev_path_point(cam, ma, r, th, dl, z);
 
             // ---- k1 of the coming step_adaptive (shares sin/cos) ------------
-            yr = r;
-            yth = th;
-            ypr = pr;
-            ypth = pth;
-            ys = s;
-            yc = c;
-            ysd = sd;
-            ycd = cd;
+            if (FAST) geo_rhs_fast(a, r, th, s, c, pr, pth, pt, pph, k1);
+            else geo_rhs(a, r, th, sd, cd, pr, pth, pt, pph, k1);
             r_prev = r;
             th_prev = th;
             ph_prev = ph;
@@ -979,161 +968,16 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
             c_base = c;
             h = cam->h0;
             att_in_step = 0;
-            stage = 0;
             phase = kAttempt;
-            break;
-        }
-
-        if (phase == kAttempt) {
-            // ---- the RHS input of this stage: y + sum_j c_j k_j ----------------
-            // RKF45 stage coefficients h * a_ij (kerr_geodesic.cpp:241-308): the
-            // camera's values at h = h0 on a step's first attempt, else formed
-            // from h; RK4: 0.5 h0 and h0 (kerr_geodesic.cpp:145-170).  Each sum
-            // runs left to right over k1, k2, ... as the reference writes it.
-            if (stage > 0) {
-                yr = r;
-                yth = th;
-                ypr = pr;
-                ypth = pth;
-                if (stage <= 5) {
-                    const bool first = att_in_step == 0;
-                    const int q0 = stage * (stage - 1) / 2;
-                    for (int j = 0; j < stage; ++j) {
-                        const int q = q0 + j;
-                        const double cf = first ? cam->c0[q]
-                                                : (kStageDen[q] == 0.0 ? h * kStageNum[q]
-                                                                       : h * kStageNum[q] / kStageDen[q]);
-                        yr = yr + cf * kst[j][0];
-                        yth = yth + cf * kst[j][1];
-                        ypr = ypr + cf * kst[j][3];
-                        ypth = ypth + cf * kst[j][4];
-                    }
-                } else {
-                    const int j = stage - 6;   // k1, q2, q3
-                    const double cf = stage == 8 ? cam->h0 : 0.5 * cam->h0;
-                    yr = yr + cf * kst[j][0];
-                    yth = yth + cf * kst[j][1];
-                    ypr = ypr + cf * kst[j][3];
-                    ypth = ypth + cf * kst[j][4];
-                }
-                if (FAST) {   // sin/cos by angle shift from the step's base angle when close
-                    const double dt = yth - th;
-                    if (fabs(dt) < 0.05) sincos_shift(s_base, c_base, dt, &ys, &yc);
-                    else sincos(yth, &ys, &yc);
-                } else {
-                    sincos_dd(yth, &ysd, &ycd);
-                }
-            }
-
-            // ---- the one right-hand side of the iteration ------------------
-            K5 kk;
-            if (FAST) geo_rhs_fast(a, yr, yth, ys, yc, ypr, ypth, pt, pph, kk);
-            else geo_rhs(a, yr, yth, ysd, ycd, ypr, ypth, pt, pph, kk);
-            const double kv[5] = {kk.r, kk.th, kk.ph, kk.pr, kk.pth};
-
-            if (stage <= 5) {
-                if (stage < 5) {
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) kst[stage][f] = kv[f];
-                }
-                // y4, y5 weights: k1 A1 B1; k3 A3 B3; k4 A4 B4; k5 -A5 -B5; k6 B6
-                // (kerr_geodesic.cpp:310-311)
-                if (stage == 0) {
-                    // (re)started below with the attempt
-                } else if (stage == 2) {
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) { ysum4[f] = ysum4[f] + A3 * kv[f]; ysum5[f] = ysum5[f] + B3 * kv[f]; }
-                } else if (stage == 3) {
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) { ysum4[f] = ysum4[f] + A4 * kv[f]; ysum5[f] = ysum5[f] + B4 * kv[f]; }
-                } else if (stage == 4) {
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) { ysum4[f] = ysum4[f] - A5 * kv[f]; ysum5[f] = ysum5[f] - B5 * kv[f]; }
-                } else if (stage == 5) {
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) ysum5[f] = ysum5[f] + B6 * kv[f];
-                }
-                bool restart = stage == 0;
-                if (stage == 5) {
-                    // ---- the attempt's verdict (kerr_geodesic.cpp:310-326) ------
-                    const double y4r = r + h * ysum4[0], y5r = r + h * ysum5[0];
-                    const double y4t = th + h * ysum4[1], y5t = th + h * ysum5[1];
-                    const double y4p = ph + h * ysum4[2], y5p = ph + h * ysum5[2];
-                    const double y4pr = pr + h * ysum4[3], y5pr = pr + h * ysum5[3];
-                    const double y4pt = pth + h * ysum4[4], y5pt = pth + h * ysum5[4];
-                    double err = 0.0;   // error_norm (kerr_geodesic.cpp:219-233); p_phi term is 0
-                    err = smax(err, fabs(y4r - y5r));
-                    err = smax(err, fabs(y4t - y5t));
-                    err = smax(err, fabs(y4p - y5p));
-                    err = smax(err, fabs(y4pr - y5pr));
-                    err = smax(err, fabs(y4pt - y5pt));
-                    err = smax(err, 0.0);
-                    ++att_total;
-                    const double h_min = cam->h_min;
-                    if (err < cam->tol || h <= h_min) {
-                        r = y5r; th = y5t; ph = y5p; pr = y5pr; pth = y5pt;
-                        ++step;
-                        phase = kStepStart;
-                    } else {
-                        const double factor = 0.8 * crm::pow025_rn(cam->tol / smax(err, 1.0e-30));
-                        h *= sclamp(factor, 0.1, 5.0);
-                        if (h < h_min) h = h_min;
-                        ++att_in_step;
-                        if (att_in_step == 50) {
-                            stage = 6;   // step_rk4 with h0: q2 next, from k1
-                        } else {
-                            restart = true;   // k1 is kept: the next attempt starts at k2
-                        }
-                    }
-                } else {
-                    ++stage;
-                }
-                if (restart) {
-                    stage = 1;
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        ysum4[f] = A1 * kst[0][f];
-                        ysum5[f] = B1 * kst[0][f];
-                    }
-                }
-            } else {
-                // ---- step_rk4 (kerr_geodesic.cpp:137-192): ysum4 carries
-                // k1 + 2 q2 + 2 q3 + q4 in the reference's order
-                if (stage == 6) {
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        kst[1][f] = kv[f];
-                        ysum4[f] = kst[0][f] + 2.0 * kv[f];
-                    }
-                    stage = 7;
-                } else if (stage == 7) {
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        kst[2][f] = kv[f];
-                        ysum4[f] = ysum4[f] + 2.0 * kv[f];
-                    }
-                    stage = 8;
-                } else {
-                    const double h0 = cam->h0;
-                    r += h0 * (ysum4[0] + kv[0]) / 6.0;
-                    th += h0 * (ysum4[1] + kv[1]) / 6.0;
-                    ph += h0 * (ysum4[2] + kv[2]) / 6.0;
-                    pr += h0 * (ysum4[3] + kv[3]) / 6.0;
-                    pth += h0 * (ysum4[4] + kv[4]) / 6.0;
-                    ++att_total;
-                    ++step;
-                    phase = kStepStart;
-                }
-            }
         }
 
         if (defer) {
-            // When a lane's buffer is full (each iteration adds at most one
-            // point per lane), or when no lane has a ray in flight, the warp
-            // replays every lane's buffered points into its bins, then
-            // finishes the waiting rays.  Warp-uniform decision.
+            // Every kRecDepth iterations (each adds at most one point per lane),
+            // or when no lane has a ray in flight, the warp replays every lane's
+            // buffered points into its bins, then finishes the waiting rays.
+            ++iter;
             const bool idle = __all_sync(0xffffffffu, phase == kDone || phase == kWaitTransfer);
-            if (__any_sync(0xffffffffu, fill >= kRecDepth) || idle) {
+            if (iter % kRecDepth == 0 || idle) {
                 deferred_transfer(A.rec_buf, A.rec_state, A.bins, A.rec_bmax, tb, slot - (tid & 31), fill, B, cam);
                 if (phase == kWaitTransfer) {
                     finish_pixel<MIXED>(A, cam, bins, B, acc, row, step, fate, att_total);
@@ -1144,6 +988,111 @@ __global__ void __launch_bounds__(kTPB, HADROS_MIN_BLOCKS) trace_kernel(const Tr
             }
         }
         if (__all_sync(0xffffffffu, phase == kDone)) break;
+        if (phase != kAttempt) continue;
+
+        // ---- one RKF45 attempt (kerr_geodesic.cpp:239-326) -----------------
+        // Stage coefficients h * a_ij (:241-308): the camera's values at
+        // h = h0 on a step's first attempt, else formed from h, each where its
+        // stage uses it so that none stays live across the attempt.  The phi
+        // components of k enter only y4 and y5: their weighted sums are
+        // accumulated as the stages produce them, in the reference's order.
+        const bool first = att_in_step == 0;
+        const double* c0 = cam->c0;
+#define HAD_CF(q, num, den) (first ? c0[q] : h * (num) / (den))
+#define HAD_CFM(q, num) (first ? c0[q] : h * (num))
+        double s4p = A1 * k1.ph, s5p = B1 * k1.ph;   // y4, y5 phi sums so far
+        K5 k2, k3, k4, k5, k6;
+        {
+            const double c = HAD_CF(0, 1.0, 4.0);
+            geo_rhs_sel<FAST>(a, r + c * k1.r, th + c * k1.th, pr + c * k1.pr, pth + c * k1.pth, pt, pph, k2,
+                              th, s_base, c_base);
+        }
+        {
+            const double c1 = HAD_CF(1, 3.0, 32.0), c2 = HAD_CF(2, 9.0, 32.0);
+            geo_rhs_sel<FAST>(a, r + c1 * k1.r + c2 * k2.r, th + c1 * k1.th + c2 * k2.th,
+                              pr + c1 * k1.pr + c2 * k2.pr, pth + c1 * k1.pth + c2 * k2.pth, pt, pph, k3, th,
+                              s_base, c_base);
+        }
+        s4p = s4p + A3 * k3.ph;
+        s5p = s5p + B3 * k3.ph;
+        {
+            const double c3 = HAD_CF(3, 1932.0, 2197.0), c4 = HAD_CF(4, -7200.0, 2197.0),
+                         c5 = HAD_CF(5, 7296.0, 2197.0);
+            geo_rhs_sel<FAST>(a, r + c3 * k1.r + c4 * k2.r + c5 * k3.r, th + c3 * k1.th + c4 * k2.th + c5 * k3.th,
+                              pr + c3 * k1.pr + c4 * k2.pr + c5 * k3.pr,
+                              pth + c3 * k1.pth + c4 * k2.pth + c5 * k3.pth, pt, pph, k4, th, s_base, c_base);
+        }
+        s4p = s4p + A4 * k4.ph;
+        s5p = s5p + B4 * k4.ph;
+        {
+            const double c6 = HAD_CF(6, 439.0, 216.0), c7 = HAD_CFM(7, -8.0), c8 = HAD_CF(8, 3680.0, 513.0),
+                         c9 = HAD_CF(9, -845.0, 4104.0);
+            geo_rhs_sel<FAST>(a, r + c6 * k1.r + c7 * k2.r + c8 * k3.r + c9 * k4.r,
+                              th + c6 * k1.th + c7 * k2.th + c8 * k3.th + c9 * k4.th,
+                              pr + c6 * k1.pr + c7 * k2.pr + c8 * k3.pr + c9 * k4.pr,
+                              pth + c6 * k1.pth + c7 * k2.pth + c8 * k3.pth + c9 * k4.pth, pt, pph, k5, th,
+                              s_base, c_base);
+        }
+        s4p = s4p - A5 * k5.ph;
+        s5p = s5p - B5 * k5.ph;
+        {
+            const double c10 = HAD_CF(10, -8.0, 27.0), c11 = HAD_CFM(11, 2.0), c12 = HAD_CF(12, -3544.0, 2565.0),
+                         c13 = HAD_CF(13, 1859.0, 4104.0), c14 = HAD_CF(14, -11.0, 40.0);
+            geo_rhs_sel<FAST>(a, r + c10 * k1.r + c11 * k2.r + c12 * k3.r + c13 * k4.r + c14 * k5.r,
+                              th + c10 * k1.th + c11 * k2.th + c12 * k3.th + c13 * k4.th + c14 * k5.th,
+                              pr + c10 * k1.pr + c11 * k2.pr + c12 * k3.pr + c13 * k4.pr + c14 * k5.pr,
+                              pth + c10 * k1.pth + c11 * k2.pth + c12 * k3.pth + c13 * k4.pth + c14 * k5.pth, pt,
+                              pph, k6, th, s_base, c_base);
+        }
+        s5p = s5p + B6 * k6.ph;
+#undef HAD_CF
+#undef HAD_CFM
+#define HAD_Y4(f) (A1 * k1.f + A3 * k3.f + A4 * k4.f - A5 * k5.f)
+#define HAD_Y5(f) (B1 * k1.f + B3 * k3.f + B4 * k4.f - B5 * k5.f + B6 * k6.f)
+        const double y4r = r + h * HAD_Y4(r), y5r = r + h * HAD_Y5(r);
+        const double y4t = th + h * HAD_Y4(th), y5t = th + h * HAD_Y5(th);
+        const double y4p = ph + h * s4p, y5p = ph + h * s5p;
+        const double y4pr = pr + h * HAD_Y4(pr), y5pr = pr + h * HAD_Y5(pr);
+        const double y4pt = pth + h * HAD_Y4(pth), y5pt = pth + h * HAD_Y5(pth);
+#undef HAD_Y4
+#undef HAD_Y5
+        double err = 0.0;   // error_norm (kerr_geodesic.cpp:219-233); p_phi term is 0
+        err = smax(err, fabs(y4r - y5r));
+        err = smax(err, fabs(y4t - y5t));
+        err = smax(err, fabs(y4p - y5p));
+        err = smax(err, fabs(y4pr - y5pr));
+        err = smax(err, fabs(y4pt - y5pt));
+        err = smax(err, 0.0);
+        ++att_total;
+        const double h_min = cam->h_min;
+        if (err < cam->tol || h <= h_min) {
+            r = y5r; th = y5t; ph = y5p; pr = y5pr; pth = y5pt;
+            ++step;
+            phase = kStepStart;
+        } else {
+            const double factor = 0.8 * crm::pow025_rn(cam->tol / smax(err, 1.0e-30));
+            h *= sclamp(factor, 0.1, 5.0);
+            if (h < h_min) h = h_min;
+            ++att_in_step;
+            if (att_in_step == 50) {   // step_rk4 with h0 (kerr_geodesic.cpp:137-192, :328)
+                const double h0 = cam->h0;
+                K5 q2, q3, q4;
+                geo_rhs_sel<FAST>(a, r + 0.5 * h0 * k1.r, th + 0.5 * h0 * k1.th, pr + 0.5 * h0 * k1.pr,
+                           pth + 0.5 * h0 * k1.pth, pt, pph, q2, th, s_base, c_base);
+                geo_rhs_sel<FAST>(a, r + 0.5 * h0 * q2.r, th + 0.5 * h0 * q2.th, pr + 0.5 * h0 * q2.pr,
+                           pth + 0.5 * h0 * q2.pth, pt, pph, q3, th, s_base, c_base);
+                geo_rhs_sel<FAST>(a, r + h0 * q3.r, th + h0 * q3.th, pr + h0 * q3.pr, pth + h0 * q3.pth,
+                           pt, pph, q4, th, s_base, c_base);
+                r += h0 * (k1.r + 2.0 * q2.r + 2.0 * q3.r + q4.r) / 6.0;
+                th += h0 * (k1.th + 2.0 * q2.th + 2.0 * q3.th + q4.th) / 6.0;
+                ph += h0 * (k1.ph + 2.0 * q2.ph + 2.0 * q3.ph + q4.ph) / 6.0;
+                pr += h0 * (k1.pr + 2.0 * q2.pr + 2.0 * q3.pr + q4.pr) / 6.0;
+                pth += h0 * (k1.pth + 2.0 * q2.pth + 2.0 * q3.pth + q4.pth) / 6.0;
+                ++att_total;
+                ++step;
+                phase = kStepStart;
+            }
+        }
     }
 }
 
