@@ -631,8 +631,13 @@ def scan_arm(args) -> None:
     t_setup = time.perf_counter()
     tpts = W.scan_points(args.train_points, seed=W.SEED + 17)
     cams = [SC.production_cam(r, t, SCAN_SIDE, SCAN_BINS) for r, t in tpts]
-    sur, info = SC.train(ctx, sig, cams, args.pixels_per_cam, 4, args.epochs, W.SEED, args.batch, args.lr,
-                         device=local)
+    if args.model and os.path.exists(args.model):
+        sur, info = SC.load_model(args.model, device=local)
+    else:
+        sur, info = SC.train(ctx, sig, cams, args.pixels_per_cam, 4, args.epochs, W.SEED, args.batch, args.lr,
+                             device=local)
+        if args.model and rank == 0:
+            SC.save_model(args.model, sur, info)
     vcams, vraw, vy = SC.held_out_samples(ctx, sig, cams, args.pixels_per_cam, W.SEED, info["i_floor"], local)
     calib = SC.calibrate(sur, sig, vcams, vraw, vy, info["i_floor"], args.bound)
     del vraw, vy
@@ -741,7 +746,7 @@ def scan_arm(args) -> None:
                           "fallback_frac_max": fb_max, "threshold": thr, "bound": args.bound,
                           "calibration": calib, "members": len(sur.nets),
                           "train": {k: info[k] for k in ("samples", "trace_s", "fit_s", "val_rms_ln_tau",
-                                                         "val_rms_ln_I") if k in info},
+                                                         "val_rms_ln_I", "loaded_from") if k in info},
                           "epochs": args.epochs, "setup_s": setup_s},
             "plain_tracer": {"seconds_per_point": plain_s, "pixel_bins_per_s": P * B / plain_s,
                              "point": k_plain, "speedup_of_surrogate_step": plain_s / per_step,
@@ -917,6 +922,9 @@ def main() -> None:
     ap.add_argument("--train-points", type=int, default=128, help="scan: training cameras (incl. held out)")
     ap.add_argument("--pixels-per-cam", type=int, default=4096, help="scan: training pixels per camera")
     ap.add_argument("--batch", type=int, default=8192, help="scan: training batch")
+    ap.add_argument("--model", default=None,
+                    help="scan: ensemble file (.npz): loaded when it exists (training record beside it), "
+                         "else trained as usual and saved there")
     ap.add_argument("--lr", type=float, default=2e-3, help="scan: peak learning rate")
     ap.add_argument("--bound", type=float, default=0.01, help="scan: intensity error bound (fallback)")
     ap.add_argument("--judge", type=float, default=0.01, help="scan: judged fraction of pixels")
