@@ -655,7 +655,10 @@ enum Phase : int { kNeedRay = 0, kStepStart = 1, kAttempt = 2, kDone = 3, kWaitT
 // Not inlined: called once every kRecDepth loop iterations, its registers are
 // saved around the call instead of crowding the RKF45 attempt's.
 // warp_slot0 is the slot of lane 0.
-constexpr int kDeferBins = 4;
+#ifndef HADROS_DEFER_BINS
+#define HADROS_DEFER_BINS 4
+#endif
+constexpr int kDeferBins = HADROS_DEFER_BINS;
 
 __device__ __noinline__ void deferred_transfer(PointRec* rec_buf, float* rec_state, const DevBin* bins, int bmax,
                                                const SmemTables tb, long long warp_slot0, int fill, int B,

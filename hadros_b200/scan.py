@@ -407,7 +407,8 @@ def run_production(a) -> dict | None:
                                       a.judge, point_rng(k), buf)
                 row["point"] = k
                 print(json.dumps({"point": k, "rank": rank, "seconds": row["seconds"],
-                                  "fallback_frac": row["fallback_frac"], "worst": row["error"]["worst"]}),
+                                  "fallback_frac": row["fallback_frac"], "worst": row["error"]["worst"],
+                                  "p99": row["error"]["p99"]}),
                       file=sys.stderr, flush=True)
                 return row
             t0 = time.perf_counter()
