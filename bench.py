@@ -411,6 +411,16 @@ def read_traffic() -> tuple[float | None, str | None]:
     return d.get("bytes_per_launch"), d.get("source")
 
 
+def read_traffic_per_step() -> tuple[float | None, str | None]:
+    """DRAM bytes per accepted step of the production trace kernel (deferred
+    transfer, 64 bins) from a committed ncu summary of a 256x256 launch."""
+    f = ROOT / "profiles" / "ncu_traffic_production.json"
+    if not f.exists():
+        return None, None
+    d = json.loads(f.read_text())
+    return d.get("bytes_per_accepted_step"), d.get("source")
+
+
 def gpu_arm(args) -> None:
     import torch
 
@@ -703,7 +713,10 @@ def scan_arm(args) -> None:
     full_check = {"point": k_plain, "pixels": int(full[0].item()), "worst": float(full[1].item()),
                   "p99": float(full[2].item()), "median": float(full[3].item())}
     del plain
-    traffic, traffic_src = read_traffic()
+    per_step, traffic_src = read_traffic_per_step()
+    traffic = per_step * steps_sum if per_step else None
+    if traffic_src:
+        traffic_src += " (bytes per accepted step of that launch x this launch's accepted steps)"
 
     # ---- e2e: the same steps from host memory to host memory --------------------
     host = runner.alloc_host()
