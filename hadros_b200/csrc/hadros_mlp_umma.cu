@@ -50,7 +50,7 @@ constexpr int kStagesPerMember = 14;         // L1: 1, L2..L4: 4 each, L5: 1
 constexpr int kLastStageBytes = 8192;        // L5: 4 chunks of [16 x 64]
 constexpr long kImageBytes = long(kStagesPerMember - 1) * kStageBytes + kLastStageBytes;
 constexpr int kActBytes = 4 * 16384;         // [128 rows x 256 K] as 4 swizzled chunks
-constexpr int kEpiWarps = 8;
+constexpr int kEpiWarps = 16;   // 4 per 32-row TMEM lane quarter: 2 accumulators x 2 column halves
 constexpr int kThreads = (kEpiWarps + 2) * 32;   // + MMA warp + producer warp
 constexpr int kMaxMembers = 8;
 
@@ -310,8 +310,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                       }
         }
     } else {
-        // ---- epilogue warps: rows of accumulator t = warp / 4 ---------------------
-        const int t = warp >> 2, qw = warp & 3;
+        // ---- epilogue warps ------------------------------------------------------
+        // Warp w takes TMEM lane quarter w % 4 (rows qw*32..+31) of accumulator
+        // t = (w / 4) % 2 and column half cpart = w / 8 (columns cpart*128..+127):
+        // two warps share each row, each evaluating half of its columns, which
+        // doubles the warps that hide the TMEM-load and barrier latency of the
+        // epilogue.  The column-half-0 ("lead") warp also does the row's last
+        // layer, the skip connection and the per-pixel reductions.
+        const int qw = warp & 3, t = (warp >> 2) & 1, cpart = warp >> 3;
+        const bool lead = cpart == 0;
         const int r = qw * 32 + lane;                 // row in the 128-row half
         const int trow = t * kTileRows + r;           // row in the 256-sample tile
         uint8_t* my_act = act + t * kActBytes;
@@ -321,53 +328,61 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
         // terms; on exit m = the pixel's maximum, se = sum exp(term - m), x1, x2
         // the pixel's sums.  Pixels of <= 32 bins reduce within a warp; larger
         // ones combine their warps through shared memory.
+        // Only the lead warps hold the values; the others take part in the
+        // group's barriers.
         auto pixel_reduce = [&](float& m, float& se, float& x1, float& x2) -> bool {
-            const int width = B < 32 ? B : 32;
-            const float v = m;
-            for (int off = 1; off < width; off <<= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
-            se = (m == -INFINITY) ? 0.0f : __expf(v - m);
-            for (int off = 1; off < width; off <<= 1) {
-                se += __shfl_xor_sync(0xffffffffu, se, off);
-                x1 += __shfl_xor_sync(0xffffffffu, x1, off);
-                x2 += __shfl_xor_sync(0xffffffffu, x2, off);
+            if (lead) {
+                const int width = B < 32 ? B : 32;
+                const float v = m;
+                for (int off = 1; off < width; off <<= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+                se = (m == -INFINITY) ? 0.0f : __expf(v - m);
+                for (int off = 1; off < width; off <<= 1) {
+                    se += __shfl_xor_sync(0xffffffffu, se, off);
+                    x1 += __shfl_xor_sync(0xffffffffu, x1, off);
+                    x2 += __shfl_xor_sync(0xffffffffu, x2, off);
+                }
             }
             if (B > 32) {
                 float* wr = red_a + (t * 4 + qw) * 4;
-                if (lane == 0) {
+                if (lead && lane == 0) {
                     wr[0] = m;
                     wr[1] = se;
                     wr[2] = x1;
                     wr[3] = x2;
                 }
                 if (!epi_sync()) return false;
-                const int nw = B / 32, w0 = t * 4 + (qw / nw) * nw;
-                float M = -INFINITY;
-                for (int j = 0; j < nw; ++j) M = fmaxf(M, red_a[(w0 + j) * 4]);
-                float S = 0.0f, X1 = 0.0f, X2 = 0.0f;
-                for (int j = 0; j < nw; ++j) {
-                    const float* q = red_a + (w0 + j) * 4;
-                    S += (q[0] == -INFINITY) ? 0.0f : q[1] * __expf(q[0] - M);
-                    X1 += q[2];
-                    X2 += q[3];
+                if (lead) {
+                    const int nw = B / 32, w0 = t * 4 + (qw / nw) * nw;
+                    float M = -INFINITY;
+                    for (int j = 0; j < nw; ++j) M = fmaxf(M, red_a[(w0 + j) * 4]);
+                    float S = 0.0f, X1 = 0.0f, X2 = 0.0f;
+                    for (int j = 0; j < nw; ++j) {
+                        const float* q = red_a + (w0 + j) * 4;
+                        S += (q[0] == -INFINITY) ? 0.0f : q[1] * __expf(q[0] - M);
+                        X1 += q[2];
+                        X2 += q[3];
+                    }
+                    m = M;
+                    se = S;
+                    x1 = X1;
+                    x2 = X2;
                 }
-                m = M;
-                se = S;
-                x1 = X1;
-                x2 = X2;
                 if (!epi_sync()) return false;   // slots free for the next reduction
             }
             return true;
         };
         const uint32_t lane_base = tmem + (uint32_t(qw * 32) << 16) + uint32_t(t * 256);
         long layer_count = 0;
-        const bool leader_possible = (trow % B) == 0;
+        const bool leader_possible = lead && (trow % B) == 0;
         for (long tile = blockIdx.x; tile < n_tiles && __all_sync(0xffffffffu, *abort_flag == 0);
              tile += gridDim.x) {
             const long s = tile * (kPair * kTileRows) + trow;
             const bool valid = s < n_samples;
             const long lp = valid ? s / B : 0;
             const int b = valid ? int(s % B) : 0;
-            uint32_t feat[kIn / 2];
+            // this warp's half of the input row: units 0..3 (hi, lo) for column
+            // half 0, units 4..7 (Fourier features) for column half 1
+            uint32_t feat[kIn / 4];
             {
                 float f[kF], xn[kF];
                 raw_features(A.cam, A.pixel_begin + lp, b, f);
@@ -376,7 +391,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                 __align__(16) bf16 row[kIn];
                 input_row(xn, row);
 #pragma unroll
-                for (int q = 0; q < kIn / 2; ++q) feat[q] = reinterpret_cast<const uint32_t*>(row)[q];
+                for (int q = 0; q < kIn / 4; ++q)
+                    feat[q] = reinterpret_cast<const uint32_t*>(row)[cpart * (kIn / 4) + q];
             }
             float sum_tau = 0.0f, sum_lnI = 0.0f;
             float w_ref = 0.0f, w_s1 = 0.0f, w_s2 = 0.0f;   // pixel leader: shifted sums of ln I_k
@@ -387,17 +403,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                 // buffer was last read two members ago, before the barrier below
                 // of the previous member)
                 {
-                    const int gt = PP ? r : trow;      // thread within the group
+                    const int gt = PP ? cpart * kTileRows + r : cpart * 2 * kTileRows + trow;   // thread in the group
                     for (int e = gt; e < 4 * kW; e += kGroupWarps * 32)   // hidden biases / 2
                         my_bias[e] = 0.5f * P[off_b(1 + e / kW) + e % kW];
                     if (gt < kOut) my_bias[4 * kW + gt] = P[kOffB5 + gt];
                     if (gt < kOut * kF) my_bias[4 * kW + kOut + gt] = P[kOffWs + gt];
                 }
-                // features -> chunk 0, the 8 16-byte units of row r
+                // features -> chunk 0: this warp's four 16-byte units of row r
 #pragma unroll
-                for (int u = 0; u < kIn / 8; ++u)
-                    *reinterpret_cast<uint4*>(my_act + r * 128 + ((u ^ (r & 7)) << 4)) =
+                for (int u = 0; u < 4; ++u) {
+                    const int uu = cpart * 4 + u;
+                    *reinterpret_cast<uint4*>(my_act + r * 128 + ((uu ^ (r & 7)) << 4)) =
                         make_uint4(feat[4 * u], feat[4 * u + 1], feat[4 * u + 2], feat[4 * u + 3]);
+                }
                 fence_async_smem();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(saddr(&act_ready[grp]));
@@ -406,19 +424,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                     if (!warp_wait(saddr(&acc_full[grp]), uint32_t(layer_count & 1), abort_flag)) goto done;
                     tc_fence_after();
                     const float* sb = my_bias + (L - 1) * kW;
-                    // two register sets: the next 32 columns load from TMEM while
-                    // the current 32 are processed
-                    uint32_t va[32], vb[32];
-                    tc_ld32(lane_base, va);
-                    tc_wait_ld(va);
+                    // this warp's 128 columns, 32 at a time (the warp that shares
+                    // the row hides this warp's TMEM-load latency)
+                    const int c0 = cpart * (kW / 2), c1 = c0 + kW / 2;
+                    uint32_t v[32];
 #pragma unroll 1
-                    for (int cb = 0; cb < kW; cb += 64) {
-                        tc_ld32(lane_base + uint32_t(cb + 32), vb);
-                        epi_chunk(va, sb, cb, my_act, r);
-                        tc_wait_ld(vb);
-                        if (cb + 64 < kW) tc_ld32(lane_base + uint32_t(cb + 64), va);
-                        epi_chunk(vb, sb, cb + 32, my_act, r);
-                        if (cb + 64 < kW) tc_wait_ld(va);
+                    for (int cb = c0; cb < c1; cb += 32) {
+                        tc_ld32(lane_base + uint32_t(cb), v);
+                        tc_wait_ld(v);
+                        epi_chunk(v, sb, cb, my_act, r);
                     }
                     tc_fence_before();
                     fence_async_smem();
@@ -429,21 +443,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
                 if (!warp_wait(saddr(&acc_full[grp]), uint32_t(layer_count & 1), abort_flag)) goto done;
                 ++layer_count;
                 tc_fence_after();
-                uint32_t o0, o1;
-                tc_ld2(lane_base, o0, o1);
-                tc_wait_ld(o0, o1);
-                tc_fence_before();
-                const float* st = my_bias + 4 * kW;
-                float a0 = __uint_as_float(o0) + st[0], a1 = __uint_as_float(o1) + st[1];
+                float ltau = 0.0f, lnI = 0.0f;
+                if (lead) {   // the lead warp holds the hi and lo units of the skip input
+                    uint32_t o0, o1;
+                    tc_ld2(lane_base, o0, o1);
+                    tc_wait_ld(o0, o1);
+                    const float* st = my_bias + 4 * kW;
+                    float a0 = __uint_as_float(o0) + st[0], a1 = __uint_as_float(o1) + st[1];
 #pragma unroll
-                for (int q = 0; q < kF / 2; ++q) {   // skip input x = hi + lo, from the feature registers
-                    const float2 hi = unpack_bf16x2(feat[q]), lo = unpack_bf16x2(feat[kF / 2 + q]);
-                    const float x0 = hi.x + lo.x, x1 = hi.y + lo.y;
-                    a0 = fmaf(st[kOut + 2 * q], x0, fmaf(st[kOut + 2 * q + 1], x1, a0));
-                    a1 = fmaf(st[kOut + kF + 2 * q], x0, fmaf(st[kOut + kF + 2 * q + 1], x1, a1));
+                    for (int q = 0; q < kF / 2; ++q) {   // skip input x = hi + lo, from the feature registers
+                        const float2 hi = unpack_bf16x2(feat[q]), lo = unpack_bf16x2(feat[kF / 2 + q]);
+                        const float x0 = hi.x + lo.x, x1 = hi.y + lo.y;
+                        a0 = fmaf(st[kOut + 2 * q], x0, fmaf(st[kOut + 2 * q + 1], x1, a0));
+                        a1 = fmaf(st[kOut + kF + 2 * q], x0, fmaf(st[kOut + kF + 2 * q + 1], x1, a1));
+                    }
+                    ltau = fmaf(a0, A.norm.out_sd[0], A.norm.out_mu[0]);
+                    lnI = fmaf(a1, A.norm.out_sd[1], A.norm.out_mu[1]);
                 }
-                const float ltau = fmaf(a0, A.norm.out_sd[0], A.norm.out_mu[0]);
-                const float lnI = fmaf(a1, A.norm.out_sd[1], A.norm.out_mu[1]);
+                tc_fence_before();
                 sum_tau += ltau;
                 sum_lnI += lnI;
                 // this member's ln I_obs (or ln tau) per pixel: log-sum-exp over the bins
@@ -463,7 +480,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_infer(const InferArgs A)
             // ensemble means -> per-sample outputs and per-pixel aggregates
             const float inv_k = 1.0f / float(K);
             const float ltau = sum_tau * inv_k, lnI = sum_lnI * inv_k;
-            if (valid) {
+            if (valid && lead) {
                 if (A.ln_tau_E) A.ln_tau_E[s] = ltau;
                 if (A.ln_I_E) A.ln_I_E[s] = lnI;
             }
