@@ -664,7 +664,7 @@ def scan_arm(args) -> None:
     jids = [torch.from_numpy(SC.judge_ids(P, args.judge, jrng)).to(device) for _ in ks]
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)   # > 126 MB L2
     for w in range(args.warmup):
-        runner.run(pars[w], thr, jids[w])
+        runner.run(pars[w], thr, jids[w], escalate=SC.ESCALATE, bound=args.bound)
         flush.zero_()
     barrier()
 
@@ -673,7 +673,8 @@ def scan_arm(args) -> None:
     with ClockSampler(gpu_index_of(local)) as clocks:
         t_start.record(stream)
         for k in range(args.steps):
-            rows.append(runner.run(pars[args.warmup + k], thr, jids[args.warmup + k]))
+            rows.append(runner.run(pars[args.warmup + k], thr, jids[args.warmup + k], escalate=SC.ESCALATE,
+                                   bound=args.bound))
             flush.zero_()
         t_end.record(stream)
         torch.cuda.synchronize()
@@ -725,7 +726,7 @@ def scan_arm(args) -> None:
     h2d = d2h = 0
     for k in range(args.steps):
         host["judge_ids"].copy_(jids[args.warmup + k].cpu())
-        r = runner.run_host(pars[args.warmup + k], thr, host)
+        r = runner.run_host(pars[args.warmup + k], thr, host, escalate=SC.ESCALATE, bound=args.bound)
         h2d, d2h = r["h2d_bytes"], r["d2h_bytes"]
     e2e_s = reduce(time.perf_counter() - t0, "max") / args.steps
     del host
@@ -786,6 +787,8 @@ def scan_arm(args) -> None:
                           "judged_pixels_per_point": rows[0]["judged"],
                           "fallback_frac_mean": statistics.mean(r["fallback_frac"] for r in rows),
                           "fallback_frac_max": fb_max, "threshold": thr, "bound": args.bound,
+                          "escalate": list(SC.ESCALATE),
+                          "steps_escalated": sum(1 for r in rows if r["escalated_pixels"] > 0),
                           "calibration": calib, "members": len(sur.nets),
                           "train": {k: info[k] for k in ("samples", "trace_s", "fit_s", "val_rms_ln_tau",
                                                          "val_rms_ln_I", "loaded_from") if k in info},

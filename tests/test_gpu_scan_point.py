@@ -103,3 +103,28 @@ def test_point_runner_judges_the_surrogate_where_nothing_falls_back(hb, gpu_ctx,
     want = SC.errors(ex["I_obs"], runner.out["I_obs"].cpu().numpy()[jids])
     assert res["error"]["n"] == want["n"]
     assert res["error"]["worst"] == pytest.approx(want["worst"], rel=1e-12)
+
+
+def test_point_runner_escalates_when_the_judge_finds_a_large_error(hb, gpu_ctx, sigma_table):
+    """An untrained ensemble errs far beyond 1 %: with no pixel sent to the
+    tracer by the first threshold, escalation to a threshold below every
+    spread traces each pixel whose spread exceeds it, after which the image is
+    the plain tracer's on those pixels and the judged error is zero."""
+    import torch
+    from hadros_b200 import scan as SC
+    torch.cuda.set_device(0)
+    p = _cam(hb)
+    sur = _untrained(hb)
+    runner = SC.PointRunner(gpu_ctx, sigma_table, sur, 16, 8, judge_frac=0.25)
+    jids = SC.judge_ids(256, 0.25, np.random.default_rng(8))
+    base = runner.run(p, 1e30, jids)
+    assert base["fallback_pixels"] == 0 and base["error"]["worst"] > 0.01
+    res = runner.run(p, 1e30, jids, escalate=(1e-30,), bound=0.01)
+    flagged = int((runner.out["spread"] > 1e-30).sum().item())
+    assert res["threshold_used"] == 1e-30 and res["escalated_pixels"] == flagged == res["fallback_pixels"]
+    plain = gpu_ctx.image(p, sigma_table, outputs=KEYS)
+    sp = runner.out["spread"].cpu().numpy()
+    for k in KEYS:
+        np.testing.assert_array_equal(runner.out[k].cpu().numpy()[sp > 1e-30], plain[k][sp > 1e-30], err_msg=k)
+    if (sp > 1e-30)[jids].all():
+        assert res["error"]["worst"] == 0.0
