@@ -89,7 +89,10 @@ struct PointRec {
     float nbdl2;   // n_b dl_cm log2(e); negative: no density
     int32_t b0, b1;// bins whose E_local lies in the sigma table's range: b0..b1 (decided in FP64)
 };
-constexpr int kRecDepth = 64;       // points a thread buffers between deferred transfers
+#ifndef HADROS_REC_DEPTH
+#define HADROS_REC_DEPTH 64
+#endif
+constexpr int kRecDepth = HADROS_REC_DEPTH;   // points a thread buffers between deferred transfers
 constexpr int kDeferMinBins = 24;   // bins from which the host picks deferred transfer
 constexpr int kAccF = 5;            // FP32 accumulators per bin in mixed precision
 
