@@ -313,7 +313,7 @@ def held_out_samples(ctx, sigma, cams, pixels_per_cam: int, seed: int, i_floor: 
     return cams[-n_val:], vraw, vy
 
 
-def calibrate(sur, sigma, cams, raw, y, i_floor: float, bound: float, q: float = 0.999, margin: float = 0.8,
+def calibrate(sur, sigma, cams, raw, y, i_floor: float, bound: float, q: float = 0.99, margin: float = 0.8,
               floor_rel: float = 1e-6) -> dict:
     """The spread threshold, chosen on held-out cameras.
 
@@ -324,7 +324,9 @@ def calibrate(sur, sigma, cams, raw, y, i_floor: float, bound: float, q: float =
     member's ln I_obs).  The threshold is the largest one (on a log grid from
     bound/30 to bound) for which, among the pixels above floor_rel of the
     brightest whose spread is at most the threshold, no more than a fraction
-    1 - q err by more than margin x bound."""
+    1 - q err by more than margin x bound.  The tail this admits is the scan's
+    per-point escalation's job (PointRunner.run): a point whose exact judge
+    finds an error above the bound lowers its threshold."""
     torch = _torch()
     B = n_bins_of(cams[0])
     bins = spectral_bins(cams[0], sigma)

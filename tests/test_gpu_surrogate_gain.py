@@ -7,7 +7,8 @@ points of the production box (collapsar_ndaf_like, density_weighted source,
 a = 0.95, rho0 in [1e9, 1e12], inclination in [10, 80] deg) at 1024 x 1024
 pixels and the production scan's 64 bins; the fallback threshold on the
 ensemble spread is calibrated on the held-out cameras.  On a scan point not
-among them, the surrogate image with its exact fallback and a 1% exact judge
+among them, the surrogate image with its exact fallback, a 1% exact judge and
+the production scan's per-point threshold escalation
 (hadros_b200.scan.PointRunner) is compared with the plain tracer's image of
 the same point: the judged worst error must be at most 1%, the pixels sent
 to the fallback must carry the exact values, and the point must be at least
@@ -41,10 +42,10 @@ def test_surrogate_meets_one_percent_and_beats_the_tracer(hb, gpu_ctx, sigma_tab
     # with it: surrogate + fallback + 1% exact judge (warmed once)
     runner = scan.PointRunner(gpu_ctx, sigma_table, sur, side, bins, 0.01)
     jids = scan.judge_ids(P, 0.01, np.random.default_rng(7))
-    runner.run(p, calib["threshold"], jids)
+    runner.run(p, calib["threshold"], jids, escalate=scan.ESCALATE, bound=0.01)
     torch.cuda.synchronize()
     a = time.perf_counter()
-    res = runner.run(p, calib["threshold"], jids)
+    res = runner.run(p, calib["threshold"], jids, escalate=scan.ESCALATE, bound=0.01)
     t_sur = time.perf_counter() - a
 
     nf = res["fallback_pixels"]

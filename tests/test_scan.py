@@ -52,7 +52,9 @@ def test_calibration_picks_the_largest_safe_threshold(hb, sigma_table):
     """calibrate(): the threshold is the largest spread below which held-out
     pixels rarely err beyond the bound.  A stand-in ensemble whose pixels have
     spread d_i and error 0.5% below spread 0.004 but 3% above it must get a
-    threshold just below 0.004."""
+    threshold just below 0.004 when no bad pixel may pass (q = 0.999), and
+    at most two steps of the threshold grid (5.8% each) above it with the
+    default q = 0.99, which admits a 1% tail for the scan's escalation."""
     import torch
 
     B, P, K = 4, 2000, 4
@@ -73,7 +75,9 @@ def test_calibration_picks_the_largest_safe_threshold(hb, sigma_table):
             return torch.from_numpy(out)
 
     raw = torch.zeros((P * B, 16))
-    c = scan.calibrate(Ens(), sigma_table, [p], raw, torch.from_numpy(y), floor, bound=0.01)
+    c = scan.calibrate(Ens(), sigma_table, [p], raw, torch.from_numpy(y), floor, bound=0.01, q=0.999)
     assert c["pixels"] > 0.5 * P
     assert 0.0025 < c["threshold"] < 0.004
     assert abs(c["fallback_frac_held_out"] - (d > c["threshold"]).mean()) < 0.02
+    c = scan.calibrate(Ens(), sigma_table, [p], raw, torch.from_numpy(y), floor, bound=0.01)
+    assert 0.0025 < c["threshold"] < 0.004 * 1.0583 ** 2
