@@ -714,8 +714,8 @@ def scan_arm(args) -> None:
     full_check = {"point": k_plain, "pixels": int(full[0].item()), "worst": float(full[1].item()),
                   "p99": float(full[2].item()), "median": float(full[3].item())}
     del plain
-    per_step, traffic_src = read_traffic_per_step()
-    traffic = per_step * steps_sum if per_step else None
+    bytes_per_accepted_step, traffic_src = read_traffic_per_step()
+    traffic = bytes_per_accepted_step * steps_sum if bytes_per_accepted_step else None
     if traffic_src:
         traffic_src += " (bytes per accepted step of that launch x this launch's accepted steps)"
 
