@@ -90,7 +90,7 @@ struct PointRec {
     int32_t b0, b1;// bins whose E_local lies in the sigma table's range: b0..b1 (decided in FP64)
 };
 #ifndef HADROS_REC_DEPTH
-#define HADROS_REC_DEPTH 64
+#define HADROS_REC_DEPTH 128
 #endif
 constexpr int kRecDepth = HADROS_REC_DEPTH;   // points a thread buffers between deferred transfers
 constexpr int kDeferMinBins = 24;   // bins from which the host picks deferred transfer
