@@ -189,8 +189,10 @@ class PointRunner:
                         for k in self.KEYS:
                             self.out[k].index_copy_(0, fb2, self.exact[k][o:o + n2])
                         n_esc += n2
-                    e2 = torch.stack(list(_device_errors(ex, self.out[key][jt]))).cpu().numpy()
-                    v[0:4] = e2
+                    pm2 = (self.exact["P_surv"][:nj] - self.out["P_surv"][jt]).abs().max().double()
+                    e2 = torch.stack([*_device_errors(ex, self.out[key][jt]), pm2]).cpu().numpy()
+                    v[0:4] = e2[:4]
+                    v[8] = e2[4]
                     if v[1] <= bound:
                         break
         nf_all = nf + n_esc
