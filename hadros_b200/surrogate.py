@@ -415,3 +415,40 @@ def trace_samples(ctx, sigma, cams, pixels_per_cam: int, seed: int = 20261203, d
         i_floor = float(I.max()) * I_FLOOR_REL if I.max() > 0 else 1e-300
     y = torch.from_numpy(targets_of(tau, I, i_floor)).to(device)
     return torch.cat(raws), y, {"i_floor": i_floor, "trace_s": t_trace, "n": int(tau.size)}
+
+
+def time_fit(rows: int = 1 << 20, epochs: int = 2, batch: int = 8192, members: int = 4, device: int = 0) -> dict:
+    """Seconds per training step of an ensemble of `members` networks on
+    `rows` synthetic samples (16 raw features with a one-hot profile block,
+    two smooth targets): one warm-up epoch (kernel loading, graph capture),
+    then `epochs` timed epochs."""
+    torch = _torch()
+    torch.cuda.set_device(device)
+    rng = np.random.default_rng(1)
+    raw = rng.normal(size=(rows, 16)).astype(np.float32)
+    raw[:, 5:13] = 0.0
+    raw[np.arange(rows), 5 + rng.integers(0, 8, rows)] = 1.0
+    y = np.stack([np.sin(raw[:, 0]) + raw[:, 15], raw[:, 1] * raw[:, 2]], axis=1).astype(np.float32)
+    sur = Surrogate(members=members, device=device, seed=1)
+    R = torch.from_numpy(raw).to(sur.device)
+    Y = torch.from_numpy(y).to(sur.device)
+    sur.fit(R, Y, epochs=1, batch=batch)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sur.fit(R, Y, epochs=epochs, batch=batch)
+    torch.cuda.synchronize()
+    steps = epochs * max(rows // batch, 1)
+    return {"rows": rows, "epochs": epochs, "batch": batch, "members": members, "steps": steps,
+            "s_per_step": (time.perf_counter() - t0) / steps, "loss": [h[-1] for h in sur.history]}
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="time the ensemble's training step on synthetic rows")
+    ap.add_argument("--rows", type=int, default=1 << 20)
+    ap.add_argument("--epochs", type=int, default=2)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--members", type=int, default=4)
+    a = ap.parse_args()
+    print(json.dumps(time_fit(a.rows, a.epochs, a.batch, a.members)))
